@@ -1,0 +1,908 @@
+// fss.cpp -- context, orchestration and the C ABI (include/fss.h).
+#include "fss.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "geometry.h"
+#include "kernels.h"
+#include "traverse.h"
+
+using namespace fss;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t b) {
+        if (b <= bytes && p) return cudaSuccess;
+        release();
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return e;
+        }
+        bytes = b;
+        return cudaSuccess;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct ProfEntry {
+    double ms = 0;
+    int64_t launches = 0;
+};
+
+}  // namespace
+
+struct fss_ctx {
+    fss_config cfg{};
+    std::string err;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    bool fp64 = false;
+    bool tree = true;
+
+    int64_t n = 0;
+    bool have = false;
+    bool stage_dirty = false;  // xs/src hold a stand-alone rhs input, not s0
+
+    // tree
+    int tree_levels = 0, leaf_level = 0;
+    int64_t nleaf = 1;
+    TreeGeometry geom;
+    std::vector<int32_t> leaf_start_h;
+    std::vector<int32_t> counts_h;
+    std::vector<Pair> pairs;
+    std::vector<int32_t> ref_loc_h, cmp_loc_h;
+    int64_t unassigned = 0;
+    ListOutput lists;
+    std::vector<int32_t> leaf_deg;
+    std::vector<double> leaf_theta;
+    int nmax = 0, level_mask = 0;
+    int parts = 1;
+    PairShape shape;
+    double direct_pairs = 0;
+
+    // device
+    DBuf in5, area_in, perm, key, key_tmp, vals_tmp, hist, leaf_start, s0, xs, acc, area_s, tracer_s, src, partials,
+        ents, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
+        wtotal, err_flag, loc;
+    int64_t src_count = 0;
+
+    // graph
+    cudaGraphExec_t graph = nullptr;
+    double graph_dt = 0, graph_omega = 0;
+
+    // profiling
+    bool prof = false;
+    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    std::vector<cudaEvent_t> ev_pool;
+    std::map<std::string, ProfEntry> prof_acc;
+    std::vector<std::string> prof_order;
+
+    std::unique_ptr<fss_ctx> alt;  // the other method, created on demand
+
+    ~fss_ctx() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (auto& p : pending) {
+            cudaEventDestroy(p.second.first);
+            cudaEventDestroy(p.second.second);
+        }
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+};
+
+namespace {
+
+int fail(fss_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    g_last_error = msg;
+    return code;
+}
+
+#define CU(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return fail(c, e_ == cudaErrorMemoryAllocation ? FSS_ERR_NOMEM : FSS_ERR_CUDA,             \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+    } while (0)
+
+#define TRY(call)                        \
+    do {                                 \
+        int r_ = (call);                 \
+        if (r_ != FSS_OK) return r_;     \
+    } while (0)
+
+cudaEvent_t ev_get(fss_ctx* c) {
+    if (!c->ev_pool.empty()) {
+        cudaEvent_t e = c->ev_pool.back();
+        c->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct ProfScope {
+    fss_ctx* c;
+    const char* name;
+    cudaEvent_t a = nullptr, b = nullptr;
+    ProfScope(fss_ctx* ctx, const char* nm) : c(ctx), name(nm) {
+        if (c->prof) {
+            a = ev_get(c);
+            b = ev_get(c);
+            cudaEventRecord(a, c->stream);
+        }
+    }
+    ~ProfScope() {
+        if (c->prof) {
+            cudaEventRecord(b, c->stream);
+            c->pending.push_back({name, {a, b}});
+        }
+    }
+};
+
+void prof_resolve(fss_ctx* c) {
+    if (c->pending.empty()) return;
+    cudaStreamSynchronize(c->stream);
+    for (auto& p : c->pending) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+        if (!c->prof_acc.count(p.first)) c->prof_order.push_back(p.first);
+        c->prof_acc[p.first].ms += ms;
+        c->prof_acc[p.first].launches += 1;
+        c->ev_pool.push_back(p.second.first);
+        c->ev_pool.push_back(p.second.second);
+    }
+    c->pending.clear();
+}
+
+int check_device_error(fss_ctx* c) {
+    int h = 0;
+    CU(cudaMemcpyAsync(&h, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    prof_resolve(c);
+    if (h != 0) {
+        cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), c->stream);
+        return fail(c, h == kErrTimeout ? FSS_ERR_TIMEOUT : FSS_ERR_TREE,
+                    h == kErrTimeout ? "a kernel's bounded wait timed out" : "tree build error");
+    }
+    return FSS_OK;
+}
+
+template <typename T>
+int upload(fss_ctx* c, DBuf& b, const std::vector<T>& v) {
+    CU(b.ensure(sizeof(T) * std::max<size_t>(v.size(), 1)));
+    if (!v.empty()) CU(cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, c->stream));
+    return FSS_OK;
+}
+
+int auto_tree_levels(const fss_config& cfg, int64_t n) {
+    if (cfg.tree_levels > 0) return cfg.tree_levels;
+    const int target = cfg.leaf_target > 0 ? cfg.leaf_target : 64;
+    int ll = 0;
+    while (ll + 1 < kMaxLevels && double(n) / (20.0 * std::pow(4.0, ll + 1)) >= target) ll++;
+    return ll + 1;
+}
+
+int src_size_ensure(fss_ctx* c, int64_t count) {
+    const size_t es = c->fp64 ? sizeof(double4) : sizeof(float4);
+    CU(c->src.ensure(es * size_t(std::max<int64_t>(count, 1))));
+    c->src_count = count;
+    return FSS_OK;
+}
+
+// Lists of the direct sum: target tiles x source chunks.
+int build_direct_lists(fss_ctx* c) {
+    const int64_t n = c->n;
+    c->shape = pairs_shape(c->fp64, c->cfg.block_threads);
+    const int TB = c->shape.threads * c->shape.per_thread;
+    const int64_t tiles = (n + TB - 1) / TB;
+    int P = c->cfg.src_parts;
+    if (P <= 0) {
+        const int64_t want = 148 * 8 * 3;
+        P = int(std::max<int64_t>(1, (want + tiles - 1) / std::max<int64_t>(tiles, 1)));
+        P = int(std::min<int64_t>(P, std::max<int64_t>(1, n / 512)));
+        P = std::min(P, 64);
+    }
+    c->parts = P;
+    ListOutput& L = c->lists;
+    L = ListOutput();
+    for (int p = 0; p < P; p++) {
+        SrcEntry e{};
+        e.start = int32_t(n * p / P);
+        e.count = int32_t(n * (p + 1) / P - e.start);
+        e.kind = 0;
+        L.entries.push_back(e);
+    }
+    for (int64_t t = 0; t < tiles; t++)
+        for (int p = 0; p < P; p++)
+            L.items.push_back(WorkItem{int32_t(t * TB), int32_t(std::min<int64_t>(TB, n - t * TB)), p, p + 1, p, 0});
+    L.pp_pairs = double(n) * double(n - 1);
+    c->direct_pairs = L.pp_pairs;
+    TRY(upload(c, c->ents, L.entries));
+    TRY(upload(c, c->items, L.items));
+    TRY(src_size_ensure(c, n));
+    CU(c->partials.ensure(sizeof(double4) * size_t(P) * size_t(std::max<int64_t>(n, 1))));
+    return FSS_OK;
+}
+
+int ensure_particle_buffers(fss_ctx* c, int64_t n) {
+    const size_t N = size_t(std::max<int64_t>(n, 1));
+    CU(c->in5.ensure(sizeof(double) * 5 * N));
+    CU(c->area_in.ensure(sizeof(double) * N));
+    CU(c->s0.ensure(sizeof(double4) * N));
+    CU(c->xs.ensure(sizeof(double4) * N));
+    CU(c->acc.ensure(sizeof(double4) * N));
+    CU(c->area_s.ensure(sizeof(double) * N));
+    CU(c->tracer_s.ensure(sizeof(double) * N));
+    CU(c->out5.ensure(sizeof(double) * 5 * N));
+    CU(c->psi.ensure(sizeof(double) * N));
+    CU(c->wtotal.ensure(sizeof(double)));
+    return FSS_OK;
+}
+
+int build_tree(fss_ctx* c);
+
+int gather(fss_ctx* c, bool write_s0) {
+    const bool treec = c->tree;
+    ProfScope ps(c, "gather");
+    launch_gather(c->stream, c->fp64, c->n, c->in5.as<double>(), c->area_in.as<double>(),
+                  treec ? c->perm.as<int32_t>() : nullptr, treec ? c->key.as<uint32_t>() : nullptr,
+                  (treec && !c->fp64) ? c->frame.as<double4>() : nullptr, write_s0 ? c->s0.as<double4>() : nullptr,
+                  c->xs.as<double4>(), c->area_s.as<double>(), c->tracer_s.as<double>(), c->src.p);
+    CU(cudaGetLastError());
+    return FSS_OK;
+}
+
+void invalidate_graph(fss_ctx* c) {
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+}
+
+int set_particles(fss_ctx* c, int64_t n, const double* state5, const double* area) {
+    if (n < 2) return fail(c, FSS_ERR_INVALID, "need at least 2 particles");
+    if (n > (int64_t(1) << 30)) return fail(c, FSS_ERR_INVALID, "too many particles");
+    if (!state5 || !area) return fail(c, FSS_ERR_INVALID, "null state or area");
+    invalidate_graph(c);
+    c->n = n;
+    TRY(ensure_particle_buffers(c, n));
+    CU(cudaMemcpyAsync(c->in5.p, state5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemcpyAsync(c->area_in.p, area, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    if (c->tree) {
+        TRY(build_tree(c));
+    } else {
+        TRY(build_direct_lists(c));
+    }
+    TRY(gather(c, true));
+    c->have = true;
+    c->stage_dirty = false;
+    return check_device_error(c);
+}
+
+int build_tree(fss_ctx* c) {
+    const int64_t n = c->n;
+    const int TL = auto_tree_levels(c->cfg, n);
+    if (TL < 1 || TL > kMaxLevels) return fail(c, FSS_ERR_INVALID, "tree_levels out of range");
+    if (TL != c->tree_levels || c->geom.tree_levels != TL) {
+        c->geom = build_tree_geometry(TL);
+        c->tree_levels = TL;
+        c->leaf_level = TL - 1;
+        c->nleaf = int64_t(20) << (2 * c->leaf_level);
+        TRY(upload(c, c->verts, c->geom.verts));
+        TRY(upload(c, c->tri_verts, c->geom.tri_verts));
+        TRY(upload(c, c->lev_off, c->geom.lev_off));
+        TRY(upload(c, c->node, c->geom.node));
+        std::vector<double4> fr(c->nleaf);
+        for (int64_t l = 0; l < c->nleaf; l++) {
+            const double* ti = &c->geom.tri_info[4 * (c->geom.lev_off[c->leaf_level] + l)];
+            fr[l] = make_double4(ti[0], ti[1], ti[2], 0.0);
+        }
+        TRY(upload(c, c->frame, fr));
+        if ((int)c->leaf_deg.size() != c->nleaf) {
+            c->leaf_deg.assign(c->nleaf, c->cfg.degree);
+            c->leaf_theta.assign(c->nleaf, c->cfg.theta);
+        }
+    }
+    const int LL = c->leaf_level;
+    const int64_t nfaces = c->geom.lev_off[TL];
+    // assignment
+    CU(c->key.ensure(sizeof(uint32_t) * n));
+    CU(c->key_tmp.ensure(sizeof(uint32_t) * n));
+    CU(c->perm.ensure(sizeof(int32_t) * n));
+    CU(c->vals_tmp.ensure(sizeof(int32_t) * n));
+    CU(c->hist.ensure(sizeof(uint32_t) * sort_scratch_words(n)));
+    CU(c->leaf_start.ensure(sizeof(int32_t) * (c->nleaf + 1)));
+    c->ref_loc_h.clear();
+    c->unassigned = 0;
+    std::vector<int32_t> ref_counts;
+    if (c->cfg.assign_mode == FSS_ASSIGN_REFERENCE) {
+        CU(c->loc.ensure(sizeof(int32_t) * size_t(TL) * n));
+        DBuf cnt;
+        CU(cnt.ensure(sizeof(int32_t) * nfaces));
+        CU(cudaMemsetAsync(cnt.p, 0, sizeof(int32_t) * nfaces, c->stream));
+        {
+            ProfScope ps(c, "tree_assign");
+            launch_assign(c->stream, n, c->in5.as<double>(), c->verts.as<double>(), c->tri_verts.as<int32_t>(),
+                          c->lev_off.as<int64_t>(), TL, 1, c->loc.as<int32_t>(), nullptr, c->err_flag.as<int>());
+        }
+        launch_level_hist(c->stream, n, TL, c->loc.as<int32_t>(), c->lev_off.as<int64_t>(), cnt.as<int32_t>());
+        c->ref_loc_h.resize(size_t(TL) * n);
+        ref_counts.resize(nfaces);
+        CU(cudaMemcpyAsync(c->ref_loc_h.data(), c->loc.p, sizeof(int32_t) * TL * n, cudaMemcpyDeviceToHost, c->stream));
+        CU(cudaMemcpyAsync(ref_counts.data(), cnt.p, sizeof(int32_t) * nfaces, cudaMemcpyDeviceToHost, c->stream));
+        CU(cudaStreamSynchronize(c->stream));
+        for (int64_t i = 0; i < n; i++)
+            if (c->ref_loc_h[size_t(LL) * n + i] < 0) c->unassigned++;
+    }
+    {
+        ProfScope ps(c, "tree_assign");
+        launch_assign(c->stream, n, c->in5.as<double>(), c->verts.as<double>(), c->tri_verts.as<int32_t>(),
+                      c->lev_off.as<int64_t>(), TL, 0, nullptr, c->key.as<uint32_t>(), c->err_flag.as<int>());
+    }
+    int bits = 0;
+    while ((int64_t(1) << bits) < c->nleaf) bits++;
+    {
+        ProfScope ps(c, "tree_sort");
+        launch_sort(c->stream, n, std::max(bits, 1), c->key.as<uint32_t>(), c->key_tmp.as<uint32_t>(),
+                    c->perm.as<int32_t>(), c->vals_tmp.as<int32_t>(), c->hist.as<uint32_t>());
+        launch_leaf_bounds(c->stream, n, c->key.as<uint32_t>(), int32_t(c->nleaf), c->leaf_start.as<int32_t>());
+    }
+    CU(cudaGetLastError());
+    c->leaf_start_h.resize(c->nleaf + 1);
+    CU(cudaMemcpyAsync(c->leaf_start_h.data(), c->leaf_start.p, sizeof(int32_t) * (c->nleaf + 1),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    // per-face counts on every level from the leaf ranges
+    c->counts_h.assign(nfaces, 0);
+    for (int l = 0; l <= LL; l++) {
+        const int64_t span = int64_t(1) << (2 * (LL - l));
+        const int64_t nf = c->geom.level_count(l);
+        for (int64_t f = 0; f < nf; f++)
+            c->counts_h[c->geom.lev_off[l] + f] = c->leaf_start_h[(f + 1) * span] - c->leaf_start_h[f * span];
+    }
+    const int K = nproxy(c->cfg.degree);
+    const int many = (c->cfg.many_count < 0) ? K : c->cfg.many_count;
+    c->pairs = dual_traverse(c->geom, (c->cfg.assign_mode == FSS_ASSIGN_REFERENCE) ? ref_counts : c->counts_h,
+                             c->cfg.theta, many);
+    std::vector<std::vector<ASrc>> al;
+    if (c->cfg.list_mode == FSS_LIST_LEAF) {
+        al = lists_per_leaf(c->geom, LL, c->counts_h, c->leaf_deg, c->leaf_theta);
+    } else {
+        const std::vector<Pair>& pp = (c->cfg.assign_mode == FSS_ASSIGN_REFERENCE)
+                                          ? dual_traverse(c->geom, c->counts_h, c->cfg.theta, many)
+                                          : c->pairs;
+        al = lists_from_pairs(c->geom, LL, pp, many, c->cfg.degree);
+    }
+    c->shape = pairs_shape(c->fp64, c->cfg.block_threads);
+    ListInput in;
+    in.g = &c->geom;
+    in.leaf_level = LL;
+    in.n = n;
+    in.leaf_start = c->leaf_start_h.data();
+    in.local_frames = !c->fp64;
+    in.threads = c->shape.threads;
+    in.per_thread = c->shape.per_thread;
+    int P = c->cfg.src_parts;
+    if (P <= 0) {
+        int64_t chunks = 0;
+        const int TB = in.threads * in.per_thread;
+        for (int64_t l = 0; l < c->nleaf; l++) chunks += (c->leaf_start_h[l + 1] - c->leaf_start_h[l] + TB - 1) / TB;
+        const double waves = double(chunks) / (148.0 * 8.0);
+        P = waves >= 3.0 ? 1 : (waves >= 1.0 ? 2 : 4);
+    }
+    in.parts = P;
+    c->parts = P;
+    build_lists(in, al, c->lists);
+    const ListOutput& L = c->lists;
+    // interpolation tables for the degrees in use
+    c->nmax = std::max(L.max_degree, 0);
+    c->level_mask = 0;
+    for (const ProxyJob& j : L.jobs) {
+        c->level_mask |= 1 << j.level;
+        for (int d = 0; d <= kMaxDegree; d++)
+            if ((j.degmask >> d) & 1) c->nmax = std::max(c->nmax, d);
+    }
+    std::vector<double> vinv_all;
+    std::vector<int32_t> vinv_off(kMaxDegree + 1, 0);
+    for (int d = 0; d <= c->nmax; d++) {
+        std::vector<double> nodes, vi;
+        interp_nodes(d, nodes, vi);
+        vinv_off[d] = int32_t(vinv_all.size());
+        vinv_all.insert(vinv_all.end(), vi.begin(), vi.end());
+    }
+    TRY(upload(c, c->vinv, vinv_all));
+    TRY(upload(c, c->vinv_off, vinv_off));
+    TRY(upload(c, c->ents, L.entries));
+    TRY(upload(c, c->items, L.items));
+    TRY(upload(c, c->jobs, L.jobs));
+    std::vector<double4> pp(L.proxy_pos.size() / 4);
+    for (size_t i = 0; i < pp.size(); i++)
+        pp[i] = make_double4(L.proxy_pos[4 * i], L.proxy_pos[4 * i + 1], L.proxy_pos[4 * i + 2], 0.0);
+    TRY(upload(c, c->proxy_pos, pp));
+    TRY(src_size_ensure(c, n + L.n_proxy));
+    CU(c->partials.ensure(sizeof(double4) * size_t(P) * size_t(n)));
+    CU(c->part_up.ensure(sizeof(double) * size_t(c->nleaf) * (LL + 1) * nproxy(c->nmax)));
+    return FSS_OK;
+}
+
+// One right-hand side on the current stage state (xs/src).
+int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
+    if (c->tree && !c->lists.jobs.empty()) {
+        {
+            ProfScope ps(c, "upward_leaf");
+            launch_up_leaf(c->stream, c->fp64, int(c->nleaf), c->src.p, c->leaf_start.as<int32_t>(),
+                           c->fp64 ? nullptr : c->frame.as<double4>(), c->node.as<NodeGeom>(), c->lev_off.as<int64_t>(),
+                           c->leaf_level, c->nmax, c->level_mask, c->part_up.as<double>());
+        }
+        {
+            ProfScope ps(c, "upward_combine");
+            launch_up_combine(c->stream, c->fp64, int(c->lists.jobs.size()), c->jobs.as<ProxyJob>(),
+                              c->part_up.as<double>(), c->leaf_level, c->nmax, c->vinv.as<double>(),
+                              c->vinv_off.as<int32_t>(), c->proxy_pos.as<double4>(), c->node.as<NodeGeom>(), !c->fp64,
+                              c->n, c->src.p);
+        }
+    }
+    {
+        ProfScope ps(c, c->fp64 ? "pairs_fp64" : "pairs_mixed");
+        CU(launch_pairs(c->stream, c->fp64, want_psi, c->shape, int(c->lists.items.size()), c->src.p,
+                        c->ents.as<SrcEntry>(), c->items.as<WorkItem>(), c->partials.as<double4>(), c->n,
+                        c->err_flag.as<int>()));
+    }
+    if (want_psi) launch_wsum(c->stream, c->n, c->xs.as<double4>(), c->area_s.as<double>(), c->wtotal.as<double>());
+    ea.n = c->n;
+    ea.parts = c->parts;
+    ea.pstride = c->n;
+    ea.partials = c->partials.as<double4>();
+    ea.xs = c->xs.as<double4>();
+    ea.area = c->area_s.as<double>();
+    ea.wtotal = c->wtotal.as<double>();
+    ea.perm = c->tree ? c->perm.as<int32_t>() : nullptr;
+    ea.src = c->src.p;
+    ea.leaf_of = c->tree ? c->key.as<uint32_t>() : nullptr;
+    ea.frame = (c->tree && !c->fp64) ? c->frame.as<double4>() : nullptr;
+    {
+        ProfScope ps(c, "epilogue");
+        launch_epilogue(c->stream, c->fp64, ea);
+    }
+    CU(cudaGetLastError());
+    return FSS_OK;
+}
+
+int rk4_once(fss_ctx* c, double dt, double omega) {
+    for (int stage = 1; stage <= 4; stage++) {
+        EpiArgs ea;
+        ea.mode = EPI_RK4;
+        ea.stage = stage;
+        ea.dt = dt;
+        ea.omega = omega;
+        ea.s0 = c->s0.as<double4>();
+        ea.acc = c->acc.as<double4>();
+        TRY(eval(c, ea, false));
+    }
+    return FSS_OK;
+}
+
+int refresh_stage(fss_ctx* c) {
+    if (!c->stage_dirty) return FSS_OK;
+    launch_refresh(c->stream, c->fp64, c->n, c->s0.as<double4>(), c->area_s.as<double>(),
+                   c->tree ? c->key.as<uint32_t>() : nullptr, (c->tree && !c->fp64) ? c->frame.as<double4>() : nullptr,
+                   c->xs.as<double4>(), c->src.p);
+    CU(cudaGetLastError());
+    c->stage_dirty = false;
+    return FSS_OK;
+}
+
+int rk4_steps(fss_ctx* c, double dt, double omega, int nsteps) {
+    if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    if (nsteps < 0) return fail(c, FSS_ERR_INVALID, "nsteps < 0");
+    TRY(refresh_stage(c));
+    const bool use_graph = c->cfg.use_graph && !c->prof;
+    if (!use_graph) {
+        for (int s = 0; s < nsteps; s++) TRY(rk4_once(c, dt, omega));
+        return FSS_OK;
+    }
+    if (!c->graph || c->graph_dt != dt || c->graph_omega != omega) {
+        invalidate_graph(c);
+        cudaGraph_t g;
+        CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int r = rk4_once(c, dt, omega);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (r != FSS_OK) return r;
+        if (e != cudaSuccess) return fail(c, FSS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(c, FSS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        c->graph_dt = dt;
+        c->graph_omega = omega;
+    }
+    for (int s = 0; s < nsteps; s++) CU(cudaGraphLaunch(c->graph, c->stream));
+    return FSS_OK;
+}
+
+int rhs_host(fss_ctx* c, const double* state5, const double* area, double omega, double* modify5, double* psi) {
+    if (!state5 || !area || !modify5) return fail(c, FSS_ERR_INVALID, "null pointer");
+    if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    CU(cudaMemcpyAsync(c->in5.p, state5, sizeof(double) * 5 * c->n, cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemcpyAsync(c->area_in.p, area, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->stream));
+    TRY(gather(c, false));
+    c->stage_dirty = true;
+    EpiArgs ea;
+    ea.mode = EPI_RHS;
+    ea.omega = omega;
+    ea.out5 = c->out5.as<double>();
+    ea.psi = psi ? c->psi.as<double>() : nullptr;
+    TRY(eval(c, ea, psi != nullptr));
+    CU(cudaMemcpyAsync(modify5, c->out5.p, sizeof(double) * 5 * c->n, cudaMemcpyDeviceToHost, c->stream));
+    if (psi) CU(cudaMemcpyAsync(psi, c->psi.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
+}
+
+fss_ctx* other_method(fss_ctx* c, int method, int* rc) {
+    *rc = FSS_OK;
+    if ((method == FSS_METHOD_TREECODE) == c->tree) return c;
+    if (!c->alt) {
+        fss_config cfg = c->cfg;
+        cfg.method = method;
+        fss_ctx* a = nullptr;
+        *rc = fss_create(&cfg, &a);
+        if (*rc != FSS_OK) return nullptr;
+        c->alt.reset(a);
+        c->alt->stream = c->stream;
+    }
+    c->alt->stream = c->stream;
+    return c->alt.get();
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+
+extern "C" {
+
+void fss_config_init(fss_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->device = 0;
+    cfg->precision = FSS_PREC_MIXED;
+    cfg->method = FSS_METHOD_TREECODE;
+    cfg->tree_levels = 0;
+    cfg->leaf_target = 64;
+    cfg->degree = 8;
+    cfg->theta = 0.7;
+    cfg->many_count = -1;
+    cfg->assign_mode = FSS_ASSIGN_COMPLETE;
+    cfg->list_mode = FSS_LIST_DUAL;
+    cfg->use_graph = 1;
+    cfg->src_parts = 0;
+    cfg->block_threads = 0;
+}
+
+int fss_create(const fss_config* cfg, fss_ctx** out) {
+    fss_ctx* c = nullptr;
+    if (!cfg || !out) return fail(c, FSS_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (cfg->degree < 0 || cfg->degree > kMaxDegree) return fail(c, FSS_ERR_INVALID, "degree must be in 0..10");
+    if (!(cfg->theta > 0)) return fail(c, FSS_ERR_INVALID, "theta must be positive");
+    if (cfg->tree_levels < 0 || cfg->tree_levels > kMaxLevels) return fail(c, FSS_ERR_INVALID, "tree_levels out of range");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(c, FSS_ERR_UNSUPPORTED, "no CUDA device");
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(c, FSS_ERR_INVALID, "bad device ordinal");
+    std::unique_ptr<fss_ctx> ctx(new fss_ctx());
+    c = ctx.get();
+    c->cfg = *cfg;
+    c->dev = cfg->device;
+    c->fp64 = cfg->precision == FSS_PREC_FP64;
+    c->tree = cfg->method == FSS_METHOD_TREECODE;
+    CU(cudaSetDevice(c->dev));
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, c->dev));
+    if (prop.major < 10) return fail(c, FSS_ERR_UNSUPPORTED, "this build targets sm_100a (Blackwell B200)");
+    CU(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    CU(c->err_flag.ensure(sizeof(int)));
+    CU(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    *out = ctx.release();
+    return FSS_OK;
+}
+
+void fss_destroy(fss_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->dev);
+    cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+}
+
+const char* fss_last_error(const fss_ctx* ctx) { return ctx ? ctx->err.c_str() : g_last_error.c_str(); }
+
+int fss_set_stream(fss_ctx* c, void* s) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    invalidate_graph(c);
+    c->stream = s ? static_cast<cudaStream_t>(s) : c->own_stream;
+    if (c->alt) c->alt->stream = c->stream;
+    return FSS_OK;
+}
+
+int fss_set_particles(fss_ctx* c, int64_t n, const double* state5, const double* area) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    CU(cudaSetDevice(c->dev));
+    return set_particles(c, n, state5, area);
+}
+
+int fss_rebuild_tree(fss_ctx* c) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    CU(cudaSetDevice(c->dev));
+    // current state back to the caller's order, then rebuild from it
+    launch_scatter_state(c->stream, c->n, c->tree ? c->perm.as<int32_t>() : nullptr, c->s0.as<double4>(),
+                         c->tracer_s.as<double>(), c->in5.as<double>());
+    std::vector<double> s5(5 * c->n), a(c->n);
+    CU(cudaMemcpyAsync(s5.data(), c->in5.p, sizeof(double) * 5 * c->n, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaMemcpyAsync(a.data(), c->area_in.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return set_particles(c, c->n, s5.data(), a.data());
+}
+
+int fss_rhs(fss_ctx* c, const double* state5, const double* area, double omega, double* modify5, double* psi) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    CU(cudaSetDevice(c->dev));
+    return rhs_host(c, state5, area, omega, modify5, psi);
+}
+
+static int rhs_method(fss_ctx* c, int method, const double* state5, const double* area, double omega, double* modify5,
+                      double* psi, int64_t n_hint) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    CU(cudaSetDevice(c->dev));
+    int rc;
+    fss_ctx* t = other_method(c, method, &rc);
+    if (!t) return fail(c, rc, fss_last_error(nullptr));
+    if (!t->have || t->n != n_hint) {
+        if (n_hint <= 0) return fail(c, FSS_ERR_STATE, "no particles set");
+        rc = set_particles(t, n_hint, state5, area);
+        if (rc != FSS_OK) return fail(c, rc, t->err);
+    }
+    rc = rhs_host(t, state5, area, omega, modify5, psi);
+    if (rc != FSS_OK) return fail(c, rc, t->err);
+    return FSS_OK;
+}
+
+int fss_rhs_direct(fss_ctx* c, const double* state5, const double* area, double omega, double* modify5, double* psi) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    return rhs_method(c, FSS_METHOD_DIRECT, state5, area, omega, modify5, psi, c->n);
+}
+
+int fss_rhs_treecode(fss_ctx* c, const double* state5, const double* area, double omega, double* modify5, double* psi) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    return rhs_method(c, FSS_METHOD_TREECODE, state5, area, omega, modify5, psi, c->n);
+}
+
+int fss_rk4_step(fss_ctx* c, double dt, double omega, int32_t nsteps) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    CU(cudaSetDevice(c->dev));
+    TRY(rk4_steps(c, dt, omega, nsteps));
+    if (c->prof) prof_resolve(c);
+    return FSS_OK;
+}
+
+int fss_rk4_step_host(fss_ctx* c, double* state5, double dt, double omega, int32_t nsteps) {
+    if (!c || !state5) return fail(c, FSS_ERR_INVALID, "null argument");
+    if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    CU(cudaSetDevice(c->dev));
+    CU(cudaMemcpyAsync(c->in5.p, state5, sizeof(double) * 5 * c->n, cudaMemcpyHostToDevice, c->stream));
+    TRY(gather(c, true));
+    c->stage_dirty = false;
+    TRY(rk4_steps(c, dt, omega, nsteps));
+    launch_scatter_state(c->stream, c->n, c->tree ? c->perm.as<int32_t>() : nullptr, c->s0.as<double4>(),
+                         c->tracer_s.as<double>(), c->out5.as<double>());
+    CU(cudaMemcpyAsync(state5, c->out5.p, sizeof(double) * 5 * c->n, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
+}
+
+int fss_get_state(fss_ctx* c, double* state5) {
+    if (!c || !state5) return fail(c, FSS_ERR_INVALID, "null argument");
+    if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    CU(cudaSetDevice(c->dev));
+    launch_scatter_state(c->stream, c->n, c->tree ? c->perm.as<int32_t>() : nullptr, c->s0.as<double4>(),
+                         c->tracer_s.as<double>(), c->out5.as<double>());
+    CU(cudaMemcpyAsync(state5, c->out5.p, sizeof(double) * 5 * c->n, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
+}
+
+int fss_rhs_current(fss_ctx* c, double omega, double* modify5, double* psi) {
+    if (!c || !modify5) return fail(c, FSS_ERR_INVALID, "null argument");
+    if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    CU(cudaSetDevice(c->dev));
+    TRY(refresh_stage(c));
+    EpiArgs ea;
+    ea.mode = EPI_RHS;
+    ea.omega = omega;
+    ea.out5 = c->out5.as<double>();
+    ea.psi = psi ? c->psi.as<double>() : nullptr;
+    TRY(eval(c, ea, psi != nullptr));
+    CU(cudaMemcpyAsync(modify5, c->out5.p, sizeof(double) * 5 * c->n, cudaMemcpyDeviceToHost, c->stream));
+    if (psi) CU(cudaMemcpyAsync(psi, c->psi.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
+}
+
+int fss_get_tree_info(fss_ctx* c, fss_tree_info* info) {
+    if (!c || !info) return fail(c, FSS_ERR_INVALID, "null argument");
+    std::memset(info, 0, sizeof(*info));
+    info->tree_levels = c->tree ? c->tree_levels : 0;
+    info->leaf_count = c->tree ? int32_t(c->nleaf) : 0;
+    info->degree = c->cfg.degree;
+    info->n_proxy = nproxy(c->cfg.degree);
+    info->n_pairs = int64_t(c->pairs.size());
+    info->n_list_entries = int64_t(c->lists.entries.size());
+    info->n_items = int64_t(c->lists.items.size());
+    info->unassigned = c->unassigned;
+    info->pp_interactions = c->lists.pp_pairs;
+    info->pc_interactions = c->lists.pc_pairs;
+    return FSS_OK;
+}
+
+int fss_get_tree(fss_ctx* c, int32_t* loc, int32_t* counts, int32_t* pairs, int64_t cap) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    if (!c->have || !c->tree) return fail(c, FSS_ERR_STATE, "no tree built");
+    const int TL = c->tree_levels, LL = c->leaf_level;
+    const int64_t n = c->n, nfaces = c->geom.lev_off[TL];
+    if (loc) {
+        if (c->cfg.assign_mode == FSS_ASSIGN_REFERENCE) {
+            std::memcpy(loc, c->ref_loc_h.data(), sizeof(int32_t) * TL * n);
+        } else {
+            std::vector<int32_t> perm(n);
+            std::vector<uint32_t> skey(n);
+            CU(cudaMemcpyAsync(perm.data(), c->perm.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+            CU(cudaMemcpyAsync(skey.data(), c->key.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+            CU(cudaStreamSynchronize(c->stream));
+            for (int64_t s = 0; s < n; s++)
+                for (int l = 0; l < TL; l++) loc[int64_t(l) * n + perm[s]] = int32_t(skey[s] >> (2 * (LL - l)));
+        }
+    }
+    if (counts) {
+        if (c->cfg.assign_mode == FSS_ASSIGN_REFERENCE) {
+            std::vector<int32_t> cc(nfaces, 0);
+            for (int l = 0; l < TL; l++)
+                for (int64_t i = 0; i < n; i++) {
+                    const int32_t f = c->ref_loc_h[size_t(l) * n + i];
+                    if (f >= 0) cc[c->geom.lev_off[l] + f]++;
+                }
+            std::memcpy(counts, cc.data(), sizeof(int32_t) * nfaces);
+        } else {
+            std::memcpy(counts, c->counts_h.data(), sizeof(int32_t) * nfaces);
+        }
+    }
+    if (pairs) {
+        if (int64_t(c->pairs.size()) > cap) return fail(c, FSS_ERR_CAPACITY, "pairs buffer too small");
+        for (size_t i = 0; i < c->pairs.size(); i++) {
+            const Pair& p = c->pairs[i];
+            int32_t* r = pairs + 7 * i;
+            r[0] = p.lt; r[1] = p.ls; r[2] = p.t; r[3] = p.s; r[4] = p.nt; r[5] = p.ns; r[6] = p.type;
+        }
+    }
+    return FSS_OK;
+}
+
+int fss_set_leaf_params(fss_ctx* c, int32_t nleaf, const int32_t* degree, const double* theta) {
+    if (!c || !degree || !theta) return fail(c, FSS_ERR_INVALID, "null argument");
+    for (int32_t i = 0; i < nleaf; i++) {
+        if (degree[i] < 0 || degree[i] > kMaxDegree) return fail(c, FSS_ERR_INVALID, "degree out of range");
+        if (!(theta[i] > 0)) return fail(c, FSS_ERR_INVALID, "theta must be positive");
+    }
+    c->leaf_deg.assign(degree, degree + nleaf);
+    c->leaf_theta.assign(theta, theta + nleaf);
+    return FSS_OK;
+}
+
+int fss_profile_enable(fss_ctx* c, int32_t on) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    prof_resolve(c);
+    c->prof = on != 0;
+    c->prof_acc.clear();
+    c->prof_order.clear();
+    return FSS_OK;
+}
+
+int fss_profile_read(fss_ctx* c, char* names, int32_t names_cap, double* ms, int64_t* launches, int32_t cap,
+                     int32_t* count) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    prof_resolve(c);
+    std::string all;
+    int32_t k = 0;
+    for (const std::string& nm : c->prof_order) {
+        if (k < cap) {
+            if (ms) ms[k] = c->prof_acc[nm].ms;
+            if (launches) launches[k] = c->prof_acc[nm].launches;
+        }
+        all += nm;
+        all += '\n';
+        k++;
+    }
+    if (count) *count = k;
+    if (names && names_cap > 0) {
+        std::strncpy(names, all.c_str(), size_t(names_cap) - 1);
+        names[names_cap - 1] = 0;
+    }
+    return FSS_OK;
+}
+
+int fss_work_per_rhs(fss_ctx* c, double* interactions, double* upward_bytes) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    if (interactions) *interactions = c->lists.pp_pairs + c->lists.pc_pairs;
+    if (upward_bytes) {
+        double b = 0;
+        if (c->tree && !c->lists.jobs.empty()) {
+            int levels = 0;
+            for (int l = 0; l <= c->leaf_level; l++) levels += (c->level_mask >> l) & 1;
+            const double es = c->fp64 ? 32.0 : 16.0;
+            b = double(c->n) * es * levels + double(c->lists.n_proxy) * es;
+        }
+        *upward_bytes = b;
+    }
+    return FSS_OK;
+}
+
+int fss_icos_counts(int32_t level, int64_t* nv, int64_t* nf) {
+    if (level < 0 || level > 11) return fail(nullptr, FSS_ERR_INVALID, "level out of range");
+    if (nv) *nv = 10 * (int64_t(1) << (2 * level)) + 2;
+    if (nf) *nf = 20 * (int64_t(1) << (2 * level));
+    return FSS_OK;
+}
+
+int fss_icos_grid(int32_t level, double* xyz, int32_t* faces) {
+    if (level < 0 || level > 11) return fail(nullptr, FSS_ERR_INVALID, "level out of range");
+    std::vector<double> v;
+    std::vector<int32_t> f;
+    icos_grid(level, v, f);
+    if (xyz) std::memcpy(xyz, v.data(), sizeof(double) * v.size());
+    if (faces) std::memcpy(faces, f.data(), sizeof(int32_t) * f.size());
+    return FSS_OK;
+}
+
+int fss_area_init(int64_t n, const double* state5, int64_t nf, const int32_t* faces, double* area) {
+    if (!state5 || !faces || !area) return fail(nullptr, FSS_ERR_INVALID, "null argument");
+    area_init(n, state5, nf, faces, area);
+    return FSS_OK;
+}
+
+int fss_vorticity_rh4_ref(int64_t n, double* state5) {
+    if (!state5) return fail(nullptr, FSS_ERR_INVALID, "null argument");
+    vorticity_rh4_ref(n, state5);
+    return FSS_OK;
+}
+
+int fss_vorticity_rh_vortices(int64_t n, double* state5, const double* area, double amp, int32_t nv, double width,
+                              uint64_t seed) {
+    if (!state5) return fail(nullptr, FSS_ERR_INVALID, "null argument");
+    vorticity_rh_vortices(n, state5, area, amp, nv, width, seed);
+    return FSS_OK;
+}
+
+const char* fss_version(void) { return "fss-b200 0.1 (sm_100a; direct sum + icosahedral BLTC; FP64 and FP32/Kahan)"; }
+
+}  // extern "C"

@@ -1,0 +1,306 @@
+// k_epi.cu -- upward pass (proxy charges), epilogue (velocity, stream
+// function, fused RK4 stage combine + renormalisation) and the total charge.
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace fss {
+
+// ---------------------------------------------------------------- upward pass
+// Proxy charges of a source face S of degree n (BLTC upward pass):
+//   q_k = sum_{j in S} w_j l_k(b_j),   l_k = sum_m Vinv[m][k] phi_m
+// with b_j the barycentric coordinates of the central projection of x_j on
+// S's plane and phi_m = T_a(2 b1 - 1) T_b(2 b2 - 1), a + b <= n.  The moments
+// M_m = sum_j w_j phi_m(b_j) are formed per leaf for every ancestor frame
+// (kernel 1, one block per leaf, particles read once per level), summed over
+// the leaves of each face and contracted with Vinv (kernel 2).  FP64.
+
+constexpr int kUpThreads = 128;
+
+template <typename T>
+__global__ void __launch_bounds__(kUpThreads) k_up_leaf(const typename Vec4<T>::type* __restrict__ src,
+                                                        const int32_t* __restrict__ leaf_start,
+                                                        const double4* __restrict__ frame,
+                                                        const NodeGeom* __restrict__ node,
+                                                        const int64_t* __restrict__ lev_off, int leaf_level,
+                                                        int nmax, int level_mask, double* __restrict__ part) {
+    __shared__ double Tw[kUpThreads][kMaxDegree + 1];
+    __shared__ double Tv[kUpThreads][kMaxDegree + 1];
+    const int leaf = blockIdx.x, tid = threadIdx.x;
+    const int KM = nproxy(nmax);
+    const int a0 = leaf_start[leaf], a1 = leaf_start[leaf + 1];
+    // basis index m -> (a, b): m = g (g + 1) / 2 + b, a = g - b
+    int ma = 0, mb = 0;
+    if (tid < KM) {
+        int g = 0;
+        while ((g + 1) * (g + 2) / 2 <= tid) g++;
+        mb = tid - g * (g + 1) / 2;
+        ma = g - mb;
+    }
+    double fx = 0, fy = 0, fz = 0;
+    if (frame) {
+        const double4 f = frame[leaf];
+        fx = f.x; fy = f.y; fz = f.z;
+    }
+    for (int l = 0; l <= leaf_level; l++) {
+        double* out = part + (int64_t(leaf) * (leaf_level + 1) + l) * KM;
+        if (!((level_mask >> l) & 1)) continue;
+        const NodeGeom ng = node[lev_off[l] + (leaf >> (2 * (leaf_level - l)))];
+        double acc = 0;
+        for (int c0 = a0; c0 < a1; c0 += kUpThreads) {
+            const int j = c0 + tid;
+            if (j < a1) {
+                const typename Vec4<T>::type q = src[j];
+                const double x = fx + double(q.x), y = fy + double(q.y), z = fz + double(q.z), w = double(q.w);
+                const double c0_ = ng.minv[0] * x + ng.minv[1] * y + ng.minv[2] * z;
+                const double c1_ = ng.minv[3] * x + ng.minv[4] * y + ng.minv[5] * z;
+                const double c2_ = ng.minv[6] * x + ng.minv[7] * y + ng.minv[8] * z;
+                const double inv = 1.0 / (c0_ + c1_ + c2_);
+                const double u = 2.0 * (c0_ * inv) - 1.0, v = 2.0 * (c1_ * inv) - 1.0;
+                double ta0 = 1.0, ta1 = u, tb0 = 1.0, tb1 = v;
+                Tw[tid][0] = w;
+                Tv[tid][0] = 1.0;
+                if (nmax >= 1) { Tw[tid][1] = w * u; Tv[tid][1] = v; }
+                for (int a = 2; a <= nmax; a++) {
+                    const double ta2 = 2.0 * u * ta1 - ta0, tb2 = 2.0 * v * tb1 - tb0;
+                    Tw[tid][a] = w * ta2;
+                    Tv[tid][a] = tb2;
+                    ta0 = ta1; ta1 = ta2; tb0 = tb1; tb1 = tb2;
+                }
+            }
+            __syncthreads();
+            if (tid < KM) {
+                const int cnt = min(kUpThreads, a1 - c0);
+                for (int jj = 0; jj < cnt; jj++) acc = fma(Tw[jj][ma], Tv[jj][mb], acc);
+            }
+            __syncthreads();
+        }
+        if (tid < KM) out[tid] = acc;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kUpThreads) k_up_combine(const ProxyJob* __restrict__ jobs, const double* __restrict__ part,
+                                                           int leaf_level, int nmax, const double* __restrict__ vinv,
+                                                           const int32_t* __restrict__ vinv_off,
+                                                           const double4* __restrict__ proxy_pos,
+                                                           const NodeGeom* __restrict__ node, int local_frames,
+                                                           int64_t n, typename Vec4<T>::type* __restrict__ src) {
+    __shared__ double M[kMaxK];
+    const ProxyJob job = jobs[blockIdx.x];
+    const int tid = threadIdx.x;
+    const int KM = nproxy(nmax);
+    if (tid < KM) {
+        double s = 0;
+        for (int lf = job.leaf_lo; lf < job.leaf_hi; lf++) s += part[(int64_t(lf) * (leaf_level + 1) + job.level) * KM + tid];
+        M[tid] = s;
+    }
+    __syncthreads();
+    double cx = 0, cy = 0, cz = 0;
+    if (local_frames) {
+        const NodeGeom& ng = node[job.node];
+        cx = ng.cx; cy = ng.cy; cz = ng.cz;
+    }
+    for (int d = 0; d <= nmax; d++) {
+        if (!((job.degmask >> d) & 1)) continue;
+        const int K = nproxy(d);
+        const double* V = vinv + vinv_off[d];
+        for (int k = tid; k < K; k += kUpThreads) {
+            double q = 0;
+            for (int m = 0; m < K; m++) q = fma(V[m * K + k], M[m], q);
+            const int64_t slot = int64_t(job.off[d]) + k;
+            const double4 y = proxy_pos[slot - n];
+            typename Vec4<T>::type o;
+            o.x = T(y.x - cx);
+            o.y = T(y.y - cy);
+            o.z = T(y.z - cz);
+            o.w = T(q);
+            src[slot] = o;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- epilogue
+
+// Sum the partial slots of each target, form the velocity (and stream
+// function), then either write the reference's modify layout (rhs_func) or
+// advance the RK4 stage:
+//   stage 1..3: acc (+)= c k;  x_next = project(s0 + h k), h = dt/2, dt/2, dt
+//   stage 4:    acc += k;      s0 = project(s0 + (dt/6) acc)
+// with project(x) = x/|x| and zeta += -2 omega (z_new - z_old)
+// (new_dynamics.cpp:281-340, helpers.h:362-372 project_points), and refresh
+// the interaction sources of the next stage.
+template <typename T>
+__global__ void k_epilogue(EpiArgs a) {
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= a.n) return;
+    double Ax = 0, Ay = 0, Az = 0, Ap = 0;
+    for (int p = 0; p < a.parts; p++) {
+        const double4 v = a.partials[int64_t(p) * a.pstride + s];
+        Ax += v.x; Ay += v.y; Az += v.z; Ap += v.w;
+    }
+    const double4 x = a.xs[s];
+    const double c = -1.0 / (2.0 * M_PI);
+    const double ux = c * (x.y * Az - x.z * Ay);
+    const double uy = c * (x.z * Ax - x.x * Az);
+    const double uz = c * (x.x * Ay - x.y * Ax);
+    const double dzeta = -2 * a.omega * uz;
+    if (a.mode == EPI_RHS) {
+        const int64_t i = a.perm ? a.perm[s] : s;
+        double* m = a.out5 + 5 * i;
+        m[0] = ux; m[1] = uy; m[2] = uz; m[3] = dzeta; m[4] = 0.0 * (-1.0 / (4.0 * M_PI));
+        if (a.psi) {
+            const double wself = x.w * a.area[s];
+            a.psi[i] = -(M_LN2 / (4.0 * M_PI)) * (Ap - (a.wtotal[0] - wself));
+        }
+        return;
+    }
+    const double4 s0 = a.s0[s];
+    double4 acc;
+    if (a.stage == 1) {
+        acc = make_double4(ux, uy, uz, dzeta);
+    } else {
+        const double f = (a.stage == 4) ? 1.0 : 2.0;
+        acc = a.acc[s];
+        acc.x += ux * f; acc.y += uy * f; acc.z += uz * f; acc.w += dzeta * f;
+    }
+    double t[4];
+    if (a.stage < 4) {
+        a.acc[s] = acc;
+        const double h = (a.stage == 3) ? a.dt : a.dt / 2;
+        t[0] = ux * h; t[1] = uy * h; t[2] = uz * h; t[3] = dzeta * h;
+        t[0] += s0.x; t[1] += s0.y; t[2] += s0.z; t[3] += s0.w;
+    } else {
+        const double h = a.dt / 6;
+        t[0] = acc.x * h; t[1] = acc.y * h; t[2] = acc.z * h; t[3] = acc.w * h;
+        t[0] += s0.x; t[1] += s0.y; t[2] += s0.z; t[3] += s0.w;
+    }
+    double nn = 0;
+    nn += t[0] * t[0];
+    nn += t[1] * t[1];
+    nn += t[2] * t[2];
+    const double sc = 1.0 / sqrt(nn);
+    const double px = t[0] * sc, py = t[1] * sc, pz = t[2] * sc;
+    const double zeta = t[3] + (-2 * a.omega) * (pz - t[2]);
+    const double4 nx = make_double4(px, py, pz, zeta);
+    if (a.stage == 4) a.s0[s] = nx;
+    a.xs[s] = nx;
+    double fx = 0, fy = 0, fz = 0;
+    if (a.frame && a.leaf_of) {
+        const double4 f = a.frame[a.leaf_of[s]];
+        fx = f.x; fy = f.y; fz = f.z;
+    }
+    typename Vec4<T>::type o;
+    o.x = T(px - fx);
+    o.y = T(py - fy);
+    o.z = T(pz - fz);
+    o.w = T(zeta * a.area[s]);
+    static_cast<typename Vec4<T>::type*>(a.src)[s] = o;
+}
+
+// Stage state and interaction sources from the step state (after a
+// stand-alone right-hand side overwrote them).
+template <typename T>
+__global__ void k_refresh(int64_t n, const double4* __restrict__ s0, const double* __restrict__ area,
+                          const uint32_t* __restrict__ leaf_of, const double4* __restrict__ frame,
+                          double4* __restrict__ xs, typename Vec4<T>::type* __restrict__ src) {
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double4 v = s0[s];
+    xs[s] = v;
+    double fx = 0, fy = 0, fz = 0;
+    if (frame && leaf_of) {
+        const double4 f = frame[leaf_of[s]];
+        fx = f.x; fy = f.y; fz = f.z;
+    }
+    typename Vec4<T>::type o;
+    o.x = T(v.x - fx);
+    o.y = T(v.y - fy);
+    o.z = T(v.z - fz);
+    o.w = T(v.w * area[s]);
+    src[s] = o;
+}
+
+// Total charge W = sum zeta_j A_j (deterministic single-block reduction).
+__global__ void __launch_bounds__(1024) k_wsum(int64_t n, const double4* __restrict__ xs, const double* __restrict__ area,
+                                               double* __restrict__ w) {
+    __shared__ double red[1024];
+    double s = 0;
+    for (int64_t i = threadIdx.x; i < n; i += 1024) s += xs[i].w * area[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 512; off > 0; off >>= 1) {
+        if (threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) w[0] = red[0];
+}
+
+// Scatter the device state back to the caller's AoS order.
+__global__ void k_scatter_state(int64_t n, const int32_t* __restrict__ perm, const double4* __restrict__ s0,
+                                const double* __restrict__ tracer, double* __restrict__ out5) {
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int64_t i = perm ? perm[s] : s;
+    const double4 v = s0[s];
+    double* o = out5 + 5 * i;
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; o[4] = tracer[s];
+}
+
+// ---------------------------------------------------------------- launchers
+
+void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, const int32_t* leaf_start,
+                    const double4* frame, const NodeGeom* node, const int64_t* lev_off, int leaf_level, int nmax,
+                    int level_mask, double* part) {
+    if (nleaf == 0 || level_mask == 0) return;
+    if (fp64)
+        k_up_leaf<double><<<nleaf, kUpThreads, 0, st>>>(static_cast<const double4*>(src), leaf_start, frame, node,
+                                                        lev_off, leaf_level, nmax, level_mask, part);
+    else
+        k_up_leaf<float><<<nleaf, kUpThreads, 0, st>>>(static_cast<const float4*>(src), leaf_start, frame, node,
+                                                       lev_off, leaf_level, nmax, level_mask, part);
+}
+
+void launch_up_combine(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part, int leaf_level,
+                       int nmax, const double* vinv, const int32_t* vinv_off, const double4* proxy_pos,
+                       const NodeGeom* node, int local_frames, int64_t n, void* src) {
+    if (njobs == 0) return;
+    if (fp64)
+        k_up_combine<double><<<njobs, kUpThreads, 0, st>>>(jobs, part, leaf_level, nmax, vinv, vinv_off, proxy_pos,
+                                                           node, local_frames, n, static_cast<double4*>(src));
+    else
+        k_up_combine<float><<<njobs, kUpThreads, 0, st>>>(jobs, part, leaf_level, nmax, vinv, vinv_off, proxy_pos,
+                                                          node, local_frames, n, static_cast<float4*>(src));
+}
+
+void launch_epilogue(cudaStream_t st, bool fp64, const EpiArgs& a) {
+    if (a.n == 0) return;
+    const unsigned g = unsigned((a.n + 255) / 256);
+    if (fp64)
+        k_epilogue<double><<<g, 256, 0, st>>>(a);
+    else
+        k_epilogue<float><<<g, 256, 0, st>>>(a);
+}
+
+void launch_refresh(cudaStream_t st, bool fp64, int64_t n, const double4* s0, const double* area,
+                    const uint32_t* leaf_of, const double4* frame, double4* xs, void* src) {
+    if (n == 0) return;
+    const unsigned g = unsigned((n + 255) / 256);
+    if (fp64)
+        k_refresh<double><<<g, 256, 0, st>>>(n, s0, area, leaf_of, frame, xs, static_cast<double4*>(src));
+    else
+        k_refresh<float><<<g, 256, 0, st>>>(n, s0, area, leaf_of, frame, xs, static_cast<float4*>(src));
+}
+
+void launch_wsum(cudaStream_t st, int64_t n, const double4* xs, const double* area, double* w) {
+    k_wsum<<<1, 1024, 0, st>>>(n, xs, area, w);
+}
+
+void launch_scatter_state(cudaStream_t st, int64_t n, const int32_t* perm, const double4* s0, const double* tracer,
+                          double* out5) {
+    if (n == 0) return;
+    k_scatter_state<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, perm, s0, tracer, out5);
+}
+
+}  // namespace fss

@@ -1,0 +1,313 @@
+// k_tree.cu -- GPU tree build: particle -> face assignment on the
+// icosahedral refinement path, stable radix key-sort, leaf ranges, and the
+// gather of the particle state into leaf order.
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace fss {
+
+// ---------------------------------------------------------------- assignment
+
+// Unnormalised cone coordinates of p in the triangle (v1, v2, v3): the 3x3
+// system [v1 v2 v3] c = p solved by LU with partial pivoting in LAPACK
+// dgetf2/dgetrs order (helpers.h:137-150 barycoords via dgesv_).  Every
+// operation is an explicitly rounded intrinsic, so no multiply-add is fused
+// and the result is bit-identical to the host FP64 arithmetic.
+__device__ __forceinline__ void cone_coords_exact(const double* v1, const double* v2, const double* v3,
+                                                  const double* p, double* b) {
+    double a[9] = {v1[0], v1[1], v1[2], v2[0], v2[1], v2[2], v3[0], v3[1], v3[2]};  // a[i + 3j]
+    b[0] = p[0]; b[1] = p[1]; b[2] = p[2];
+    int ipiv[3];
+    bool singular = false;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        int pr = k;
+        double mx = fabs(a[k + 3 * k]);
+#pragma unroll
+        for (int i = k + 1; i < 3; i++)
+            if (fabs(a[i + 3 * k]) > mx) { mx = fabs(a[i + 3 * k]); pr = i; }
+        ipiv[k] = pr;
+        if (a[pr + 3 * k] == 0.0) { singular = true; continue; }
+        if (pr != k) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) { double t = a[k + 3 * j]; a[k + 3 * j] = a[pr + 3 * j]; a[pr + 3 * j] = t; }
+        }
+        const double r = __drcp_rn(a[k + 3 * k]);
+#pragma unroll
+        for (int i = k + 1; i < 3; i++) a[i + 3 * k] = __dmul_rn(a[i + 3 * k], r);
+#pragma unroll
+        for (int j = k + 1; j < 3; j++)
+#pragma unroll
+            for (int i = k + 1; i < 3; i++) a[i + 3 * j] = __dsub_rn(a[i + 3 * j], __dmul_rn(a[i + 3 * k], a[k + 3 * j]));
+    }
+    if (singular) return;  // dgesv_ leaves b = p
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const int pr = ipiv[k];
+        if (pr != k) { double t = b[k]; b[k] = b[pr]; b[pr] = t; }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int i = k + 1; i < 3; i++) b[i] = __dsub_rn(b[i], __dmul_rn(a[i + 3 * k], b[k]));
+#pragma unroll
+    for (int k = 2; k >= 0; k--) {
+        b[k] = __ddiv_rn(b[k], a[k + 3 * k]);
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+            if (i < k) b[i] = __dsub_rn(b[i], __dmul_rn(a[i + 3 * k], b[k]));
+    }
+}
+
+// icos_utils.h:145-170 point_assign for every particle.  Level 0 searches
+// the 20 faces, level l the four children of the level l-1 face; the first
+// face whose cone coordinates are all >= 0 wins.  In reference mode a
+// particle with no match is left out of the level (loc = -1) and the next
+// level searches the children of face 0, as the reference does with its
+// zero-initialised tree_point_locs.  In complete mode the particle goes to
+// the candidate whose smallest cone coordinate is largest, so every particle
+// has exactly one leaf.  key[i] = leaf face (complete mode only).
+__global__ void k_assign(int64_t n, const double* __restrict__ in5, const double* __restrict__ verts,
+                         const int32_t* __restrict__ tri_verts, const int64_t* __restrict__ lev_off,
+                         int tree_levels, int reference_mode, int32_t* __restrict__ loc, uint32_t* __restrict__ key,
+                         int* __restrict__ err) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double p[3] = {in5[5 * i], in5[5 * i + 1], in5[5 * i + 2]};
+    int prev = 0;
+    for (int l = 0; l < tree_levels; l++) {
+        const int lb = (l > 0) ? 4 * prev : 0, ub = (l > 0) ? lb + 4 : 20;
+        int found = -1, best = lb;
+        double best_min = -1e300;
+        for (int j = lb; j < ub; j++) {
+            const int32_t* tv = tri_verts + 3 * (lev_off[l] + j);
+            double c[3];
+            cone_coords_exact(verts + 3 * int64_t(tv[0]), verts + 3 * int64_t(tv[1]), verts + 3 * int64_t(tv[2]), p, c);
+            if (c[0] >= 0 && c[1] >= 0 && c[2] >= 0) { found = j; break; }
+            const double m = fmin(c[0], fmin(c[1], c[2]));
+            if (m > best_min) { best_min = m; best = j; }
+        }
+        if (reference_mode) {
+            if (loc) loc[int64_t(l) * n + i] = found;
+            prev = (found >= 0) ? found : 0;
+        } else {
+            const int f = (found >= 0) ? found : best;
+            if (loc) loc[int64_t(l) * n + i] = f;
+            prev = f;
+        }
+    }
+    if (key) key[i] = uint32_t(prev);
+    (void)err;
+}
+
+// Per-face member counts of every level from loc (reference-mode parity).
+__global__ void k_level_hist(int64_t n, int tree_levels, const int32_t* __restrict__ loc,
+                             const int64_t* __restrict__ lev_off, int32_t* __restrict__ counts) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int l = 0; l < tree_levels; l++) {
+        const int32_t f = loc[int64_t(l) * n + i];
+        if (f >= 0) atomicAdd(&counts[lev_off[l] + f], 1);
+    }
+}
+
+// ---------------------------------------------------------------- radix sort
+// Stable LSD radix sort of (key, value) with 8-bit digits.  Each block owns
+// a tile of kSortTile consecutive elements; warps own consecutive 512-element
+// slices of it, so ranks computed warp by warp, round by round, lane by lane
+// preserve the input order within every digit.
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortPerWarp = 512;
+constexpr int kSortTile = kSortWarps * kSortPerWarp;  // 4096
+
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(int64_t n, const uint32_t* __restrict__ keys, int shift,
+                                                             uint32_t* __restrict__ hist, int nblk) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = int64_t(blockIdx.x) * kSortTile;
+    for (int k = threadIdx.x; k < kSortTile; k += kSortThreads) {
+        const int64_t i = base + k;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[int64_t(threadIdx.x) * nblk + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of m entries in one block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ a, int64_t m) {
+    __shared__ uint32_t part[1024];
+    const int t = threadIdx.x;
+    const int64_t per = (m + 1023) / 1024;
+    const int64_t lo = t * per, hi = (lo + per < m) ? lo + per : m;
+    uint32_t s = 0;
+    for (int64_t i = lo; i < hi; i++) s += a[i];
+    part[t] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const uint32_t v = (t >= off) ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = (t > 0) ? part[t - 1] : 0u;
+    for (int64_t i = lo; i < hi; i++) {
+        const uint32_t v = a[i];
+        a[i] = run;
+        run += v;
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(int64_t n, const uint32_t* __restrict__ kin,
+                                                                const int32_t* __restrict__ vin,
+                                                                uint32_t* __restrict__ kout, int32_t* __restrict__ vout,
+                                                                int shift, const uint32_t* __restrict__ gofs,
+                                                                int nblk) {
+    __shared__ uint32_t cnt[kSortWarps][256];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = lane; d < 256; d += 32) cnt[w][d] = 0;
+    __syncwarp();
+    const int64_t base = int64_t(blockIdx.x) * kSortTile + int64_t(w) * kSortPerWarp;
+    for (int r = 0; r < kSortPerWarp / 32; r++) {
+        const int64_t i = base + r * 32 + lane;
+        if (i < n) atomicAdd(&cnt[w][(kin[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    // per digit: exclusive prefix over warps
+    {
+        const int d = threadIdx.x;  // 256 threads <-> 256 digits
+        uint32_t run = 0;
+        for (int ww = 0; ww < kSortWarps; ww++) {
+            const uint32_t c = cnt[ww][d];
+            cnt[ww][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    for (int r = 0; r < kSortPerWarp / 32; r++) {
+        const int64_t i = base + r * 32 + lane;
+        const bool valid = i < n;
+        const uint32_t k = valid ? kin[i] : 0u;
+        const uint32_t d = (k >> shift) & 255u;
+        const uint32_t tag = valid ? d : (256u + lane);
+        const uint32_t peers = __match_any_sync(0xffffffffu, tag);
+        const uint32_t rank = __popc(peers & lt_mask);
+        uint32_t basepos = 0;
+        if (valid) basepos = cnt[w][d];
+        __syncwarp();
+        if (valid) {
+            const uint64_t pos = uint64_t(gofs[int64_t(d) * nblk + blockIdx.x]) + basepos + rank;
+            kout[pos] = k;
+            vout[pos] = vin ? vin[i] : int32_t(i);
+            if ((__ffs(peers) - 1) == lane) cnt[w][d] += __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+// leaf_start[k] = first sorted position whose key is >= k (k = 0..nleaf).
+__global__ void k_leaf_bounds(int64_t n, const uint32_t* __restrict__ skey, int32_t nleaf,
+                              int32_t* __restrict__ leaf_start) {
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s > n) return;
+    const int64_t prev = (s == 0) ? -1 : int64_t(skey[s - 1]);
+    const int64_t cur = (s == n) ? int64_t(nleaf) : int64_t(skey[s]);
+    for (int64_t k = prev + 1; k <= cur && k <= nleaf; k++) leaf_start[k] = int32_t(s);
+}
+
+// ---------------------------------------------------------------- gather
+
+// Sorted (leaf-order) FP64 state from the caller's AoS state, and the
+// interaction sources: local coordinates against the leaf's frame centre
+// (mixed precision) or absolute coordinates (FP64 / direct sum), w = zeta*A.
+template <typename T>
+__global__ void k_gather(int64_t n, const double* __restrict__ in5, const double* __restrict__ area_in,
+                         const int32_t* __restrict__ perm, const uint32_t* __restrict__ leaf_of,
+                         const double4* __restrict__ frame, double4* __restrict__ s0, double4* __restrict__ xs,
+                         double* __restrict__ area_s, double* __restrict__ tracer_s,
+                         typename Vec4<T>::type* __restrict__ src) {
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int64_t i = perm ? perm[s] : s;
+    const double4 v = make_double4(in5[5 * i], in5[5 * i + 1], in5[5 * i + 2], in5[5 * i + 3]);
+    const double a = area_in[i];
+    if (s0) s0[s] = v;
+    xs[s] = v;
+    area_s[s] = a;
+    if (tracer_s) tracer_s[s] = in5[5 * i + 4];
+    double cx = 0, cy = 0, cz = 0;
+    if (frame && leaf_of) {
+        const double4 f = frame[leaf_of[s]];
+        cx = f.x; cy = f.y; cz = f.z;
+    }
+    typename Vec4<T>::type o;
+    o.x = T(v.x - cx);
+    o.y = T(v.y - cy);
+    o.z = T(v.z - cz);
+    o.w = T(v.w * a);
+    src[s] = o;
+}
+
+// ---------------------------------------------------------------- launchers
+
+void launch_assign(cudaStream_t st, int64_t n, const double* in5, const double* verts, const int32_t* tri_verts,
+                   const int64_t* lev_off, int tree_levels, int reference_mode, int32_t* loc, uint32_t* key, int* err) {
+    if (n == 0) return;
+    k_assign<<<unsigned((n + 127) / 128), 128, 0, st>>>(n, in5, verts, tri_verts, lev_off, tree_levels, reference_mode,
+                                                        loc, key, err);
+}
+
+void launch_level_hist(cudaStream_t st, int64_t n, int tree_levels, const int32_t* loc, const int64_t* lev_off,
+                       int32_t* counts) {
+    if (n == 0) return;
+    k_level_hist<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, tree_levels, loc, lev_off, counts);
+}
+
+int64_t sort_scratch_words(int64_t n) {
+    const int64_t nblk = (n + kSortTile - 1) / kSortTile;
+    return 256 * nblk;
+}
+
+void launch_sort(cudaStream_t st, int64_t n, int bits, uint32_t* keys, uint32_t* keys_tmp, int32_t* vals,
+                 int32_t* vals_tmp, uint32_t* hist) {
+    if (n == 0) return;
+    const int nblk = int((n + kSortTile - 1) / kSortTile);
+    uint32_t *ki = keys, *ko = keys_tmp;
+    int32_t *vi = nullptr, *vo = vals;
+    int pass = 0;
+    for (int shift = 0; shift < bits; shift += 8, pass++) {
+        k_radix_hist<<<nblk, kSortThreads, 0, st>>>(n, ki, shift, hist, nblk);
+        k_scan_exclusive<<<1, 1024, 0, st>>>(hist, int64_t(256) * nblk);
+        k_radix_scatter<<<nblk, kSortThreads, 0, st>>>(n, ki, vi, ko, vo, shift, hist, nblk);
+        std::swap(ki, ko);
+        vi = vo;
+        vo = (vo == vals) ? vals_tmp : vals;
+    }
+    // results end in (ki, vi); make sure they are in (keys, vals)
+    if (ki != keys) cudaMemcpyAsync(keys, ki, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
+    if (vi != vals) cudaMemcpyAsync(vals, vi, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st);
+}
+
+void launch_leaf_bounds(cudaStream_t st, int64_t n, const uint32_t* skey, int32_t nleaf, int32_t* leaf_start) {
+    k_leaf_bounds<<<unsigned((n + 1 + 255) / 256), 256, 0, st>>>(n, skey, nleaf, leaf_start);
+}
+
+void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, const double* area_in, const int32_t* perm,
+                   const uint32_t* leaf_of, const double4* frame, double4* s0, double4* xs, double* area_s,
+                   double* tracer_s, void* src) {
+    if (n == 0) return;
+    const unsigned g = unsigned((n + 255) / 256);
+    if (fp64)
+        k_gather<double><<<g, 256, 0, st>>>(n, in5, area_in, perm, leaf_of, frame, s0, xs, area_s, tracer_s,
+                                            static_cast<double4*>(src));
+    else
+        k_gather<float><<<g, 256, 0, st>>>(n, in5, area_in, perm, leaf_of, frame, s0, xs, area_s, tracer_s,
+                                           static_cast<float4*>(src));
+}
+
+}  // namespace fss

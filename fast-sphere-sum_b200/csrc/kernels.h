@@ -1,0 +1,74 @@
+// kernels.h -- host-callable launchers of the sm_100a kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "fss_internal.h"
+
+namespace fss {
+
+enum EpiMode { EPI_RHS = 0, EPI_RK4 = 1 };
+
+struct EpiArgs {
+    int64_t n = 0;
+    int parts = 1;
+    int64_t pstride = 0;
+    const double4* partials = nullptr;
+    double4* xs = nullptr;          // current stage state (x, y, z, zeta), sorted; updated in RK4 mode
+    const double* area = nullptr;   // sorted
+    double omega = 0;
+    int mode = EPI_RHS;
+    // rhs output (caller's order through perm)
+    const int32_t* perm = nullptr;
+    double* out5 = nullptr;
+    double* psi = nullptr;
+    const double* wtotal = nullptr;  // device scalar: sum zeta A
+    // RK4
+    int stage = 1;
+    double dt = 0;
+    double4* s0 = nullptr;
+    double4* acc = nullptr;
+    // interaction sources of the next stage
+    void* src = nullptr;
+    const uint32_t* leaf_of = nullptr;
+    const double4* frame = nullptr;
+};
+
+struct PairShape {
+    int threads = 128;
+    int per_thread = 1;
+};
+
+// k_tree.cu
+void launch_assign(cudaStream_t st, int64_t n, const double* in5, const double* verts, const int32_t* tri_verts,
+                   const int64_t* lev_off, int tree_levels, int reference_mode, int32_t* loc, uint32_t* key, int* err);
+void launch_level_hist(cudaStream_t st, int64_t n, int tree_levels, const int32_t* loc, const int64_t* lev_off,
+                       int32_t* counts);
+int64_t sort_scratch_words(int64_t n);
+void launch_sort(cudaStream_t st, int64_t n, int bits, uint32_t* keys, uint32_t* keys_tmp, int32_t* vals,
+                 int32_t* vals_tmp, uint32_t* hist);
+void launch_leaf_bounds(cudaStream_t st, int64_t n, const uint32_t* skey, int32_t nleaf, int32_t* leaf_start);
+void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, const double* area_in, const int32_t* perm,
+                   const uint32_t* leaf_of, const double4* frame, double4* s0, double4* xs, double* area_s,
+                   double* tracer_s, void* src);
+
+// k_pairs.cu
+PairShape pairs_shape(bool fp64, int threads_hint);
+cudaError_t launch_pairs(cudaStream_t st, bool fp64, bool psi, PairShape shape, int nitems, const void* src,
+                         const SrcEntry* ents, const WorkItem* items, double4* partials, int64_t pstride, int* err);
+
+// k_epi.cu
+void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, const int32_t* leaf_start,
+                    const double4* frame, const NodeGeom* node, const int64_t* lev_off, int leaf_level, int nmax,
+                    int level_mask, double* part);
+void launch_up_combine(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part, int leaf_level,
+                       int nmax, const double* vinv, const int32_t* vinv_off, const double4* proxy_pos,
+                       const NodeGeom* node, int local_frames, int64_t n, void* src);
+void launch_epilogue(cudaStream_t st, bool fp64, const EpiArgs& a);
+void launch_refresh(cudaStream_t st, bool fp64, int64_t n, const double4* s0, const double* area,
+                    const uint32_t* leaf_of, const double4* frame, double4* xs, void* src);
+void launch_wsum(cudaStream_t st, int64_t n, const double4* xs, const double* area, double* w);
+void launch_scatter_state(cudaStream_t st, int64_t n, const int32_t* perm, const double4* s0, const double* tracer,
+                          double* out5);
+
+}  // namespace fss

@@ -1,0 +1,295 @@
+// traverse.cpp -- treecode interaction lists (host).
+//
+// dual_traverse() is compiled with -ffp-contract=off and follows
+// fast_rhs.h:16-91 tree_traverse operation for operation, so its pair list
+// is bit-identical to the reference's for the same per-face counts.
+#include "traverse.h"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <stdexcept>
+
+namespace fss {
+
+std::vector<Pair> dual_traverse(const TreeGeometry& g, const std::vector<int32_t>& counts, double theta,
+                                int many_count) {
+    const int L = g.tree_levels;
+    std::vector<Pair> out;
+    struct Q { int32_t t, s, lt, ls; };
+    std::vector<Q> q;
+    q.reserve(1 << 16);
+    size_t head = 0;
+    for (int i = 0; i < 20; i++)
+        for (int j = 0; j < 20; j++) q.push_back({i, j, 0, 0});
+    while (head < q.size()) {
+        const Q e = q[head++];
+        const int nt = counts[g.lev_off[e.lt] + e.t], ns = counts[g.lev_off[e.ls] + e.s];
+        if (nt == 0 || ns == 0) continue;  // fast_rhs.h:40
+        const double* ti = &g.tri_info[4 * (g.lev_off[e.lt] + e.t)];
+        const double* si = &g.tri_info[4 * (g.lev_off[e.ls] + e.s)];
+        const double dist = great_circ_dist(ti, si, 1.0);
+        const double sep = (ti[3] + si[3]) / dist;
+        if (dist > 0 && sep < theta) {  // fast_rhs.h:46-58
+            const int ty = ((nt > many_count) ? 2 : 0) + ((ns > many_count) ? 1 : 0);
+            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, ty, 1});
+        } else if (nt < many_count && ns < many_count) {  // :60
+            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, 0, 0});
+        } else if (e.lt == L - 1 && e.ls == L - 1) {  // :63
+            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, 0, 0});
+        } else if (e.lt == L - 1) {  // :66 refine the source
+            for (int c = 0; c < 4; c++) q.push_back({e.t, 4 * e.s + c, e.lt, e.ls + 1});
+        } else if (e.ls == L - 1) {  // :71 refine the target
+            for (int c = 0; c < 4; c++) q.push_back({4 * e.t + c, e.s, e.lt + 1, e.ls});
+        } else if (nt >= ns) {  // :77
+            for (int c = 0; c < 4; c++) q.push_back({4 * e.t + c, e.s, e.lt + 1, e.ls});
+        } else {
+            for (int c = 0; c < 4; c++) q.push_back({e.t, 4 * e.s + c, e.lt, e.ls + 1});
+        }
+        if (head > (1u << 20) && head * 2 > q.size()) {  // keep the FIFO compact
+            q.erase(q.begin(), q.begin() + head);
+            head = 0;
+        }
+    }
+    return out;
+}
+
+std::vector<std::vector<ASrc>> lists_from_pairs(const TreeGeometry& g, int leaf_level, const std::vector<Pair>& pairs,
+                                                int many_count, int degree) {
+    (void)g;
+    const int64_t nleaf = int64_t(20) << (2 * leaf_level);
+    std::vector<std::vector<ASrc>> lists(nleaf);
+    for (const Pair& p : pairs) {
+        const int64_t span = int64_t(1) << (2 * (leaf_level - p.lt));
+        const ASrc src = (p.far && p.ns > many_count) ? ASrc{1, p.ls, p.s, degree} : ASrc{0, p.ls, p.s, 0};
+        for (int64_t lf = p.t * span; lf < (p.t + 1) * span; lf++) lists[lf].push_back(src);
+    }
+    return lists;
+}
+
+std::vector<std::vector<ASrc>> lists_per_leaf(const TreeGeometry& g, int leaf_level, const std::vector<int32_t>& counts,
+                                              const std::vector<int32_t>& leaf_degree,
+                                              const std::vector<double>& leaf_theta) {
+    const int64_t nleaf = int64_t(20) << (2 * leaf_level);
+    std::vector<std::vector<ASrc>> lists(nleaf);
+    struct S { int32_t l, s; };
+    std::vector<S> st;
+    for (int64_t lf = 0; lf < nleaf; lf++) {
+        if (counts[g.lev_off[leaf_level] + lf] == 0) continue;
+        const int deg = leaf_degree[lf];
+        const int K = nproxy(deg);
+        const double th = leaf_theta[lf];
+        const double* ti = &g.tri_info[4 * (g.lev_off[leaf_level] + lf)];
+        st.clear();
+        for (int r = 19; r >= 0; r--) st.push_back({0, r});
+        while (!st.empty()) {
+            const S e = st.back();
+            st.pop_back();
+            const int ns = counts[g.lev_off[e.l] + e.s];
+            if (ns == 0) continue;
+            const double* si = &g.tri_info[4 * (g.lev_off[e.l] + e.s)];
+            const double dist = great_circ_dist(ti, si, 1.0);
+            if (dist > 0 && (ti[3] + si[3]) / dist < th) {
+                lists[lf].push_back(ns > K ? ASrc{1, e.l, e.s, deg} : ASrc{0, e.l, e.s, 0});
+            } else if (e.l == leaf_level) {
+                lists[lf].push_back({0, e.l, e.s, 0});
+            } else {
+                for (int c = 3; c >= 0; c--) st.push_back({e.l + 1, 4 * e.s + c});
+            }
+        }
+    }
+    return lists;
+}
+
+void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& lists, ListOutput& out) {
+    const TreeGeometry& g = *in.g;
+    const int LL = in.leaf_level;
+    const int64_t nleaf = int64_t(20) << (2 * LL);
+    out = ListOutput();
+    // proxy slots in first-use order
+    std::map<std::pair<int64_t, int>, int64_t> slot;  // (global face, degree) -> offset
+    std::map<int64_t, size_t> job_of;                 // global face -> job index
+    std::map<int, std::vector<double>> node_cache;    // degree -> barycentric nodes
+    for (int64_t lf = 0; lf < nleaf; lf++)
+        for (const ASrc& a : lists[lf]) {
+            if (!a.proxy) continue;
+            const int64_t gf = g.lev_off[a.level] + a.node;
+            auto key = std::make_pair(gf, a.deg);
+            if (slot.count(key)) continue;
+            slot[key] = out.n_proxy;
+            auto it = job_of.find(gf);
+            if (it == job_of.end()) {
+                ProxyJob j{};
+                j.level = a.level;
+                j.node = int32_t(gf);
+                j.local = a.node;
+                const int64_t span = int64_t(1) << (2 * (LL - a.level));
+                j.leaf_lo = int32_t(a.node * span);
+                j.leaf_hi = int32_t((a.node + 1) * span);
+                for (int d = 0; d < 12; d++) j.off[d] = -1;
+                job_of[gf] = out.jobs.size();
+                out.jobs.push_back(j);
+                it = job_of.find(gf);
+            }
+            ProxyJob& j = out.jobs[it->second];
+            j.degmask |= 1 << a.deg;
+            j.off[a.deg] = int32_t(in.n + out.n_proxy);
+            out.max_degree = std::max(out.max_degree, a.deg);
+            // proxy positions: y_k = normalise(sum_m l_km v_m)
+            if (!node_cache.count(a.deg)) {
+                std::vector<double> vinv;
+                interp_nodes(a.deg, node_cache[a.deg], vinv);
+            }
+            const std::vector<double>& nodes = node_cache[a.deg];
+            const int K = nproxy(a.deg);
+            const int32_t* tv = &g.tri_verts[3 * gf];
+            const double* v[3] = {&g.verts[3 * int64_t(tv[0])], &g.verts[3 * int64_t(tv[1])], &g.verts[3 * int64_t(tv[2])]};
+            for (int k = 0; k < K; k++) {
+                double y[3];
+                for (int c = 0; c < 3; c++) y[c] = nodes[3 * k] * v[0][c] + nodes[3 * k + 1] * v[1][c] + nodes[3 * k + 2] * v[2][c];
+                const double nn = std::sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+                out.proxy_pos.push_back(y[0] / nn);
+                out.proxy_pos.push_back(y[1] / nn);
+                out.proxy_pos.push_back(y[2] / nn);
+                out.proxy_pos.push_back(0.0);
+                out.proxy_node.push_back(int32_t(gf));
+            }
+            out.n_proxy += K;
+        }
+    // entries and items
+    const int TB = in.threads * in.per_thread;
+    const int P = std::max(1, in.parts);
+    auto centre = [&](int64_t gf, double* c) {
+        if (in.local_frames) {
+            c[0] = g.tri_info[4 * gf]; c[1] = g.tri_info[4 * gf + 1]; c[2] = g.tri_info[4 * gf + 2];
+        } else {
+            c[0] = c[1] = c[2] = 0;
+        }
+    };
+    struct Cost { double cost; WorkItem it; };
+    std::vector<Cost> items;
+    for (int64_t lf = 0; lf < nleaf; lf++) {
+        const int32_t t0 = in.leaf_start[lf], nt = in.leaf_start[lf + 1] - t0;
+        if (nt == 0) continue;
+        double ct[3];
+        centre(g.lev_off[LL] + lf, ct);
+        const int32_t e_begin = int32_t(out.entries.size());
+        for (const ASrc& a : lists[lf]) {
+            const int64_t gf = g.lev_off[a.level] + a.node;
+            if (a.proxy) {
+                SrcEntry e{};
+                e.start = int32_t(in.n + slot[std::make_pair(gf, a.deg)]);
+                e.count = nproxy(a.deg);
+                e.kind = 1;
+                double cs[3];
+                centre(gf, cs);
+                e.dx = cs[0] - ct[0]; e.dy = cs[1] - ct[1]; e.dz = cs[2] - ct[2];
+                out.entries.push_back(e);
+                out.pc_pairs += double(nt) * e.count;
+            } else {
+                const int64_t span = int64_t(1) << (2 * (LL - a.level));
+                for (int64_t l2 = a.node * span; l2 < (a.node + 1) * span; l2++) {
+                    const int32_t s0 = in.leaf_start[l2], ns = in.leaf_start[l2 + 1] - s0;
+                    if (ns == 0) continue;
+                    SrcEntry e{};
+                    e.start = s0;
+                    e.count = ns;
+                    e.kind = 0;
+                    double cs[3];
+                    centre(g.lev_off[LL] + l2, cs);
+                    e.dx = cs[0] - ct[0]; e.dy = cs[1] - ct[1]; e.dz = cs[2] - ct[2];
+                    out.entries.push_back(e);
+                    out.pp_pairs += double(nt) * ns - ((l2 == lf) ? nt : 0);
+                }
+            }
+        }
+        const int32_t e_end = int32_t(out.entries.size());
+        // split [e_begin, e_end) into P parts of similar source counts
+        double total = 0;
+        for (int32_t e = e_begin; e < e_end; e++) total += out.entries[e].count;
+        std::vector<int32_t> cut(P + 1, e_end);
+        cut[0] = e_begin;
+        {
+            double acc = 0;
+            int p = 1;
+            for (int32_t e = e_begin; e < e_end && p < P; e++) {
+                acc += out.entries[e].count;
+                if (acc >= total * p / P) cut[p++] = e + 1;
+            }
+            for (; p < P; p++) cut[p] = e_end;
+        }
+        for (int32_t c0 = 0; c0 < nt; c0 += TB) {
+            const int32_t cn = std::min(TB, nt - c0);
+            for (int p = 0; p < P; p++) {
+                double w = 0;
+                for (int32_t e = cut[p]; e < cut[p + 1]; e++) w += out.entries[e].count;
+                items.push_back({w * cn, WorkItem{t0 + c0, cn, cut[p], cut[p + 1], p, int32_t(lf)}});
+            }
+        }
+    }
+    std::stable_sort(items.begin(), items.end(), [](const Cost& a, const Cost& b) { return a.cost > b.cost; });
+    out.items.reserve(items.size());
+    for (auto& c : items) out.items.push_back(c.it);
+}
+
+// ---------------------------------------------------------------- interpolation
+
+void interp_nodes(int n, std::vector<double>& nodes, std::vector<double>& vinv) {
+    const int K = nproxy(n);
+    nodes.assign(3 * K, 0.0);
+    if (n == 0) {
+        nodes[0] = nodes[1] = nodes[2] = 1.0 / 3.0;
+        vinv.assign(1, 1.0);
+        return;
+    }
+    std::vector<double> v(n + 1);
+    for (int m = 0; m <= n; m++) v[m] = 0.5 * (1.0 - std::cos(M_PI * m / n));
+    int k = 0;
+    for (int i = 0; i <= n; i++)
+        for (int j = 0; j <= n - i; j++, k++) {
+            const int l = n - i - j;
+            nodes[3 * k] = (1 + 2 * v[i] - v[j] - v[l]) / 3.0;
+            nodes[3 * k + 1] = (1 + 2 * v[j] - v[i] - v[l]) / 3.0;
+            nodes[3 * k + 2] = 1.0 - nodes[3 * k] - nodes[3 * k + 1];
+        }
+    // Vandermonde V[k][m], basis m <-> (a, b): degree g = a + b, m = g(g+1)/2 + b
+    std::vector<double> V(size_t(K) * K);
+    std::vector<double> Ta(n + 1), Tb(n + 1);
+    for (int q = 0; q < K; q++) {
+        const double x = 2 * nodes[3 * q] - 1, y = 2 * nodes[3 * q + 1] - 1;
+        Ta[0] = 1; Tb[0] = 1;
+        if (n >= 1) { Ta[1] = x; Tb[1] = y; }
+        for (int a = 2; a <= n; a++) { Ta[a] = 2 * x * Ta[a - 1] - Ta[a - 2]; Tb[a] = 2 * y * Tb[a - 1] - Tb[a - 2]; }
+        for (int gdeg = 0, m = 0; gdeg <= n; gdeg++)
+            for (int b = 0; b <= gdeg; b++, m++) V[size_t(q) * K + m] = Ta[gdeg - b] * Tb[b];
+    }
+    // Gauss-Jordan inverse with partial pivoting
+    std::vector<double> A(V), I(size_t(K) * K, 0.0);
+    for (int i = 0; i < K; i++) I[size_t(i) * K + i] = 1;
+    for (int c = 0; c < K; c++) {
+        int p = c;
+        for (int r = c + 1; r < K; r++)
+            if (std::fabs(A[size_t(r) * K + c]) > std::fabs(A[size_t(p) * K + c])) p = r;
+        if (A[size_t(p) * K + c] == 0.0) throw std::runtime_error("singular interpolation matrix");
+        if (p != c)
+            for (int j = 0; j < K; j++) {
+                std::swap(A[size_t(p) * K + j], A[size_t(c) * K + j]);
+                std::swap(I[size_t(p) * K + j], I[size_t(c) * K + j]);
+            }
+        const double inv = 1.0 / A[size_t(c) * K + c];
+        for (int j = 0; j < K; j++) { A[size_t(c) * K + j] *= inv; I[size_t(c) * K + j] *= inv; }
+        for (int r = 0; r < K; r++) {
+            if (r == c) continue;
+            const double f = A[size_t(r) * K + c];
+            if (f == 0.0) continue;
+            for (int j = 0; j < K; j++) {
+                A[size_t(r) * K + j] -= f * A[size_t(c) * K + j];
+                I[size_t(r) * K + j] -= f * I[size_t(c) * K + j];
+            }
+        }
+    }
+    // I = V^{-1}: I[m][k]; l_k(x) = sum_m I[m][k] phi_m(x)
+    vinv = I;
+}
+
+}  // namespace fss

@@ -1,0 +1,77 @@
+// traverse.h -- interaction lists of the icosahedral treecode (host).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "fss_internal.h"
+#include "geometry.h"
+
+namespace fss {
+
+// One record of fast_rhs.h:16-91 tree_traverse (struct_list.h:6-14
+// interaction_pair) plus whether it came from the well-separated branch.
+struct Pair {
+    int32_t lt, ls, t, s, nt, ns, type;  // type: 0 pp, 1 pc, 2 cp, 3 cc
+    int32_t far;
+};
+
+// The reference's dual traversal, bit-exact: FIFO over (target, source)
+// faces seeded with all 20x20 level-0 pairs; counts are per-face particle
+// counts (levels concatenated).
+std::vector<Pair> dual_traverse(const TreeGeometry& g, const std::vector<int32_t>& counts, double theta,
+                                int many_count);
+
+// Source of one target leaf before materialisation: the particles of face
+// (level, node), or the degree-`deg` proxies of that face.
+struct ASrc {
+    int32_t proxy;  // 0 particles, 1 proxies
+    int32_t level, node, deg;
+};
+
+struct ListInput {
+    const TreeGeometry* g = nullptr;
+    int leaf_level = 0;                 // tree_levels - 1
+    int64_t n = 0;                      // particles
+    const int32_t* leaf_start = nullptr;  // nleaf + 1 (sorted order)
+    bool local_frames = true;           // mixed: leaf / node centre frames
+    int threads = 128, per_thread = 1;  // targets per block = threads * per_thread
+    int parts = 1;                      // source-list split
+};
+
+struct ListOutput {
+    std::vector<SrcEntry> entries;
+    std::vector<WorkItem> items;
+    std::vector<ProxyJob> jobs;
+    std::vector<double> proxy_pos;  // 4 doubles per proxy slot: y (on sphere) and pad
+    std::vector<int32_t> proxy_node;  // proxy slot -> face (global index)
+    int64_t n_proxy = 0;            // proxy slots after the n particles
+    double pp_pairs = 0, pc_pairs = 0;
+    int max_degree = 0;
+};
+
+// Per-target-leaf source lists from the reference's pair list: every pair
+// (T, S) gives each leaf under T either S's proxies (well separated and S
+// holds more than many_count particles) or S's particles, leaf by leaf.
+std::vector<std::vector<ASrc>> lists_from_pairs(const TreeGeometry& g, int leaf_level,
+                                                const std::vector<Pair>& pairs, int many_count, int degree);
+
+// Per-target-leaf traversal with its own (degree, theta): a source face is
+// taken as proxies when (r_t + r_s)/d < theta and it holds more particles
+// than its proxy count, as particles when well separated but small or when
+// it is a leaf, otherwise its four children are visited.
+std::vector<std::vector<ASrc>> lists_per_leaf(const TreeGeometry& g, int leaf_level,
+                                              const std::vector<int32_t>& counts,
+                                              const std::vector<int32_t>& leaf_degree,
+                                              const std::vector<double>& leaf_theta);
+
+// Materialise entries, work items, proxy slots and upward-pass jobs.
+void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& lists, ListOutput& out);
+
+// Proxy node set: barycentric interpolation points of degree n on a
+// triangle (Blyth-Pozrikidis construction on Chebyshev-Lobatto points) and
+// the inverse of the Vandermonde matrix of the Chebyshev product basis
+// T_a(2 l1 - 1) T_b(2 l2 - 1), a + b <= n.  nodes: 3 doubles each; vinv: K x K
+// row-major with vinv[m*K + k] = coefficient of basis m in Lagrange poly k.
+void interp_nodes(int n, std::vector<double>& nodes, std::vector<double>& vinv);
+
+}  // namespace fss

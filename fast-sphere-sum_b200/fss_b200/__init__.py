@@ -1,0 +1,295 @@
+"""fss_b200 -- ctypes front end of ``libfss.so`` (the C ABI in include/fss.h).
+
+The product path is the CUDA library; this module only marshals numpy
+arrays.  There is no CPU fallback: if ``libfss.so`` is missing or has no GPU,
+the calls raise.
+
+Mirrors the reference's interface (cygnari/fast-sphere-sum,
+Old-BVE-code/rhs_eval.h:47 ``rhs_func(modify, curr_state, area, omega,
+config1)``): state arrays are (N, 5) float64 ``[x, y, z, zeta, tracer]`` and
+``rhs`` returns ``modify`` in the same layout.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfss.so")
+CSRC = os.path.join(os.path.dirname(HERE), "csrc")
+
+OMEGA = 2.0 * np.pi
+PREC_FP64, PREC_MIXED = 0, 1
+METHOD_DIRECT, METHOD_TREECODE = 0, 1
+ASSIGN_COMPLETE, ASSIGN_REFERENCE = 0, 1
+LIST_DUAL, LIST_LEAF = 0, 1
+STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NOMEM", 4: "TIMEOUT", 5: "TREE", 6: "STATE",
+          7: "UNSUPPORTED", 8: "CAPACITY"}
+
+
+class FssError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"fss error {STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("precision", C.c_int32), ("method", C.c_int32),
+                ("tree_levels", C.c_int32), ("leaf_target", C.c_int32), ("degree", C.c_int32),
+                ("theta", C.c_double), ("many_count", C.c_int32), ("assign_mode", C.c_int32),
+                ("list_mode", C.c_int32), ("use_graph", C.c_int32), ("src_parts", C.c_int32),
+                ("block_threads", C.c_int32), ("reserved", C.c_int32 * 8)]
+
+
+class TreeInfo(C.Structure):
+    _fields_ = [("tree_levels", C.c_int32), ("leaf_count", C.c_int32), ("degree", C.c_int32),
+                ("n_proxy", C.c_int32), ("n_pairs", C.c_int64), ("n_list_entries", C.c_int64),
+                ("n_items", C.c_int64), ("unassigned", C.c_int64), ("pp_interactions", C.c_double),
+                ("pc_interactions", C.c_double)]
+
+
+def build():
+    """Compile libfss.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-j8", "-C", CSRC], check=True)
+
+
+_lib = None
+_D = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_I = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+_i64 = C.c_int64
+
+# every symbol include/fss.h declares
+SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fss_set_stream",
+           "fss_set_particles", "fss_rebuild_tree", "fss_rhs", "fss_rhs_direct", "fss_rhs_treecode",
+           "fss_rk4_step", "fss_rk4_step_host", "fss_get_state", "fss_rhs_current", "fss_get_tree_info",
+           "fss_get_tree", "fss_set_leaf_params", "fss_profile_enable", "fss_profile_read",
+           "fss_work_per_rhs", "fss_icos_counts", "fss_icos_grid", "fss_area_init",
+           "fss_vorticity_rh4_ref", "fss_vorticity_rh_vortices", "fss_version"]
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FssError(7, f"{LIB_PATH} is not built (run __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    L.fss_config_init.argtypes = [P(Config)]
+    L.fss_config_init.restype = None
+    L.fss_create.argtypes = [P(Config), P(_vp)]
+    L.fss_destroy.argtypes = [_vp]
+    L.fss_destroy.restype = None
+    L.fss_last_error.argtypes = [_vp]
+    L.fss_last_error.restype = C.c_char_p
+    L.fss_set_stream.argtypes = [_vp, _vp]
+    L.fss_set_particles.argtypes = [_vp, _i64, _D, _D]
+    L.fss_rebuild_tree.argtypes = [_vp]
+    for nm in ("fss_rhs", "fss_rhs_direct", "fss_rhs_treecode"):
+        getattr(L, nm).argtypes = [_vp, _D, _D, C.c_double, _D, _vp]
+    L.fss_rk4_step.argtypes = [_vp, C.c_double, C.c_double, C.c_int32]
+    L.fss_rk4_step_host.argtypes = [_vp, _vp, C.c_double, C.c_double, C.c_int32]
+    L.fss_get_state.argtypes = [_vp, _D]
+    L.fss_rhs_current.argtypes = [_vp, C.c_double, _D, _vp]
+    L.fss_get_tree_info.argtypes = [_vp, P(TreeInfo)]
+    L.fss_get_tree.argtypes = [_vp, _vp, _vp, _vp, _i64]
+    L.fss_set_leaf_params.argtypes = [_vp, C.c_int32, _I, _D]
+    L.fss_profile_enable.argtypes = [_vp, C.c_int32]
+    L.fss_profile_read.argtypes = [_vp, C.c_char_p, C.c_int32, _vp, _vp, C.c_int32, P(C.c_int32)]
+    L.fss_work_per_rhs.argtypes = [_vp, P(C.c_double), P(C.c_double)]
+    L.fss_icos_counts.argtypes = [C.c_int32, P(_i64), P(_i64)]
+    L.fss_icos_grid.argtypes = [C.c_int32, _D, _I]
+    L.fss_area_init.argtypes = [_i64, _D, _i64, _I, _D]
+    L.fss_vorticity_rh4_ref.argtypes = [_i64, _D]
+    L.fss_vorticity_rh_vortices.argtypes = [_i64, _D, _vp, C.c_double, C.c_int32, C.c_double, C.c_uint64]
+    L.fss_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _check(rc, ctx=None):
+    if rc != 0:
+        msg = lib().fss_last_error(ctx).decode()
+        raise FssError(rc, msg)
+
+
+# ------------------------------------------------------------------ inputs
+
+def icos_grid(level):
+    """Level-`level` icosahedral vertices (icos_init order) and faces."""
+    nv, nf = _i64(), _i64()
+    _check(lib().fss_icos_counts(level, C.byref(nv), C.byref(nf)))
+    xyz = np.zeros((nv.value, 3))
+    faces = np.zeros((nf.value, 3), dtype=np.int32)
+    _check(lib().fss_icos_grid(level, xyz.reshape(-1), faces.reshape(-1)))
+    return xyz, faces
+
+
+def area_init(state5, faces):
+    s = np.ascontiguousarray(state5, dtype=np.float64)
+    f = np.ascontiguousarray(faces, dtype=np.int32)
+    area = np.zeros(s.shape[0])
+    _check(lib().fss_area_init(s.shape[0], s.reshape(-1), f.shape[0], f.reshape(-1), area))
+    return area
+
+
+RH_AMP = 7.848e-6 * 86400.0  # w = K of the Rossby-Haurwitz wave, per day
+
+
+def make_state(level, field="rh4_ref", n_vortex=0, seed=1, amp=RH_AMP, width=0.1):
+    """(state5 (N,5), area (N,)) on the level-`level` icosahedral grid.
+
+    field 'rh4_ref': the reference's rossby_haurwitz_4 (vorticity_functions.h:13).
+    field 'rh_vortices': RH R=4 wave (w = K = amp) + n_vortex seeded Gaussian vortices.
+    """
+    xyz, faces = icos_grid(level)
+    s = np.zeros((xyz.shape[0], 5))
+    s[:, :3] = xyz
+    area = area_init(s, faces)
+    if field == "rh4_ref":
+        _check(lib().fss_vorticity_rh4_ref(s.shape[0], s.reshape(-1)))
+    elif field == "rh_vortices":
+        _check(lib().fss_vorticity_rh_vortices(s.shape[0], s.reshape(-1), area.ctypes.data_as(_vp), amp,
+                                               n_vortex, width, seed))
+    else:
+        raise ValueError(field)
+    return s, area
+
+
+# ------------------------------------------------------------------ context
+
+class Context:
+    """One problem on one GPU.  Keyword arguments set fss_config fields."""
+
+    def __init__(self, **kw):
+        L = lib()
+        cfg = Config()
+        L.fss_config_init(C.byref(cfg))
+        for k, v in kw.items():
+            if not hasattr(cfg, k):
+                raise TypeError(f"unknown config field {k}")
+            setattr(cfg, k, v)
+        self.cfg = cfg
+        h = _vp()
+        _check(L.fss_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fss_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, rc):
+        _check(rc, self.h)
+
+    def set_stream(self, stream_handle):
+        self._c(lib().fss_set_stream(self.h, stream_handle))
+
+    def set_particles(self, state5, area):
+        s = np.ascontiguousarray(state5, dtype=np.float64)
+        a = np.ascontiguousarray(area, dtype=np.float64)
+        self._c(lib().fss_set_particles(self.h, s.shape[0], s.reshape(-1), a))
+        self.n = s.shape[0]
+
+    def rebuild_tree(self):
+        self._c(lib().fss_rebuild_tree(self.h))
+
+    def _rhs(self, fn, state5, area, omega, psi):
+        s = np.ascontiguousarray(state5, dtype=np.float64)
+        a = np.ascontiguousarray(area, dtype=np.float64)
+        out = np.zeros_like(s)
+        p = np.zeros(s.shape[0]) if psi else None
+        self._c(fn(self.h, s.reshape(-1), a, omega, out.reshape(-1), p.ctypes.data_as(_vp) if psi else None))
+        return (out, p) if psi else out
+
+    def rhs(self, state5, area, omega=OMEGA, psi=False):
+        """rhs_eval.h:47 rhs_func: modify (N,5) [and psi (N,)]."""
+        return self._rhs(lib().fss_rhs, state5, area, omega, psi)
+
+    def rhs_direct(self, state5, area, omega=OMEGA, psi=False):
+        return self._rhs(lib().fss_rhs_direct, state5, area, omega, psi)
+
+    def rhs_treecode(self, state5, area, omega=OMEGA, psi=False):
+        return self._rhs(lib().fss_rhs_treecode, state5, area, omega, psi)
+
+    def rhs_current(self, omega=OMEGA, psi=False):
+        out = np.zeros((self.n, 5))
+        p = np.zeros(self.n) if psi else None
+        self._c(lib().fss_rhs_current(self.h, omega, out.reshape(-1), p.ctypes.data_as(_vp) if psi else None))
+        return (out, p) if psi else out
+
+    def rk4_step(self, dt, omega=OMEGA, nsteps=1):
+        self._c(lib().fss_rk4_step(self.h, dt, omega, nsteps))
+
+    def rk4_step_host(self, state5, dt, omega=OMEGA, nsteps=1):
+        """In place on a C-contiguous float64 (N,5) array (may be pinned)."""
+        assert state5.dtype == np.float64 and state5.flags.c_contiguous
+        self._c(lib().fss_rk4_step_host(self.h, state5.ctypes.data_as(_vp), dt, omega, nsteps))
+        return state5
+
+    def rk4_step_host_ptr(self, ptr, dt, omega=OMEGA, nsteps=1):
+        self._c(lib().fss_rk4_step_host(self.h, ptr, dt, omega, nsteps))
+
+    def get_state(self):
+        out = np.zeros((self.n, 5))
+        self._c(lib().fss_get_state(self.h, out.reshape(-1)))
+        return out
+
+    def tree_info(self):
+        ti = TreeInfo()
+        self._c(lib().fss_get_tree_info(self.h, C.byref(ti)))
+        return {k: getattr(ti, k) for k, _ in TreeInfo._fields_}
+
+    def get_tree(self):
+        """(loc[levels, N], counts, pairs[P, 7]) in the reference's formats."""
+        ti = self.tree_info()
+        TL = ti["tree_levels"]
+        nf = sum(20 * 4 ** l for l in range(TL))
+        loc = np.zeros((TL, self.n), dtype=np.int32)
+        counts = np.zeros(nf, dtype=np.int32)
+        pairs = np.zeros((ti["n_pairs"], 7), dtype=np.int32)
+        self._c(lib().fss_get_tree(self.h, loc.ctypes.data_as(_vp), counts.ctypes.data_as(_vp),
+                                   pairs.ctypes.data_as(_vp), ti["n_pairs"]))
+        return loc, counts, pairs
+
+    def set_leaf_params(self, degree, theta):
+        d = np.ascontiguousarray(degree, dtype=np.int32)
+        t = np.ascontiguousarray(theta, dtype=np.float64)
+        self._c(lib().fss_set_leaf_params(self.h, d.size, d, t))
+
+    def profile(self, on=True):
+        self._c(lib().fss_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self):
+        names = C.create_string_buffer(4096)
+        ms = np.zeros(64)
+        ln = np.zeros(64, dtype=np.int64)
+        cnt = C.c_int32()
+        self._c(lib().fss_profile_read(self.h, names, 4096, ms.ctypes.data_as(_vp), ln.ctypes.data_as(_vp), 64,
+                                       C.byref(cnt)))
+        nm = names.value.decode().split("\n")[:cnt.value]
+        return {n: (float(ms[i]), int(ln[i])) for i, n in enumerate(nm)}
+
+    def work_per_rhs(self):
+        a, b = C.c_double(), C.c_double()
+        self._c(lib().fss_work_per_rhs(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+
+def version():
+    return lib().fss_version().decode()

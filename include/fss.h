@@ -1,0 +1,197 @@
+/*
+ * fss.h -- C ABI of the B200 barotropic-vorticity right-hand side.
+ *
+ * Drop-in replacement for the right-hand-side evaluators of
+ * cygnari/fast-sphere-sum (Old-BVE-code/rhs_eval.h):
+ *
+ *   rhs_func(modify, curr_state, area, omega, run_information&)  rhs_eval.h:47-56
+ *   rhs_direct_sum(modify, curr_state, area, omega, points)     rhs_eval.h:15-32
+ *   rhs_fast_sum(modify, curr_state, area, config1, omega)      rhs_eval.h:34-45
+ *
+ * plus the tree set-up those evaluators read from run_information
+ * (icos_utils.h:135 icosahedron_init, :172 points_assign, fast_rhs.h:16
+ * tree_traverse, interp_utils.h:61 interp_init) and the RK4 particle loop
+ * that calls them (new_dynamics.cpp:281-340, helpers.h:362 project_points).
+ *
+ * Conventions (the reference's): particle state is an array of 5 doubles per
+ * particle {x, y, z, zeta (relative vorticity), tracer}; area is one double
+ * per particle; modify has the same layout as the state and is fully
+ * overwritten with {u_x, u_y, u_z, dzeta/dt = -2 omega u_z, 0}.  Time is in
+ * days, the sphere has radius 1, omega = 2 pi.
+ *
+ * Every entry point returns an fss_status (0 = success); no exception
+ * crosses this boundary.  A context is not thread-safe: one host thread at a
+ * time.  Host pointers are plain (pageable or pinned) host memory unless a
+ * function says "device".
+ */
+#ifndef FSS_H
+#define FSS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fss_status {
+    FSS_OK = 0,
+    FSS_ERR_INVALID = 1,      /* bad argument or configuration */
+    FSS_ERR_CUDA = 2,         /* CUDA runtime error (see fss_last_error) */
+    FSS_ERR_NOMEM = 3,        /* device or host allocation failed */
+    FSS_ERR_TIMEOUT = 4,      /* a kernel's bounded wait ran out */
+    FSS_ERR_TREE = 5,         /* tree build failed (e.g. unassigned particles) */
+    FSS_ERR_STATE = 6,        /* call order (e.g. no particles set) */
+    FSS_ERR_UNSUPPORTED = 7,  /* compiled without this feature / no GPU */
+    FSS_ERR_CAPACITY = 8      /* an output buffer is too small */
+} fss_status;
+
+typedef enum fss_precision {
+    FSS_PREC_FP64 = 0,   /* FP64 everywhere (the plain FP64 path) */
+    FSS_PREC_MIXED = 1   /* FP32 interactions + Kahan, FP64 RK4/renorm/interp */
+} fss_precision;
+
+typedef enum fss_method {
+    FSS_METHOD_DIRECT = 0,    /* rhs_direct_sum: all pairs */
+    FSS_METHOD_TREECODE = 1   /* icosahedral-tree barycentric Lagrange treecode */
+} fss_method;
+
+typedef enum fss_assign_mode {
+    FSS_ASSIGN_COMPLETE = 0,  /* reference first-match rule; particles it drops
+                                 go to their most-inside child instead */
+    FSS_ASSIGN_REFERENCE = 1  /* exactly the reference's points_assign
+                                 (membership/pair parity only) */
+} fss_assign_mode;
+
+typedef enum fss_list_mode {
+    FSS_LIST_DUAL = 0,   /* the reference's dual traversal (fast_rhs.h:16) */
+    FSS_LIST_LEAF = 1    /* per-target-leaf traversal with per-leaf (n, theta) */
+} fss_list_mode;
+
+typedef struct fss_config {
+    int32_t device;        /* CUDA device ordinal */
+    int32_t precision;     /* fss_precision */
+    int32_t method;        /* fss_method (reference: run_information::use_fast) */
+    int32_t tree_levels;   /* reference -l: levels 0..tree_levels-1, leaves on the
+                              last; 0 = smallest depth whose mean leaf holds at
+                              least leaf_target particles */
+    int32_t leaf_target;   /* for tree_levels == 0 (default 64) */
+    int32_t degree;        /* interpolation degree n (K = (n+1)(n+2)/2 proxies) */
+    double theta;          /* MAC (reference -h, default 0.7) */
+    int32_t many_count;    /* reference cluster threshold; < 0 means K */
+    int32_t assign_mode;   /* fss_assign_mode */
+    int32_t list_mode;     /* fss_list_mode */
+    int32_t use_graph;     /* capture the RK4 step in a CUDA graph */
+    int32_t src_parts;     /* split each target's source list in this many parts
+                              (0 = automatic) */
+    int32_t block_threads; /* threads per interaction block (0 = automatic) */
+    int32_t reserved[8];
+} fss_config;
+
+typedef struct fss_ctx fss_ctx;
+
+/* Defaults: FP64... see fss.cpp; mixed precision, treecode, auto depth. */
+void fss_config_init(fss_config* cfg);
+
+int fss_create(const fss_config* cfg, fss_ctx** out);
+void fss_destroy(fss_ctx* ctx);
+/* Message for the last failing call on this context (or on a NULL context). */
+const char* fss_last_error(const fss_ctx* ctx);
+/* Launch stream for all later work (a cudaStream_t; NULL = the context's own). */
+int fss_set_stream(fss_ctx* ctx, void* cuda_stream);
+
+/* Upload a particle set (host, 5 doubles per particle, in the caller's order)
+ * and, for the treecode, build the tree once, as the reference does before
+ * its time loop (new_dynamics.cpp:187-199).  The tree stays fixed until the
+ * next fss_set_particles or fss_rebuild_tree. */
+int fss_set_particles(fss_ctx* ctx, int64_t n, const double* state5, const double* area);
+/* Re-assign particles and rebuild the interaction lists from the current
+ * device state (new_dynamics.cpp:335, after AMR, calls points_assign again). */
+int fss_rebuild_tree(fss_ctx* ctx);
+
+/* rhs_eval.h:47 rhs_func.  state5/area/modify5 are host arrays in the
+ * caller's order; psi (nullable) receives the stream function.  The tree of
+ * fss_set_particles is reused; if the particle count differs, the particles
+ * are set first.  Uses the context's method. */
+int fss_rhs(fss_ctx* ctx, const double* state5, const double* area, double omega,
+            double* modify5, double* psi);
+/* rhs_eval.h:15 rhs_direct_sum (then scaled and dzeta/dt set as rhs_func). */
+int fss_rhs_direct(fss_ctx* ctx, const double* state5, const double* area, double omega,
+                   double* modify5, double* psi);
+/* rhs_eval.h:34 rhs_fast_sum, through the treecode (then scaled as rhs_func). */
+int fss_rhs_treecode(fss_ctx* ctx, const double* state5, const double* area, double omega,
+                     double* modify5, double* psi);
+
+/* RK4 steps on the device-resident state (new_dynamics.cpp:281-340 order:
+ * stage states projected onto the sphere, zeta adjusted by -2 omega dz). */
+int fss_rk4_step(fss_ctx* ctx, double dt, double omega, int32_t nsteps);
+/* Same, with the state uploaded from and downloaded to host memory. */
+int fss_rk4_step_host(fss_ctx* ctx, double* state5, double dt, double omega, int32_t nsteps);
+/* Download the device-resident state (caller's order, 5 doubles each). */
+int fss_get_state(fss_ctx* ctx, double* state5);
+/* Velocity of the device-resident state into host modify5 (and psi). */
+int fss_rhs_current(fss_ctx* ctx, double omega, double* modify5, double* psi);
+
+/* Tree summary of the last build. */
+typedef struct fss_tree_info {
+    int32_t tree_levels;     /* levels 0..tree_levels-1 */
+    int32_t leaf_count;      /* 20 * 4^(tree_levels-1) */
+    int32_t degree, n_proxy; /* n and K */
+    int64_t n_pairs;         /* reference-format interactions (dual traversal) */
+    int64_t n_list_entries;  /* source ranges over all target leaves */
+    int64_t n_items;         /* interaction work items per RHS */
+    int64_t unassigned;      /* particles without a leaf (reference mode) */
+    double pp_interactions;  /* particle-particle pair count per RHS */
+    double pc_interactions;  /* particle-proxy pair count per RHS */
+} fss_tree_info;
+int fss_get_tree_info(fss_ctx* ctx, fss_tree_info* info);
+
+/* Membership and interaction list of the last build, in the reference's
+ * formats: loc[l*n + i] = face of particle i on level l or -1 (icos_utils.h
+ * tree_point_locs / tree_tri_points); counts = member counts per face, levels
+ * concatenated; pairs = 7 ints per interaction {lev_t, lev_s, t, s, n_t, n_s,
+ * type} with type 0 "pp", 1 "pc", 2 "cp", 3 "cc" (struct_list.h:6-14), in the
+ * order tree_traverse emits them.  Any pointer may be NULL. */
+int fss_get_tree(fss_ctx* ctx, int32_t* loc, int32_t* counts, int32_t* pairs, int64_t pairs_cap);
+
+/* Per-leaf (degree, theta) choice for FSS_LIST_LEAF, applied at the next
+ * build: degree[leaf], theta[leaf] for every leaf. */
+int fss_set_leaf_params(fss_ctx* ctx, int32_t nleaf, const int32_t* degree, const double* theta);
+
+/* Per-kernel device time.  When enabled, every launch is bracketed by CUDA
+ * events on the launch stream (graphs are not used while enabled). */
+int fss_profile_enable(fss_ctx* ctx, int32_t on);
+/* names: '\n'-separated kernel names; ms[i], launches[i] per kernel; returns
+ * the number of kernels through *count. */
+int fss_profile_read(fss_ctx* ctx, char* names, int32_t names_cap, double* ms, int64_t* launches,
+                     int32_t cap, int32_t* count);
+/* Algorithmic work of one RHS evaluation: pair interactions (23 flops each),
+ * and bytes of the upward pass. */
+int fss_work_per_rhs(fss_ctx* ctx, double* interactions, double* upward_bytes);
+
+/* ----------------------------------------------------------------- inputs
+ * Synthetic inputs: the reference's missing CSV initial conditions
+ * (helpers.h:299 read_points) are regenerated from icos_init. */
+
+/* Vertices and faces after `level` refinements (icos_utils.h:15 icos_init,
+ * same vertex order): n = 10*4^level + 2, faces = 20*4^level. */
+int fss_icos_counts(int32_t level, int64_t* n_verts, int64_t* n_faces);
+int fss_icos_grid(int32_t level, double* xyz, int32_t* faces);
+/* helpers.h:344 area_init */
+int fss_area_init(int64_t n, const double* state5, int64_t n_faces, const int32_t* faces, double* area);
+/* vorticity_functions.h:13 rossby_haurwitz_4 (zeta and tracer). */
+int fss_vorticity_rh4_ref(int64_t n, double* state5);
+/* Rossby-Haurwitz R=4 with w = K = amp (per day), zeta = 2 w sin(lat) -
+ * K (R+1)(R+2) cos^R(lat) sin(lat) cos(R lon), plus n_vortex Gaussian vortices
+ * a exp(-(d/width)^2) (centres uniform on the sphere, a ~ N(0, 2 pi^2)) from
+ * a 64-bit Mersenne twister seeded with `seed`, area-weighted mean removed;
+ * tracer = 2 + lat. */
+int fss_vorticity_rh_vortices(int64_t n, double* state5, const double* area, double amp,
+                              int32_t n_vortex, double width, uint64_t seed);
+
+/* Library build string (architecture, features). */
+const char* fss_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FSS_H */

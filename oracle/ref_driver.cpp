@@ -1,0 +1,198 @@
+// ref_driver.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// Thin extern "C" driver around the reference's own hot-path headers
+// (cygnari/fast-sphere-sum Old-BVE-code/*.h), compiled from the reference's
+// sources in place by oracle/Makefile into oracle/_ref/libref.so.  Nothing
+// of the reference is copied here: this file includes its headers and calls
+// its functions.  Used by tests (bit-exact pins of the oracle) and by the
+// CPU baseline of the benchmark.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "helpers.h"
+#include "struct_list.h"
+#include "vorticity_functions.h"
+#include "rhs_eval.h"
+#include "icos_utils.h"
+#include "fast_rhs.h"
+#include "interp_utils.h"
+
+using std::vector;
+
+static vector<double> to_state(int64_t n, const double* s5) { return vector<double>(s5, s5 + 5 * n); }
+
+extern "C" {
+
+// icos_utils.h:15 icos_init.  Outputs as in oracle/fss_oracle.c orc_icos_init.
+int64_t ref_icos_init(int levels, double radius, double* verts, int* tri_verts, double* tri_info) {
+    run_information c;
+    icos_init(c, levels, radius);
+    for (size_t i = 0; i < c.tree_verts.size(); i++)
+        for (int k = 0; k < 3; k++) verts[3 * i + k] = c.tree_verts[i][k];
+    int64_t f = 0;
+    for (size_t l = 0; l < c.tree_tri_verts.size(); l++)
+        for (size_t j = 0; j < c.tree_tri_verts[l].size(); j++, f++)
+            for (int k = 0; k < 3; k++) {
+                tri_verts[3 * f + k] = c.tree_tri_verts[l][j][k];
+                if (tri_info) tri_info[4 * f + k] = c.tree_tri_info[l][j][k];
+                if (tri_info && k == 2) tri_info[4 * f + 3] = c.tree_tri_info[l][j][3];
+            }
+    return (int64_t)c.tree_verts.size();
+}
+
+// helpers.h:344 area_init
+void ref_area_init(int64_t n, const double* state5, int64_t ntri, const int* tris, double* area) {
+    vector<double> s = to_state(n, state5), a(n, 0.0);
+    vector<vector<int>> t(ntri, vector<int>(3));
+    for (int64_t i = 0; i < ntri; i++)
+        for (int k = 0; k < 3; k++) t[i][k] = tris[3 * i + k];
+    area_init(s, a, t, (int)ntri);
+    std::memcpy(area, a.data(), sizeof(double) * n);
+}
+
+// vorticity_functions.h:13 rossby_haurwitz_4
+void ref_rossby_haurwitz_4(int64_t n, double* state5) {
+    vector<double> s = to_state(n, state5);
+    rossby_haurwitz_4(s, (int)n);
+    std::memcpy(state5, s.data(), sizeof(double) * 5 * n);
+}
+
+// vorticity_functions.h:26 gauss_vortex
+void ref_gauss_vortex(int64_t n, double* state5, const double* area) {
+    vector<double> s = to_state(n, state5), a(area, area + n);
+    gauss_vortex(s, a, (int)n);
+    std::memcpy(state5, s.data(), sizeof(double) * 5 * n);
+}
+
+// rhs_eval.h:47 rhs_func with use_fast == false (direct sum).
+void ref_rhs_func_direct(int64_t n, const double* state5, const double* area, double omega,
+                         double* modify5) {
+    run_information c;
+    c.point_count = (int)n;
+    c.use_fast = false;
+    vector<double> s = to_state(n, state5), a(area, area + n), m(5 * n, 0.0);
+    rhs_func(m, s, a, omega, c);
+    std::memcpy(modify5, m.data(), sizeof(double) * 5 * n);
+}
+
+// The loop of rhs_eval.h:15-32 rhs_direct_sum restricted to a set of target
+// rows (the row-range form the reference's MPI program uses,
+// direct_sum_mpi.cpp:18-55), built on the reference's own BVE_gfunc, slice,
+// scalar_mult and vec_add, and scaled by -1/(4 pi) as rhs_func does.
+// Rows are split over `threads` OS threads.
+void ref_rhs_direct_rows(int64_t n, const double* state5, const double* area, int64_t nrows,
+                         const int64_t* rows, double* out3, int threads) {
+    vector<double> s = to_state(n, state5);
+    vector<double> a(area, area + n);
+    if (threads < 1) threads = 1;
+    auto work = [&](int64_t lo, int64_t hi) {
+        vector<double> pos_change, particle_i, particle_j, contribution;
+        for (int64_t r = lo; r < hi; r++) {
+            int64_t i = rows ? rows[r] : r;
+            pos_change = {0, 0, 0};
+            particle_i = slice(s, 5 * (int)i, 1, 3);
+            for (int64_t j = 0; j < n; j++) {
+                if (i != j) {
+                    particle_j = slice(s, 5 * (int)j, 1, 3);
+                    contribution = BVE_gfunc(particle_i, particle_j);
+                    scalar_mult(contribution, s[5 * j + 3] * a[j]);
+                    vec_add(pos_change, contribution);
+                }
+            }
+            scalar_mult(pos_change, -1.0 / (4.0 * M_PI));
+            for (int k = 0; k < 3; k++) out3[3 * r + k] = pos_change[k];
+        }
+    };
+    if (threads == 1) { work(0, nrows); return; }
+    vector<std::thread> th;
+    for (int t = 0; t < threads; t++)
+        th.emplace_back(work, nrows * t / threads, nrows * (t + 1) / threads);
+    for (auto& x : th) x.join();
+}
+
+// helpers.h:362 project_points
+void ref_project_points(int64_t n, double* state5, double omega) {
+    vector<double> s = to_state(n, state5);
+    project_points(s, (int)n, omega);
+    std::memcpy(state5, s.data(), sizeof(double) * 5 * n);
+}
+
+// icos_utils.h:135 icosahedron_init + :172 points_assign + fast_rhs.h:16
+// tree_traverse.  loc[l*n+i] = face holding particle i on level l or -1;
+// counts = faces' member counts (levels concatenated); pairs = 7 ints per
+// interaction (lev_t, lev_s, t, s, n_t, n_s, type 0 pp / 1 pc / 2 cp / 3 cc).
+// Returns the number of interactions (or -needed if pairs_cap is short).
+int64_t ref_tree(int tree_levels, double theta, int many_count, int64_t n, const double* state5,
+                 int* loc, int* counts, int* pairs, int64_t pairs_cap) {
+    run_information c;
+    c.point_count = (int)n;
+    c.tree_levels = tree_levels;
+    c.theta = theta;
+    c.many_count = many_count;
+    icosahedron_init(c, 1.0);
+    vector<double> s = to_state(n, state5);
+    points_assign(c, s);
+    tree_traverse(c);
+    int64_t f = 0;
+    for (int l = 0; l < tree_levels; l++) {
+        for (int64_t i = 0; i < n; i++) loc[l * n + i] = -1;
+        for (size_t j = 0; j < c.tree_tri_points[l].size(); j++, f++) {
+            counts[f] = (int)c.tree_tri_points[l][j].size();
+            for (int id : c.tree_tri_points[l][j]) loc[l * n + id] = (int)j;
+        }
+    }
+    int64_t np = (int64_t)c.tree_interactions.size();
+    if (np > pairs_cap) return -np;
+    for (int64_t i = 0; i < np; i++) {
+        const interaction_pair& p = c.tree_interactions[i];
+        int ty = (p.type[0] == 'c' ? 2 : 0) + (p.type[1] == 'c' ? 1 : 0);
+        int* r = pairs + 7 * i;
+        r[0] = p.lev_target; r[1] = p.lev_source; r[2] = p.curr_target; r[3] = p.curr_source;
+        r[4] = p.count_target; r[5] = p.count_source; r[6] = ty;
+    }
+    return np;
+}
+
+// Ordered member list of one face (for membership comparisons).
+int64_t ref_tree_members(int tree_levels, int64_t n, const double* state5, int level, int face,
+                         int* out, int64_t cap) {
+    run_information c;
+    c.point_count = (int)n;
+    c.tree_levels = tree_levels;
+    icosahedron_init(c, 1.0);
+    vector<double> s = to_state(n, state5);
+    points_assign(c, s);
+    const vector<int>& m = c.tree_tri_points[level][face];
+    for (size_t i = 0; i < m.size() && (int64_t)i < cap; i++) out[i] = m[i];
+    return (int64_t)m.size();
+}
+
+// The reference's fast sum end to end (interp_utils.h:61 interp_init,
+// points_assign, tree_traverse, rhs_func with use_fast): its only working
+// setting is degree 2.  Returns dgetrf's info for the interpolation matrix.
+int ref_rhs_fast(int64_t n, const double* state5, const double* area, double omega, int tree_levels,
+                 double theta, int many_count, int degree, double* modify5) {
+    run_information c;
+    c.point_count = (int)n;
+    c.tree_levels = tree_levels;
+    c.theta = theta;
+    c.many_count = many_count;
+    c.degree = degree;
+    icosahedron_init(c, 1.0);
+    interp_init(c);
+    vector<double> s = to_state(n, state5), a(area, area + n), m(5 * n, 0.0);
+    points_assign(c, s);
+    tree_traverse(c);
+    c.use_fast = true;
+    rhs_func(m, s, a, omega, c);
+    std::memcpy(modify5, m.data(), sizeof(double) * 5 * n);
+    return c.info;
+}
+
+}  // extern "C"
