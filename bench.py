@@ -1,0 +1,367 @@
+"""Benchmark: RK4 steps/s of the barotropic-vorticity treecode on B200.
+
+Headline workload: 655,362 particles (icosahedral level 8), Rossby-Haurwitz
+R=4 wave + 32 seeded Gaussian vortices, mixed-precision BLTC (FP32
+interactions with Kahan accumulation, FP64 RK4 / renormalisation /
+interpolation weights), dt = 0.01 day, static tree built once (as the
+reference does before its time loop).  Beside it: the plain FP64 BLTC
+(n = 8, theta = 0.7) on the same GPU, the velocity error of both against the
+FP64 direct sum, an end-to-end number through the C ABI with host buffers,
+the pair kernel's roofline, and the reference's CPU direct sum timed on this
+host's cores.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With N > 1 (torchrun) every rank runs an independent replica (the path does
+not shard: replicas only); value = all ranks' steps / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "fast-sphere-sum_b200"))
+
+METRIC = "RK4 steps/s, N=655,362: mixed+learned BLTC vs FP64 plain @ rel-L2≤1e-6"
+UNIT = "steps/s"
+FLOPS_PER_PAIR = 23  # algorithmic flops of one velocity pair interaction
+DT = 0.01
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--level", type=int, default=8)
+    p.add_argument("--degree", type=int, default=8)
+    p.add_argument("--theta", type=float, default=0.7)
+    p.add_argument("--vortices", type=int, default=32)
+    p.add_argument("--seed", type=int, default=2)
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-sample", type=int, default=2048, help="targets in one CPU-baseline sample")
+    return p.parse_args()
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """SM clock, power and clock-event reasons sampled through NVML every
+    10 ms in a background thread while the timed region runs."""
+
+    BITS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown"}
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.rows = []
+        self.h = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            try:
+                bus = torch.cuda.get_device_properties(dev).pci_bus_id
+                self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(dev)
+            self.max = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.h = None
+
+    def _reasons(self):
+        f = getattr(self.nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            getattr(self.nv, "nvmlDeviceGetCurrentClocksThrottleReasons")
+        return f(self.h)
+
+    def _run(self):
+        while not self.stop:
+            try:
+                self.rows.append((self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM),
+                                  self.nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0, self._reasons()))
+            except Exception:
+                pass
+            time.sleep(0.01)
+
+    def __enter__(self):
+        import threading
+        self.stop = False
+        if self.h is not None:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop = True
+        if self.h is not None:
+            self.t.join()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = np.array([r[0] for r in self.rows], dtype=float)
+        load = sm[sm > 0.5 * self.max] if (sm > 0.5 * self.max).any() else sm
+        reasons = sorted({nm for r in self.rows for b, nm in self.BITS.items() if r[2] & b})
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": float(self.max), "reasons": reasons,
+                "power_w_max": float(max(r[1] for r in self.rows)), "samples": len(self.rows),
+                "source": "NVML, 10 ms"}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def profiled_traffic(name):
+    """Per-launch DRAM bytes of a kernel from its committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"{name}.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+def time_steps(ctx, stream, steps, flush):
+    """Sum of per-step device times (CUDA events on the launch stream); the
+    L2 is flushed between steps, outside the timed intervals."""
+    import torch
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            ctx.rk4_step(DT, nsteps=1)
+            b.record(stream)
+    stream.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs) / 1e3
+
+
+def make_arm(fss, state, area, stream, prec, args, dev):
+    ctx = fss.Context(method=fss.METHOD_TREECODE, precision=prec, degree=args.degree, theta=args.theta,
+                      device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_particles(state, area)
+    return ctx
+
+
+def warm(ctx, stream, w):
+    for _ in range(w):
+        ctx.rk4_step(DT, nsteps=1)
+    stream.synchronize()
+
+
+def cpu_reference_sample(state, area, sample, seed=7):
+    """Reference direct sum (its own BVE_gfunc/slice/vec_add, row-range
+    partition of direct_sum_mpi.cpp) on `sample` seeded targets, all cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    use_ref = O.ref() is not None
+    rows = np.sort(np.random.default_rng(seed).choice(state.shape[0], sample, replace=False))
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    O.rhs_direct_rows(state, area, rows, threads=threads, use_ref=use_ref)
+    dt = time.perf_counter() - t0
+    n = state.shape[0]
+    t_rhs = dt * n / sample
+    return {"value": 1.0 / (4.0 * t_rhs), "unit": UNIT, "cores": threads,
+            "kind": "reference" if use_ref else "port",
+            "sample": f"reference direct sum rhs_direct_sum/BVE_gfunc (oracle/_ref) on {sample} seeded targets x "
+                      f"{n} sources, {threads} threads, {dt:.2f} s; scaled by N/sample to one RHS, x4 per RK4 step"}
+
+
+def main_reference(args, ws, rank):
+    if rank != 0:
+        return
+    import fss_b200 as fss
+    state, area = fss.make_state(args.level, "rh_vortices", n_vortex=args.vortices, seed=args.seed)
+    for _ in range(args.warmup):
+        cpu_reference_sample(state, area, max(64, args.cpu_sample // 8))
+    vals, secs = [], 0.0
+    cb = None
+    for k in range(args.steps):
+        cb = cpu_reference_sample(state, area, args.cpu_sample, seed=100 + k)
+        vals.append(cb["value"])
+        secs += 1.0 / cb["value"]
+    value = args.steps / secs
+    cb["value"] = value
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"BVE RHS RK4 step, {state.shape[0]} particles (icosahedral level {args.level}), "
+                                   f"RH4 + {args.vortices} vortices; reference FP64 direct sum on host cores",
+                       "n_particles": int(state.shape[0])},
+            "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        main_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import torch
+    import fss_b200 as fss
+    torch.cuda.set_device(local)
+    dev = local
+    state, area = fss.make_state(args.level, "rh_vortices", n_vortex=args.vortices, seed=args.seed)
+    n = state.shape[0]
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")  # 256 MB > L2
+
+    # accuracy reference: the FP64 direct sum on the GPU (parity-tested against the oracle)
+    with fss.Context(method=fss.METHOD_DIRECT, precision=fss.PREC_FP64, device=dev) as dctx:
+        dctx.set_stream(stream.cuda_stream)
+        dctx.set_particles(state, area)
+        u_ref = dctx.rhs(state, area)[:, :3]
+
+    def rel_err(ctx):
+        u = ctx.rhs(state, area)[:, :3]
+        return float(np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref)), float(
+            np.max(np.linalg.norm(u - u_ref, axis=1)) / np.max(np.linalg.norm(u_ref, axis=1)))
+
+    # ---------------- headline arm: mixed precision BLTC
+    ctx = make_arm(fss, state, area, stream, fss.PREC_MIXED, args, dev)
+    err_l2, err_max = rel_err(ctx)
+    warm(ctx, stream, args.warmup)
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        t = time_steps(ctx, stream, args.steps, flush)
+    torch.cuda.synchronize()
+    barrier(ws)
+    t_max = max_over_ranks(t, ws)
+    value = ws * args.steps / t_max
+    clocks = clk.summary()
+
+    # kernel-level pass (events around every launch, no graph): shares and roofline
+    ctx.profile(True)
+    ctx.rk4_step(DT, nsteps=args.steps)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    inter, up_bytes = ctx.work_per_rhs()
+    pk = "pairs_mixed"
+    pairs_ms = prof[pk][0] / prof[pk][1]
+    launches_per_step = sum(v[1] for v in prof.values()) / args.steps
+    total_ms = sum(v[0] for v in prof.values())
+    peaks = load_peaks()
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s, nominal at max SM clock
+    achieved = FLOPS_PER_PAIR * inter / (pairs_ms * 1e-3) / 1e12
+    traffic = profiled_traffic("pairs_mixed_level8")
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": traffic,
+                "kernel": pk, "kernel_ms": pairs_ms, "interactions_per_launch": inter,
+                "flops_per_interaction": FLOPS_PER_PAIR,
+                "peak_source": f"nominal FP32 148 SM x 128 lanes x 2 x {sm_max:.0f} MHz (MEASURED_PEAKS.json has no FP32 figure)",
+                "frac_at_sampled_clock": (achieved / (fp32_peak * clocks["sm_mhz"] / sm_max)) if clocks.get("sm_mhz") else None,
+                "kernel_shares": {k: round(v[0] / total_ms, 4) for k, v in prof.items()},
+                "upward_bytes_per_rhs": up_bytes}
+    info = ctx.tree_info()
+
+    # ---------------- plain FP64 BLTC (the ratio's denominator)
+    fp64 = None
+    if not args.no_fp64:
+        c64 = make_arm(fss, state, area, stream, fss.PREC_FP64, args, dev)
+        e64 = rel_err(c64)
+        warm(c64, stream, args.warmup)
+        t64 = max_over_ranks(time_steps(c64, stream, args.steps, flush), ws)
+        fp64 = {"value": ws * args.steps / t64, "ms_per_step": 1e3 * t64 / args.steps, "rel_l2": e64[0],
+                "rel_max": e64[1], "degree": args.degree, "theta": args.theta}
+        c64.close()
+
+    # ---------------- end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = torch.from_numpy(state.copy()).pin_memory()
+        ptr = host.data_ptr()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for _ in range(args.warmup):
+            ctx.rk4_step_host_ptr(ptr, DT, nsteps=1)
+        with torch.cuda.stream(stream):
+            for a, b in evs:
+                flush.zero_()
+                a.record(stream)
+                ctx.rk4_step_host_ptr(ptr, DT, nsteps=1)  # H2D state, 4 stages, D2H state
+                b.record(stream)
+        stream.synchronize()
+        te = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs) / 1e3, ws)
+        e2e = {"value": ws * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": int(state.nbytes),
+               "d2h_bytes_per_step": int(state.nbytes)}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_reference_sample(state, area, args.cpu_sample)
+
+    ctx.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"BVE RK4 step (4 RHS), {n} particles (icosahedral level {args.level}), "
+                                       f"RH4 wave + {args.vortices} seeded vortices, BLTC n={args.degree} "
+                                       f"theta={args.theta}, tree_levels={info['tree_levels']}, static tree",
+                           "n_particles": n, "degree": args.degree, "theta": args.theta,
+                           "precision": "FP32 interactions + Kahan; FP64 RK4, renormalisation, interpolation",
+                           "selector": "none (fixed degree/theta)", "l2": "flushed between timed steps (256 MB write)",
+                           "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+                "rel_l2": err_l2, "rel_max": err_max,
+                "fp64_plain": fp64,
+                "ratio_vs_fp64_plain": (value / fp64["value"]) if fp64 else None,
+                "interactions_per_rhs": inter, "tree": info,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": int(round(launches_per_step * args.steps)),
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -84,7 +84,7 @@ struct fss_ctx {
 
     // device
     DBuf in5, area_in, perm, key, key_tmp, vals_tmp, hist, leaf_start, s0, xs, acc, area_s, tracer_s, src, partials,
-        ents, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
+        copies, tiles, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
         wtotal, err_flag, loc;
     int64_t src_count = 0;
 
@@ -237,12 +237,18 @@ int build_direct_lists(fss_ctx* c) {
         e.kind = 0;
         L.entries.push_back(e);
     }
-    for (int64_t t = 0; t < tiles; t++)
-        for (int p = 0; p < P; p++)
-            L.items.push_back(WorkItem{int32_t(t * TB), int32_t(std::min<int64_t>(TB, n - t * TB)), p, p + 1, p, 0});
+    for (int64_t t = 0; t < tiles; t++) {
+        const int64_t t0 = t * TB, nt = std::min<int64_t>(TB, n - t0);
+        for (int p = 0; p < P; p++) {
+            const int32_t k0 = int32_t(L.tiles.size());
+            pack_tiles(L.entries, p, p + 1, c->shape.tile, t0, t0 + nt, L.copies, L.tiles);
+            L.items.push_back(WorkItem{int32_t(t0), int32_t(nt), k0, int32_t(L.tiles.size()), p, 0});
+        }
+    }
     L.pp_pairs = double(n) * double(n - 1);
     c->direct_pairs = L.pp_pairs;
-    TRY(upload(c, c->ents, L.entries));
+    TRY(upload(c, c->copies, L.copies));
+    TRY(upload(c, c->tiles, L.tiles));
     TRY(upload(c, c->items, L.items));
     TRY(src_size_ensure(c, n));
     CU(c->partials.ensure(sizeof(double4) * size_t(P) * size_t(std::max<int64_t>(n, 1))));
@@ -271,7 +277,7 @@ int gather(fss_ctx* c, bool write_s0) {
     ProfScope ps(c, "gather");
     launch_gather(c->stream, c->fp64, c->n, c->in5.as<double>(), c->area_in.as<double>(),
                   treec ? c->perm.as<int32_t>() : nullptr, treec ? c->key.as<uint32_t>() : nullptr,
-                  (treec && !c->fp64) ? c->frame.as<double4>() : nullptr, write_s0 ? c->s0.as<double4>() : nullptr,
+                  nullptr, write_s0 ? c->s0.as<double4>() : nullptr,
                   c->xs.as<double4>(), c->area_s.as<double>(), c->tracer_s.as<double>(), c->src.p);
     CU(cudaGetLastError());
     return FSS_OK;
@@ -402,7 +408,7 @@ int build_tree(fss_ctx* c) {
     in.leaf_level = LL;
     in.n = n;
     in.leaf_start = c->leaf_start_h.data();
-    in.local_frames = !c->fp64;
+    in.tile = c->shape.tile;
     in.threads = c->shape.threads;
     in.per_thread = c->shape.per_thread;
     int P = c->cfg.src_parts;
@@ -435,7 +441,8 @@ int build_tree(fss_ctx* c) {
     }
     TRY(upload(c, c->vinv, vinv_all));
     TRY(upload(c, c->vinv_off, vinv_off));
-    TRY(upload(c, c->ents, L.entries));
+    TRY(upload(c, c->copies, L.copies));
+    TRY(upload(c, c->tiles, L.tiles));
     TRY(upload(c, c->items, L.items));
     TRY(upload(c, c->jobs, L.jobs));
     std::vector<double4> pp(L.proxy_pos.size() / 4);
@@ -453,23 +460,23 @@ int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
     if (c->tree && !c->lists.jobs.empty()) {
         {
             ProfScope ps(c, "upward_leaf");
-            launch_up_leaf(c->stream, c->fp64, int(c->nleaf), c->src.p, c->leaf_start.as<int32_t>(),
-                           c->fp64 ? nullptr : c->frame.as<double4>(), c->node.as<NodeGeom>(), c->lev_off.as<int64_t>(),
+            launch_up_leaf(c->stream, c->fp64, int(c->nleaf), c->src.p, c->leaf_start.as<int32_t>(), nullptr,
+                           c->node.as<NodeGeom>(), c->lev_off.as<int64_t>(),
                            c->leaf_level, c->nmax, c->level_mask, c->part_up.as<double>());
         }
         {
             ProfScope ps(c, "upward_combine");
             launch_up_combine(c->stream, c->fp64, int(c->lists.jobs.size()), c->jobs.as<ProxyJob>(),
                               c->part_up.as<double>(), c->leaf_level, c->nmax, c->vinv.as<double>(),
-                              c->vinv_off.as<int32_t>(), c->proxy_pos.as<double4>(), c->node.as<NodeGeom>(), !c->fp64,
+                              c->vinv_off.as<int32_t>(), c->proxy_pos.as<double4>(), c->node.as<NodeGeom>(), 0,
                               c->n, c->src.p);
         }
     }
     {
         ProfScope ps(c, c->fp64 ? "pairs_fp64" : "pairs_mixed");
         CU(launch_pairs(c->stream, c->fp64, want_psi, c->shape, int(c->lists.items.size()), c->src.p,
-                        c->ents.as<SrcEntry>(), c->items.as<WorkItem>(), c->partials.as<double4>(), c->n,
-                        c->err_flag.as<int>()));
+                        c->copies.as<Copy>(), c->tiles.as<Tile>(), c->items.as<WorkItem>(), c->partials.as<double4>(),
+                        c->n, c->err_flag.as<int>()));
     }
     if (want_psi) launch_wsum(c->stream, c->n, c->xs.as<double4>(), c->area_s.as<double>(), c->wtotal.as<double>());
     ea.n = c->n;
@@ -481,8 +488,8 @@ int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
     ea.wtotal = c->wtotal.as<double>();
     ea.perm = c->tree ? c->perm.as<int32_t>() : nullptr;
     ea.src = c->src.p;
-    ea.leaf_of = c->tree ? c->key.as<uint32_t>() : nullptr;
-    ea.frame = (c->tree && !c->fp64) ? c->frame.as<double4>() : nullptr;
+    ea.leaf_of = nullptr;
+    ea.frame = nullptr;  // interaction sources in absolute coordinates
     {
         ProfScope ps(c, "epilogue");
         launch_epilogue(c->stream, c->fp64, ea);
@@ -507,8 +514,7 @@ int rk4_once(fss_ctx* c, double dt, double omega) {
 
 int refresh_stage(fss_ctx* c) {
     if (!c->stage_dirty) return FSS_OK;
-    launch_refresh(c->stream, c->fp64, c->n, c->s0.as<double4>(), c->area_s.as<double>(),
-                   c->tree ? c->key.as<uint32_t>() : nullptr, (c->tree && !c->fp64) ? c->frame.as<double4>() : nullptr,
+    launch_refresh(c->stream, c->fp64, c->n, c->s0.as<double4>(), c->area_s.as<double>(), nullptr, nullptr,
                    c->xs.as<double4>(), c->src.p);
     CU(cudaGetLastError());
     c->stage_dirty = false;
@@ -759,6 +765,7 @@ int fss_get_tree_info(fss_ctx* c, fss_tree_info* info) {
     info->n_proxy = nproxy(c->cfg.degree);
     info->n_pairs = int64_t(c->pairs.size());
     info->n_list_entries = int64_t(c->lists.entries.size());
+    info->n_tiles = int64_t(c->lists.tiles.size());
     info->n_items = int64_t(c->lists.items.size());
     info->unassigned = c->unassigned;
     info->pp_interactions = c->lists.pp_pairs;
@@ -900,6 +907,41 @@ int fss_vorticity_rh_vortices(int64_t n, double* state5, const double* area, dou
                               uint64_t seed) {
     if (!state5) return fail(nullptr, FSS_ERR_INVALID, "null argument");
     vorticity_rh_vortices(n, state5, area, amp, nv, width, seed);
+    return FSS_OK;
+}
+
+int fss_tree_traverse(int32_t tree_levels, double theta, int32_t many_count, const int32_t* counts, int32_t* pairs,
+                      int64_t cap, int64_t* n_pairs) {
+    if (tree_levels < 1 || tree_levels > kMaxLevels || !counts)
+        return fail(nullptr, FSS_ERR_INVALID, "bad tree_levels or counts");
+    TreeGeometry g = build_tree_geometry(tree_levels);
+    std::vector<int32_t> cnt(counts, counts + g.lev_off[tree_levels]);
+    std::vector<Pair> pp = dual_traverse(g, cnt, theta, many_count);
+    if (n_pairs) *n_pairs = int64_t(pp.size());
+    if (int64_t(pp.size()) > cap) return fail(nullptr, FSS_ERR_CAPACITY, "pairs buffer too small");
+    if (pairs)
+        for (size_t i = 0; i < pp.size(); i++) {
+            int32_t* r = pairs + 7 * i;
+            r[0] = pp[i].lt; r[1] = pp[i].ls; r[2] = pp[i].t; r[3] = pp[i].s;
+            r[4] = pp[i].nt; r[5] = pp[i].ns; r[6] = pp[i].type;
+        }
+    return FSS_OK;
+}
+
+int fss_interp_nodes(int32_t degree, double* nodes, double* vinv) {
+    if (degree < 0 || degree > kMaxDegree) return fail(nullptr, FSS_ERR_INVALID, "degree must be in 0..10");
+    std::vector<double> nd, vi;
+    interp_nodes(degree, nd, vi);
+    if (nodes) std::memcpy(nodes, nd.data(), sizeof(double) * nd.size());
+    if (vinv) std::memcpy(vinv, vi.data(), sizeof(double) * vi.size());
+    return FSS_OK;
+}
+
+int fss_tree_geometry(int32_t tree_levels, double* tri_info) {
+    if (tree_levels < 1 || tree_levels > kMaxLevels || !tri_info)
+        return fail(nullptr, FSS_ERR_INVALID, "bad tree_levels");
+    TreeGeometry g = build_tree_geometry(tree_levels);
+    std::memcpy(tri_info, g.tri_info.data(), sizeof(double) * 4 * g.lev_off[tree_levels]);
     return FSS_OK;
 }
 

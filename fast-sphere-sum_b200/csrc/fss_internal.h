@@ -17,26 +17,40 @@ enum : int { kErrNone = 0, kErrTimeout = 1, kErrTree = 2 };
 
 // One contiguous run of sources seen by one target leaf: `count` entries of
 // the unified source array starting at `start` (particles [0, n), proxies
-// after them).  (dx, dy, dz) = source frame centre - target frame centre; the
-// kernels add it to the source's local coordinates so that displacements are
-// formed from small numbers (frames are leaf/node circumcentres in mixed
-// precision and the origin in FP64).
+// after them).  Host-side list element before packing into tiles.
 struct SrcEntry {
     int32_t start;
     int32_t count;
     int32_t kind;   // 0 particles (near or small far cluster), 1 proxies
     int32_t pad;
-    double dx, dy, dz;
+};
+
+// One bulk copy global -> shared: `count` sources from `start`.
+struct Copy {
+    int32_t start;
+    int32_t count;
+};
+
+// One shared-memory tile: copies [c0, c1) placed back to back, `count`
+// sources in all; guard = 1 when a copy overlaps the block's own targets
+// (the self pair must be skipped).
+struct Tile {
+    int32_t c0, c1;
+    int32_t count;
+    int32_t guard;
 };
 
 // One block's work: targets [t0, t0 + nt) (one leaf, sorted order) against
-// entries [e0, e1); results go to partial slot `part`.
+// tiles [k0, k1); results go to partial slot `part`.
 struct WorkItem {
     int32_t t0, nt;
-    int32_t e0, e1;
+    int32_t k0, k1;
     int32_t part;
     int32_t leaf;
 };
+
+// Sources per shared-memory tile: 256 float4 (4 KB) or 128 double4 (4 KB).
+FSS_HD constexpr int tile_capacity(bool fp64) { return fp64 ? 128 : 256; }
 
 // Upward-pass combine work: node `node` (global index, levels concatenated)
 // on `level`; proxies of degree set `degmask` (bit d = degree d) written at

@@ -37,6 +37,7 @@ struct EpiArgs {
 struct PairShape {
     int threads = 128;
     int per_thread = 1;
+    int tile = 256;
 };
 
 // k_tree.cu
@@ -55,7 +56,8 @@ void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, con
 // k_pairs.cu
 PairShape pairs_shape(bool fp64, int threads_hint);
 cudaError_t launch_pairs(cudaStream_t st, bool fp64, bool psi, PairShape shape, int nitems, const void* src,
-                         const SrcEntry* ents, const WorkItem* items, double4* partials, int64_t pstride, int* err);
+                         const Copy* copies, const Tile* tiles, const WorkItem* items, double4* partials,
+                         int64_t pstride, int* err);
 
 // k_epi.cu
 void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, const int32_t* leaf_start,

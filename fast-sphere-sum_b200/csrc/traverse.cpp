@@ -159,21 +159,13 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
     // entries and items
     const int TB = in.threads * in.per_thread;
     const int P = std::max(1, in.parts);
-    auto centre = [&](int64_t gf, double* c) {
-        if (in.local_frames) {
-            c[0] = g.tri_info[4 * gf]; c[1] = g.tri_info[4 * gf + 1]; c[2] = g.tri_info[4 * gf + 2];
-        } else {
-            c[0] = c[1] = c[2] = 0;
-        }
-    };
     struct Cost { double cost; WorkItem it; };
     std::vector<Cost> items;
+    std::vector<SrcEntry> ents;
     for (int64_t lf = 0; lf < nleaf; lf++) {
         const int32_t t0 = in.leaf_start[lf], nt = in.leaf_start[lf + 1] - t0;
         if (nt == 0) continue;
-        double ct[3];
-        centre(g.lev_off[LL] + lf, ct);
-        const int32_t e_begin = int32_t(out.entries.size());
+        ents.clear();
         for (const ASrc& a : lists[lf]) {
             const int64_t gf = g.lev_off[a.level] + a.node;
             if (a.proxy) {
@@ -181,28 +173,24 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
                 e.start = int32_t(in.n + slot[std::make_pair(gf, a.deg)]);
                 e.count = nproxy(a.deg);
                 e.kind = 1;
-                double cs[3];
-                centre(gf, cs);
-                e.dx = cs[0] - ct[0]; e.dy = cs[1] - ct[1]; e.dz = cs[2] - ct[2];
-                out.entries.push_back(e);
+                ents.push_back(e);
                 out.pc_pairs += double(nt) * e.count;
             } else {
                 const int64_t span = int64_t(1) << (2 * (LL - a.level));
-                for (int64_t l2 = a.node * span; l2 < (a.node + 1) * span; l2++) {
-                    const int32_t s0 = in.leaf_start[l2], ns = in.leaf_start[l2 + 1] - s0;
-                    if (ns == 0) continue;
-                    SrcEntry e{};
-                    e.start = s0;
-                    e.count = ns;
-                    e.kind = 0;
-                    double cs[3];
-                    centre(g.lev_off[LL] + l2, cs);
-                    e.dx = cs[0] - ct[0]; e.dy = cs[1] - ct[1]; e.dz = cs[2] - ct[2];
-                    out.entries.push_back(e);
-                    out.pp_pairs += double(nt) * ns - ((l2 == lf) ? nt : 0);
-                }
+                // the particles of S are contiguous in leaf order
+                const int32_t s0 = in.leaf_start[a.node * span], s1 = in.leaf_start[(a.node + 1) * span];
+                if (s1 == s0) continue;
+                SrcEntry e{};
+                e.start = s0;
+                e.count = s1 - s0;
+                e.kind = 0;
+                ents.push_back(e);
+                const bool self = (t0 >= s0 && t0 < s1);
+                out.pp_pairs += double(nt) * e.count - (self ? nt : 0);
             }
         }
+        const int32_t e_begin = int32_t(out.entries.size());
+        out.entries.insert(out.entries.end(), ents.begin(), ents.end());
         const int32_t e_end = int32_t(out.entries.size());
         // split [e_begin, e_end) into P parts of similar source counts
         double total = 0;
@@ -223,13 +211,39 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
             for (int p = 0; p < P; p++) {
                 double w = 0;
                 for (int32_t e = cut[p]; e < cut[p + 1]; e++) w += out.entries[e].count;
-                items.push_back({w * cn, WorkItem{t0 + c0, cn, cut[p], cut[p + 1], p, int32_t(lf)}});
+                const int32_t k0 = int32_t(out.tiles.size());
+                pack_tiles(out.entries, cut[p], cut[p + 1], in.tile, t0 + c0, t0 + c0 + cn, out.copies, out.tiles);
+                const int32_t k1 = int32_t(out.tiles.size());
+                items.push_back({w * cn, WorkItem{t0 + c0, cn, k0, k1, p, int32_t(lf)}});
             }
         }
     }
     std::stable_sort(items.begin(), items.end(), [](const Cost& a, const Cost& b) { return a.cost > b.cost; });
     out.items.reserve(items.size());
     for (auto& c : items) out.items.push_back(c.it);
+}
+
+void pack_tiles(const std::vector<SrcEntry>& entries, int32_t e0, int32_t e1, int cap, int64_t t0, int64_t t1,
+                std::vector<Copy>& copies, std::vector<Tile>& tiles) {
+    Tile cur{int32_t(copies.size()), int32_t(copies.size()), 0, 0};
+    for (int32_t e = e0; e < e1; e++) {
+        int32_t off = 0;
+        const SrcEntry& en = entries[e];
+        while (off < en.count) {
+            const int32_t take = std::min(en.count - off, cap - cur.count);
+            const int64_t a = int64_t(en.start) + off, b = a + take;
+            copies.push_back({int32_t(a), take});
+            if (a < t1 && b > t0) cur.guard = 1;
+            cur.count += take;
+            cur.c1 = int32_t(copies.size());
+            off += take;
+            if (cur.count == cap) {
+                tiles.push_back(cur);
+                cur = Tile{int32_t(copies.size()), int32_t(copies.size()), 0, 0};
+            }
+        }
+    }
+    if (cur.count > 0) tiles.push_back(cur);
 }
 
 // ---------------------------------------------------------------- interpolation

@@ -33,13 +33,15 @@ struct ListInput {
     int leaf_level = 0;                 // tree_levels - 1
     int64_t n = 0;                      // particles
     const int32_t* leaf_start = nullptr;  // nleaf + 1 (sorted order)
-    bool local_frames = true;           // mixed: leaf / node centre frames
     int threads = 128, per_thread = 1;  // targets per block = threads * per_thread
+    int tile = 256;                     // sources per shared-memory tile
     int parts = 1;                      // source-list split
 };
 
 struct ListOutput {
-    std::vector<SrcEntry> entries;
+    std::vector<SrcEntry> entries;  // per target leaf, in list order
+    std::vector<Copy> copies;
+    std::vector<Tile> tiles;
     std::vector<WorkItem> items;
     std::vector<ProxyJob> jobs;
     std::vector<double> proxy_pos;  // 4 doubles per proxy slot: y (on sphere) and pad
@@ -63,6 +65,12 @@ std::vector<std::vector<ASrc>> lists_per_leaf(const TreeGeometry& g, int leaf_le
                                               const std::vector<int32_t>& counts,
                                               const std::vector<int32_t>& leaf_degree,
                                               const std::vector<double>& leaf_theta);
+
+// Pack source ranges [e0, e1) of `entries` into tiles of at most `cap`
+// sources (ranges split across tile boundaries as needed); guard marks tiles
+// holding any of the targets [t0, t1).
+void pack_tiles(const std::vector<SrcEntry>& entries, int32_t e0, int32_t e1, int cap, int64_t t0, int64_t t1,
+                std::vector<Copy>& copies, std::vector<Tile>& tiles);
 
 // Materialise entries, work items, proxy slots and upward-pass jobs.
 void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& lists, ListOutput& out);

@@ -44,7 +44,7 @@ class Config(C.Structure):
 class TreeInfo(C.Structure):
     _fields_ = [("tree_levels", C.c_int32), ("leaf_count", C.c_int32), ("degree", C.c_int32),
                 ("n_proxy", C.c_int32), ("n_pairs", C.c_int64), ("n_list_entries", C.c_int64),
-                ("n_items", C.c_int64), ("unassigned", C.c_int64), ("pp_interactions", C.c_double),
+                ("n_items", C.c_int64), ("n_tiles", C.c_int64), ("unassigned", C.c_int64), ("pp_interactions", C.c_double),
                 ("pc_interactions", C.c_double)]
 
 
@@ -66,7 +66,8 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_rk4_step", "fss_rk4_step_host", "fss_get_state", "fss_rhs_current", "fss_get_tree_info",
            "fss_get_tree", "fss_set_leaf_params", "fss_profile_enable", "fss_profile_read",
            "fss_work_per_rhs", "fss_icos_counts", "fss_icos_grid", "fss_area_init",
-           "fss_vorticity_rh4_ref", "fss_vorticity_rh_vortices", "fss_version"]
+           "fss_vorticity_rh4_ref", "fss_vorticity_rh_vortices", "fss_tree_traverse", "fss_interp_nodes",
+           "fss_tree_geometry", "fss_version"]
 
 
 def lib():
@@ -104,6 +105,9 @@ def lib():
     L.fss_area_init.argtypes = [_i64, _D, _i64, _I, _D]
     L.fss_vorticity_rh4_ref.argtypes = [_i64, _D]
     L.fss_vorticity_rh_vortices.argtypes = [_i64, _D, _vp, C.c_double, C.c_int32, C.c_double, C.c_uint64]
+    L.fss_tree_traverse.argtypes = [C.c_int32, C.c_double, C.c_int32, _I, _vp, _i64, P(_i64)]
+    L.fss_interp_nodes.argtypes = [C.c_int32, _D, _D]
+    L.fss_tree_geometry.argtypes = [C.c_int32, _D]
     L.fss_version.restype = C.c_char_p
     _lib = L
     return L
@@ -156,6 +160,36 @@ def make_state(level, field="rh4_ref", n_vortex=0, seed=1, amp=RH_AMP, width=0.1
     else:
         raise ValueError(field)
     return s, area
+
+
+def tree_traverse(tree_levels, theta, many_count, counts):
+    """fast_rhs.h:16 tree_traverse on per-face counts (host): pairs (P, 7)."""
+    cnt = np.ascontiguousarray(counts, dtype=np.int32)
+    npairs = _i64()
+    rc = lib().fss_tree_traverse(tree_levels, theta, many_count, cnt, None, 0, C.byref(npairs))
+    if rc not in (0, 8):
+        _check(rc)
+    pairs = np.zeros((max(npairs.value, 1), 7), dtype=np.int32)
+    _check(lib().fss_tree_traverse(tree_levels, theta, many_count, cnt, pairs.ctypes.data_as(_vp), npairs.value,
+                                   C.byref(npairs)))
+    return pairs[:npairs.value]
+
+
+def interp_nodes(degree):
+    """(nodes (K, 3) barycentric, vinv (K, K)) of the degree-n proxy set."""
+    K = (degree + 1) * (degree + 2) // 2
+    nodes = np.zeros((K, 3))
+    vinv = np.zeros((K, K))
+    _check(lib().fss_interp_nodes(degree, nodes.reshape(-1), vinv.reshape(-1)))
+    return nodes, vinv
+
+
+def tree_geometry(tree_levels):
+    """Circumcentre + circumradius per face, levels 0..tree_levels-1 concatenated."""
+    nf = sum(20 * 4 ** l for l in range(tree_levels))
+    ti = np.zeros((nf, 4))
+    _check(lib().fss_tree_geometry(tree_levels, ti.reshape(-1)))
+    return ti
 
 
 # ------------------------------------------------------------------ context

@@ -89,7 +89,9 @@ typedef struct fss_config {
 
 typedef struct fss_ctx fss_ctx;
 
-/* Defaults: FP64... see fss.cpp; mixed precision, treecode, auto depth. */
+/* Defaults: mixed precision treecode, degree 8, theta 0.7, automatic depth
+ * (leaves of >= 64 particles), complete assignment, dual (reference)
+ * traversal, CUDA graph on, device 0. */
 void fss_config_init(fss_config* cfg);
 
 int fss_create(const fss_config* cfg, fss_ctx** out);
@@ -138,7 +140,8 @@ typedef struct fss_tree_info {
     int32_t degree, n_proxy; /* n and K */
     int64_t n_pairs;         /* reference-format interactions (dual traversal) */
     int64_t n_list_entries;  /* source ranges over all target leaves */
-    int64_t n_items;         /* interaction work items per RHS */
+    int64_t n_items;         /* interaction work items (blocks) per RHS */
+    int64_t n_tiles;         /* shared-memory source tiles over all items */
     int64_t unassigned;      /* particles without a leaf (reference mode) */
     double pp_interactions;  /* particle-particle pair count per RHS */
     double pc_interactions;  /* particle-proxy pair count per RHS */
@@ -187,6 +190,23 @@ int fss_vorticity_rh4_ref(int64_t n, double* state5);
  * tracer = 2 + lat. */
 int fss_vorticity_rh_vortices(int64_t n, double* state5, const double* area, double amp,
                               int32_t n_vortex, double width, uint64_t seed);
+
+/* Host-only, no GPU needed. ---------------------------------------------- */
+
+/* fast_rhs.h:16 tree_traverse on given per-face particle counts (levels
+ * 0..tree_levels-1 concatenated, 20*4^l faces on level l): the reference's
+ * pair list, 7 ints per pair as in fss_get_tree, into pairs[cap*7]; the
+ * number of pairs goes to *n_pairs (FSS_ERR_CAPACITY if it exceeds cap). */
+int fss_tree_traverse(int32_t tree_levels, double theta, int32_t many_count, const int32_t* counts,
+                      int32_t* pairs, int64_t cap, int64_t* n_pairs);
+/* Interpolation points of degree n (K = (n+1)(n+2)/2 barycentric triples)
+ * and the K x K inverse Vandermonde matrix of the Chebyshev product basis
+ * (vinv[m*K + k]: coefficient of basis function m in Lagrange polynomial k);
+ * replaces interp_utils.h:12-75 (fekete_init / interp_mat_init). */
+int fss_interp_nodes(int32_t degree, double* nodes, double* vinv);
+/* icos_utils.h:15 icos_init tree geometry for levels 0..tree_levels-1:
+ * circumcentre and circumradius per face (4 doubles), levels concatenated. */
+int fss_tree_geometry(int32_t tree_levels, double* tri_info);
 
 /* Library build string (architecture, features). */
 const char* fss_version(void);

@@ -76,6 +76,7 @@ def _setup_ref(R):
     R.ref_rhs_func_direct.argtypes = [i64, _D, _D, C.c_double, _D]
     R.ref_rhs_direct_rows.argtypes = [i64, _D, _D, i64, C.c_void_p, _D, C.c_int]
     R.ref_project_points.argtypes = [i64, _D, C.c_double]
+    R.ref_rk4_step.argtypes = [i64, _D, _D, C.c_double, C.c_double]
     R.ref_tree.argtypes = [C.c_int, C.c_double, C.c_int, i64, _D, _I, _I, _I, i64]
     R.ref_tree.restype = i64
     R.ref_tree_members.argtypes = [C.c_int, i64, _D, C.c_int, C.c_int, _I, i64]
@@ -167,10 +168,13 @@ def stream_rows(state5, area, rows):
     return out
 
 
-def rk4_step(state5, area, dt, omega=OMEGA, threads=None):
+def rk4_step(state5, area, dt, omega=OMEGA, threads=None, use_ref=False):
     s = np.array(state5, dtype=np.float64).reshape(-1)
-    lib().orc_rk4_step(s.size // 5, s, np.ascontiguousarray(area, dtype=np.float64), omega, dt,
-                       threads or os.cpu_count())
+    a = np.ascontiguousarray(area, dtype=np.float64)
+    if use_ref:
+        ref().ref_rk4_step(s.size // 5, s, a, omega, dt)
+    else:
+        lib().orc_rk4_step(s.size // 5, s, a, omega, dt, threads or os.cpu_count())
     return s.reshape(-1, 5)
 
 

@@ -123,6 +123,45 @@ void ref_project_points(int64_t n, double* state5, double omega) {
     std::memcpy(state5, s.data(), sizeof(double) * 5 * n);
 }
 
+// One RK4 step in the order of new_dynamics.cpp:281-340 (the loop as it is
+// meant to run: its stage buffers intermediate_1..3 and c_1..c_4 are only
+// commented-out declarations there), built from the reference's rhs_func,
+// scalar_mult, vec_add and project_points with the direct sum.
+void ref_rk4_step(int64_t n, double* state5, const double* area, double omega, double dt) {
+    run_information c;
+    c.point_count = (int)n;
+    c.use_fast = false;
+    vector<double> s = to_state(n, state5), a(area, area + n);
+    vector<double> c_1(5 * n), c_2(5 * n), c_3(5 * n), c_4(5 * n), c1234;
+    vector<double> intermediate_1, intermediate_2, intermediate_3;
+    rhs_func(c_1, s, a, omega, c);
+    intermediate_1 = c_1;
+    scalar_mult(intermediate_1, dt / 2);
+    vec_add(intermediate_1, s);
+    project_points(intermediate_1, (int)n, omega);
+    rhs_func(c_2, intermediate_1, a, omega, c);
+    intermediate_2 = c_2;
+    scalar_mult(intermediate_2, dt / 2);
+    vec_add(intermediate_2, s);
+    project_points(intermediate_2, (int)n, omega);
+    rhs_func(c_3, intermediate_2, a, omega, c);
+    intermediate_3 = c_3;
+    scalar_mult(intermediate_3, dt);
+    vec_add(intermediate_3, s);
+    project_points(intermediate_3, (int)n, omega);
+    rhs_func(c_4, intermediate_3, a, omega, c);
+    c1234 = c_1;
+    scalar_mult(c_2, 2);
+    vec_add(c1234, c_2);
+    scalar_mult(c_3, 2);
+    vec_add(c1234, c_3);
+    vec_add(c1234, c_4);
+    scalar_mult(c1234, dt / 6);
+    vec_add(s, c1234);
+    project_points(s, (int)n, omega);
+    std::memcpy(state5, s.data(), sizeof(double) * 5 * n);
+}
+
 // icos_utils.h:135 icosahedron_init + :172 points_assign + fast_rhs.h:16
 // tree_traverse.  loc[l*n+i] = face holding particle i on level l or -1;
 // counts = faces' member counts (levels concatenated); pairs = 7 ints per
