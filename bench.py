@@ -95,11 +95,16 @@ class ClockSampler:
             import torch
             pynvml.nvmlInit()
             self.nv = pynvml
-            try:
-                bus = torch.cuda.get_device_properties(dev).pci_bus_id
-                self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
-            except Exception:
-                self.h = pynvml.nvmlDeviceGetHandleByIndex(dev)
+            # match the CUDA device to its NVML handle by PCI location
+            # (integers from both sides; no string/pointer conversions)
+            prop = torch.cuda.get_device_properties(dev)
+            want = (int(prop.pci_domain_id), int(prop.pci_bus_id), int(prop.pci_device_id))
+            for i in range(pynvml.nvmlDeviceGetCount()):
+                h = pynvml.nvmlDeviceGetHandleByIndex(i)
+                pci = pynvml.nvmlDeviceGetPciInfo(h)
+                if (int(pci.domain), int(pci.bus), int(pci.device)) == want:
+                    self.h = h
+                    break
             self.max = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
         except Exception:
             self.h = None
