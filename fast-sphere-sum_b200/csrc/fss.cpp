@@ -584,6 +584,11 @@ fss_ctx* other_method(fss_ctx* c, int method, int* rc) {
 
 }  // namespace
 
+namespace fss {
+// Message for fss_last_error(NULL), for entry points outside this file.
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace fss
+
 // =================================================================== C ABI
 
 extern "C" {

@@ -67,7 +67,9 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_get_tree", "fss_set_leaf_params", "fss_profile_enable", "fss_profile_read",
            "fss_work_per_rhs", "fss_icos_counts", "fss_icos_grid", "fss_area_init",
            "fss_vorticity_rh4_ref", "fss_vorticity_rh_vortices", "fss_tree_traverse", "fss_interp_nodes",
-           "fss_tree_geometry", "fss_version"]
+           "fss_tree_geometry", "fss_rhs_direct_noalloc", "fss_version"]
+
+NOALLOC_MAX_PARTICLES = 262144  # FSS_NOALLOC_MAX_PARTICLES in include/fss.h
 
 
 def lib():
@@ -108,6 +110,7 @@ def lib():
     L.fss_tree_traverse.argtypes = [C.c_int32, C.c_double, C.c_int32, _I, _vp, _i64, P(_i64)]
     L.fss_interp_nodes.argtypes = [C.c_int32, _D, _D]
     L.fss_tree_geometry.argtypes = [C.c_int32, _D]
+    L.fss_rhs_direct_noalloc.argtypes = [_i64, _vp, _vp, C.c_double, _vp, _vp]
     L.fss_version.restype = C.c_char_p
     _lib = L
     return L
@@ -323,6 +326,12 @@ class Context:
         a, b = C.c_double(), C.c_double()
         self._c(lib().fss_work_per_rhs(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+
+def rhs_direct_noalloc(n, state5_dev_ptr, area_dev_ptr, out5_dev_ptr, stream_handle=None, omega=OMEGA):
+    """fss_rhs_direct_noalloc on caller-owned device buffers (raw pointers);
+    asynchronous on the given stream.  Raises FssError on a bad size."""
+    _check(lib().fss_rhs_direct_noalloc(n, state5_dev_ptr, area_dev_ptr, omega, out5_dev_ptr, stream_handle))
 
 
 def version():

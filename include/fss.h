@@ -208,6 +208,28 @@ int fss_interp_nodes(int32_t degree, double* nodes, double* vinv);
  * circumcentre and circumradius per face (4 doubles), levels concatenated. */
 int fss_tree_geometry(int32_t tree_levels, double* tri_info);
 
+/* Direct sum without any allocation.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory: real-time loops in which a
+ * cudaMalloc or cudaFree could synchronise the device and stall it, and
+ * plugins whose host application owns the whole device memory budget.  The
+ * caller passes device buffers: state5 (n x 5 doubles, the reference's
+ * layout), area (n doubles) and modify5 (n x 5 doubles, overwritten as by
+ * rhs_func with the direct sum, mixed precision: FP32 pairs, Kahan-compensated
+ * sums).  Kernels go to `stream` (a cudaStream_t, NULL = the default stream)
+ * and run asynchronously; the call does not synchronise.
+ *
+ * Limit: n <= FSS_NOALLOC_MAX_PARTICLES; larger n returns FSS_ERR_CAPACITY
+ * with a message in fss_last_error(NULL).  The scratch is a fixed device
+ * array of FSS_NOALLOC_MAX_PARTICLES x 16 bytes (4 MiB) that every GPU
+ * loading the library holds until the process exits.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress, with the
+ * device current); make that first call before any stream capture.  All
+ * calls share the array: two calls whose kernels overlap on the GPU race. */
+#define FSS_NOALLOC_MAX_PARTICLES 262144
+int fss_rhs_direct_noalloc(int64_t n, const double* state5, const double* area, double omega, double* modify5,
+                           void* stream);
+
 /* Library build string (architecture, features). */
 const char* fss_version(void);
 
