@@ -75,6 +75,8 @@ struct fss_ctx {
     std::vector<int32_t> ref_loc_h, cmp_loc_h;
     int64_t unassigned = 0;
     ListOutput lists;
+    std::vector<std::vector<ASrc>> alists;  // per-leaf sources before packing
+    std::vector<std::pair<PairShape, double>> tuned;  // autotuner: shape, ms per pair pass
     std::vector<int32_t> leaf_deg;
     std::vector<double> leaf_theta;
     int nmax = 0, level_mask = 0;
@@ -217,7 +219,7 @@ int src_size_ensure(fss_ctx* c, int64_t count) {
 // Lists of the direct sum: target tiles x source chunks.
 int build_direct_lists(fss_ctx* c) {
     const int64_t n = c->n;
-    c->shape = pairs_shape(c->fp64, c->cfg.block_threads);
+    c->shape = pairs_shape(c->fp64, c->cfg.block_threads, c->cfg.targets_per_thread);
     const int TB = c->shape.threads * c->shape.per_thread;
     const int64_t tiles = (n + TB - 1) / TB;
     int P = c->cfg.src_parts;
@@ -271,6 +273,9 @@ int ensure_particle_buffers(fss_ctx* c, int64_t n) {
 }
 
 int build_tree(fss_ctx* c);
+PairShape choose_shape(fss_ctx* c);
+int materialize(fss_ctx* c, PairShape shape);
+int autotune(fss_ctx* c);
 
 int gather(fss_ctx* c, bool write_s0) {
     const bool treec = c->tree;
@@ -305,6 +310,7 @@ int set_particles(fss_ctx* c, int64_t n, const double* state5, const double* are
     TRY(gather(c, true));
     c->have = true;
     c->stage_dirty = false;
+    if (c->tree && c->cfg.autotune) TRY(autotune(c));
     return check_device_error(c);
 }
 
@@ -402,15 +408,37 @@ int build_tree(fss_ctx* c) {
                                           : c->pairs;
         al = lists_from_pairs(c->geom, LL, pp, many, c->cfg.degree);
     }
-    c->shape = pairs_shape(c->fp64, c->cfg.block_threads);
+    c->alists = std::move(al);
+    TRY(materialize(c, choose_shape(c)));
+    return FSS_OK;
+}
+
+// Block shape for the treecode's pair kernel: the configured one, or the
+// smallest supported block whose targets cover the largest leaf (so that
+// no leaf spills a tail block).
+PairShape choose_shape(fss_ctx* c) {
+    if (c->cfg.block_threads > 0) return pairs_shape(c->fp64, c->cfg.block_threads, c->cfg.targets_per_thread);
+    int maxleaf = 1;
+    for (int64_t l = 0; l < c->nleaf; l++) maxleaf = std::max(maxleaf, c->leaf_start_h[l + 1] - c->leaf_start_h[l]);
+    for (const PairShape& sh : pair_shapes(c->fp64))
+        if (sh.per_thread == 1 && sh.threads >= maxleaf) return sh;
+    return pair_shapes(c->fp64).back();
+}
+
+// Work items, tiles and copies of the current lists for one block shape;
+// proxy slots, upward-pass jobs and interpolation tables.
+int materialize(fss_ctx* c, PairShape shape) {
+    const int64_t n = c->n;
+    const int LL = c->leaf_level;
+    c->shape = shape;
     ListInput in;
     in.g = &c->geom;
     in.leaf_level = LL;
     in.n = n;
     in.leaf_start = c->leaf_start_h.data();
-    in.tile = c->shape.tile;
-    in.threads = c->shape.threads;
-    in.per_thread = c->shape.per_thread;
+    in.tile = shape.tile;
+    in.threads = shape.threads;
+    in.per_thread = shape.per_thread;
     int P = c->cfg.src_parts;
     if (P <= 0) {
         int64_t chunks = 0;
@@ -421,7 +449,7 @@ int build_tree(fss_ctx* c) {
     }
     in.parts = P;
     c->parts = P;
-    build_lists(in, al, c->lists);
+    build_lists(in, c->alists, c->lists);
     const ListOutput& L = c->lists;
     // interpolation tables for the degrees in use
     c->nmax = std::max(L.max_degree, 0);
@@ -495,6 +523,46 @@ int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
         launch_epilogue(c->stream, c->fp64, ea);
     }
     CU(cudaGetLastError());
+    return FSS_OK;
+}
+
+// Autotuner: time the pair kernel (after the upward pass) for every
+// supported block shape on the current lists and keep the fastest.
+int autotune(fss_ctx* c) {
+    c->tuned.clear();
+    const bool prof_was = c->prof;
+    c->prof = false;
+    cudaEvent_t a, b;
+    CU(cudaEventCreate(&a));
+    CU(cudaEventCreate(&b));
+    PairShape best = c->shape;
+    double best_ms = 1e30;
+    for (const PairShape& sh : pair_shapes(c->fp64)) {
+        TRY(materialize(c, sh));
+        EpiArgs ea;
+        ea.mode = EPI_RHS;
+        ea.out5 = c->out5.as<double>();
+        TRY(eval(c, ea, false));  // warm (and proxies)
+        CU(cudaEventRecord(a, c->stream));
+        for (int r = 0; r < 2; r++)
+            CU(launch_pairs(c->stream, c->fp64, false, c->shape, int(c->lists.items.size()), c->src.p,
+                            c->copies.as<Copy>(), c->tiles.as<Tile>(), c->items.as<WorkItem>(),
+                            c->partials.as<double4>(), c->n, c->err_flag.as<int>()));
+        CU(cudaEventRecord(b, c->stream));
+        CU(cudaEventSynchronize(b));
+        float ms = 0;
+        CU(cudaEventElapsedTime(&ms, a, b));
+        c->tuned.push_back({sh, ms / 2});
+        if (ms / 2 < best_ms) {
+            best_ms = ms / 2;
+            best = sh;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    TRY(materialize(c, best));
+    c->prof = prof_was;
+    c->stage_dirty = true;  // the timing passes overwrote the stage sources
     return FSS_OK;
 }
 
@@ -609,6 +677,8 @@ void fss_config_init(fss_config* cfg) {
     cfg->use_graph = 1;
     cfg->src_parts = 0;
     cfg->block_threads = 0;
+    cfg->targets_per_thread = 1;
+    cfg->autotune = 0;
 }
 
 int fss_create(const fss_config* cfg, fss_ctx** out) {
@@ -775,6 +845,9 @@ int fss_get_tree_info(fss_ctx* c, fss_tree_info* info) {
     info->unassigned = c->unassigned;
     info->pp_interactions = c->lists.pp_pairs;
     info->pc_interactions = c->lists.pc_pairs;
+    info->block_threads = c->shape.threads;
+    info->targets_per_thread = c->shape.per_thread;
+    info->src_parts = c->parts;
     return FSS_OK;
 }
 

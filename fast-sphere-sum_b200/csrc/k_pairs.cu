@@ -203,31 +203,46 @@ static cudaError_t run_pairs(cudaStream_t st, int nitems, const void* src, const
     return cudaGetLastError();
 }
 
-PairShape pairs_shape(bool fp64, int threads_hint) {
-    PairShape s;
-    s.threads = 128;
-    s.per_thread = 1;
-    if (!fp64 && threads_hint == 64) {
-        s.threads = 64;
-        s.per_thread = 2;
+const std::vector<PairShape>& pair_shapes(bool fp64) {
+    static const std::vector<PairShape> f32 = {{128, 1, 256}, {160, 1, 256}, {192, 1, 256}, {256, 1, 256},
+                                               {64, 2, 256},  {96, 2, 256},  {128, 2, 256}};
+    static const std::vector<PairShape> f64 = {{128, 1, 128}, {160, 1, 128}, {192, 1, 128}, {256, 1, 128}};
+    return fp64 ? f64 : f32;
+}
+
+PairShape pairs_shape(bool fp64, int threads, int per_thread) {
+    for (const PairShape& s : pair_shapes(fp64))
+        if (s.threads == threads && s.per_thread == (per_thread > 0 ? per_thread : 1)) return s;
+    return pair_shapes(fp64).front();
+}
+
+template <typename T, bool PSI>
+static cudaError_t dispatch(cudaStream_t st, PairShape sh, int nitems, const void* src, const Copy* copies,
+                            const Tile* tiles, const WorkItem* items, double4* partials, int64_t pstride, int* err) {
+#define FSS_SHAPE(TH, R)                                                                                   \
+    if (sh.threads == TH && sh.per_thread == R)                                                            \
+        return run_pairs<T, TH, R, PSI>(st, nitems, src, copies, tiles, items, partials, pstride, err);
+    FSS_SHAPE(128, 1)
+    FSS_SHAPE(160, 1)
+    FSS_SHAPE(192, 1)
+    FSS_SHAPE(256, 1)
+    if (sizeof(T) == 4) {
+        FSS_SHAPE(64, 2)
+        FSS_SHAPE(96, 2)
+        FSS_SHAPE(128, 2)
     }
-    s.tile = tile_capacity(fp64);
-    return s;
+#undef FSS_SHAPE
+    return cudaErrorInvalidConfiguration;
 }
 
 cudaError_t launch_pairs(cudaStream_t st, bool fp64, bool psi, PairShape shape, int nitems, const void* src,
                          const Copy* copies, const Tile* tiles, const WorkItem* items, double4* partials,
                          int64_t pstride, int* err) {
-    if (fp64) {
-        return psi ? run_pairs<double, 128, 1, true>(st, nitems, src, copies, tiles, items, partials, pstride, err)
-                   : run_pairs<double, 128, 1, false>(st, nitems, src, copies, tiles, items, partials, pstride, err);
-    }
-    if (shape.threads == 64) {
-        return psi ? run_pairs<float, 64, 2, true>(st, nitems, src, copies, tiles, items, partials, pstride, err)
-                   : run_pairs<float, 64, 2, false>(st, nitems, src, copies, tiles, items, partials, pstride, err);
-    }
-    return psi ? run_pairs<float, 128, 1, true>(st, nitems, src, copies, tiles, items, partials, pstride, err)
-               : run_pairs<float, 128, 1, false>(st, nitems, src, copies, tiles, items, partials, pstride, err);
+    if (fp64)
+        return psi ? dispatch<double, true>(st, shape, nitems, src, copies, tiles, items, partials, pstride, err)
+                   : dispatch<double, false>(st, shape, nitems, src, copies, tiles, items, partials, pstride, err);
+    return psi ? dispatch<float, true>(st, shape, nitems, src, copies, tiles, items, partials, pstride, err)
+               : dispatch<float, false>(st, shape, nitems, src, copies, tiles, items, partials, pstride, err);
 }
 
 }  // namespace fss

@@ -1,6 +1,7 @@
 // kernels.h -- host-callable launchers of the sm_100a kernels.
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "fss_internal.h"
@@ -54,7 +55,10 @@ void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, con
                    double* tracer_s, void* src);
 
 // k_pairs.cu
-PairShape pairs_shape(bool fp64, int threads_hint);
+// Supported (threads, targets per thread) shapes of the pair kernel.
+const std::vector<PairShape>& pair_shapes(bool fp64);
+// The supported shape for (threads, per_thread), or the default (128, 1).
+PairShape pairs_shape(bool fp64, int threads, int per_thread);
 cudaError_t launch_pairs(cudaStream_t st, bool fp64, bool psi, PairShape shape, int nitems, const void* src,
                          const Copy* copies, const Tile* tiles, const WorkItem* items, double4* partials,
                          int64_t pstride, int* err);

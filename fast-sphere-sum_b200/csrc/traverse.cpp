@@ -214,7 +214,9 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
                 const int32_t k0 = int32_t(out.tiles.size());
                 pack_tiles(out.entries, cut[p], cut[p + 1], in.tile, t0 + c0, t0 + c0 + cn, out.copies, out.tiles);
                 const int32_t k1 = int32_t(out.tiles.size());
-                items.push_back({w * cn, WorkItem{t0 + c0, cn, k0, k1, p, int32_t(lf)}});
+                // a block's run time follows its source count (its warps
+                // run side by side), so the longest source lists go first
+                items.push_back({w, WorkItem{t0 + c0, cn, k0, k1, p, int32_t(lf)}});
             }
         }
     }

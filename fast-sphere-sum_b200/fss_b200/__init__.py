@@ -38,14 +38,16 @@ class Config(C.Structure):
                 ("tree_levels", C.c_int32), ("leaf_target", C.c_int32), ("degree", C.c_int32),
                 ("theta", C.c_double), ("many_count", C.c_int32), ("assign_mode", C.c_int32),
                 ("list_mode", C.c_int32), ("use_graph", C.c_int32), ("src_parts", C.c_int32),
-                ("block_threads", C.c_int32), ("reserved", C.c_int32 * 8)]
+                ("block_threads", C.c_int32), ("targets_per_thread", C.c_int32), ("autotune", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 class TreeInfo(C.Structure):
     _fields_ = [("tree_levels", C.c_int32), ("leaf_count", C.c_int32), ("degree", C.c_int32),
                 ("n_proxy", C.c_int32), ("n_pairs", C.c_int64), ("n_list_entries", C.c_int64),
                 ("n_items", C.c_int64), ("n_tiles", C.c_int64), ("unassigned", C.c_int64), ("pp_interactions", C.c_double),
-                ("pc_interactions", C.c_double)]
+                ("pc_interactions", C.c_double), ("block_threads", C.c_int32),
+                ("targets_per_thread", C.c_int32), ("src_parts", C.c_int32), ("pad", C.c_int32)]
 
 
 def build():

@@ -83,8 +83,12 @@ typedef struct fss_config {
     int32_t use_graph;     /* capture the RK4 step in a CUDA graph */
     int32_t src_parts;     /* split each target's source list in this many parts
                               (0 = automatic) */
-    int32_t block_threads; /* threads per interaction block (0 = automatic) */
-    int32_t reserved[8];
+    int32_t block_threads; /* threads per interaction block (0 = automatic: the
+                              smallest block that holds the largest leaf) */
+    int32_t targets_per_thread; /* with block_threads: 1 or 2 */
+    int32_t autotune;      /* at fss_set_particles, time every supported block
+                              shape on the actual lists and keep the fastest */
+    int32_t reserved[6];
 } fss_config;
 
 typedef struct fss_ctx fss_ctx;
@@ -145,6 +149,10 @@ typedef struct fss_tree_info {
     int64_t unassigned;      /* particles without a leaf (reference mode) */
     double pp_interactions;  /* particle-particle pair count per RHS */
     double pc_interactions;  /* particle-proxy pair count per RHS */
+    int32_t block_threads;   /* pair-kernel block shape in use */
+    int32_t targets_per_thread;
+    int32_t src_parts;
+    int32_t pad;
 } fss_tree_info;
 int fss_get_tree_info(fss_ctx* ctx, fss_tree_info* info);
 
