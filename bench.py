@@ -47,6 +47,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=2048, help="targets in one CPU-baseline sample")
+    p.add_argument("--tol", type=float, default=1e-6, help="selector: relative L2 velocity error target")
+    p.add_argument("--safety", type=float, default=2.0, help="selector: predicted-error safety factor")
+    p.add_argument("--fixed", action="store_true", help="headline arm without the learned selector")
     return p.parse_args()
 
 
@@ -190,6 +193,18 @@ def make_arm(fss, state, area, stream, prec, args, dev):
     return ctx
 
 
+def make_learned_arm(fss, state, area, stream, args, dev):
+    """Mixed precision with the learned per-leaf (degree, theta) and per-leaf
+    interaction lists; block shape chosen by the autotuner."""
+    from fss_b200 import selector
+    ctx = fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, list_mode=fss.LIST_LEAF,
+                      degree=args.degree, theta=args.theta, device=dev, autotune=1)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_particles(state, area)
+    choice = selector.apply(ctx, tol=args.tol, safety=args.safety, device=dev)
+    return ctx, np.bincount(choice, minlength=selector.NCLS).tolist()
+
+
 def warm(ctx, stream, w):
     for _ in range(w):
         ctx.rk4_step(DT, nsteps=1)
@@ -271,7 +286,13 @@ def main():
             np.max(np.linalg.norm(u - u_ref, axis=1)) / np.max(np.linalg.norm(u_ref, axis=1)))
 
     # ---------------- headline arm: mixed precision BLTC
-    ctx = make_arm(fss, state, area, stream, fss.PREC_MIXED, args, dev)
+    from fss_b200 import selector as _sel
+    learned = (not args.fixed) and os.path.exists(_sel.WEIGHTS)
+    classes = None
+    if learned:
+        ctx, classes = make_learned_arm(fss, state, area, stream, args, dev)
+    else:
+        ctx = make_arm(fss, state, area, stream, fss.PREC_MIXED, args, dev)
     err_l2, err_max = rel_err(ctx)
     warm(ctx, stream, args.warmup)
     barrier(ws)
@@ -349,11 +370,15 @@ def main():
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": f"BVE RK4 step (4 RHS), {n} particles (icosahedral level {args.level}), "
-                                       f"RH4 wave + {args.vortices} seeded vortices, BLTC n={args.degree} "
-                                       f"theta={args.theta}, tree_levels={info['tree_levels']}, static tree",
+                                       f"RH4 wave + {args.vortices} seeded vortices, mixed-precision BLTC "
+                                       f"({'learned per-leaf degree/theta' if learned else f'n={args.degree} theta={args.theta}'}), "
+                                       f"tree_levels={info['tree_levels']}, static tree",
                            "n_particles": n, "degree": args.degree, "theta": args.theta,
                            "precision": "FP32 interactions + Kahan; FP64 RK4, renormalisation, interpolation",
-                           "selector": "none (fixed degree/theta)", "l2": "flushed between timed steps (256 MB write)",
+                           "selector": (f"learned per-leaf (n, theta), tol {args.tol}, safety {args.safety}, "
+                                        f"class counts {classes}") if learned else "none (fixed degree/theta)",
+                           "lists": "per-leaf" if learned else "dual (reference traversal)",
+                           "l2": "flushed between timed steps (256 MB write)",
                            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
                 "rel_l2": err_l2, "rel_max": err_max,
                 "fp64_plain": fp64,

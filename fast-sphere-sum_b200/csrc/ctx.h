@@ -1,0 +1,116 @@
+// ctx.h -- the context behind fss_ctx (private to the library).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fss.h"
+#include "geometry.h"
+#include "kernels.h"
+#include "traverse.h"
+
+namespace fss {
+
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t b) {
+        if (b <= bytes && p) return cudaSuccess;
+        release();
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return e;
+        }
+        bytes = b;
+        return cudaSuccess;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct ProfEntry {
+    double ms = 0;
+    int64_t launches = 0;
+};
+
+}  // namespace fss
+
+struct fss_ctx {
+    using DBuf = fss::DBuf;
+    using ProfEntry = fss::ProfEntry;
+    using TreeGeometry = fss::TreeGeometry;
+    using Pair = fss::Pair;
+    using ListOutput = fss::ListOutput;
+    using ASrc = fss::ASrc;
+    using PairShape = fss::PairShape;
+    fss_config cfg{};
+    std::string err;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    bool fp64 = false;
+    bool tree = true;
+
+    int64_t n = 0;
+    bool have = false;
+    bool stage_dirty = false;  // xs/src hold a stand-alone rhs input, not s0
+
+    // tree
+    int tree_levels = 0, leaf_level = 0;
+    int64_t nleaf = 1;
+    TreeGeometry geom;
+    std::vector<int32_t> leaf_start_h;
+    std::vector<int32_t> counts_h;
+    std::vector<Pair> pairs;
+    std::vector<int32_t> ref_loc_h, cmp_loc_h;
+    int64_t unassigned = 0;
+    ListOutput lists;
+    std::vector<std::vector<ASrc>> alists;  // per-leaf sources before packing
+    std::vector<std::pair<fss::PairShape, double>> tuned;  // autotuner: shape, ms per pair pass
+    std::vector<int32_t> leaf_deg;
+    std::vector<double> leaf_theta;
+    int nmax = 0, level_mask = 0;
+    int parts = 1;
+    PairShape shape;
+    double direct_pairs = 0;
+
+    // device
+    DBuf in5, area_in, perm, key, key_tmp, vals_tmp, hist, leaf_start, s0, xs, acc, area_s, tracer_s, src, partials,
+        copies, tiles, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
+        wtotal, err_flag, loc;
+    int64_t src_count = 0;
+
+    // graph
+    cudaGraphExec_t graph = nullptr;
+    double graph_dt = 0, graph_omega = 0;
+
+    // profiling
+    bool prof = false;
+    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    std::vector<cudaEvent_t> ev_pool;
+    std::map<std::string, ProfEntry> prof_acc;
+    std::vector<std::string> prof_order;
+
+    std::unique_ptr<fss_ctx> alt;  // the other method, created on demand
+
+    ~fss_ctx() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (auto& p : pending) {
+            cudaEventDestroy(p.second.first);
+            cudaEventDestroy(p.second.second);
+        }
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+};
+

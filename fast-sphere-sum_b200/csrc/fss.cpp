@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "ctx.h"
 #include "geometry.h"
 #include "kernels.h"
 #include "traverse.h"
@@ -21,98 +22,7 @@ namespace {
 
 thread_local std::string g_last_error;
 
-struct DBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    ~DBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    cudaError_t ensure(size_t b) {
-        if (b <= bytes && p) return cudaSuccess;
-        release();
-        if (b == 0) b = 16;
-        cudaError_t e = cudaMalloc(&p, b);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return e;
-        }
-        bytes = b;
-        return cudaSuccess;
-    }
-    template <typename T> T* as() const { return static_cast<T*>(p); }
-};
-
-struct ProfEntry {
-    double ms = 0;
-    int64_t launches = 0;
-};
-
 }  // namespace
-
-struct fss_ctx {
-    fss_config cfg{};
-    std::string err;
-    int dev = 0;
-    cudaStream_t stream = nullptr;
-    cudaStream_t own_stream = nullptr;
-    bool fp64 = false;
-    bool tree = true;
-
-    int64_t n = 0;
-    bool have = false;
-    bool stage_dirty = false;  // xs/src hold a stand-alone rhs input, not s0
-
-    // tree
-    int tree_levels = 0, leaf_level = 0;
-    int64_t nleaf = 1;
-    TreeGeometry geom;
-    std::vector<int32_t> leaf_start_h;
-    std::vector<int32_t> counts_h;
-    std::vector<Pair> pairs;
-    std::vector<int32_t> ref_loc_h, cmp_loc_h;
-    int64_t unassigned = 0;
-    ListOutput lists;
-    std::vector<std::vector<ASrc>> alists;  // per-leaf sources before packing
-    std::vector<std::pair<PairShape, double>> tuned;  // autotuner: shape, ms per pair pass
-    std::vector<int32_t> leaf_deg;
-    std::vector<double> leaf_theta;
-    int nmax = 0, level_mask = 0;
-    int parts = 1;
-    PairShape shape;
-    double direct_pairs = 0;
-
-    // device
-    DBuf in5, area_in, perm, key, key_tmp, vals_tmp, hist, leaf_start, s0, xs, acc, area_s, tracer_s, src, partials,
-        copies, tiles, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
-        wtotal, err_flag, loc;
-    int64_t src_count = 0;
-
-    // graph
-    cudaGraphExec_t graph = nullptr;
-    double graph_dt = 0, graph_omega = 0;
-
-    // profiling
-    bool prof = false;
-    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
-    std::vector<cudaEvent_t> ev_pool;
-    std::map<std::string, ProfEntry> prof_acc;
-    std::vector<std::string> prof_order;
-
-    std::unique_ptr<fss_ctx> alt;  // the other method, created on demand
-
-    ~fss_ctx() {
-        if (graph) cudaGraphExecDestroy(graph);
-        for (auto& p : pending) {
-            cudaEventDestroy(p.second.first);
-            cudaEventDestroy(p.second.second);
-        }
-        for (auto e : ev_pool) cudaEventDestroy(e);
-        if (own_stream) cudaStreamDestroy(own_stream);
-    }
-};
 
 namespace {
 
@@ -211,7 +121,9 @@ int auto_tree_levels(const fss_config& cfg, int64_t n) {
 
 int src_size_ensure(fss_ctx* c, int64_t count) {
     const size_t es = c->fp64 ? sizeof(double4) : sizeof(float4);
+    void* before = c->src.p;
     CU(c->src.ensure(es * size_t(std::max<int64_t>(count, 1))));
+    if (c->src.p != before) c->stage_dirty = true;  // particle sources must be rewritten
     c->src_count = count;
     return FSS_OK;
 }
@@ -276,6 +188,8 @@ int build_tree(fss_ctx* c);
 PairShape choose_shape(fss_ctx* c);
 int materialize(fss_ctx* c, PairShape shape);
 int autotune(fss_ctx* c);
+int refresh_stage(fss_ctx* c);
+int eval(fss_ctx* c, EpiArgs& ea, bool want_psi);
 
 int gather(fss_ctx* c, bool write_s0) {
     const bool treec = c->tree;
@@ -311,6 +225,7 @@ int set_particles(fss_ctx* c, int64_t n, const double* state5, const double* are
     c->have = true;
     c->stage_dirty = false;
     if (c->tree && c->cfg.autotune) TRY(autotune(c));
+    TRY(refresh_stage(c));
     return check_device_error(c);
 }
 
@@ -539,6 +454,7 @@ int autotune(fss_ctx* c) {
     double best_ms = 1e30;
     for (const PairShape& sh : pair_shapes(c->fp64)) {
         TRY(materialize(c, sh));
+        TRY(refresh_stage(c));
         EpiArgs ea;
         ea.mode = EPI_RHS;
         ea.out5 = c->out5.as<double>();
@@ -655,6 +571,36 @@ fss_ctx* other_method(fss_ctx* c, int method, int* rc) {
 namespace fss {
 // Message for fss_last_error(NULL), for entry points outside this file.
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+// Interaction lists again from the current mode and per-leaf parameters.
+int internal_relist(fss_ctx* c) {
+    invalidate_graph(c);
+    const int LL = c->leaf_level;
+    if (c->cfg.list_mode == FSS_LIST_LEAF) {
+        c->alists = lists_per_leaf(c->geom, LL, c->counts_h, c->leaf_deg, c->leaf_theta);
+    } else {
+        const int many = (c->cfg.many_count < 0) ? nproxy(c->cfg.degree) : c->cfg.many_count;
+        c->alists = lists_from_pairs(c->geom, LL, dual_traverse(c->geom, c->counts_h, c->cfg.theta, many), many,
+                                     c->cfg.degree);
+    }
+    TRY(materialize(c, choose_shape(c)));
+    c->stage_dirty = true;
+    TRY(refresh_stage(c));
+    return check_device_error(c);
+}
+
+// Velocity of the current stage state into a host array (caller's order).
+int internal_rhs_current(fss_ctx* c, std::vector<double>& out5) {
+    TRY(refresh_stage(c));
+    EpiArgs ea;
+    ea.mode = EPI_RHS;
+    ea.omega = 2 * M_PI;
+    ea.out5 = c->out5.as<double>();
+    TRY(eval(c, ea, false));
+    out5.resize(5 * c->n);
+    CU(cudaMemcpyAsync(out5.data(), c->out5.p, sizeof(double) * 5 * c->n, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
+}
 }  // namespace fss
 
 // =================================================================== C ABI

@@ -69,7 +69,10 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_get_tree", "fss_set_leaf_params", "fss_profile_enable", "fss_profile_read",
            "fss_work_per_rhs", "fss_icos_counts", "fss_icos_grid", "fss_area_init",
            "fss_vorticity_rh4_ref", "fss_vorticity_rh_vortices", "fss_tree_traverse", "fss_interp_nodes",
-           "fss_tree_geometry", "fss_rhs_direct_noalloc", "fss_version"]
+           "fss_tree_geometry", "fss_rhs_direct_noalloc", "fss_mlp_create", "fss_mlp_destroy",
+           "fss_mlp_param_count", "fss_mlp_init", "fss_mlp_set_params", "fss_mlp_get_params", "fss_mlp_set_data",
+           "fss_mlp_gradient", "fss_mlp_train", "fss_mlp_predict", "fss_selector_features", "fss_select_classes",
+           "fss_selector_apply", "fss_version"]
 
 NOALLOC_MAX_PARTICLES = 262144  # FSS_NOALLOC_MAX_PARTICLES in include/fss.h
 

@@ -216,6 +216,46 @@ int fss_interp_nodes(int32_t degree, double* nodes, double* vinv);
  * circumcentre and circumradius per face (4 doubles), levels concatenated. */
 int fss_tree_geometry(int32_t tree_levels, double* tri_info);
 
+/* ------------------------------------------------------------ selector
+ * Learned per-leaf interpolation degree and MAC (no counterpart in the
+ * reference, which fixes degree 2 and one theta: new_dynamics.cpp:78-79,
+ * run_config.h:100).  Classes c = 0..11: degree 4 + 2 (c / 3), theta
+ * 0.5 + 0.1 (c % 3).  The network is a 16-64-64-12 MLP (ReLU) with BF16
+ * weights and FP32 accumulation; it predicts log10(e_l(c) / U) for every
+ * leaf l, e_l the L2 velocity error over the leaf's particles and U the RMS
+ * speed. */
+#define FSS_SELECTOR_CLASSES 12
+#define FSS_SELECTOR_FEATURES 16
+typedef struct fss_mlp fss_mlp;
+int fss_mlp_create(int32_t device, fss_mlp** out);
+void fss_mlp_destroy(fss_mlp* m);
+/* Number of parameters: W1[64][16], b1[64], W2[64][64], b2[64], W3[12][64], b3[12]. */
+int32_t fss_mlp_param_count(void);
+int fss_mlp_init(fss_mlp* m, uint64_t seed);
+int fss_mlp_set_params(fss_mlp* m, const float* params);
+int fss_mlp_get_params(fss_mlp* m, float* params);
+/* Training set: n rows of 16 features, 12 targets and an optional 0/1 mask. */
+int fss_mlp_set_data(fss_mlp* m, int64_t n, const float* x, const float* t, const float* mask);
+/* Loss = mean over rows of sum_o mask (y - t)^2 and its gradient (no update). */
+int fss_mlp_gradient(fss_mlp* m, float* grad, double* loss);
+/* Adam (beta 0.9/0.999), shuffled mini-batches (multiples of 128); mean
+ * batch loss per epoch into losses[epochs]. */
+int fss_mlp_train(fss_mlp* m, int32_t epochs, int32_t batch, double lr, uint64_t seed, double* losses);
+int fss_mlp_predict(fss_mlp* m, int64_t n, const float* x, float* y);
+/* Features (16 per leaf) and exact interaction counts (12 per leaf, one per
+ * class) of the current tree and state, and the RMS speed U. */
+int fss_selector_features(fss_ctx* ctx, float* features, double* costs, double* u_rms);
+/* Per leaf the class minimising cost + mu * 10^(2 y) with mu chosen by
+ * bisection so that sum_l 10^(2 y_l) <= budget (host only). */
+int fss_select_classes(int64_t nleaf, int32_t nclass, const double* pred_log_err, const double* cost,
+                       double budget, int32_t* choice);
+/* Predict with `m` (features standardised with mean/std), choose classes
+ * for a relative L2 tolerance tol (budget (tol/safety)^2 N), switch the
+ * context to per-leaf lists with those parameters.  choice_out: nleaf ints
+ * (nullable). */
+int fss_selector_apply(fss_ctx* ctx, fss_mlp* m, const float* feat_mean, const float* feat_std, double tol,
+                       double safety, int32_t* choice_out);
+
 /* Direct sum without any allocation.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory: real-time loops in which a

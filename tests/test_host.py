@@ -16,7 +16,7 @@ def bits(a):
 
 def test_library_exports_every_declared_symbol(fss):
     header = open(os.path.join(ROOT, "include", "fss.h")).read()
-    declared = sorted(set(re.findall(r"^(?:int|void|const char\s*\*)\s+(fss_[a-z0-9_]+)\s*\(", header, re.M)))
+    declared = sorted(set(re.findall(r"^(?:int|int32_t|int64_t|void|const char\s*\*)\s+(fss_[a-z0-9_]+)\s*\(", header, re.M)))
     assert len(declared) > 20
     L = fss.lib()
     missing = [s for s in declared if not hasattr(L, s)]

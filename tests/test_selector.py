@@ -1,0 +1,92 @@
+"""Learned degree/MAC selector: the MLP kernels against the FP64 oracle,
+the budgeted class selection, and what the trained network gains."""
+import os
+
+import numpy as np
+import pytest
+
+
+def test_select_classes_respects_budget_and_minimises_cost(fss):
+    from fss_b200 import selector as S
+    rng = np.random.default_rng(0)
+    nleaf, ncls = 40, 12
+    pred = rng.uniform(-9, -4, (nleaf, ncls))
+    cost = rng.uniform(1, 10, (nleaf, ncls))
+    for budget in (1e-10, 1e-9, 1e-8):
+        ch = S.select(pred, cost, budget)
+        e = np.sum(10.0 ** (2 * pred[np.arange(nleaf), ch]))
+        assert e <= budget * (1 + 1e-9) or np.array_equal(ch, pred.argmin(1))
+        # no single leaf can be moved to a cheaper class without breaking the budget
+        for l in range(nleaf):
+            for k in range(ncls):
+                if cost[l, k] < cost[l, ch[l]]:
+                    e2 = e - 10.0 ** (2 * pred[l, ch[l]]) + 10.0 ** (2 * pred[l, k])
+                    assert e2 > budget * 0.999 or cost[l, k] >= cost[l, ch[l]]
+
+
+def test_select_unreachable_budget_takes_least_error(fss):
+    from fss_b200 import selector as S
+    pred = np.array([[-3.0, -4.0, -5.0]] * 3)
+    cost = np.array([[1.0, 2.0, 3.0]] * 3)
+    assert np.array_equal(S.select(pred, cost, 1e-30), [2, 2, 2])
+
+
+def test_weights_file_is_consistent(fss):
+    from fss_b200 import selector as S
+    if not os.path.exists(S.WEIGHTS):
+        pytest.skip("no trained weights")
+    p, mean, std = S.load()
+    assert p.shape == (6028,) and mean.shape == (16,) and std.shape == (16,)
+    assert np.all(np.isfinite(p)) and np.all(std > 0)
+
+
+@pytest.mark.gpu
+def test_mlp_gradient_matches_oracle(fss):
+    import mlp_oracle as M
+    from fss_b200 import selector as S
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((1000, 16)).astype(np.float32)
+    t = rng.standard_normal((1000, 12)).astype(np.float32)
+    mask = (rng.uniform(size=(1000, 12)) > 0.2).astype(np.float32)
+    m = S.MLP(seed=3)
+    p = m.params()
+    m.set_data(x, t, mask)
+    g, loss = m.gradient()
+    lo, go = M.loss_and_grad(p, x, t, mask)
+    assert abs(loss - lo) < 1e-5 * abs(lo)
+    assert np.linalg.norm(g - go) < 1e-4 * np.linalg.norm(go)
+    # per parameter block
+    for a, b in zip(S.unpack(g), S.unpack(go)):
+        assert np.linalg.norm(a - b) <= 1e-3 * np.linalg.norm(b) + 1e-9
+    y = m.predict(x)
+    assert np.abs(y - M.forward(p, x)[3]).max() < 1e-4 * np.abs(M.forward(p, x)[3]).max()
+    m.close()
+
+
+@pytest.mark.gpu
+def test_mlp_training_fits_a_smooth_target(fss):
+    from fss_b200 import selector as S
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((8192, 16)).astype(np.float32)
+    t = np.stack([np.sin(x[:, k % 16]) + 0.5 * x[:, (k + 3) % 16] for k in range(12)], 1).astype(np.float32)
+    m = S.MLP(seed=4)
+    m.set_data(x, t)
+    _, l0 = m.gradient()
+    losses = m.train(30, batch=1024, lr=3e-3)
+    _, l1 = m.gradient()
+    assert l1 < 0.1 * l0, (l0, l1, losses[-5:])
+    m.close()
+
+
+@pytest.mark.gpu
+def test_selector_gain_over_fixed_degree(fss):
+    """On a field outside the training set, the learned per-leaf (n, theta)
+    keeps rel-L2 <= 1e-6 against the FP64 direct sum with fewer interactions
+    than the fixed n = 8, theta = 0.7 treecode."""
+    from fss_b200 import selector as S
+    if not os.path.exists(S.WEIGHTS):
+        pytest.skip("no trained weights")
+    r = S.evaluate(S.WEIGHTS, level=7, seed=4242, tol=1e-6, safety=2.0, n_vortex=16)
+    assert r["learned"]["rel_l2"] <= 1e-6, r
+    assert r["fixed"]["rel_l2"] <= 1e-6, r
+    assert r["interaction_ratio"] > 1.0, r
