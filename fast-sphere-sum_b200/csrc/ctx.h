@@ -60,6 +60,7 @@ struct fss_ctx {
     cudaStream_t own_stream = nullptr;
     bool fp64 = false;
     bool tree = true;
+    bool resort = false;  // re-sort particles into their current leaves every RK4 step
 
     int64_t n = 0;
     bool have = false;
@@ -86,8 +87,8 @@ struct fss_ctx {
 
     // device
     DBuf in5, area_in, perm, key, key_tmp, vals_tmp, hist, leaf_start, s0, xs, acc, area_s, tracer_s, src, partials,
-        copies, tiles, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
-        wtotal, err_flag, loc;
+        segs, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
+        wtotal, err_flag, loc, sortq;
     int64_t src_count = 0;
 
     // graph

@@ -128,7 +128,7 @@ int src_size_ensure(fss_ctx* c, int64_t count) {
     return FSS_OK;
 }
 
-// Lists of the direct sum: target tiles x source chunks.
+// Lists of the direct sum: blocks of targets x P chunks of the sources.
 int build_direct_lists(fss_ctx* c) {
     const int64_t n = c->n;
     c->shape = pairs_shape(c->fp64, c->cfg.block_threads, c->cfg.targets_per_thread);
@@ -144,29 +144,36 @@ int build_direct_lists(fss_ctx* c) {
     c->parts = P;
     ListOutput& L = c->lists;
     L = ListOutput();
-    for (int p = 0; p < P; p++) {
-        SrcEntry e{};
-        e.start = int32_t(n * p / P);
-        e.count = int32_t(n * (p + 1) / P - e.start);
-        e.kind = 0;
-        L.entries.push_back(e);
-    }
+    for (int p = 0; p < P; p++) L.segs.push_back(Segment{1, int32_t(n * p / P), int32_t(n * (p + 1) / P), 0});
     for (int64_t t = 0; t < tiles; t++) {
         const int64_t t0 = t * TB, nt = std::min<int64_t>(TB, n - t0);
         for (int p = 0; p < P; p++) {
-            const int32_t k0 = int32_t(L.tiles.size());
-            pack_tiles(L.entries, p, p + 1, c->shape.tile, t0, t0 + nt, L.copies, L.tiles);
-            L.items.push_back(WorkItem{int32_t(t0), int32_t(nt), k0, int32_t(L.tiles.size()), p, 0});
+            L.items.push_back(WorkItem{int32_t(t0), int32_t(nt), p, p + 1, p, -1});
+            L.n_tiles += (L.segs[p].b - L.segs[p].a + c->shape.tile - 1) / c->shape.tile;
         }
     }
     L.pp_pairs = double(n) * double(n - 1);
     c->direct_pairs = L.pp_pairs;
-    TRY(upload(c, c->copies, L.copies));
-    TRY(upload(c, c->tiles, L.tiles));
+    TRY(upload(c, c->segs, L.segs));
     TRY(upload(c, c->items, L.items));
     TRY(src_size_ensure(c, n));
     CU(c->partials.ensure(sizeof(double4) * size_t(P) * size_t(std::max<int64_t>(n, 1))));
     return FSS_OK;
+}
+
+// Per-leaf source lists of the configured mode.  With re-sorting, faces
+// empty at the build may fill later, so no face is pruned for being empty.
+void make_alists(fss_ctx* c, const std::vector<int32_t>& dual_counts) {
+    const int LL = c->leaf_level;
+    if (c->cfg.list_mode == FSS_LIST_LEAF) {
+        c->alists = lists_per_leaf(c->geom, LL, c->counts_h, c->leaf_deg, c->leaf_theta, c->resort);
+        return;
+    }
+    const int many = (c->cfg.many_count < 0) ? nproxy(c->cfg.degree) : c->cfg.many_count;
+    std::vector<int32_t> cc = dual_counts;
+    if (c->resort)
+        for (int32_t& x : cc) x = std::max(x, 1);
+    c->alists = lists_from_pairs(c->geom, LL, dual_traverse(c->geom, cc, c->cfg.theta, many), many, c->cfg.degree);
 }
 
 int ensure_particle_buffers(fss_ctx* c, int64_t n) {
@@ -232,6 +239,8 @@ int set_particles(fss_ctx* c, int64_t n, const double* state5, const double* are
 int build_tree(fss_ctx* c) {
     const int64_t n = c->n;
     const int TL = auto_tree_levels(c->cfg, n);
+    c->resort = c->cfg.rebuild == FSS_REBUILD_RESORT ||
+                (c->cfg.rebuild == FSS_REBUILD_AUTO && c->cfg.assign_mode != FSS_ASSIGN_REFERENCE);
     if (TL < 1 || TL > kMaxLevels) return fail(c, FSS_ERR_INVALID, "tree_levels out of range");
     if (TL != c->tree_levels || c->geom.tree_levels != TL) {
         c->geom = build_tree_geometry(TL);
@@ -260,6 +269,7 @@ int build_tree(fss_ctx* c) {
     CU(c->key_tmp.ensure(sizeof(uint32_t) * n));
     CU(c->perm.ensure(sizeof(int32_t) * n));
     CU(c->vals_tmp.ensure(sizeof(int32_t) * n));
+    CU(c->sortq.ensure(sizeof(int32_t) * n));
     CU(c->hist.ensure(sizeof(uint32_t) * sort_scratch_words(n)));
     CU(c->leaf_start.ensure(sizeof(int32_t) * (c->nleaf + 1)));
     c->ref_loc_h.clear();
@@ -312,18 +322,14 @@ int build_tree(fss_ctx* c) {
     }
     const int K = nproxy(c->cfg.degree);
     const int many = (c->cfg.many_count < 0) ? K : c->cfg.many_count;
+    // the reference-format pair list (fss_get_tree) of this build
     c->pairs = dual_traverse(c->geom, (c->cfg.assign_mode == FSS_ASSIGN_REFERENCE) ? ref_counts : c->counts_h,
                              c->cfg.theta, many);
-    std::vector<std::vector<ASrc>> al;
-    if (c->cfg.list_mode == FSS_LIST_LEAF) {
-        al = lists_per_leaf(c->geom, LL, c->counts_h, c->leaf_deg, c->leaf_theta);
+    if (c->cfg.list_mode == FSS_LIST_DUAL && !c->resort && c->cfg.assign_mode != FSS_ASSIGN_REFERENCE) {
+        c->alists = lists_from_pairs(c->geom, LL, c->pairs, many, c->cfg.degree);
     } else {
-        const std::vector<Pair>& pp = (c->cfg.assign_mode == FSS_ASSIGN_REFERENCE)
-                                          ? dual_traverse(c->geom, c->counts_h, c->cfg.theta, many)
-                                          : c->pairs;
-        al = lists_from_pairs(c->geom, LL, pp, many, c->cfg.degree);
+        make_alists(c, c->counts_h);
     }
-    c->alists = std::move(al);
     TRY(materialize(c, choose_shape(c)));
     return FSS_OK;
 }
@@ -363,6 +369,7 @@ int materialize(fss_ctx* c, PairShape shape) {
         P = waves >= 3.0 ? 1 : (waves >= 1.0 ? 2 : 4);
     }
     in.parts = P;
+    in.all_leaves = c->resort;
     c->parts = P;
     build_lists(in, c->alists, c->lists);
     const ListOutput& L = c->lists;
@@ -384,8 +391,7 @@ int materialize(fss_ctx* c, PairShape shape) {
     }
     TRY(upload(c, c->vinv, vinv_all));
     TRY(upload(c, c->vinv_off, vinv_off));
-    TRY(upload(c, c->copies, L.copies));
-    TRY(upload(c, c->tiles, L.tiles));
+    TRY(upload(c, c->segs, L.segs));
     TRY(upload(c, c->items, L.items));
     TRY(upload(c, c->jobs, L.jobs));
     std::vector<double4> pp(L.proxy_pos.size() / 4);
@@ -418,8 +424,8 @@ int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
     {
         ProfScope ps(c, c->fp64 ? "pairs_fp64" : "pairs_mixed");
         CU(launch_pairs(c->stream, c->fp64, want_psi, c->shape, int(c->lists.items.size()), c->src.p,
-                        c->copies.as<Copy>(), c->tiles.as<Tile>(), c->items.as<WorkItem>(), c->partials.as<double4>(),
-                        c->n, c->err_flag.as<int>()));
+                        c->segs.as<Segment>(), c->leaf_start.as<int32_t>(), c->items.as<WorkItem>(),
+                        c->partials.as<double4>(), c->n, c->err_flag.as<int>()));
     }
     if (want_psi) launch_wsum(c->stream, c->n, c->xs.as<double4>(), c->area_s.as<double>(), c->wtotal.as<double>());
     ea.n = c->n;
@@ -462,7 +468,7 @@ int autotune(fss_ctx* c) {
         CU(cudaEventRecord(a, c->stream));
         for (int r = 0; r < 2; r++)
             CU(launch_pairs(c->stream, c->fp64, false, c->shape, int(c->lists.items.size()), c->src.p,
-                            c->copies.as<Copy>(), c->tiles.as<Tile>(), c->items.as<WorkItem>(),
+                            c->segs.as<Segment>(), c->leaf_start.as<int32_t>(), c->items.as<WorkItem>(),
                             c->partials.as<double4>(), c->n, c->err_flag.as<int>()));
         CU(cudaEventRecord(b, c->stream));
         CU(cudaEventSynchronize(b));
@@ -482,7 +488,28 @@ int autotune(fss_ctx* c) {
     return FSS_OK;
 }
 
+// Particles into the leaves they are in now (start of an RK4 step): keys,
+// stable key sort (order q), state permuted in place, leaf ranges, stage-1
+// sources.
+int resort(fss_ctx* c) {
+    ProfScope ps(c, "resort");
+    const int64_t n = c->n;
+    launch_reassign(c->stream, n, c->s0.as<double4>(), nullptr, c->leaf_level, c->verts.as<double>(),
+                    c->tri_verts.as<int32_t>(), c->lev_off.as<int64_t>(), c->key.as<uint32_t>());
+    int bits = 0;
+    while ((int64_t(1) << bits) < c->nleaf) bits++;
+    launch_sort(c->stream, n, std::max(bits, 1), c->key.as<uint32_t>(), c->key_tmp.as<uint32_t>(),
+                c->sortq.as<int32_t>(), c->vals_tmp.as<int32_t>(), c->hist.as<uint32_t>());
+    launch_resort(c->stream, c->fp64, n, c->sortq.as<int32_t>(), c->s0.as<double4>(), c->area_s.as<double>(),
+                  c->tracer_s.as<double>(), c->perm.as<int32_t>(), c->xs.as<double4>(), c->acc.as<double4>(),
+                  c->src.p);
+    launch_leaf_bounds(c->stream, n, c->key.as<uint32_t>(), int32_t(c->nleaf), c->leaf_start.as<int32_t>());
+    CU(cudaGetLastError());
+    return FSS_OK;
+}
+
 int rk4_once(fss_ctx* c, double dt, double omega) {
+    if (c->tree && c->resort) TRY(resort(c));
     for (int stage = 1; stage <= 4; stage++) {
         EpiArgs ea;
         ea.mode = EPI_RK4;
@@ -575,14 +602,7 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 // Interaction lists again from the current mode and per-leaf parameters.
 int internal_relist(fss_ctx* c) {
     invalidate_graph(c);
-    const int LL = c->leaf_level;
-    if (c->cfg.list_mode == FSS_LIST_LEAF) {
-        c->alists = lists_per_leaf(c->geom, LL, c->counts_h, c->leaf_deg, c->leaf_theta);
-    } else {
-        const int many = (c->cfg.many_count < 0) ? nproxy(c->cfg.degree) : c->cfg.many_count;
-        c->alists = lists_from_pairs(c->geom, LL, dual_traverse(c->geom, c->counts_h, c->cfg.theta, many), many,
-                                     c->cfg.degree);
-    }
+    make_alists(c, c->counts_h);
     TRY(materialize(c, choose_shape(c)));
     c->stage_dirty = true;
     TRY(refresh_stage(c));
@@ -785,8 +805,8 @@ int fss_get_tree_info(fss_ctx* c, fss_tree_info* info) {
     info->degree = c->cfg.degree;
     info->n_proxy = nproxy(c->cfg.degree);
     info->n_pairs = int64_t(c->pairs.size());
-    info->n_list_entries = int64_t(c->lists.entries.size());
-    info->n_tiles = int64_t(c->lists.tiles.size());
+    info->n_list_entries = int64_t(c->lists.segs.size());
+    info->n_tiles = c->lists.n_tiles;
     info->n_items = int64_t(c->lists.items.size());
     info->unassigned = c->unassigned;
     info->pp_interactions = c->lists.pp_pairs;

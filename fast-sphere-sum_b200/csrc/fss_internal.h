@@ -15,36 +15,28 @@ namespace fss {
 // Error codes a kernel records in the context's device error word.
 enum : int { kErrNone = 0, kErrTimeout = 1, kErrTree = 2 };
 
-// One contiguous run of sources seen by one target leaf: `count` entries of
-// the unified source array starting at `start` (particles [0, n), proxies
-// after them).  Host-side list element before packing into tiles.
-struct SrcEntry {
-    int32_t start;
-    int32_t count;
-    int32_t kind;   // 0 particles (near or small far cluster), 1 proxies
+// One run of sources of a work item.  The pair kernel resolves it to a
+// range [lo, hi) of the unified source array (particles [0, n), proxies
+// after them) when it runs:
+//   kind 0: the particles of leaves [a, b), i.e. [leaf_start[a],
+//           leaf_start[b]) -- read on the device, since particles are
+//           re-sorted into the leaves they have moved into;
+//   kind 1: the fixed range [a, b) (far-cluster proxies, or a chunk of the
+//           direct sum).
+// The kernel packs consecutive runs into shared-memory tiles as it goes.
+struct Segment {
+    int32_t kind;
+    int32_t a, b;
     int32_t pad;
 };
 
-// One bulk copy global -> shared: `count` sources from `start`.
-struct Copy {
-    int32_t start;
-    int32_t count;
-};
-
-// One shared-memory tile: copies [c0, c1) placed back to back, `count`
-// sources in all; guard = 1 when a copy overlaps the block's own targets
-// (the self pair must be skipped).
-struct Tile {
-    int32_t c0, c1;
-    int32_t count;
-    int32_t guard;
-};
-
-// One block's work: targets [t0, t0 + nt) (one leaf, sorted order) against
-// tiles [k0, k1); results go to partial slot `part`.
+// One block's work.  leaf >= 0: the targets are that leaf's current
+// particles, taken in chunks of the block size; leaf < 0: the targets are
+// [t0, t0 + nt).  Sources: segments [g0, g1).  Results go to partial slot
+// `part`.
 struct WorkItem {
     int32_t t0, nt;
-    int32_t k0, k1;
+    int32_t g0, g1;
     int32_t part;
     int32_t leaf;
 };
@@ -61,6 +53,18 @@ struct ProxyJob {
     int32_t degmask;
     int32_t off[12];              // by degree, -1 when not wanted
     int32_t pad;
+};
+
+// One leaf of an ensemble member for the batched upward pass: its index in
+// the concatenated leaf_start (particles [leaf_start[g], leaf_start[g+1])
+// of the concatenated arrays), its member's leaf level, its index on that
+// level, the first of its (leaf_level + 1) x K moment slots, and the levels
+// whose faces carry proxies in its member.
+struct EnsLeaf {
+    int32_t gleaf;
+    int32_t leaf_level, local;
+    int32_t level_mask;
+    int64_t part_base;
 };
 
 // Per-node geometry for the upward pass: inverse of [v1 v2 v3] (columns),

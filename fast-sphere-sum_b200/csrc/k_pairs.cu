@@ -1,14 +1,17 @@
 // k_pairs.cu -- the pair engine shared by the direct sum, the near field and
 // the particle-cluster far field.
 //
-// A block owns up to THREADS*R targets of one leaf (or of one tile of the
-// direct sum).  Its sources -- particles of near leaves, proxy charges of far
-// clusters, or a chunk of all particles -- arrive as a sequence of
-// shared-memory tiles.  Each tile is several source ranges placed back to
-// back by bulk TMA copies (cp.async.bulk, issued by one lane of warp 0,
-// completion counted on the tile slot's mbarrier; no multicast), in a ring
-// of kDepth slots released by the consumer warps through a second mbarrier.
-// Each thread keeps R targets in registers.  Per pair (23 algorithmic flops):
+// A block works on one work item: the targets of one leaf (taken in chunks
+// of the block size; the leaf's current particle range is read from
+// leaf_start on the device, since particles are re-sorted into the leaves
+// they have moved into) or an explicit target range (direct sum).  Its
+// sources are a list of segments -- the particles of a run of leaves (range
+// read at run time) or a fixed range of far-cluster proxies -- which warp 0
+// packs back to back into shared-memory tiles as it goes, issuing one bulk
+// TMA copy (cp.async.bulk, no multicast) per piece with completion counted
+// on the tile slot's mbarrier.  Tiles circulate in a ring of kDepth slots
+// released by the consumer warps through a second mbarrier; an empty tile
+// ends a chunk.  One target per thread.  Per pair (23 algorithmic flops):
 //
 //   d   = x_j - x_i
 //   r2  = |d|^2           (= 2 (1 - x_i.x_j) on the unit sphere, no cancellation)
@@ -27,27 +30,24 @@ namespace fss {
 
 constexpr int kDepth = 4;  // ring depth (tiles in flight)
 
-template <typename T, int R, bool PSI, bool GUARD>
-__device__ __forceinline__ void tile_pairs(const typename Vec4<T>::type* __restrict__ s, int cnt, const T* tx,
-                                           const T* ty, const T* tz, T* ax, T* ay, T* az, T* ap) {
+template <typename T, bool PSI, bool GUARD>
+__device__ __forceinline__ void tile_pairs(const typename Vec4<T>::type* __restrict__ s, int cnt, T tx, T ty, T tz,
+                                           T& ax, T& ay, T& az, T& ap) {
 #pragma unroll 8
     for (int j = 0; j < cnt; j++) {
         const typename Vec4<T>::type q = s[j];
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-            const T dx = q.x - tx[r], dy = q.y - ty[r], dz = q.z - tz[r];
-            const T r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-            T inv = rcp_fast(r2);
-            if (GUARD) inv = (r2 > T(0)) ? inv : T(0);
-            const T sc = q.w * inv;
-            ax[r] = fma(sc, dx, ax[r]);
-            ay[r] = fma(sc, dy, ay[r]);
-            az[r] = fma(sc, dz, az[r]);
-            if (PSI) {
-                T lg = lg2_fast(r2);
-                if (GUARD) lg = (r2 > T(0)) ? lg : T(0);
-                ap[r] = fma(q.w, lg, ap[r]);
-            }
+        const T dx = q.x - tx, dy = q.y - ty, dz = q.z - tz;
+        const T r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+        T inv = rcp_fast(r2);
+        if (GUARD) inv = (r2 > T(0)) ? inv : T(0);
+        const T sc = q.w * inv;
+        ax = fma(sc, dx, ax);
+        ay = fma(sc, dy, ay);
+        az = fma(sc, dz, az);
+        if (PSI) {
+            T lg = lg2_fast(r2);
+            if (GUARD) lg = (r2 > T(0)) ? lg : T(0);
+            ap = fma(q.w, lg, ap);
         }
     }
 }
@@ -60,189 +60,303 @@ __device__ __forceinline__ void kahan_add(T& sum, T& comp, T x) {
     sum = t;
 }
 
-template <typename T, int THREADS, int R, bool PSI, int TILE>
-__global__ void __launch_bounds__(THREADS) k_pairs(const typename Vec4<T>::type* __restrict__ src,
-                                                   const Copy* __restrict__ copies, const Tile* __restrict__ tiles,
-                                                   const WorkItem* __restrict__ items, double4* __restrict__ partials,
-                                                   int64_t pstride, int* __restrict__ err) {
+// Producer side of the ring: warp 0 packs the next tile of a work item's
+// sources.  Lane i resolves segment g + i to its range [lo, hi) (kind 0
+// through leaf_start), a warp scan places the ranges back to back, and each
+// lane issues the bulk copy of its piece; the segment cut by the end of the
+// tile is resumed at `off` by the next tile.  Returns the tile's source
+// count (0: the item's sources are exhausted); `guard` is set when a piece
+// overlaps the targets [t0, t1) (a source that is one of the block's own
+// targets must skip the self pair).  The transaction bytes of each round
+// are expected on `bar` by lane 0 before any lane issues its copy.
+template <typename S4, int TILE>
+__device__ __forceinline__ int pack_tile(const Segment* __restrict__ segs, const int32_t* __restrict__ leaf_start,
+                                         int g1, int& g, int& off, int t0, int t1, const S4* __restrict__ src,
+                                         S4* dst, uint64_t* bar, bool& guard) {
+    const int lane = threadIdx.x & 31;
+    int count = 0;
+    bool gd = false;
+    while (g < g1 && count < TILE) {
+        const int gi = g + lane;
+        int lo = 0, hi = 0;
+        if (gi < g1) {
+            const Segment sg = segs[gi];
+            if (sg.kind == 0) {
+                lo = leaf_start[sg.a];
+                hi = leaf_start[sg.b];
+            } else {
+                lo = sg.a;
+                hi = sg.b;
+            }
+            if (lane == 0) lo += off;
+        }
+        const int len = max(hi - lo, 0);
+        int incl = len;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += y;
+        }
+        const int excl = incl - len;
+        const int room = TILE - count;
+        const int take = max(0, min(len, room - excl));
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        const int placed = min(total, room);
+        if (lane == 0 && placed > 0) mbar_expect_tx(bar, uint32_t(placed) * uint32_t(sizeof(S4)));
+        __syncwarp();
+        if (take > 0) {
+            bulk_g2s(dst + count + excl, src + lo, uint32_t(take) * uint32_t(sizeof(S4)), bar);
+            if (lo < t1 && lo + take > t0) gd = true;
+        }
+        if (total <= room) {
+            g = min(g + 32, g1);
+            off = 0;
+            count += total;
+        } else {
+            const int k = __ffs(__ballot_sync(0xffffffffu, incl > room)) - 1;
+            const int ek = __shfl_sync(0xffffffffu, excl, k);
+            off = (k == 0 ? off : 0) + (room - ek);
+            g += k;
+            count = TILE;
+        }
+    }
+    guard = __any_sync(0xffffffffu, gd) != 0;
+    return count;
+}
+
+// Tile header written by the producer before the slot's arrive (the
+// consumers read it after the slot's phase completes).
+struct SlotHdr {
+    int count, guard;
+};
+
+struct RingState {
+    int64_t issued, consumed;
+    bool failed;
+};
+
+// One work item: every chunk of targets against every tile of its segments.
+template <typename T, int THREADS, int TILE, bool PSI>
+__device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4<T>::type* __restrict__ src,
+                                         const Segment* __restrict__ segs, const int32_t* __restrict__ leaf_start,
+                                         double4* __restrict__ partials, int64_t pstride,
+                                         typename Vec4<T>::type* ring, SlotHdr* hdr, uint64_t* full_bar,
+                                         uint64_t* empty_bar, RingState& rs) {
     using S4 = typename Vec4<T>::type;
     constexpr bool kKahan = sizeof(T) == 4;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    S4* ring = reinterpret_cast<S4*>(smem_raw);
-    __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int t0 = it.t0, nt = it.nt;
+    if (it.leaf >= 0) {
+        t0 = leaf_start[it.leaf];
+        nt = leaf_start[it.leaf + 1] - t0;
+    }
+    for (int c0 = 0; c0 < nt && !rs.failed; c0 += THREADS) {
+        const int cn = min(THREADS, nt - c0);
+        const bool active = warp * 32 < cn;
+        const S4 v = src[t0 + c0 + ((tid < cn) ? tid : 0)];
+        const T tx = v.x, ty = v.y, tz = v.z;
+        T ax = 0, ay = 0, az = 0, ap = 0, sx = 0, sy = 0, sz = 0, sp = 0, cx = 0, cy = 0, cz = 0, cp = 0;
+        int pg = it.g0, poff = 0;
+        bool pdone = false;
+        // producer: warp 0; one tile per call, then one empty tile that ends
+        // the chunk
+        auto produce = [&]() {
+            if (pdone || rs.failed) return;
+            const int slot = int(rs.issued % kDepth);
+            bool ok = true;
+            if (rs.issued >= kDepth) ok = mbar_wait_bounded(&empty_bar[slot], uint32_t((rs.issued / kDepth) - 1) & 1);
+            if (!__all_sync(0xffffffffu, ok)) {
+                rs.failed = true;
+                return;
+            }
+            bool gd = false;
+            const int cnt = pack_tile<S4, TILE>(segs, leaf_start, it.g1, pg, poff, t0 + c0, t0 + c0 + cn, src,
+                                                ring + slot * TILE, &full_bar[slot], gd);
+            if (lane == 0) {
+                hdr[slot].count = cnt;
+                hdr[slot].guard = gd ? 1 : 0;
+                mbar_arrive(&full_bar[slot]);
+            }
+            __syncwarp();
+            if (cnt == 0) pdone = true;
+            rs.issued++;
+        };
+        if (warp == 0)
+            for (int d = 0; d < kDepth - 1; d++) produce();
+        for (;;) {
+            if (warp == 0) produce();
+            const int slot = int(rs.consumed % kDepth);
+            if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full_bar[slot], uint32_t(rs.consumed / kDepth) & 1))) {
+                rs.failed = true;
+                break;
+            }
+            const SlotHdr h = hdr[slot];
+            if (active && h.count > 0) {
+                const S4* tile = ring + slot * TILE;
+                if (h.guard)
+                    tile_pairs<T, PSI, true>(tile, h.count, tx, ty, tz, ax, ay, az, ap);
+                else
+                    tile_pairs<T, PSI, false>(tile, h.count, tx, ty, tz, ax, ay, az, ap);
+                if (kKahan) {
+                    kahan_add(sx, cx, ax);
+                    kahan_add(sy, cy, ay);
+                    kahan_add(sz, cz, az);
+                    if (PSI) kahan_add(sp, cp, ap);
+                    ax = ay = az = ap = T(0);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty_bar[slot]);
+            rs.consumed++;
+            if (h.count == 0) break;
+        }
+        // every tile produced for this chunk has been consumed, so the
+        // counters agree in every warp unless a wait gave up
+        rs.failed = __syncthreads_or(rs.failed) != 0;
+        if (rs.failed) return;
+        if (tid < cn) {
+            double4 o;
+            if (kKahan)
+                o = make_double4(double(sx) - double(cx), double(sy) - double(cy), double(sz) - double(cz),
+                                 double(sp) - double(cp));
+            else
+                o = make_double4(double(ax), double(ay), double(az), double(ap));
+            partials[int64_t(it.part) * pstride + t0 + c0 + tid] = o;
+        }
+    }
+}
 
-    const WorkItem it = items[blockIdx.x];
-    const int tid = threadIdx.x, lane = tid & 31;
-
-    // Warps whose targets all lie beyond nt have nothing to compute (the
-    // tail chunk of a leaf larger than one block): they leave at once, and
-    // the slot-release barrier counts only the active warps.
-    const int need = (it.nt + 32 * R - 1) / (32 * R);
-    const int active_warps = need < THREADS / 32 ? need : THREADS / 32;
-    if (tid == 0) {
-#pragma unroll
+__device__ __forceinline__ void init_ring(uint64_t* full_bar, uint64_t* empty_bar, int warps) {
+    if (threadIdx.x == 0) {
         for (int d = 0; d < kDepth; d++) {
             mbar_init(&full_bar[d], 1);
-            mbar_init(&empty_bar[d], active_warps);
+            mbar_init(&empty_bar[d], warps);
         }
         mbar_init_fence();
     }
     __syncthreads();
-    if ((tid >> 5) >= active_warps) return;
+}
 
-    T tx[R], ty[R], tz[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        const int k = tid * R + r;
-        const S4 v = src[it.t0 + ((k < it.nt) ? k : 0)];
-        tx[r] = v.x; ty[r] = v.y; tz[r] = v.z;
-    }
-    T ax[R], ay[R], az[R], ap[R];
-    T sx[R], sy[R], sz[R], sp[R], cx[R], cy[R], cz[R], cp[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        ax[r] = ay[r] = az[r] = ap[r] = T(0);
-        sx[r] = sy[r] = sz[r] = sp[r] = T(0);
-        cx[r] = cy[r] = cz[r] = cp[r] = T(0);
-    }
+// One block per work item.
+template <typename T, int THREADS, bool PSI, int TILE>
+__global__ void __launch_bounds__(THREADS) k_pairs(const typename Vec4<T>::type* __restrict__ src,
+                                                   const Segment* __restrict__ segs,
+                                                   const int32_t* __restrict__ leaf_start,
+                                                   const WorkItem* __restrict__ items, double4* __restrict__ partials,
+                                                   int64_t pstride, int* __restrict__ err) {
+    using S4 = typename Vec4<T>::type;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth];
+    __shared__ SlotHdr hdr[kDepth];
+    init_ring(full_bar, empty_bar, THREADS / 32);
+    RingState rs{0, 0, false};
+    const WorkItem it = items[blockIdx.x];
+    run_item<T, THREADS, TILE, PSI>(it, src, segs, leaf_start, partials, pstride, reinterpret_cast<S4*>(smem_raw),
+                                    hdr, full_bar, empty_bar, rs);
+    if (rs.failed && threadIdx.x == 0) set_error(err, kErrTimeout);
+}
 
-    // Producer: warp 0 as a whole (it never diverges from its own consumer
-    // work); lane 0 issues the copies of one tile.
-    const bool producer = (tid >> 5) == 0;
-    int pk = it.k0;  // next tile to issue
-    bool failed = false;
-    auto produce = [&]() {
-        if (pk >= it.k1) return;
-        const int k = pk - it.k0;
-        const int slot = k % kDepth;
-        bool ok = true;
-        if (k >= kDepth) ok = mbar_wait_bounded(&empty_bar[slot], ((k / kDepth) - 1) & 1);
-        if (!__all_sync(0xffffffffu, ok)) {
-            failed = true;
-            return;
-        }
-        if (lane == 0) {
-            const Tile tl = tiles[pk];
-            mbar_arrive_expect_tx(&full_bar[slot], uint32_t(tl.count) * uint32_t(sizeof(S4)));
-            S4* dst = ring + slot * TILE;
-            for (int c = tl.c0; c < tl.c1; c++) {
-                const Copy cp = copies[c];
-                bulk_g2s(dst, src + cp.start, uint32_t(cp.count) * uint32_t(sizeof(S4)), &full_bar[slot]);
-                dst += cp.count;
-            }
-        }
-        __syncwarp();
-        pk++;
-    };
-    if (producer)
-        for (int d = 0; d < kDepth - 1 && !failed; d++) produce();
-
-    int kfail = it.k1;
-    for (int kt = it.k0; kt < it.k1; kt++) {
-        if (producer && !failed) produce();
-        const int k = kt - it.k0;
-        const int slot = k % kDepth;
-        const Tile tl = tiles[kt];
-        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full_bar[slot], (k / kDepth) & 1))) {
-            failed = true;
-            kfail = kt;
-            break;
-        }
-        const S4* tile = ring + slot * TILE;
-        if (tl.guard)
-            tile_pairs<T, R, PSI, true>(tile, tl.count, tx, ty, tz, ax, ay, az, ap);
-        else
-            tile_pairs<T, R, PSI, false>(tile, tl.count, tx, ty, tz, ax, ay, az, ap);
-        if (kKahan) {
-#pragma unroll
-            for (int r = 0; r < R; r++) {
-                kahan_add(sx[r], cx[r], ax[r]);
-                kahan_add(sy[r], cy[r], ay[r]);
-                kahan_add(sz[r], cz[r], az[r]);
-                if (PSI) kahan_add(sp[r], cp[r], ap[r]);
-                ax[r] = ay[r] = az[r] = ap[r] = T(0);
-            }
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty_bar[slot]);
+// Persistent blocks pulling work items from one global queue (reset to 0
+// before every launch); the ring counters run on from item to item.
+template <typename T, int THREADS, int TILE>
+__global__ void __launch_bounds__(THREADS) k_pairs_persistent(const typename Vec4<T>::type* __restrict__ src,
+                                                              const Segment* __restrict__ segs,
+                                                              const int32_t* __restrict__ leaf_start,
+                                                              const WorkItem* __restrict__ items, int nitems,
+                                                              int* __restrict__ queue, double4* __restrict__ partials,
+                                                              int64_t pstride, int* __restrict__ err) {
+    using S4 = typename Vec4<T>::type;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth];
+    __shared__ SlotHdr hdr[kDepth];
+    __shared__ int next_item;
+    init_ring(full_bar, empty_bar, THREADS / 32);
+    RingState rs{0, 0, false};
+    for (;;) {
+        if (threadIdx.x == 0) next_item = atomicAdd(queue, 1);
+        __syncthreads();
+        const int item = next_item;
+        __syncthreads();
+        if (item >= nitems) break;
+        const WorkItem it = items[item];
+        run_item<T, THREADS, TILE, false>(it, src, segs, leaf_start, partials, pstride,
+                                          reinterpret_cast<S4*>(smem_raw), hdr, full_bar, empty_bar, rs);
+        if (rs.failed) break;
     }
-    if (failed) {
-        set_error(err, kErrTimeout);
-        // wait (bounded) for copies issued but not consumed before leaving
-        if (producer && lane == 0)
-            for (int kk = kfail; kk < pk; kk++)
-                mbar_wait_bounded(&full_bar[(kk - it.k0) % kDepth], ((kk - it.k0) / kDepth) & 1);
-        return;
-    }
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        const int kk = tid * R + r;
-        if (kk >= it.nt) continue;
-        double4 o;
-        if (kKahan) {
-            o = make_double4(double(sx[r]) - double(cx[r]), double(sy[r]) - double(cy[r]),
-                             double(sz[r]) - double(cz[r]), double(sp[r]) - double(cp[r]));
-        } else {
-            o = make_double4(double(ax[r]), double(ay[r]), double(az[r]), double(ap[r]));
-        }
-        partials[int64_t(it.part) * pstride + it.t0 + kk] = o;
-    }
+    if (rs.failed && threadIdx.x == 0) set_error(err, kErrTimeout);
 }
 
 // ---------------------------------------------------------------- dispatch
 
-template <typename T, int THREADS, int R, bool PSI>
-static cudaError_t run_pairs(cudaStream_t st, int nitems, const void* src, const Copy* copies, const Tile* tiles,
-                             const WorkItem* items, double4* partials, int64_t pstride, int* err) {
+template <typename T, int THREADS, bool PSI>
+static cudaError_t run_pairs(cudaStream_t st, int nitems, const void* src, const Segment* segs,
+                             const int32_t* leaf_start, const WorkItem* items, double4* partials, int64_t pstride,
+                             int* err) {
     constexpr int TILE = tile_capacity(sizeof(T) == 8);
     constexpr size_t smem = size_t(kDepth) * TILE * sizeof(typename Vec4<T>::type);
     static_assert(smem <= 48 * 1024, "ring must fit the default dynamic shared memory limit");
     if (nitems == 0) return cudaSuccess;
-    k_pairs<T, THREADS, R, PSI, TILE><<<nitems, THREADS, smem, st>>>(
-        static_cast<const typename Vec4<T>::type*>(src), copies, tiles, items, partials, pstride, err);
+    k_pairs<T, THREADS, PSI, TILE><<<nitems, THREADS, smem, st>>>(static_cast<const typename Vec4<T>::type*>(src),
+                                                                   segs, leaf_start, items, partials,
+                                                                   pstride, err);
     return cudaGetLastError();
 }
 
 const std::vector<PairShape>& pair_shapes(bool fp64) {
-    static const std::vector<PairShape> f32 = {{128, 1, 256}, {160, 1, 256}, {192, 1, 256}, {256, 1, 256},
-                                               {64, 2, 256},  {96, 2, 256},  {128, 2, 256}};
+    static const std::vector<PairShape> f32 = {{128, 1, 256}, {160, 1, 256}, {192, 1, 256}, {256, 1, 256}};
     static const std::vector<PairShape> f64 = {{128, 1, 128}, {160, 1, 128}, {192, 1, 128}, {256, 1, 128}};
     return fp64 ? f64 : f32;
 }
 
 PairShape pairs_shape(bool fp64, int threads, int per_thread) {
+    (void)per_thread;
     for (const PairShape& s : pair_shapes(fp64))
-        if (s.threads == threads && s.per_thread == (per_thread > 0 ? per_thread : 1)) return s;
+        if (s.threads == threads) return s;
     return pair_shapes(fp64).front();
 }
 
 template <typename T, bool PSI>
-static cudaError_t dispatch(cudaStream_t st, PairShape sh, int nitems, const void* src, const Copy* copies,
-                            const Tile* tiles, const WorkItem* items, double4* partials, int64_t pstride, int* err) {
-#define FSS_SHAPE(TH, R)                                                                                   \
-    if (sh.threads == TH && sh.per_thread == R)                                                            \
-        return run_pairs<T, TH, R, PSI>(st, nitems, src, copies, tiles, items, partials, pstride, err);
-    FSS_SHAPE(128, 1)
-    FSS_SHAPE(160, 1)
-    FSS_SHAPE(192, 1)
-    FSS_SHAPE(256, 1)
-    if (sizeof(T) == 4) {
-        FSS_SHAPE(64, 2)
-        FSS_SHAPE(96, 2)
-        FSS_SHAPE(128, 2)
-    }
+static cudaError_t dispatch(cudaStream_t st, PairShape sh, int nitems, const void* src, const Segment* segs,
+                            const int32_t* leaf_start, const WorkItem* items, double4* partials,
+                            int64_t pstride, int* err) {
+#define FSS_SHAPE(TH)                                                                                            \
+    if (sh.threads == TH)                                                                                        \
+        return run_pairs<T, TH, PSI>(st, nitems, src, segs, leaf_start, items, partials, pstride, err);
+    FSS_SHAPE(128)
+    FSS_SHAPE(160)
+    FSS_SHAPE(192)
+    FSS_SHAPE(256)
 #undef FSS_SHAPE
     return cudaErrorInvalidConfiguration;
 }
 
 cudaError_t launch_pairs(cudaStream_t st, bool fp64, bool psi, PairShape shape, int nitems, const void* src,
-                         const Copy* copies, const Tile* tiles, const WorkItem* items, double4* partials,
-                         int64_t pstride, int* err) {
+                         const Segment* segs, const int32_t* leaf_start, const WorkItem* items,
+                         double4* partials, int64_t pstride, int* err) {
     if (fp64)
-        return psi ? dispatch<double, true>(st, shape, nitems, src, copies, tiles, items, partials, pstride, err)
-                   : dispatch<double, false>(st, shape, nitems, src, copies, tiles, items, partials, pstride, err);
-    return psi ? dispatch<float, true>(st, shape, nitems, src, copies, tiles, items, partials, pstride, err)
-               : dispatch<float, false>(st, shape, nitems, src, copies, tiles, items, partials, pstride, err);
+        return psi ? dispatch<double, true>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err)
+                   : dispatch<double, false>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err);
+    return psi ? dispatch<float, true>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err)
+               : dispatch<float, false>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err);
+}
+
+cudaError_t launch_pairs_persistent(cudaStream_t st, int nitems, const void* src, const Segment* segs,
+                                    const int32_t* leaf_start, const WorkItem* items, int* queue,
+                                    double4* partials, int64_t pstride, int* err, int blocks) {
+    constexpr int TILE = tile_capacity(false);
+    constexpr size_t smem = size_t(kDepth) * TILE * sizeof(float4);
+    if (nitems == 0) return cudaSuccess;
+    k_pairs_persistent<float, kPersistentThreads, TILE><<<blocks, kPersistentThreads, smem, st>>>(
+        static_cast<const float4*>(src), segs, leaf_start, items, nitems, queue, partials, pstride, err);
+    return cudaGetLastError();
+}
+
+int persistent_blocks_per_sm() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pairs_persistent<float, kPersistentThreads, tile_capacity(false)>,
+                                                  kPersistentThreads,
+                                                  size_t(kDepth) * tile_capacity(false) * sizeof(float4));
+    return nb > 0 ? nb : 1;
 }
 
 }  // namespace fss

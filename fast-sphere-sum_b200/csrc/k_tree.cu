@@ -253,6 +253,88 @@ __global__ void k_gather(int64_t n, const double* __restrict__ in5, const double
     src[s] = o;
 }
 
+// ---------------------------------------------------------------- re-sort
+
+// Particles move between RK4 steps; at the start of a step each is put in
+// the leaf it is in now.  Its previous leaf key[s] is kept when the
+// particle is still inside it (all cone coordinates >= 0), otherwise it
+// descends from the 20 root faces in complete mode (the first child that
+// contains it, else the most-inside one).  With `leaves` the keys are global
+// leaf indices of an ensemble (each member's leaf level and the leaf's
+// index on it from the table; a member's leaves are consecutive); without,
+// leaf indices of one tree with leaves on `leaf_level`.
+__global__ void k_reassign(int64_t n, const double4* __restrict__ pos, const EnsLeaf* __restrict__ leaves,
+                           int leaf_level, const double* __restrict__ verts, const int32_t* __restrict__ tri_verts,
+                           const int64_t* __restrict__ lev_off, uint32_t* __restrict__ key) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 q = pos[i];
+    const double p[3] = {q.x, q.y, q.z};
+    const uint32_t g = key[i];
+    int LL = leaf_level, local = int(g);
+    if (leaves) {
+        const EnsLeaf lf = leaves[g];
+        LL = lf.leaf_level;
+        local = lf.local;
+    }
+    double c[3];
+    {
+        const int32_t* tv = tri_verts + 3 * (lev_off[LL] + local);
+        cone_coords_exact(verts + 3 * int64_t(tv[0]), verts + 3 * int64_t(tv[1]), verts + 3 * int64_t(tv[2]), p, c);
+        if (c[0] >= 0 && c[1] >= 0 && c[2] >= 0) return;
+    }
+    int prev = 0;
+    for (int l = 0; l <= LL; l++) {
+        const int lb = (l > 0) ? 4 * prev : 0, ub = (l > 0) ? lb + 4 : 20;
+        int found = -1, best = lb;
+        double best_min = -1e300;
+        for (int j = lb; j < ub; j++) {
+            const int32_t* tv = tri_verts + 3 * (lev_off[l] + j);
+            cone_coords_exact(verts + 3 * int64_t(tv[0]), verts + 3 * int64_t(tv[1]), verts + 3 * int64_t(tv[2]), p, c);
+            if (c[0] >= 0 && c[1] >= 0 && c[2] >= 0) { found = j; break; }
+            const double m = fmin(c[0], fmin(c[1], c[2]));
+            if (m > best_min) { best_min = m; best = j; }
+        }
+        prev = (found >= 0) ? found : best;
+    }
+    key[i] = uint32_t(int64_t(g) - local + prev);
+}
+
+// New order q (sorted position -> old position): the step state, areas,
+// tracers and caller indices gathered into the free stage buffers (xs, and
+// acc as {area, tracer, caller index, 0}).
+__global__ void k_resort_gather(int64_t n, const int32_t* __restrict__ q, const double4* __restrict__ s0,
+                                const double* __restrict__ area, const double* __restrict__ tracer,
+                                const int32_t* __restrict__ perm, double4* __restrict__ xs, double4* __restrict__ acc) {
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int64_t j = q[s];
+    xs[s] = s0[j];
+    acc[s] = make_double4(area[j], tracer[j], double(perm[j]), 0.0);
+}
+
+// Back into place, with the stage-1 state (xs = s0) and interaction
+// sources (x, y, z, zeta A) of the new order.
+template <typename T>
+__global__ void k_resort_commit(int64_t n, const double4* __restrict__ xs, const double4* __restrict__ acc,
+                                double4* __restrict__ s0, double* __restrict__ area, double* __restrict__ tracer,
+                                int32_t* __restrict__ perm, typename Vec4<T>::type* __restrict__ src) {
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double4 v = xs[s];
+    const double4 t = acc[s];
+    s0[s] = v;
+    area[s] = t.x;
+    tracer[s] = t.y;
+    perm[s] = int32_t(t.z);
+    typename Vec4<T>::type o;
+    o.x = T(v.x);
+    o.y = T(v.y);
+    o.z = T(v.z);
+    o.w = T(v.w * t.x);
+    src[s] = o;
+}
+
 // ---------------------------------------------------------------- launchers
 
 void launch_assign(cudaStream_t st, int64_t n, const double* in5, const double* verts, const int32_t* tri_verts,
@@ -308,6 +390,23 @@ void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, con
     else
         k_gather<float><<<g, 256, 0, st>>>(n, in5, area_in, perm, leaf_of, frame, s0, xs, area_s, tracer_s,
                                            static_cast<float4*>(src));
+}
+
+void launch_reassign(cudaStream_t st, int64_t n, const double4* pos, const EnsLeaf* leaves, int leaf_level,
+                     const double* verts, const int32_t* tri_verts, const int64_t* lev_off, uint32_t* key) {
+    if (n == 0) return;
+    k_reassign<<<unsigned((n + 127) / 128), 128, 0, st>>>(n, pos, leaves, leaf_level, verts, tri_verts, lev_off, key);
+}
+
+void launch_resort(cudaStream_t st, bool fp64, int64_t n, const int32_t* q, double4* s0, double* area,
+                   double* tracer, int32_t* perm, double4* xs, double4* acc, void* src) {
+    if (n == 0) return;
+    const unsigned g = unsigned((n + 255) / 256);
+    k_resort_gather<<<g, 256, 0, st>>>(n, q, s0, area, tracer, perm, xs, acc);
+    if (fp64)
+        k_resort_commit<double><<<g, 256, 0, st>>>(n, xs, acc, s0, area, tracer, perm, static_cast<double4*>(src));
+    else
+        k_resort_commit<float><<<g, 256, 0, st>>>(n, xs, acc, s0, area, tracer, perm, static_cast<float4*>(src));
 }
 
 }  // namespace fss

@@ -50,18 +50,32 @@ int64_t sort_scratch_words(int64_t n);
 void launch_sort(cudaStream_t st, int64_t n, int bits, uint32_t* keys, uint32_t* keys_tmp, int32_t* vals,
                  int32_t* vals_tmp, uint32_t* hist);
 void launch_leaf_bounds(cudaStream_t st, int64_t n, const uint32_t* skey, int32_t nleaf, int32_t* leaf_start);
+// Re-sort at the start of an RK4 step: new leaf keys (the previous leaf
+// when the particle is still inside it), then, after the key sort gave the
+// order q, the state, areas, tracers and caller indices permuted in place
+// (through the free stage buffers xs and acc) and the stage-1 sources
+// rewritten.
+void launch_reassign(cudaStream_t st, int64_t n, const double4* pos, const EnsLeaf* leaves, int leaf_level,
+                     const double* verts, const int32_t* tri_verts, const int64_t* lev_off, uint32_t* key);
+void launch_resort(cudaStream_t st, bool fp64, int64_t n, const int32_t* q, double4* s0, double* area,
+                   double* tracer, int32_t* perm, double4* xs, double4* acc, void* src);
 void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, const double* area_in, const int32_t* perm,
                    const uint32_t* leaf_of, const double4* frame, double4* s0, double4* xs, double* area_s,
                    double* tracer_s, void* src);
 
 // k_pairs.cu
-// Supported (threads, targets per thread) shapes of the pair kernel.
+// Supported block shapes of the pair kernel (threads; one target each).
 const std::vector<PairShape>& pair_shapes(bool fp64);
-// The supported shape for (threads, per_thread), or the default (128, 1).
+// The supported shape with `threads`, or the default (128).
 PairShape pairs_shape(bool fp64, int threads, int per_thread);
 cudaError_t launch_pairs(cudaStream_t st, bool fp64, bool psi, PairShape shape, int nitems, const void* src,
-                         const Copy* copies, const Tile* tiles, const WorkItem* items, double4* partials,
+                         const Segment* segs, const int32_t* leaf_start, const WorkItem* items, double4* partials,
                          int64_t pstride, int* err);
+constexpr int kPersistentThreads = 160;
+cudaError_t launch_pairs_persistent(cudaStream_t st, int nitems, const void* src, const Segment* segs,
+                                    const int32_t* leaf_start, const WorkItem* items, int* queue, double4* partials,
+                                    int64_t pstride, int* err, int blocks);
+int persistent_blocks_per_sm();
 
 // k_epi.cu
 void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, const int32_t* leaf_start,
@@ -76,5 +90,13 @@ void launch_refresh(cudaStream_t st, bool fp64, int64_t n, const double4* s0, co
 void launch_wsum(cudaStream_t st, int64_t n, const double4* xs, const double* area, double* w);
 void launch_scatter_state(cudaStream_t st, int64_t n, const int32_t* perm, const double4* s0, const double* tracer,
                           double* out5);
+
+// k_ensemble.cu
+void launch_up_leaf_batch(cudaStream_t st, int nleaf, const void* src, const EnsLeaf* leaves,
+                          const int32_t* leaf_start, const NodeGeom* node, const int64_t* lev_off, int nmax,
+                          double* part);
+void launch_up_combine_batch(cudaStream_t st, int njobs, const ProxyJob* jobs, const EnsLeaf* leaves,
+                             const double* part, int nmax, const double* vinv, const int32_t* vinv_off,
+                             const double4* proxy_pos, int64_t n, void* src);
 
 }  // namespace fss

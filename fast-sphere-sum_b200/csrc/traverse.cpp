@@ -69,13 +69,13 @@ std::vector<std::vector<ASrc>> lists_from_pairs(const TreeGeometry& g, int leaf_
 
 std::vector<std::vector<ASrc>> lists_per_leaf(const TreeGeometry& g, int leaf_level, const std::vector<int32_t>& counts,
                                               const std::vector<int32_t>& leaf_degree,
-                                              const std::vector<double>& leaf_theta) {
+                                              const std::vector<double>& leaf_theta, bool keep_empty) {
     const int64_t nleaf = int64_t(20) << (2 * leaf_level);
     std::vector<std::vector<ASrc>> lists(nleaf);
     struct S { int32_t l, s; };
     std::vector<S> st;
     for (int64_t lf = 0; lf < nleaf; lf++) {
-        if (counts[g.lev_off[leaf_level] + lf] == 0) continue;
+        if (!keep_empty && counts[g.lev_off[leaf_level] + lf] == 0) continue;
         const int deg = leaf_degree[lf];
         const int K = nproxy(deg);
         const double th = leaf_theta[lf];
@@ -86,7 +86,10 @@ std::vector<std::vector<ASrc>> lists_per_leaf(const TreeGeometry& g, int leaf_le
             const S e = st.back();
             st.pop_back();
             const int ns = counts[g.lev_off[e.l] + e.s];
-            if (ns == 0) continue;
+            if (ns == 0) {
+                if (keep_empty) lists[lf].push_back({0, e.l, e.s, 0});
+                continue;
+            }
             const double* si = &g.tri_info[4 * (g.lev_off[e.l] + e.s)];
             const double dist = great_circ_dist(ti, si, 1.0);
             if (dist > 0 && (ti[3] + si[3]) / dist < th) {
@@ -156,96 +159,75 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
             }
             out.n_proxy += K;
         }
-    // entries and items
+    // segments and items
     const int TB = in.threads * in.per_thread;
     const int P = std::max(1, in.parts);
     struct Cost { double cost; WorkItem it; };
     std::vector<Cost> items;
-    std::vector<SrcEntry> ents;
+    std::vector<Segment> sg;
+    std::vector<double> est;  // sources per segment at the build
     for (int64_t lf = 0; lf < nleaf; lf++) {
-        const int32_t t0 = in.leaf_start[lf], nt = in.leaf_start[lf + 1] - t0;
-        if (nt == 0) continue;
-        ents.clear();
+        const int32_t nt = in.leaf_start[lf + 1] - in.leaf_start[lf];
+        if (lists[lf].empty() || (nt == 0 && !in.all_leaves)) continue;
+        sg.clear();
+        est.clear();
         for (const ASrc& a : lists[lf]) {
             const int64_t gf = g.lev_off[a.level] + a.node;
+            Segment e{};
+            double cnt;
             if (a.proxy) {
-                SrcEntry e{};
-                e.start = int32_t(in.n + slot[std::make_pair(gf, a.deg)]);
-                e.count = nproxy(a.deg);
                 e.kind = 1;
-                ents.push_back(e);
-                out.pc_pairs += double(nt) * e.count;
+                e.a = int32_t(in.n + slot[std::make_pair(gf, a.deg)]);
+                e.b = e.a + nproxy(a.deg);
+                cnt = nproxy(a.deg);
+                out.pc_pairs += double(nt) * cnt;
             } else {
                 const int64_t span = int64_t(1) << (2 * (LL - a.level));
-                // the particles of S are contiguous in leaf order
-                const int32_t s0 = in.leaf_start[a.node * span], s1 = in.leaf_start[(a.node + 1) * span];
-                if (s1 == s0) continue;
-                SrcEntry e{};
-                e.start = s0;
-                e.count = s1 - s0;
                 e.kind = 0;
-                ents.push_back(e);
-                const bool self = (t0 >= s0 && t0 < s1);
-                out.pp_pairs += double(nt) * e.count - (self ? nt : 0);
+                e.a = int32_t(a.node * span);
+                e.b = int32_t((a.node + 1) * span);
+                // the particles of a face are contiguous in leaf order
+                const int32_t s0 = in.leaf_start[e.a], s1 = in.leaf_start[e.b];
+                cnt = s1 - s0;
+                const bool self = (lf >= e.a && lf < e.b);
+                out.pp_pairs += double(nt) * cnt - (self ? nt : 0);
+            }
+            if (!sg.empty() && sg.back().kind == e.kind && sg.back().b == e.a) {
+                sg.back().b = e.b;
+                est.back() += cnt;
+            } else {
+                sg.push_back(e);
+                est.push_back(cnt);
             }
         }
-        const int32_t e_begin = int32_t(out.entries.size());
-        out.entries.insert(out.entries.end(), ents.begin(), ents.end());
-        const int32_t e_end = int32_t(out.entries.size());
-        // split [e_begin, e_end) into P parts of similar source counts
+        const int32_t base = int32_t(out.segs.size());
+        out.segs.insert(out.segs.end(), sg.begin(), sg.end());
+        // split the segments into P parts of similar source counts
         double total = 0;
-        for (int32_t e = e_begin; e < e_end; e++) total += out.entries[e].count;
-        std::vector<int32_t> cut(P + 1, e_end);
-        cut[0] = e_begin;
+        for (double c : est) total += c;
+        std::vector<int32_t> cut(P + 1, int32_t(sg.size()));
+        cut[0] = 0;
         {
             double acc = 0;
             int p = 1;
-            for (int32_t e = e_begin; e < e_end && p < P; e++) {
-                acc += out.entries[e].count;
-                if (acc >= total * p / P) cut[p++] = e + 1;
+            for (size_t k = 0; k < sg.size() && p < P; k++) {
+                acc += est[k];
+                if (acc >= total * p / P) cut[p++] = int32_t(k + 1);
             }
-            for (; p < P; p++) cut[p] = e_end;
         }
-        for (int32_t c0 = 0; c0 < nt; c0 += TB) {
-            const int32_t cn = std::min(TB, nt - c0);
-            for (int p = 0; p < P; p++) {
-                double w = 0;
-                for (int32_t e = cut[p]; e < cut[p + 1]; e++) w += out.entries[e].count;
-                const int32_t k0 = int32_t(out.tiles.size());
-                pack_tiles(out.entries, cut[p], cut[p + 1], in.tile, t0 + c0, t0 + c0 + cn, out.copies, out.tiles);
-                const int32_t k1 = int32_t(out.tiles.size());
-                // a block's run time follows its source count (its warps
-                // run side by side), so the longest source lists go first
-                items.push_back({w, WorkItem{t0 + c0, cn, k0, k1, p, int32_t(lf)}});
-            }
+        const int chunks = std::max(1, (nt + TB - 1) / TB);
+        for (int p = 0; p < P; p++) {
+            double w = 0;
+            for (int32_t k = cut[p]; k < cut[p + 1]; k++) w += est[k];
+            out.n_tiles += int64_t(chunks) * (int64_t(w + in.tile - 1) / in.tile);
+            // a block's run time follows its source count (its warps run
+            // side by side), so the longest source lists go first
+            items.push_back({w * chunks, WorkItem{0, 0, base + cut[p], base + cut[p + 1], p, int32_t(lf)}});
         }
     }
     std::stable_sort(items.begin(), items.end(), [](const Cost& a, const Cost& b) { return a.cost > b.cost; });
     out.items.reserve(items.size());
     for (auto& c : items) out.items.push_back(c.it);
-}
-
-void pack_tiles(const std::vector<SrcEntry>& entries, int32_t e0, int32_t e1, int cap, int64_t t0, int64_t t1,
-                std::vector<Copy>& copies, std::vector<Tile>& tiles) {
-    Tile cur{int32_t(copies.size()), int32_t(copies.size()), 0, 0};
-    for (int32_t e = e0; e < e1; e++) {
-        int32_t off = 0;
-        const SrcEntry& en = entries[e];
-        while (off < en.count) {
-            const int32_t take = std::min(en.count - off, cap - cur.count);
-            const int64_t a = int64_t(en.start) + off, b = a + take;
-            copies.push_back({int32_t(a), take});
-            if (a < t1 && b > t0) cur.guard = 1;
-            cur.count += take;
-            cur.c1 = int32_t(copies.size());
-            off += take;
-            if (cur.count == cap) {
-                tiles.push_back(cur);
-                cur = Tile{int32_t(copies.size()), int32_t(copies.size()), 0, 0};
-            }
-        }
-    }
-    if (cur.count > 0) tiles.push_back(cur);
 }
 
 // ---------------------------------------------------------------- interpolation

@@ -32,21 +32,21 @@ struct ListInput {
     const TreeGeometry* g = nullptr;
     int leaf_level = 0;                 // tree_levels - 1
     int64_t n = 0;                      // particles
-    const int32_t* leaf_start = nullptr;  // nleaf + 1 (sorted order)
+    const int32_t* leaf_start = nullptr;  // nleaf + 1 (sorted order) at the build; estimates only
     int threads = 128, per_thread = 1;  // targets per block = threads * per_thread
     int tile = 256;                     // sources per shared-memory tile
     int parts = 1;                      // source-list split
+    bool all_leaves = false;            // items also for leaves empty at the build
 };
 
 struct ListOutput {
-    std::vector<SrcEntry> entries;  // per target leaf, in list order
-    std::vector<Copy> copies;
-    std::vector<Tile> tiles;
+    std::vector<Segment> segs;      // per work item, in list order
     std::vector<WorkItem> items;
     std::vector<ProxyJob> jobs;
     std::vector<double> proxy_pos;  // 4 doubles per proxy slot: y (on sphere) and pad
     std::vector<int32_t> proxy_node;  // proxy slot -> face (global index)
     int64_t n_proxy = 0;            // proxy slots after the n particles
+    int64_t n_tiles = 0;            // shared-memory tiles per RHS at the build's leaf counts
     double pp_pairs = 0, pc_pairs = 0;
     int max_degree = 0;
 };
@@ -60,19 +60,19 @@ std::vector<std::vector<ASrc>> lists_from_pairs(const TreeGeometry& g, int leaf_
 // Per-target-leaf traversal with its own (degree, theta): a source face is
 // taken as proxies when (r_t + r_s)/d < theta and it holds more particles
 // than its proxy count, as particles when well separated but small or when
-// it is a leaf, otherwise its four children are visited.
+// it is a leaf, otherwise its four children are visited.  Faces empty at
+// the build are skipped, unless keep_empty (particles re-sorted every step
+// may move into them): then every leaf gets a list and an empty face is
+// taken as particles, whatever it holds when the kernel runs.
 std::vector<std::vector<ASrc>> lists_per_leaf(const TreeGeometry& g, int leaf_level,
                                               const std::vector<int32_t>& counts,
                                               const std::vector<int32_t>& leaf_degree,
-                                              const std::vector<double>& leaf_theta);
+                                              const std::vector<double>& leaf_theta, bool keep_empty);
 
-// Pack source ranges [e0, e1) of `entries` into tiles of at most `cap`
-// sources (ranges split across tile boundaries as needed); guard marks tiles
-// holding any of the targets [t0, t1).
-void pack_tiles(const std::vector<SrcEntry>& entries, int32_t e0, int32_t e1, int cap, int64_t t0, int64_t t1,
-                std::vector<Copy>& copies, std::vector<Tile>& tiles);
-
-// Materialise entries, work items, proxy slots and upward-pass jobs.
+// Materialise segments, work items (one per target leaf and source part),
+// proxy slots and upward-pass jobs.  A face's particles become a kind-0
+// segment over its leaves (adjacent ones merged), a face's proxies a kind-1
+// segment over its proxy slots.
 void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& lists, ListOutput& out);
 
 // Proxy node set: barycentric interpolation points of degree n on a

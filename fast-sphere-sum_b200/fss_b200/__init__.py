@@ -23,6 +23,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 METHOD_DIRECT, METHOD_TREECODE = 0, 1
 ASSIGN_COMPLETE, ASSIGN_REFERENCE = 0, 1
 LIST_DUAL, LIST_LEAF = 0, 1
+REBUILD_AUTO, REBUILD_STATIC, REBUILD_RESORT = 0, 1, 2
 STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NOMEM", 4: "TIMEOUT", 5: "TREE", 6: "STATE",
           7: "UNSUPPORTED", 8: "CAPACITY"}
 
@@ -39,7 +40,7 @@ class Config(C.Structure):
                 ("theta", C.c_double), ("many_count", C.c_int32), ("assign_mode", C.c_int32),
                 ("list_mode", C.c_int32), ("use_graph", C.c_int32), ("src_parts", C.c_int32),
                 ("block_threads", C.c_int32), ("targets_per_thread", C.c_int32), ("autotune", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("rebuild", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class TreeInfo(C.Structure):
@@ -72,7 +73,9 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_tree_geometry", "fss_rhs_direct_noalloc", "fss_mlp_create", "fss_mlp_destroy",
            "fss_mlp_param_count", "fss_mlp_init", "fss_mlp_set_params", "fss_mlp_get_params", "fss_mlp_set_data",
            "fss_mlp_gradient", "fss_mlp_train", "fss_mlp_predict", "fss_selector_features", "fss_select_classes",
-           "fss_selector_apply", "fss_version"]
+           "fss_selector_apply", "fss_ensemble_create", "fss_ensemble_destroy", "fss_ensemble_set_stream",
+           "fss_ensemble_add", "fss_ensemble_build", "fss_ensemble_rk4_step", "fss_ensemble_get_state",
+           "fss_ensemble_info", "fss_version"]
 
 NOALLOC_MAX_PARTICLES = 262144  # FSS_NOALLOC_MAX_PARTICLES in include/fss.h
 
@@ -116,6 +119,15 @@ def lib():
     L.fss_interp_nodes.argtypes = [C.c_int32, _D, _D]
     L.fss_tree_geometry.argtypes = [C.c_int32, _D]
     L.fss_rhs_direct_noalloc.argtypes = [_i64, _vp, _vp, C.c_double, _vp, _vp]
+    L.fss_ensemble_create.argtypes = [P(Config), P(_vp)]
+    L.fss_ensemble_destroy.argtypes = [_vp]
+    L.fss_ensemble_destroy.restype = None
+    L.fss_ensemble_set_stream.argtypes = [_vp, _vp]
+    L.fss_ensemble_add.argtypes = [_vp, _i64, _D, _D, P(C.c_int32)]
+    L.fss_ensemble_build.argtypes = [_vp]
+    L.fss_ensemble_rk4_step.argtypes = [_vp, C.c_double, C.c_double, C.c_int32]
+    L.fss_ensemble_get_state.argtypes = [_vp, C.c_int32, _D]
+    L.fss_ensemble_info.argtypes = [_vp, P(C.c_int32), P(_i64), P(C.c_double), P(_i64)]
     L.fss_version.restype = C.c_char_p
     _lib = L
     return L
@@ -337,6 +349,70 @@ def rhs_direct_noalloc(n, state5_dev_ptr, area_dev_ptr, out5_dev_ptr, stream_han
     """fss_rhs_direct_noalloc on caller-owned device buffers (raw pointers);
     asynchronous on the given stream.  Raises FssError on a bad size."""
     _check(lib().fss_rhs_direct_noalloc(n, state5_dev_ptr, area_dev_ptr, omega, out5_dev_ptr, stream_handle))
+
+
+class Ensemble:
+    """Independent problems of uneven size advanced together (mixed-precision
+    treecode): one persistent pair-kernel launch per RK stage for all members,
+    one CUDA graph per RK4 step."""
+
+    def __init__(self, **kw):
+        L = lib()
+        cfg = Config()
+        L.fss_config_init(C.byref(cfg))
+        for k, v in kw.items():
+            if not hasattr(cfg, k):
+                raise TypeError(f"unknown config field {k}")
+            setattr(cfg, k, v)
+        h = _vp()
+        _check(L.fss_ensemble_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.sizes = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fss_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_handle):
+        _check(lib().fss_ensemble_set_stream(self.h, stream_handle))
+
+    def add(self, state5, area):
+        s = np.ascontiguousarray(state5, dtype=np.float64)
+        a = np.ascontiguousarray(area, dtype=np.float64)
+        m = C.c_int32()
+        _check(lib().fss_ensemble_add(self.h, s.shape[0], s.reshape(-1), a, C.byref(m)))
+        self.sizes.append(s.shape[0])
+        return m.value
+
+    def build(self):
+        _check(lib().fss_ensemble_build(self.h))
+
+    def rk4_step(self, dt, omega=OMEGA, nsteps=1):
+        _check(lib().fss_ensemble_rk4_step(self.h, dt, omega, nsteps))
+
+    def get_state(self, member):
+        out = np.zeros((self.sizes[member], 5))
+        _check(lib().fss_ensemble_get_state(self.h, member, out.reshape(-1)))
+        return out
+
+    def info(self):
+        m, n, w = C.c_int32(), _i64(), _i64()
+        inter = C.c_double()
+        _check(lib().fss_ensemble_info(self.h, C.byref(m), C.byref(n), C.byref(inter), C.byref(w)))
+        return {"members": m.value, "particles": n.value, "interactions_per_rhs": inter.value, "work_items": w.value}
 
 
 def version():

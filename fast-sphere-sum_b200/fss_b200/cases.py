@@ -3,6 +3,12 @@
     python -m fss_b200.cases rhs  --level 8 --precision mixed [--repeat 2]
     python -m fss_b200.cases rk4  --level 8 --precision mixed --steps 2
     python -m fss_b200.cases direct --level 6 --precision mixed
+    python -m fss_b200.cases ensemble --members 64 --steps 20
+
+The ensemble case: members on icosahedral levels drawn uniformly from 5-8,
+each an RH R=4 wave with a seeded +-5% amplitude perturbation and 4-16
+Gaussian vortices; mixed-precision BLTC n=8, theta=0.7; one CUDA graph per
+RK4 step for all members.
 
 Inputs: icosahedral grid of the given level, RH4 wave + seeded vortices.
 Prints one line with the wall time; exits non-zero on any library error.
@@ -12,12 +18,14 @@ import time
 
 import numpy as np
 
-from . import (METHOD_DIRECT, METHOD_TREECODE, PREC_FP64, PREC_MIXED, Context, make_state)
+from . import (METHOD_DIRECT, METHOD_TREECODE, PREC_FP64, PREC_MIXED, RH_AMP, Context, Ensemble, make_state)
 
 
 def main(argv=None):
     p = argparse.ArgumentParser()
-    p.add_argument("case", choices=["rhs", "rk4", "direct"])
+    p.add_argument("case", choices=["rhs", "rk4", "direct", "ensemble"])
+    p.add_argument("--members", type=int, default=64)
+    p.add_argument("--seed", type=int, default=100)
     p.add_argument("--level", type=int, default=8)
     p.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     p.add_argument("--degree", type=int, default=8)
@@ -28,6 +36,8 @@ def main(argv=None):
     p.add_argument("--no-graph", action="store_true")
     a = p.parse_args(argv)
     prec = PREC_MIXED if a.precision == "mixed" else PREC_FP64
+    if a.case == "ensemble":
+        return ensemble_case(a)
     s, area = make_state(a.level, "rh_vortices", n_vortex=a.vortices, seed=2)
     method = METHOD_DIRECT if a.case == "direct" else METHOD_TREECODE
     t0 = time.perf_counter()
@@ -44,6 +54,36 @@ def main(argv=None):
     assert np.all(np.isfinite(out))
     print(f"case={a.case} level={a.level} n={s.shape[0]} precision={a.precision} "
           f"items={info['n_items']} wall={time.perf_counter() - t0:.3f}s")
+
+
+def ensemble_case(a):
+    import json
+    rng = np.random.default_rng(a.seed)
+    t0 = time.perf_counter()
+    with Ensemble(degree=a.degree, theta=a.theta) as ens:
+        levels = []
+        for m in range(a.members):
+            level = int(rng.integers(5, 9))
+            nv = int(rng.integers(4, 17))
+            amp = float(rng.uniform(0.95, 1.05))
+            s, area = make_state(level, "rh_vortices", n_vortex=nv, seed=a.seed + m, amp=RH_AMP * amp)
+            ens.add(s, area)
+            levels.append(level)
+        ens.build()
+        t_build = time.perf_counter() - t0
+        info = ens.info()
+        ens.rk4_step(0.01, nsteps=1)
+        _ = ens.get_state(0)                       # sync
+        t1 = time.perf_counter()
+        ens.rk4_step(0.01, nsteps=a.steps)
+        out = ens.get_state(0)
+        dt = time.perf_counter() - t1
+    assert np.all(np.isfinite(out))
+    print(json.dumps(dict(case="ensemble", members=a.members, levels=np.bincount(levels, minlength=9)[5:].tolist(),
+                          particles=info["particles"], work_items=info["work_items"],
+                          interactions_per_rhs=info["interactions_per_rhs"], steps=a.steps,
+                          wall_s=dt, steps_per_s=a.steps / dt,
+                          pairs_per_s=4 * a.steps * info["interactions_per_rhs"] / dt, build_s=t_build)))
 
 
 if __name__ == "__main__":

@@ -67,6 +67,19 @@ typedef enum fss_list_mode {
     FSS_LIST_LEAF = 1    /* per-target-leaf traversal with per-leaf (n, theta) */
 } fss_list_mode;
 
+/* What happens to the tree as particles move (treecode). */
+typedef enum fss_rebuild_policy {
+    FSS_REBUILD_AUTO = 0,    /* RESORT, or STATIC with FSS_ASSIGN_REFERENCE */
+    FSS_REBUILD_STATIC = 1,  /* the reference's: membership and lists of the last
+                                build are kept (new_dynamics.cpp:87-88 assigns
+                                once before the time loop) */
+    FSS_REBUILD_RESORT = 2   /* at the start of every RK4 step each particle is
+                                put in the leaf it is in now and the particles
+                                are re-sorted on the GPU; leaf geometry and
+                                interaction lists (which refer to leaves, not
+                                particles) stay those of the last build */
+} fss_rebuild_policy;
+
 typedef struct fss_config {
     int32_t device;        /* CUDA device ordinal */
     int32_t precision;     /* fss_precision */
@@ -88,7 +101,8 @@ typedef struct fss_config {
     int32_t targets_per_thread; /* with block_threads: 1 or 2 */
     int32_t autotune;      /* at fss_set_particles, time every supported block
                               shape on the actual lists and keep the fastest */
-    int32_t reserved[6];
+    int32_t rebuild;       /* fss_rebuild_policy */
+    int32_t reserved[5];
 } fss_config;
 
 typedef struct fss_ctx fss_ctx;
@@ -106,9 +120,10 @@ const char* fss_last_error(const fss_ctx* ctx);
 int fss_set_stream(fss_ctx* ctx, void* cuda_stream);
 
 /* Upload a particle set (host, 5 doubles per particle, in the caller's order)
- * and, for the treecode, build the tree once, as the reference does before
- * its time loop (new_dynamics.cpp:187-199).  The tree stays fixed until the
- * next fss_set_particles or fss_rebuild_tree. */
+ * and, for the treecode, build the tree, as the reference does before its
+ * time loop (new_dynamics.cpp:87-88).  The lists stay fixed until the next
+ * fss_set_particles or fss_rebuild_tree; with FSS_REBUILD_RESORT the
+ * particles are re-sorted into their current leaves at every RK4 step. */
 int fss_set_particles(fss_ctx* ctx, int64_t n, const double* state5, const double* area);
 /* Re-assign particles and rebuild the interaction lists from the current
  * device state (new_dynamics.cpp:335, after AMR, calls points_assign again). */
@@ -143,9 +158,10 @@ typedef struct fss_tree_info {
     int32_t leaf_count;      /* 20 * 4^(tree_levels-1) */
     int32_t degree, n_proxy; /* n and K */
     int64_t n_pairs;         /* reference-format interactions (dual traversal) */
-    int64_t n_list_entries;  /* source ranges over all target leaves */
+    int64_t n_list_entries;  /* source segments (leaf runs, proxy runs) over all items */
     int64_t n_items;         /* interaction work items (blocks) per RHS */
-    int64_t n_tiles;         /* shared-memory source tiles over all items */
+    int64_t n_tiles;         /* shared-memory source tiles over all items at the
+                                build's leaf counts */
     int64_t unassigned;      /* particles without a leaf (reference mode) */
     double pp_interactions;  /* particle-particle pair count per RHS */
     double pc_interactions;  /* particle-proxy pair count per RHS */
@@ -215,6 +231,28 @@ int fss_interp_nodes(int32_t degree, double* nodes, double* vinv);
 /* icos_utils.h:15 icos_init tree geometry for levels 0..tree_levels-1:
  * circumcentre and circumradius per face (4 doubles), levels concatenated. */
 int fss_tree_geometry(int32_t tree_levels, double* tri_info);
+
+/* ------------------------------------------------------------ ensemble
+ * Many independent problems of uneven size (mixed-precision treecode) that
+ * advance together: per RK stage one batched upward pass, one persistent
+ * pair-kernel launch over a global (member, target leaf, source run) work
+ * queue and one epilogue; each RK4 step is one CUDA graph.  No counterpart in
+ * the reference (which runs one problem per process). */
+typedef struct fss_ensemble fss_ensemble;
+/* cfg: precision FSS_PREC_MIXED, method FSS_METHOD_TREECODE; degree, theta,
+ * tree_levels (0 = automatic per member) apply to every member. */
+int fss_ensemble_create(const fss_config* cfg, fss_ensemble** out);
+void fss_ensemble_destroy(fss_ensemble* e);
+int fss_ensemble_set_stream(fss_ensemble* e, void* cuda_stream);
+/* Add one member (host state, 5 doubles per particle, and areas); its tree
+ * and lists are built now.  *member receives its index. */
+int fss_ensemble_add(fss_ensemble* e, int64_t n, const double* state5, const double* area, int32_t* member);
+/* Concatenate all members' state and work lists on the device. */
+int fss_ensemble_build(fss_ensemble* e);
+int fss_ensemble_rk4_step(fss_ensemble* e, double dt, double omega, int32_t nsteps);
+int fss_ensemble_get_state(fss_ensemble* e, int32_t member, double* state5);
+int fss_ensemble_info(fss_ensemble* e, int32_t* members, int64_t* particles, double* interactions_per_rhs,
+                      int64_t* work_items);
 
 /* ------------------------------------------------------------ selector
  * Learned per-leaf interpolation degree and MAC (no counterpart in the

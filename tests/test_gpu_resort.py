@@ -1,0 +1,66 @@
+"""Re-sorting particles into the leaves they are in now at every RK4 step
+(FSS_REBUILD_RESORT, the default for complete assignment) against the
+reference's fixed tree (FSS_REBUILD_STATIC; new_dynamics.cpp:87-88 assigns
+once before the time loop) and the FP64 direct sum."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _steps(fss, s, a, nsteps, **kw):
+    with fss.Context(**kw) as ctx:
+        ctx.set_particles(s, a)
+        ctx.rk4_step(0.01, nsteps=nsteps)
+        loc = ctx.get_tree()[0] if kw.get("method", fss.METHOD_TREECODE) == fss.METHOD_TREECODE else None
+        return ctx.get_state(), loc
+
+
+def test_resort_membership_follows_particles(fss, oracle):
+    """After k steps the leaves are those of the state at the start of step k."""
+    s, a = fss.make_state(5, "rh_vortices", n_vortex=8, seed=4)
+    kw = dict(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, tree_levels=4, rebuild=fss.REBUILD_RESORT)
+    _, loc0 = _steps(fss, s, a, 0, **kw)
+    s5, _ = _steps(fss, s, a, 5, **kw)
+    _, loc6 = _steps(fss, s, a, 6, **kw)
+    ref = oracle.points_assign(4, s5)
+    ok = ref[3] >= 0
+    # the oracle takes the first containing face, the re-sort keeps the
+    # previous leaf while it still contains the particle: they differ only
+    # for particles on a shared edge
+    agree = np.mean(loc6[3][ok] == ref[3][ok])
+    assert agree > 0.995, agree
+    assert np.any(loc6[3] != loc0[3])             # particles changed leaves
+    for l in range(3):
+        assert np.array_equal(loc6[l], loc6[3] >> (2 * (3 - l)))
+
+
+def test_static_policy_keeps_build_membership(fss):
+    s, a = fss.make_state(5, "rh_vortices", n_vortex=8, seed=4)
+    kw = dict(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, tree_levels=4, rebuild=fss.REBUILD_STATIC)
+    _, loc0 = _steps(fss, s, a, 0, **kw)
+    _, loc3 = _steps(fss, s, a, 3, **kw)
+    assert np.array_equal(loc0, loc3)
+
+
+@pytest.mark.parametrize("list_mode", [0, 1])
+def test_resort_tracks_direct_over_many_steps(fss, list_mode):
+    """Twenty steps of a vortex field (particles cross many leaves)."""
+    s, a = fss.make_state(6, "rh_vortices", n_vortex=16, seed=11)
+    ref, _ = _steps(fss, s, a, 20, method=fss.METHOD_DIRECT, precision=fss.PREC_FP64)
+    got, _ = _steps(fss, s, a, 20, method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, degree=8, theta=0.7,
+                    list_mode=list_mode, rebuild=fss.REBUILD_RESORT)
+    assert np.all(np.isfinite(got))
+    disp = ref[:, :3] - s[:, :3]
+    err = np.linalg.norm(got[:, :3] - ref[:, :3]) / np.linalg.norm(disp)
+    assert err < 2e-6, err
+    dz = np.linalg.norm(got[:, 3] - ref[:, 3]) / np.linalg.norm(ref[:, 3])
+    assert dz < 1e-6, dz
+    assert np.array_equal(got[:, 4], s[:, 4])    # tracers ride along with their particles
+
+
+def test_resort_graph_equals_eager(fss):
+    s, a = fss.make_state(5, "rh_vortices", n_vortex=8, seed=12)
+    outs = [_steps(fss, s, a, 4, method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, use_graph=g,
+                   rebuild=fss.REBUILD_RESORT)[0] for g in (0, 1)]
+    assert np.array_equal(outs[0], outs[1])

@@ -36,9 +36,16 @@ def test_rk4_host_equals_device(fss):
         ctx.set_particles(s, a)
         ctx.rk4_step(0.01, nsteps=2)
         dev = ctx.get_state()
-        host = np.ascontiguousarray(s.copy())
-        ctx.rk4_step_host(host, 0.01, nsteps=2)
+        # the same start again after two steps: the particles were re-sorted
+        # in between, so sums run in another order (equal to rounding)
+        again = ctx.rk4_step_host(np.ascontiguousarray(s.copy()), 0.01, nsteps=2)
+    with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as ctx:
+        ctx.set_particles(s, a)
+        host = ctx.rk4_step_host(np.ascontiguousarray(s.copy()), 0.01, nsteps=2)
     assert np.array_equal(dev, host)
+    disp = dev[:, :3] - s[:, :3]
+    assert np.linalg.norm(again[:, :3] - dev[:, :3]) / np.linalg.norm(disp) < 1e-6
+    assert np.array_equal(again[:, 4], dev[:, 4])
 
 
 def test_rhs_between_steps_does_not_disturb(fss):
