@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--tol", type=float, default=1e-6, help="selector: relative L2 velocity error target")
     p.add_argument("--safety", type=float, default=2.0, help="selector: predicted-error safety factor")
     p.add_argument("--fixed", action="store_true", help="headline arm without the learned selector")
+    p.add_argument("--no-clusters", action="store_true",
+                   help="headline arm without target clusters (far sources summed at the target particles)")
     return p.parse_args()
 
 
@@ -185,20 +187,21 @@ def time_steps(ctx, stream, steps, flush):
     return sum(a.elapsed_time(b) for a, b in evs) / 1e3
 
 
-def make_arm(fss, state, area, stream, prec, args, dev):
+def make_arm(fss, state, area, stream, prec, args, dev, clusters=False):
     ctx = fss.Context(method=fss.METHOD_TREECODE, precision=prec, degree=args.degree, theta=args.theta,
-                      device=dev)
+                      cluster_targets=int(clusters), device=dev)
     ctx.set_stream(stream.cuda_stream)
     ctx.set_particles(state, area)
     return ctx
 
 
-def make_learned_arm(fss, state, area, stream, args, dev):
-    """Mixed precision with the learned per-leaf (degree, theta) and per-leaf
-    interaction lists; block shape chosen by the autotuner."""
+def make_learned_arm(fss, state, area, stream, args, dev, clusters=True):
+    """Mixed precision with the learned per-leaf (degree, theta) (with target
+    clusters: carried up to the faces of a dual traversal); block shape
+    chosen by the autotuner."""
     from fss_b200 import selector
     ctx = fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, list_mode=fss.LIST_LEAF,
-                      degree=args.degree, theta=args.theta, device=dev, autotune=1)
+                      cluster_targets=int(clusters), degree=args.degree, theta=args.theta, device=dev, autotune=1)
     ctx.set_stream(stream.cuda_stream)
     ctx.set_particles(state, area)
     choice = selector.apply(ctx, tol=args.tol, safety=args.safety, device=dev)
@@ -287,12 +290,13 @@ def main():
 
     # ---------------- headline arm: mixed precision BLTC
     from fss_b200 import selector as _sel
-    learned = (not args.fixed) and os.path.exists(_sel.WEIGHTS)
+    clusters = not args.no_clusters
+    learned = (not args.fixed) and os.path.exists(_sel.default_weights(clusters))
     classes = None
     if learned:
-        ctx, classes = make_learned_arm(fss, state, area, stream, args, dev)
+        ctx, classes = make_learned_arm(fss, state, area, stream, args, dev, clusters)
     else:
-        ctx = make_arm(fss, state, area, stream, fss.PREC_MIXED, args, dev)
+        ctx = make_arm(fss, state, area, stream, fss.PREC_MIXED, args, dev, clusters)
     err_l2, err_max = rel_err(ctx)
     warm(ctx, stream, args.warmup)
     barrier(ws)
@@ -312,7 +316,7 @@ def main():
     ctx.profile(False)
     inter, up_bytes = ctx.work_per_rhs()
     pk = "pairs_mixed"
-    pairs_ms = prof[pk][0] / prof[pk][1]
+    pairs_ms = prof[pk][0] / (4 * args.steps)  # per RHS (target-leaf and target-cluster launches)
     launches_per_step = sum(v[1] for v in prof.values()) / args.steps
     total_ms = sum(v[0] for v in prof.values())
     peaks = load_peaks()
@@ -322,7 +326,8 @@ def main():
     traffic = profiled_traffic("pairs_mixed_level8")
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp32_peak, "traffic": traffic,
-                "kernel": pk, "kernel_ms": pairs_ms, "interactions_per_launch": inter,
+                "kernel": "k_pairs (target-leaf + target-cluster launches of one RHS)", "kernel_ms": pairs_ms,
+                "interactions_per_launch": inter,
                 "flops_per_interaction": FLOPS_PER_PAIR,
                 "peak_source": f"nominal FP32 148 SM x 128 lanes x 2 x {sm_max:.0f} MHz (MEASURED_PEAKS.json has no FP32 figure)",
                 "frac_at_sampled_clock": (achieved / (fp32_peak * clocks["sm_mhz"] / sm_max)) if clocks.get("sm_mhz") else None,
@@ -330,16 +335,23 @@ def main():
                 "upward_bytes_per_rhs": up_bytes}
     info = ctx.tree_info()
 
-    # ---------------- plain FP64 BLTC (the ratio's denominator)
-    fp64 = None
+    # ---------------- FP64 arms: plain BLTC (the ratio's denominator: fixed n, theta,
+    # far sources summed at the target particles) and the same algorithm as the
+    # headline arm's (target clusters) in FP64, for reference
+    fp64 = fp64c = None
     if not args.no_fp64:
-        c64 = make_arm(fss, state, area, stream, fss.PREC_FP64, args, dev)
-        e64 = rel_err(c64)
-        warm(c64, stream, args.warmup)
-        t64 = max_over_ranks(time_steps(c64, stream, args.steps, flush), ws)
-        fp64 = {"value": ws * args.steps / t64, "ms_per_step": 1e3 * t64 / args.steps, "rel_l2": e64[0],
-                "rel_max": e64[1], "degree": args.degree, "theta": args.theta}
-        c64.close()
+        for cl in (False, True):
+            c64 = make_arm(fss, state, area, stream, fss.PREC_FP64, args, dev, clusters=cl)
+            e64 = rel_err(c64)
+            warm(c64, stream, args.warmup)
+            t64 = max_over_ranks(time_steps(c64, stream, args.steps, flush), ws)
+            r = {"value": ws * args.steps / t64, "ms_per_step": 1e3 * t64 / args.steps, "rel_l2": e64[0],
+                 "rel_max": e64[1], "degree": args.degree, "theta": args.theta, "target_clusters": cl}
+            c64.close()
+            if cl:
+                fp64c = r
+            else:
+                fp64 = r
 
     # ---------------- end to end through the C ABI with pinned host buffers
     e2e = None
@@ -371,18 +383,25 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": f"BVE RK4 step (4 RHS), {n} particles (icosahedral level {args.level}), "
                                        f"RH4 wave + {args.vortices} seeded vortices, mixed-precision BLTC "
-                                       f"({'learned per-leaf degree/theta' if learned else f'n={args.degree} theta={args.theta}'}), "
-                                       f"tree_levels={info['tree_levels']}, static tree",
+                                       f"({'learned per-leaf degree/theta' if learned else f'n={args.degree} theta={args.theta}'}"
+                                       f"{', target clusters (reference cp/cc types)' if clusters else ''}), "
+                                       f"tree_levels={info['tree_levels']}, particles re-sorted into their current leaves every step",
                            "n_particles": n, "degree": args.degree, "theta": args.theta,
                            "precision": "FP32 interactions + Kahan; FP64 RK4, renormalisation, interpolation",
                            "selector": (f"learned per-leaf (n, theta), tol {args.tol}, safety {args.safety}, "
+                                        f"classes (n, theta) {list(zip(*_sel.class_table(clusters)))}, "
                                         f"class counts {classes}") if learned else "none (fixed degree/theta)",
-                           "lists": "per-leaf" if learned else "dual (reference traversal)",
+                           "lists": ("dual traversal with per-face parameters from the per-leaf choice" if learned
+                                     else "dual (reference traversal)") if clusters else
+                                    ("per-leaf" if learned else "dual (reference traversal)"),
+                           "target_clusters": clusters,
                            "l2": "flushed between timed steps (256 MB write)",
                            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
                 "rel_l2": err_l2, "rel_max": err_max,
                 "fp64_plain": fp64,
                 "ratio_vs_fp64_plain": (value / fp64["value"]) if fp64 else None,
+                "fp64_same_algorithm": fp64c,
+                "ratio_vs_fp64_same_algorithm": (value / fp64c["value"]) if fp64c else None,
                 "interactions_per_rhs": inter, "tree": info,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(round(launches_per_step * args.steps)),

@@ -43,11 +43,19 @@ struct ProfEntry {
     int64_t launches = 0;
 };
 
+// One profiled range: its events and the number of kernels launched in it.
+struct ProfPending {
+    std::string name;
+    cudaEvent_t a, b;
+    int kernels;
+};
+
 }  // namespace fss
 
 struct fss_ctx {
     using DBuf = fss::DBuf;
     using ProfEntry = fss::ProfEntry;
+    using ProfPending = fss::ProfPending;
     using TreeGeometry = fss::TreeGeometry;
     using Pair = fss::Pair;
     using ListOutput = fss::ListOutput;
@@ -77,18 +85,20 @@ struct fss_ctx {
     int64_t unassigned = 0;
     ListOutput lists;
     std::vector<std::vector<ASrc>> alists;  // per-leaf sources before packing
+    std::vector<fss::TList> tlists;         // target clusters (cp/cc) and their sources
     std::vector<std::pair<fss::PairShape, double>> tuned;  // autotuner: shape, ms per pair pass
     std::vector<int32_t> leaf_deg;
     std::vector<double> leaf_theta;
     int nmax = 0, level_mask = 0;
     int parts = 1;
+    int64_t pstride = 0;  // partial slot stride: n, or n + proxy slots with target clusters
     PairShape shape;
     double direct_pairs = 0;
 
     // device
     DBuf in5, area_in, perm, key, key_tmp, vals_tmp, hist, leaf_start, s0, xs, acc, area_s, tracer_s, src, partials,
         segs, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
-        wtotal, err_flag, loc, sortq;
+        wtotal, err_flag, loc, sortq, down_jobs, down_of_face, down_coef;
     int64_t src_count = 0;
 
     // graph
@@ -97,7 +107,7 @@ struct fss_ctx {
 
     // profiling
     bool prof = false;
-    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    std::vector<ProfPending> pending;
     std::vector<cudaEvent_t> ev_pool;
     std::map<std::string, ProfEntry> prof_acc;
     std::vector<std::string> prof_order;
@@ -107,8 +117,8 @@ struct fss_ctx {
     ~fss_ctx() {
         if (graph) cudaGraphExecDestroy(graph);
         for (auto& p : pending) {
-            cudaEventDestroy(p.second.first);
-            cudaEventDestroy(p.second.second);
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
         }
         for (auto e : ev_pool) cudaEventDestroy(e);
         if (own_stream) cudaStreamDestroy(own_stream);

@@ -145,6 +145,7 @@ int fss_ensemble_create(const fss_config* cfg, fss_ensemble** out) {
     e->cfg.src_parts = 1;
     e->cfg.autotune = 0;
     e->cfg.use_graph = 0;
+    e->cfg.cluster_targets = 0;  // members' far fields are summed at their particles
     e->dev = cfg->device;
     ECU(cudaSetDevice(e->dev));
     ECU(cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking));
@@ -251,7 +252,7 @@ int fss_ensemble_build(fss_ensemble* e) {
         for (ProxyJob j : L.jobs) {
             j.leaf_lo += int32_t(lo);
             j.leaf_hi += int32_t(lo);
-            for (int d = 0; d < 12; d++)
+            for (int d = 0; d <= kMaxDegree; d++)
                 if (j.off[d] >= 0) j.off[d] = int32_t(j.off[d] - c->n + pxo);
             jobs.push_back(j);
         }

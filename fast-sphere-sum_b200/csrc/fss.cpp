@@ -57,11 +57,13 @@ cudaEvent_t ev_get(fss_ctx* c) {
     return e;
 }
 
+// Device time of a range of launches (`kernels` of them) under profiling.
 struct ProfScope {
     fss_ctx* c;
     const char* name;
+    int kernels;
     cudaEvent_t a = nullptr, b = nullptr;
-    ProfScope(fss_ctx* ctx, const char* nm) : c(ctx), name(nm) {
+    ProfScope(fss_ctx* ctx, const char* nm, int nk = 1) : c(ctx), name(nm), kernels(nk) {
         if (c->prof) {
             a = ev_get(c);
             b = ev_get(c);
@@ -71,7 +73,7 @@ struct ProfScope {
     ~ProfScope() {
         if (c->prof) {
             cudaEventRecord(b, c->stream);
-            c->pending.push_back({name, {a, b}});
+            c->pending.push_back({name, a, b, kernels});
         }
     }
 };
@@ -81,12 +83,12 @@ void prof_resolve(fss_ctx* c) {
     cudaStreamSynchronize(c->stream);
     for (auto& p : c->pending) {
         float ms = 0;
-        cudaEventElapsedTime(&ms, p.second.first, p.second.second);
-        if (!c->prof_acc.count(p.first)) c->prof_order.push_back(p.first);
-        c->prof_acc[p.first].ms += ms;
-        c->prof_acc[p.first].launches += 1;
-        c->ev_pool.push_back(p.second.first);
-        c->ev_pool.push_back(p.second.second);
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        if (!c->prof_acc.count(p.name)) c->prof_order.push_back(p.name);
+        c->prof_acc[p.name].ms += ms;
+        c->prof_acc[p.name].launches += p.kernels;
+        c->ev_pool.push_back(p.a);
+        c->ev_pool.push_back(p.b);
     }
     c->pending.clear();
 }
@@ -152,11 +154,13 @@ int build_direct_lists(fss_ctx* c) {
             L.n_tiles += (L.segs[p].b - L.segs[p].a + c->shape.tile - 1) / c->shape.tile;
         }
     }
+    L.n_leaf_items = int64_t(L.items.size());
     L.pp_pairs = double(n) * double(n - 1);
     c->direct_pairs = L.pp_pairs;
     TRY(upload(c, c->segs, L.segs));
     TRY(upload(c, c->items, L.items));
     TRY(src_size_ensure(c, n));
+    c->pstride = n;
     CU(c->partials.ensure(sizeof(double4) * size_t(P) * size_t(std::max<int64_t>(n, 1))));
     return FSS_OK;
 }
@@ -165,15 +169,26 @@ int build_direct_lists(fss_ctx* c) {
 // empty at the build may fill later, so no face is pruned for being empty.
 void make_alists(fss_ctx* c, const std::vector<int32_t>& dual_counts) {
     const int LL = c->leaf_level;
+    c->tlists.clear();
+    std::vector<int32_t> cc = dual_counts;
+    if (c->resort)
+        for (int32_t& x : cc) x = std::max(x, 1);
+    if (c->cfg.list_mode == FSS_LIST_LEAF && c->cfg.cluster_targets) {
+        // per-leaf (n, theta) carried up to the target faces of a dual traversal
+        std::vector<int32_t> fdeg;
+        std::vector<double> fth;
+        face_params(c->geom, LL, c->leaf_deg, c->leaf_theta, fdeg, fth);
+        c->alists = lists_from_pairs(c->geom, LL, dual_traverse_faces(c->geom, cc, fth, fdeg), 0, c->cfg.degree,
+                                     &c->tlists);
+        return;
+    }
     if (c->cfg.list_mode == FSS_LIST_LEAF) {
         c->alists = lists_per_leaf(c->geom, LL, c->counts_h, c->leaf_deg, c->leaf_theta, c->resort);
         return;
     }
     const int many = (c->cfg.many_count < 0) ? nproxy(c->cfg.degree) : c->cfg.many_count;
-    std::vector<int32_t> cc = dual_counts;
-    if (c->resort)
-        for (int32_t& x : cc) x = std::max(x, 1);
-    c->alists = lists_from_pairs(c->geom, LL, dual_traverse(c->geom, cc, c->cfg.theta, many), many, c->cfg.degree);
+    c->alists = lists_from_pairs(c->geom, LL, dual_traverse(c->geom, cc, c->cfg.theta, many), many, c->cfg.degree,
+                                 c->cfg.cluster_targets ? &c->tlists : nullptr);
 }
 
 int ensure_particle_buffers(fss_ctx* c, int64_t n) {
@@ -326,7 +341,9 @@ int build_tree(fss_ctx* c) {
     c->pairs = dual_traverse(c->geom, (c->cfg.assign_mode == FSS_ASSIGN_REFERENCE) ? ref_counts : c->counts_h,
                              c->cfg.theta, many);
     if (c->cfg.list_mode == FSS_LIST_DUAL && !c->resort && c->cfg.assign_mode != FSS_ASSIGN_REFERENCE) {
-        c->alists = lists_from_pairs(c->geom, LL, c->pairs, many, c->cfg.degree);
+        c->tlists.clear();
+        c->alists = lists_from_pairs(c->geom, LL, c->pairs, many, c->cfg.degree,
+                                     c->cfg.cluster_targets ? &c->tlists : nullptr);
     } else {
         make_alists(c, c->counts_h);
     }
@@ -371,7 +388,7 @@ int materialize(fss_ctx* c, PairShape shape) {
     in.parts = P;
     in.all_leaves = c->resort;
     c->parts = P;
-    build_lists(in, c->alists, c->lists);
+    build_lists(in, c->alists, c->tlists, c->lists);
     const ListOutput& L = c->lists;
     // interpolation tables for the degrees in use
     c->nmax = std::max(L.max_degree, 0);
@@ -394,13 +411,36 @@ int materialize(fss_ctx* c, PairShape shape) {
     TRY(upload(c, c->segs, L.segs));
     TRY(upload(c, c->items, L.items));
     TRY(upload(c, c->jobs, L.jobs));
+    TRY(upload(c, c->down_jobs, L.down));
+    TRY(upload(c, c->down_of_face, L.down_of_face));
+    CU(c->down_coef.ensure(sizeof(double4) * size_t(std::max<int64_t>(L.n_coef, 1))));
     std::vector<double4> pp(L.proxy_pos.size() / 4);
     for (size_t i = 0; i < pp.size(); i++)
         pp[i] = make_double4(L.proxy_pos[4 * i], L.proxy_pos[4 * i + 1], L.proxy_pos[4 * i + 2], 0.0);
     TRY(upload(c, c->proxy_pos, pp));
     TRY(src_size_ensure(c, n + L.n_proxy));
-    CU(c->partials.ensure(sizeof(double4) * size_t(P) * size_t(n)));
+    // target clusters write partials at their interpolation points (slots
+    // after the particles) and the down pass one more slot per particle
+    const bool down = !L.down.empty();
+    c->pstride = down ? n + L.n_proxy : n;
+    CU(c->partials.ensure(sizeof(double4) * size_t(P + (down ? 1 : 0)) * size_t(c->pstride)));
     CU(c->part_up.ensure(sizeof(double) * size_t(c->nleaf) * (LL + 1) * nproxy(c->nmax)));
+    return FSS_OK;
+}
+
+// The pair kernel over all work items: target leaves with the block shape
+// of the context, target clusters with a block fitted to their
+// interpolation point count.
+int launch_all_pairs(fss_ctx* c, bool want_psi) {
+    const ListOutput& L = c->lists;
+    const int nl = int(L.n_leaf_items), nall = int(L.items.size());
+    CU(launch_pairs(c->stream, c->fp64, want_psi, c->shape, nl, c->src.p, c->segs.as<Segment>(),
+                    c->leaf_start.as<int32_t>(), c->items.as<WorkItem>(), c->partials.as<double4>(), c->pstride,
+                    c->err_flag.as<int>()));
+    if (nall > nl)
+        CU(launch_pairs(c->stream, c->fp64, want_psi, cluster_shape(c->fp64, L.max_cluster_k), nall - nl, c->src.p,
+                        c->segs.as<Segment>(), c->leaf_start.as<int32_t>(), c->items.as<WorkItem>() + nl,
+                        c->partials.as<double4>(), c->pstride, c->err_flag.as<int>()));
     return FSS_OK;
 }
 
@@ -422,15 +462,22 @@ int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
         }
     }
     {
-        ProfScope ps(c, c->fp64 ? "pairs_fp64" : "pairs_mixed");
-        CU(launch_pairs(c->stream, c->fp64, want_psi, c->shape, int(c->lists.items.size()), c->src.p,
-                        c->segs.as<Segment>(), c->leaf_start.as<int32_t>(), c->items.as<WorkItem>(),
-                        c->partials.as<double4>(), c->n, c->err_flag.as<int>()));
+        ProfScope ps(c, c->fp64 ? "pairs_fp64" : "pairs_mixed", c->lists.n_leaf_items < int64_t(c->lists.items.size()) ? 2 : 1);
+        TRY(launch_all_pairs(c, want_psi));
+    }
+    const bool down = c->tree && !c->lists.down.empty();
+    if (down) {
+        ProfScope ps(c, "downward", 2);
+        launch_down(c->stream, want_psi, int(c->lists.down.size()), c->down_jobs.as<DownJob>(), c->partials.as<double4>(),
+                    c->parts, c->pstride, c->vinv.as<double>(), c->vinv_off.as<int32_t>(), c->down_coef.as<double4>(),
+                    int(c->nleaf), c->xs.as<double4>(), c->leaf_start.as<int32_t>(), c->node.as<NodeGeom>(),
+                    c->lev_off.as<int64_t>(), c->leaf_level, c->down_of_face.as<int32_t>(),
+                    c->partials.as<double4>() + int64_t(c->parts) * c->pstride);
     }
     if (want_psi) launch_wsum(c->stream, c->n, c->xs.as<double4>(), c->area_s.as<double>(), c->wtotal.as<double>());
     ea.n = c->n;
-    ea.parts = c->parts;
-    ea.pstride = c->n;
+    ea.parts = c->parts + (down ? 1 : 0);
+    ea.pstride = c->pstride;
     ea.partials = c->partials.as<double4>();
     ea.xs = c->xs.as<double4>();
     ea.area = c->area_s.as<double>();
@@ -467,9 +514,7 @@ int autotune(fss_ctx* c) {
         TRY(eval(c, ea, false));  // warm (and proxies)
         CU(cudaEventRecord(a, c->stream));
         for (int r = 0; r < 2; r++)
-            CU(launch_pairs(c->stream, c->fp64, false, c->shape, int(c->lists.items.size()), c->src.p,
-                            c->segs.as<Segment>(), c->leaf_start.as<int32_t>(), c->items.as<WorkItem>(),
-                            c->partials.as<double4>(), c->n, c->err_flag.as<int>()));
+            TRY(launch_all_pairs(c, false));
         CU(cudaEventRecord(b, c->stream));
         CU(cudaEventSynchronize(b));
         float ms = 0;
@@ -492,13 +537,15 @@ int autotune(fss_ctx* c) {
 // stable key sort (order q), state permuted in place, leaf ranges, stage-1
 // sources.
 int resort(fss_ctx* c) {
-    ProfScope ps(c, "resort");
+    int bits = 0;
+    while ((int64_t(1) << bits) < c->nleaf) bits++;
+    bits = std::max(bits, 1);
+    // reassign, 3 per 8-bit sort pass, gather + commit, leaf bounds
+    ProfScope ps(c, "resort", 1 + 3 * ((bits + 7) / 8) + 2 + 1);
     const int64_t n = c->n;
     launch_reassign(c->stream, n, c->s0.as<double4>(), nullptr, c->leaf_level, c->verts.as<double>(),
                     c->tri_verts.as<int32_t>(), c->lev_off.as<int64_t>(), c->key.as<uint32_t>());
-    int bits = 0;
-    while ((int64_t(1) << bits) < c->nleaf) bits++;
-    launch_sort(c->stream, n, std::max(bits, 1), c->key.as<uint32_t>(), c->key_tmp.as<uint32_t>(),
+    launch_sort(c->stream, n, bits, c->key.as<uint32_t>(), c->key_tmp.as<uint32_t>(),
                 c->sortq.as<int32_t>(), c->vals_tmp.as<int32_t>(), c->hist.as<uint32_t>());
     launch_resort(c->stream, c->fp64, n, c->sortq.as<int32_t>(), c->s0.as<double4>(), c->area_s.as<double>(),
                   c->tracer_s.as<double>(), c->perm.as<int32_t>(), c->xs.as<double4>(), c->acc.as<double4>(),
@@ -651,7 +698,7 @@ int fss_create(const fss_config* cfg, fss_ctx** out) {
     fss_ctx* c = nullptr;
     if (!cfg || !out) return fail(c, FSS_ERR_INVALID, "null argument");
     *out = nullptr;
-    if (cfg->degree < 0 || cfg->degree > kMaxDegree) return fail(c, FSS_ERR_INVALID, "degree must be in 0..10");
+    if (cfg->degree < 0 || cfg->degree > kMaxDegree) return fail(c, FSS_ERR_INVALID, "degree must be in 0..12");
     if (!(cfg->theta > 0)) return fail(c, FSS_ERR_INVALID, "theta must be positive");
     if (cfg->tree_levels < 0 || cfg->tree_levels > kMaxLevels) return fail(c, FSS_ERR_INVALID, "tree_levels out of range");
     int ndev = 0;
@@ -814,6 +861,9 @@ int fss_get_tree_info(fss_ctx* c, fss_tree_info* info) {
     info->block_threads = c->shape.threads;
     info->targets_per_thread = c->shape.per_thread;
     info->src_parts = c->parts;
+    info->target_clusters = int32_t(c->lists.down.size());
+    info->cp_interactions = c->lists.cp_pairs;
+    info->cc_interactions = c->lists.cc_pairs;
     return FSS_OK;
 }
 
@@ -904,7 +954,7 @@ int fss_profile_read(fss_ctx* c, char* names, int32_t names_cap, double* ms, int
 
 int fss_work_per_rhs(fss_ctx* c, double* interactions, double* upward_bytes) {
     if (!c) return fail(c, FSS_ERR_INVALID, "null context");
-    if (interactions) *interactions = c->lists.pp_pairs + c->lists.pc_pairs;
+    if (interactions) *interactions = c->lists.pp_pairs + c->lists.pc_pairs + c->lists.cp_pairs + c->lists.cc_pairs;
     if (upward_bytes) {
         double b = 0;
         if (c->tree && !c->lists.jobs.empty()) {
@@ -973,7 +1023,7 @@ int fss_tree_traverse(int32_t tree_levels, double theta, int32_t many_count, con
 }
 
 int fss_interp_nodes(int32_t degree, double* nodes, double* vinv) {
-    if (degree < 0 || degree > kMaxDegree) return fail(nullptr, FSS_ERR_INVALID, "degree must be in 0..10");
+    if (degree < 0 || degree > kMaxDegree) return fail(nullptr, FSS_ERR_INVALID, "degree must be in 0..12");
     std::vector<double> nd, vi;
     interp_nodes(degree, nd, vi);
     if (nodes) std::memcpy(nodes, nd.data(), sizeof(double) * nd.size());

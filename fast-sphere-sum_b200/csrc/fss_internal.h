@@ -51,8 +51,7 @@ struct ProxyJob {
     int32_t level, node, local;   // local = index within its level
     int32_t leaf_lo, leaf_hi;     // leaves under the node
     int32_t degmask;
-    int32_t off[12];              // by degree, -1 when not wanted
-    int32_t pad;
+    int32_t off[16];              // by degree (0..kMaxDegree), -1 when not wanted
 };
 
 // One leaf of an ensemble member for the batched upward pass: its index in
@@ -67,6 +66,17 @@ struct EnsLeaf {
     int64_t part_base;
 };
 
+// Downward pass of a target cluster: a face that receives far sources at
+// its K = nproxy(deg) interpolation points (fast_rhs.h cp and cc).  The
+// field there (unified indices [slot, slot + K)) becomes coefficients of the
+// Chebyshev product basis (K double4 from `coef`), evaluated at every
+// particle of the face.
+struct DownJob {
+    int32_t level, node, local, deg;  // node = global face index
+    int32_t slot;                     // first interpolation point (unified index)
+    int32_t coef;                     // first coefficient (double4 units)
+};
+
 // Per-node geometry for the upward pass: inverse of [v1 v2 v3] (columns),
 // row-major, and the frame centre.
 struct NodeGeom {
@@ -74,8 +84,8 @@ struct NodeGeom {
     double cx, cy, cz;
 };
 
-constexpr int kMaxDegree = 10;
-constexpr int kMaxK = (kMaxDegree + 1) * (kMaxDegree + 2) / 2;  // 66
+constexpr int kMaxDegree = 12;
+constexpr int kMaxK = (kMaxDegree + 1) * (kMaxDegree + 2) / 2;  // 91
 constexpr int kMaxLevels = 8;  // tree_levels supported
 
 FSS_HD inline int nproxy(int n) { return (n + 1) * (n + 2) / 2; }

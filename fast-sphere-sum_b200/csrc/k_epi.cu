@@ -248,6 +248,114 @@ __global__ void k_scatter_state(int64_t n, const int32_t* __restrict__ perm, con
     o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; o[4] = tracer[s];
 }
 
+// ---------------------------------------------------------------- downward pass
+// Target clusters (fast_rhs.h cp and cc): the sum A of a face's far
+// sources at its interpolation points y_k is interpolated to its particles,
+//   A(x_i) = sum_k A(y_k) l_k(b_i) = sum_m c_m phi_m(b_i),   c_m = sum_k Vinv[m][k] A(y_k),
+// with b_i the barycentric coordinates of the central projection of x_i on
+// the face's plane and phi_m the Chebyshev product basis of the upward pass.
+// Kernel 1 forms c for every target cluster; kernel 2, one block per leaf,
+// evaluates the polynomials of all the leaf's ancestors that are target
+// clusters at its particles and writes the sum (x, y, z and, when the
+// stream function is wanted, its log term) to the down-pass partial slot of
+// every particle.  FP64.
+
+template <bool PSI>
+__global__ void __launch_bounds__(kUpThreads) k_down_combine(const DownJob* __restrict__ jobs,
+                                                             const double4* __restrict__ partials, int parts,
+                                                             int64_t pstride, const double* __restrict__ vinv,
+                                                             const int32_t* __restrict__ vinv_off,
+                                                             double4* __restrict__ coef) {
+    __shared__ double4 A[kMaxK];
+    const DownJob job = jobs[blockIdx.x];
+    const int K = nproxy(job.deg);
+    for (int k = threadIdx.x; k < K; k += kUpThreads) {
+        double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int p = 0; p < parts; p++) {
+            const double4 v = partials[int64_t(p) * pstride + job.slot + k];
+            a.x += v.x; a.y += v.y; a.z += v.z; a.w += v.w;
+        }
+        A[k] = a;
+    }
+    __syncthreads();
+    const double* V = vinv + vinv_off[job.deg];
+    for (int m = threadIdx.x; m < K; m += kUpThreads) {
+        double4 c = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int k = 0; k < K; k++) {
+            const double w = V[m * K + k];
+            const double4 v = A[k];
+            c.x = fma(w, v.x, c.x); c.y = fma(w, v.y, c.y); c.z = fma(w, v.z, c.z);
+            if (PSI) c.w = fma(w, v.w, c.w);
+        }
+        coef[int64_t(job.coef) + m] = c;
+    }
+}
+
+template <bool PSI>
+__global__ void __launch_bounds__(kUpThreads) k_down_leaf(const double4* __restrict__ xs,
+                                                          const int32_t* __restrict__ leaf_start,
+                                                          const NodeGeom* __restrict__ node,
+                                                          const int64_t* __restrict__ lev_off, int leaf_level,
+                                                          const int32_t* __restrict__ down_of_face,
+                                                          const DownJob* __restrict__ jobs,
+                                                          const double4* __restrict__ coef,
+                                                          double4* __restrict__ out) {
+    __shared__ double4 C[kMaxLevels][kMaxK];
+    __shared__ int deg_s[kMaxLevels];
+    const int leaf = blockIdx.x, tid = threadIdx.x;
+    const int a0 = leaf_start[leaf], a1 = leaf_start[leaf + 1];
+    if (a0 == a1) return;
+    for (int l = 0; l <= leaf_level; l++) {
+        const int j = down_of_face[lev_off[l] + (leaf >> (2 * (leaf_level - l)))];
+        if (j < 0) {
+            if (tid == 0) deg_s[l] = -1;
+            continue;
+        }
+        const DownJob job = jobs[j];
+        if (tid == 0) deg_s[l] = job.deg;
+        const int K = nproxy(job.deg);
+        for (int k = tid; k < K; k += kUpThreads) C[l][k] = coef[int64_t(job.coef) + k];
+    }
+    __syncthreads();
+    for (int i = a0 + tid; i < a1; i += kUpThreads) {
+        const double4 x = xs[i];
+        double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int l = 0; l <= leaf_level; l++) {
+            const int deg = deg_s[l];
+            if (deg < 0) continue;
+            const NodeGeom& ng = node[lev_off[l] + (leaf >> (2 * (leaf_level - l)))];
+            const double c0 = ng.minv[0] * x.x + ng.minv[1] * x.y + ng.minv[2] * x.z;
+            const double c1 = ng.minv[3] * x.x + ng.minv[4] * x.y + ng.minv[5] * x.z;
+            const double c2 = ng.minv[6] * x.x + ng.minv[7] * x.y + ng.minv[8] * x.z;
+            const double inv = 1.0 / (c0 + c1 + c2);
+            const double u = 2.0 * (c0 * inv) - 1.0, v = 2.0 * (c1 * inv) - 1.0;
+            double Tu[kMaxDegree + 1], Tv[kMaxDegree + 1];
+            Tu[0] = 1.0; Tv[0] = 1.0;
+            Tu[1] = u; Tv[1] = v;
+#pragma unroll
+            for (int a = 2; a <= kMaxDegree; a++) {
+                Tu[a] = 2.0 * u * Tu[a - 1] - Tu[a - 2];
+                Tv[a] = 2.0 * v * Tv[a - 1] - Tv[a - 2];
+            }
+            const double4* Cl = C[l];
+#pragma unroll
+            for (int g = 0; g <= kMaxDegree; g++) {
+                if (g > deg) break;
+#pragma unroll
+                for (int b = 0; b <= g; b++) {
+                    const double phi = Tu[g - b] * Tv[b];
+                    const double4 cm = Cl[g * (g + 1) / 2 + b];
+                    acc.x = fma(phi, cm.x, acc.x);
+                    acc.y = fma(phi, cm.y, acc.y);
+                    acc.z = fma(phi, cm.z, acc.z);
+                    if (PSI) acc.w = fma(phi, cm.w, acc.w);
+                }
+            }
+        }
+        out[i] = acc;
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 
 void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, const int32_t* leaf_start,
@@ -301,6 +409,22 @@ void launch_scatter_state(cudaStream_t st, int64_t n, const int32_t* perm, const
                           double* out5) {
     if (n == 0) return;
     k_scatter_state<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, perm, s0, tracer, out5);
+}
+
+void launch_down(cudaStream_t st, bool psi, int njobs, const DownJob* jobs, const double4* partials, int parts,
+                 int64_t pstride, const double* vinv, const int32_t* vinv_off, double4* coef, int nleaf,
+                 const double4* xs, const int32_t* leaf_start, const NodeGeom* node, const int64_t* lev_off,
+                 int leaf_level, const int32_t* down_of_face, double4* out) {
+    if (njobs == 0) return;
+    if (psi) {
+        k_down_combine<true><<<njobs, kUpThreads, 0, st>>>(jobs, partials, parts, pstride, vinv, vinv_off, coef);
+        k_down_leaf<true><<<nleaf, kUpThreads, 0, st>>>(xs, leaf_start, node, lev_off, leaf_level, down_of_face, jobs,
+                                                        coef, out);
+    } else {
+        k_down_combine<false><<<njobs, kUpThreads, 0, st>>>(jobs, partials, parts, pstride, vinv, vinv_off, coef);
+        k_down_leaf<false><<<nleaf, kUpThreads, 0, st>>>(xs, leaf_start, node, lev_off, leaf_level, down_of_face,
+                                                         jobs, coef, out);
+    }
 }
 
 }  // namespace fss

@@ -315,6 +315,13 @@ PairShape pairs_shape(bool fp64, int threads, int per_thread) {
     return pair_shapes(fp64).front();
 }
 
+PairShape cluster_shape(bool fp64, int k) {
+    const int tile = tile_capacity(fp64);
+    if (k <= 64) return PairShape{64, 1, tile};
+    if (k <= 96) return PairShape{96, 1, tile};
+    return pairs_shape(fp64, 128, 1);
+}
+
 template <typename T, bool PSI>
 static cudaError_t dispatch(cudaStream_t st, PairShape sh, int nitems, const void* src, const Segment* segs,
                             const int32_t* leaf_start, const WorkItem* items, double4* partials,
@@ -322,6 +329,8 @@ static cudaError_t dispatch(cudaStream_t st, PairShape sh, int nitems, const voi
 #define FSS_SHAPE(TH)                                                                                            \
     if (sh.threads == TH)                                                                                        \
         return run_pairs<T, TH, PSI>(st, nitems, src, segs, leaf_start, items, partials, pstride, err);
+    FSS_SHAPE(64)
+    FSS_SHAPE(96)
     FSS_SHAPE(128)
     FSS_SHAPE(160)
     FSS_SHAPE(192)

@@ -68,6 +68,9 @@ void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, con
 const std::vector<PairShape>& pair_shapes(bool fp64);
 // The supported shape with `threads`, or the default (128).
 PairShape pairs_shape(bool fp64, int threads, int per_thread);
+// Block for work items of k targets (target clusters: their interpolation
+// points): the smallest of 64, 96, 128 threads that holds them.
+PairShape cluster_shape(bool fp64, int k);
 cudaError_t launch_pairs(cudaStream_t st, bool fp64, bool psi, PairShape shape, int nitems, const void* src,
                          const Segment* segs, const int32_t* leaf_start, const WorkItem* items, double4* partials,
                          int64_t pstride, int* err);
@@ -84,6 +87,13 @@ void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, cons
 void launch_up_combine(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part, int leaf_level,
                        int nmax, const double* vinv, const int32_t* vinv_off, const double4* proxy_pos,
                        const NodeGeom* node, int local_frames, int64_t n, void* src);
+// Downward pass of the target clusters: coefficients from the field at
+// their interpolation points (parts partial slots of stride pstride), then
+// their sum at every particle into `out` (the down-pass partial slot).
+void launch_down(cudaStream_t st, bool psi, int njobs, const DownJob* jobs, const double4* partials, int parts,
+                 int64_t pstride, const double* vinv, const int32_t* vinv_off, double4* coef, int nleaf,
+                 const double4* xs, const int32_t* leaf_start, const NodeGeom* node, const int64_t* lev_off,
+                 int leaf_level, const int32_t* down_of_face, double4* out);
 void launch_epilogue(cudaStream_t st, bool fp64, const EpiArgs& a);
 void launch_refresh(cudaStream_t st, bool fp64, int64_t n, const double4* s0, const double* area,
                     const uint32_t* leaf_of, const double4* frame, double4* xs, void* src);

@@ -1,7 +1,10 @@
 // selector.cpp -- learned per-leaf interpolation degree and MAC.
 //
-// For every target leaf the selector chooses one of 12 classes,
-//   (n, theta) in {4, 6, 8, 10} x {0.5, 0.6, 0.7},   class c = 3 i + j, n = 4 + 2i, theta = 0.5 + 0.1 j,
+// For every target leaf the selector chooses one of 12 classes c = 3 i + j,
+//   target-leaf evaluation: (n, theta) in {4, 6, 8, 10} x {0.5, 0.6, 0.7}  (n = 4 + 2i, theta = 0.5 + 0.1 j),
+//   target clusters:        (n, theta) in {6, 8, 10, 12} x {0.7, 0.8, 0.9}  (n = 6 + 2i, theta = 0.7 + 0.1 j)
+// (with target clusters a face takes the most accurate choice of its
+// leaves and interpolates at both ends, so its useful range sits higher),
 // so that the relative L2 velocity error stays below a tolerance at least
 // interaction count.  A target leaf's velocity error depends only on its own
 // class (its far clusters and their degree-n proxies), and squared errors
@@ -10,7 +13,8 @@
 // The network predicts y_l(c) = log10(e_l(c) / U) with U the RMS speed
 // (from 16 leaf features: geometry, charge statistics and far-field
 // statistics of the leaf's theta = 0.7 interaction list); the costs cost_l(c)
-// are exact interaction counts from one traversal per theta.  The choice
+// are exact interaction counts from one traversal per theta (per class, with
+// target clusters, whose work is shared among their leaves).  The choice
 // minimises sum cost + mu sum 10^(2y) leaf by leaf, with mu set by bisection
 // so that the predicted budget sum_l 10^(2 y_l) <= (tol / safety)^2 N holds.
 #include <algorithm>
@@ -31,8 +35,9 @@ void set_last_error(const std::string& msg);
 
 constexpr int kClasses = 12;
 constexpr int kFeatures = 16;
-inline int class_degree(int c) { return 4 + 2 * (c / 3); }
-inline double class_theta(int c) { return 0.5 + 0.1 * (c % 3); }
+inline int class_degree(int c, bool clusters) { return (clusters ? 6 : 4) + 2 * (c / 3); }
+inline double class_theta(int c, bool clusters) { return (clusters ? 0.7 : 0.5) + 0.1 * (c % 3); }
+constexpr double kFeatureTheta = 0.7;  // far-field features come from this traversal
 
 struct ThetaLists {
     std::vector<int64_t> near;               // near-field particles per leaf
@@ -168,22 +173,42 @@ static int features_and_costs(fss_ctx* c, std::vector<float>& feat, std::vector<
             qabs[g.lev_off[l] + f] = q;
         }
     }
-    // traversals per theta, costs per class
+    // costs per class: exact interaction counts of each class used everywhere
     cost.assign(size_t(nleaf) * kClasses, 0);
-    ThetaLists t07;
-    for (int j = 0; j < 3; j++) {
-        const double th = class_theta(j);
-        ThetaLists tl = traverse_theta(g, LL, c->counts_h, th);
-        for (int64_t l = 0; l < nleaf; l++) {
-            const double nt = c->leaf_start_h[l + 1] - c->leaf_start_h[l];
-            for (int i = 0; i < 4; i++) {
-                const int K = nproxy(4 + 2 * i);
-                double s = double(tl.near[l]);
-                for (int32_t gf : tl.far[l]) s += std::min<double>(K, c->counts_h[gf]);
-                cost[size_t(l) * kClasses + 3 * i + j] = nt * s;
+    ThetaLists t07 = traverse_theta(g, LL, c->counts_h, kFeatureTheta);
+    const bool clusters = c->cfg.cluster_targets != 0;
+    if (clusters) {
+        // dual traversal per class; a target cluster's work (its
+        // interpolation points against its sources) is shared among its
+        // leaves by particle count
+        for (int k = 0; k < kClasses; k++) {
+            const int K = nproxy(class_degree(k, true));
+            const std::vector<Pair> pairs = dual_traverse(g, c->counts_h, class_theta(k, true), K);
+            for (const Pair& p : pairs) {
+                const int64_t span = int64_t(1) << (2 * (LL - p.lt));
+                const bool cl = p.far && p.nt > K;
+                const double per_src = (p.far && p.ns > K) ? K : p.ns;
+                for (int64_t lf = p.t * span; lf < (p.t + 1) * span; lf++) {
+                    const double nl = c->leaf_start_h[lf + 1] - c->leaf_start_h[lf];
+                    cost[size_t(lf) * kClasses + k] += cl ? double(K) * per_src * nl / double(p.nt) : nl * per_src;
+                }
             }
         }
-        if (j == 2) t07 = std::move(tl);
+    } else {
+        for (int j = 0; j < 3; j++) {
+            const double th = class_theta(j, false);
+            const ThetaLists tl = (th == kFeatureTheta) ? ThetaLists() : traverse_theta(g, LL, c->counts_h, th);
+            const ThetaLists& t = (th == kFeatureTheta) ? t07 : tl;
+            for (int64_t l = 0; l < nleaf; l++) {
+                const double nt = c->leaf_start_h[l + 1] - c->leaf_start_h[l];
+                for (int i = 0; i < 4; i++) {
+                    const int K = nproxy(class_degree(3 * i, false));
+                    double s = double(t.near[l]);
+                    for (int32_t gf : t.far[l]) s += std::min<double>(K, c->counts_h[gf]);
+                    cost[size_t(l) * kClasses + 3 * i + j] = nt * s;
+                }
+            }
+        }
     }
     // features
     feat.assign(size_t(nleaf) * kFeatures, 0.f);
@@ -239,6 +264,18 @@ int fss_selector_features(fss_ctx* c, float* features, double* costs, double* u_
     return FSS_OK;
 }
 
+int fss_selector_class_table(int32_t clusters, int32_t* degree, double* theta) {
+    if (!degree || !theta) {
+        set_last_error("fss_selector_class_table: null argument");
+        return FSS_ERR_INVALID;
+    }
+    for (int k = 0; k < kClasses; k++) {
+        degree[k] = class_degree(k, clusters != 0);
+        theta[k] = class_theta(k, clusters != 0);
+    }
+    return FSS_OK;
+}
+
 int fss_select_classes(int64_t nleaf, int32_t nclass, const double* pred_log_err, const double* cost, double budget,
                        int32_t* choice) {
     if (nleaf < 0 || nclass <= 0 || !pred_log_err || !cost || !choice) {
@@ -277,12 +314,13 @@ int fss_selector_apply(fss_ctx* c, fss_mlp* m, const float* feat_mean, const flo
     std::vector<int32_t> choice(nleaf, 0);
     const double budget = (tol / safety) * (tol / safety) * double(c->n);
     select(nleaf, kClasses, yd.data(), k.data(), budget, choice.data());
+    const bool clusters = c->cfg.cluster_targets != 0;
     for (int64_t l = 0; l < nleaf; l++) {
-        c->leaf_deg[l] = class_degree(choice[l]);
-        c->leaf_theta[l] = class_theta(choice[l]);
+        c->leaf_deg[l] = class_degree(choice[l], clusters);
+        c->leaf_theta[l] = class_theta(choice[l], clusters);
     }
     if (choice_out) std::memcpy(choice_out, choice.data(), sizeof(int32_t) * nleaf);
-    c->cfg.list_mode = FSS_LIST_LEAF;
+    c->cfg.list_mode = FSS_LIST_LEAF;  // with cluster_targets: per-face dual traversal
     return internal_relist(c);
 }
 

@@ -32,11 +32,11 @@ std::vector<Pair> dual_traverse(const TreeGeometry& g, const std::vector<int32_t
         const double sep = (ti[3] + si[3]) / dist;
         if (dist > 0 && sep < theta) {  // fast_rhs.h:46-58
             const int ty = ((nt > many_count) ? 2 : 0) + ((ns > many_count) ? 1 : 0);
-            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, ty, 1});
+            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, ty, 1, -1});
         } else if (nt < many_count && ns < many_count) {  // :60
-            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, 0, 0});
+            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, 0, 0, -1});
         } else if (e.lt == L - 1 && e.ls == L - 1) {  // :63
-            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, 0, 0});
+            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, 0, 0, -1});
         } else if (e.lt == L - 1) {  // :66 refine the source
             for (int c = 0; c < 4; c++) q.push_back({e.t, 4 * e.s + c, e.lt, e.ls + 1});
         } else if (e.ls == L - 1) {  // :71 refine the target
@@ -54,14 +54,89 @@ std::vector<Pair> dual_traverse(const TreeGeometry& g, const std::vector<int32_t
     return out;
 }
 
+std::vector<Pair> dual_traverse_faces(const TreeGeometry& g, const std::vector<int32_t>& counts,
+                                      const std::vector<double>& face_theta, const std::vector<int32_t>& face_deg) {
+    const int L = g.tree_levels;
+    std::vector<Pair> out;
+    struct Q { int32_t t, s, lt, ls; };
+    std::vector<Q> q;
+    q.reserve(1 << 16);
+    size_t head = 0;
+    for (int i = 0; i < 20; i++)
+        for (int j = 0; j < 20; j++) q.push_back({i, j, 0, 0});
+    while (head < q.size()) {
+        const Q e = q[head++];
+        const int64_t gt = g.lev_off[e.lt] + e.t, gs = g.lev_off[e.ls] + e.s;
+        const int nt = counts[gt], ns = counts[gs];
+        if (nt == 0 || ns == 0) continue;
+        const int deg = face_deg[gt];
+        const int many = nproxy(deg);
+        const double* ti = &g.tri_info[4 * gt];
+        const double* si = &g.tri_info[4 * gs];
+        const double dist = great_circ_dist(ti, si, 1.0);
+        if (dist > 0 && (ti[3] + si[3]) / dist < face_theta[gt]) {
+            const int ty = ((nt > many) ? 2 : 0) + ((ns > many) ? 1 : 0);
+            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, ty, 1, deg});
+        } else if ((nt < many && ns < many) || (e.lt == L - 1 && e.ls == L - 1)) {
+            out.push_back({e.lt, e.ls, e.t, e.s, nt, ns, 0, 0, deg});
+        } else if (e.lt == L - 1) {
+            for (int c = 0; c < 4; c++) q.push_back({e.t, 4 * e.s + c, e.lt, e.ls + 1});
+        } else if (e.ls == L - 1 || nt >= ns) {
+            for (int c = 0; c < 4; c++) q.push_back({4 * e.t + c, e.s, e.lt + 1, e.ls});
+        } else {
+            for (int c = 0; c < 4; c++) q.push_back({e.t, 4 * e.s + c, e.lt, e.ls + 1});
+        }
+        if (head > (1u << 20) && head * 2 > q.size()) {
+            q.erase(q.begin(), q.begin() + head);
+            head = 0;
+        }
+    }
+    return out;
+}
+
+void face_params(const TreeGeometry& g, int leaf_level, const std::vector<int32_t>& leaf_deg,
+                 const std::vector<double>& leaf_theta, std::vector<int32_t>& face_deg,
+                 std::vector<double>& face_theta) {
+    const int64_t nf = g.lev_off[leaf_level + 1];
+    face_deg.assign(nf, 0);
+    face_theta.assign(nf, 1e300);
+    const int64_t nleaf = g.level_count(leaf_level);
+    for (int64_t l = 0; l < nleaf; l++) {
+        face_deg[g.lev_off[leaf_level] + l] = leaf_deg[l];
+        face_theta[g.lev_off[leaf_level] + l] = leaf_theta[l];
+    }
+    for (int lv = leaf_level - 1; lv >= 0; lv--)
+        for (int64_t f = 0; f < g.level_count(lv); f++) {
+            const int64_t p = g.lev_off[lv] + f;
+            for (int c = 0; c < 4; c++) {
+                const int64_t ch = g.lev_off[lv + 1] + 4 * f + c;
+                face_deg[p] = std::max(face_deg[p], face_deg[ch]);
+                face_theta[p] = std::min(face_theta[p], face_theta[ch]);
+            }
+        }
+}
+
 std::vector<std::vector<ASrc>> lists_from_pairs(const TreeGeometry& g, int leaf_level, const std::vector<Pair>& pairs,
-                                                int many_count, int degree) {
-    (void)g;
+                                                int many_count, int degree, std::vector<TList>* clusters) {
     const int64_t nleaf = int64_t(20) << (2 * leaf_level);
     std::vector<std::vector<ASrc>> lists(nleaf);
+    std::map<int64_t, size_t> cl_of;  // global face -> cluster list
+    if (clusters) clusters->clear();
     for (const Pair& p : pairs) {
+        const int deg = p.deg >= 0 ? p.deg : degree;
+        const int many = p.deg >= 0 ? nproxy(p.deg) : many_count;
+        const ASrc src = (p.far && p.ns > many) ? ASrc{1, p.ls, p.s, deg} : ASrc{0, p.ls, p.s, 0};
+        if (clusters && p.far && p.nt > many) {  // fast_rhs.h cp / cc
+            const int64_t gf = g.lev_off[p.lt] + p.t;
+            auto it = cl_of.find(gf);
+            if (it == cl_of.end()) {
+                it = cl_of.emplace(gf, clusters->size()).first;
+                clusters->push_back(TList{p.lt, p.t, deg, {}});
+            }
+            (*clusters)[it->second].src.push_back(src);
+            continue;
+        }
         const int64_t span = int64_t(1) << (2 * (leaf_level - p.lt));
-        const ASrc src = (p.far && p.ns > many_count) ? ASrc{1, p.ls, p.s, degree} : ASrc{0, p.ls, p.s, 0};
         for (int64_t lf = p.t * span; lf < (p.t + 1) * span; lf++) lists[lf].push_back(src);
     }
     return lists;
@@ -104,7 +179,8 @@ std::vector<std::vector<ASrc>> lists_per_leaf(const TreeGeometry& g, int leaf_le
     return lists;
 }
 
-void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& lists, ListOutput& out) {
+void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& lists,
+                 const std::vector<TList>& clusters, ListOutput& out) {
     const TreeGeometry& g = *in.g;
     const int LL = in.leaf_level;
     const int64_t nleaf = int64_t(20) << (2 * LL);
@@ -113,52 +189,63 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
     std::map<std::pair<int64_t, int>, int64_t> slot;  // (global face, degree) -> offset
     std::map<int64_t, size_t> job_of;                 // global face -> job index
     std::map<int, std::vector<double>> node_cache;    // degree -> barycentric nodes
-    for (int64_t lf = 0; lf < nleaf; lf++)
-        for (const ASrc& a : lists[lf]) {
-            if (!a.proxy) continue;
-            const int64_t gf = g.lev_off[a.level] + a.node;
-            auto key = std::make_pair(gf, a.deg);
-            if (slot.count(key)) continue;
-            slot[key] = out.n_proxy;
-            auto it = job_of.find(gf);
-            if (it == job_of.end()) {
-                ProxyJob j{};
-                j.level = a.level;
-                j.node = int32_t(gf);
-                j.local = a.node;
-                const int64_t span = int64_t(1) << (2 * (LL - a.level));
-                j.leaf_lo = int32_t(a.node * span);
-                j.leaf_hi = int32_t((a.node + 1) * span);
-                for (int d = 0; d < 12; d++) j.off[d] = -1;
-                job_of[gf] = out.jobs.size();
-                out.jobs.push_back(j);
-                it = job_of.find(gf);
-            }
-            ProxyJob& j = out.jobs[it->second];
-            j.degmask |= 1 << a.deg;
-            j.off[a.deg] = int32_t(in.n + out.n_proxy);
-            out.max_degree = std::max(out.max_degree, a.deg);
-            // proxy positions: y_k = normalise(sum_m l_km v_m)
-            if (!node_cache.count(a.deg)) {
-                std::vector<double> vinv;
-                interp_nodes(a.deg, node_cache[a.deg], vinv);
-            }
-            const std::vector<double>& nodes = node_cache[a.deg];
-            const int K = nproxy(a.deg);
-            const int32_t* tv = &g.tri_verts[3 * gf];
-            const double* v[3] = {&g.verts[3 * int64_t(tv[0])], &g.verts[3 * int64_t(tv[1])], &g.verts[3 * int64_t(tv[2])]};
-            for (int k = 0; k < K; k++) {
-                double y[3];
-                for (int c = 0; c < 3; c++) y[c] = nodes[3 * k] * v[0][c] + nodes[3 * k + 1] * v[1][c] + nodes[3 * k + 2] * v[2][c];
-                const double nn = std::sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
-                out.proxy_pos.push_back(y[0] / nn);
-                out.proxy_pos.push_back(y[1] / nn);
-                out.proxy_pos.push_back(y[2] / nn);
-                out.proxy_pos.push_back(0.0);
-                out.proxy_node.push_back(int32_t(gf));
-            }
-            out.n_proxy += K;
+    // proxy slot of (face, degree), created in first-use order with its
+    // upward-pass job (which writes the slot's positions and charges)
+    auto need_slot = [&](int level, int node, int deg) -> int64_t {
+        const int64_t gf = g.lev_off[level] + node;
+        auto key = std::make_pair(gf, deg);
+        auto found = slot.find(key);
+        if (found != slot.end()) return found->second;
+        slot[key] = out.n_proxy;
+        auto it = job_of.find(gf);
+        if (it == job_of.end()) {
+            ProxyJob j{};
+            j.level = level;
+            j.node = int32_t(gf);
+            j.local = node;
+            const int64_t span = int64_t(1) << (2 * (LL - level));
+            j.leaf_lo = int32_t(node * span);
+            j.leaf_hi = int32_t((node + 1) * span);
+            for (int d = 0; d < 16; d++) j.off[d] = -1;
+            job_of[gf] = out.jobs.size();
+            out.jobs.push_back(j);
+            it = job_of.find(gf);
         }
+        ProxyJob& j = out.jobs[it->second];
+        j.degmask |= 1 << deg;
+        j.off[deg] = int32_t(in.n + out.n_proxy);
+        out.max_degree = std::max(out.max_degree, deg);
+        // proxy positions: y_k = normalise(sum_m l_km v_m)
+        if (!node_cache.count(deg)) {
+            std::vector<double> vinv;
+            interp_nodes(deg, node_cache[deg], vinv);
+        }
+        const std::vector<double>& nodes = node_cache[deg];
+        const int K = nproxy(deg);
+        const int32_t* tv = &g.tri_verts[3 * gf];
+        const double* v[3] = {&g.verts[3 * int64_t(tv[0])], &g.verts[3 * int64_t(tv[1])], &g.verts[3 * int64_t(tv[2])]};
+        for (int k = 0; k < K; k++) {
+            double y[3];
+            for (int c = 0; c < 3; c++) y[c] = nodes[3 * k] * v[0][c] + nodes[3 * k + 1] * v[1][c] + nodes[3 * k + 2] * v[2][c];
+            const double nn = std::sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+            out.proxy_pos.push_back(y[0] / nn);
+            out.proxy_pos.push_back(y[1] / nn);
+            out.proxy_pos.push_back(y[2] / nn);
+            out.proxy_pos.push_back(0.0);
+            out.proxy_node.push_back(int32_t(gf));
+        }
+        const int64_t off = out.n_proxy;
+        out.n_proxy += K;
+        return off;
+    };
+    for (int64_t lf = 0; lf < nleaf; lf++)
+        for (const ASrc& a : lists[lf])
+            if (a.proxy) need_slot(a.level, a.node, a.deg);
+    for (const TList& t : clusters) {
+        need_slot(t.level, t.node, t.deg);
+        for (const ASrc& a : t.src)
+            if (a.proxy) need_slot(a.level, a.node, a.deg);
+    }
     // segments and items
     const int TB = in.threads * in.per_thread;
     const int P = std::max(1, in.parts);
@@ -166,12 +253,13 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
     std::vector<Cost> items;
     std::vector<Segment> sg;
     std::vector<double> est;  // sources per segment at the build
-    for (int64_t lf = 0; lf < nleaf; lf++) {
-        const int32_t nt = in.leaf_start[lf + 1] - in.leaf_start[lf];
-        if (lists[lf].empty() || (nt == 0 && !in.all_leaves)) continue;
+    // segments of one source list for nt targets; `self_leaf` is the target
+    // leaf (-1 for a target cluster); returns pp and proxy pair counts
+    auto make_segments = [&](const std::vector<ASrc>& list, double nt, int64_t self_leaf, double& npp, double& npc) {
         sg.clear();
         est.clear();
-        for (const ASrc& a : lists[lf]) {
+        npp = npc = 0;
+        for (const ASrc& a : list) {
             const int64_t gf = g.lev_off[a.level] + a.node;
             Segment e{};
             double cnt;
@@ -180,7 +268,7 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
                 e.a = int32_t(in.n + slot[std::make_pair(gf, a.deg)]);
                 e.b = e.a + nproxy(a.deg);
                 cnt = nproxy(a.deg);
-                out.pc_pairs += double(nt) * cnt;
+                npc += nt * cnt;
             } else {
                 const int64_t span = int64_t(1) << (2 * (LL - a.level));
                 e.kind = 0;
@@ -189,8 +277,8 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
                 // the particles of a face are contiguous in leaf order
                 const int32_t s0 = in.leaf_start[e.a], s1 = in.leaf_start[e.b];
                 cnt = s1 - s0;
-                const bool self = (lf >= e.a && lf < e.b);
-                out.pp_pairs += double(nt) * cnt - (self ? nt : 0);
+                const bool self = (self_leaf >= e.a && self_leaf < e.b);
+                npp += nt * cnt - (self ? nt : 0);
             }
             if (!sg.empty() && sg.back().kind == e.kind && sg.back().b == e.a) {
                 sg.back().b = e.b;
@@ -200,9 +288,12 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
                 est.push_back(cnt);
             }
         }
+    };
+    // split the current segments into P parts of similar source counts and
+    // queue one item per part
+    auto add_items = [&](int32_t t0, int32_t nt_item, int32_t leaf, int nt_est) {
         const int32_t base = int32_t(out.segs.size());
         out.segs.insert(out.segs.end(), sg.begin(), sg.end());
-        // split the segments into P parts of similar source counts
         double total = 0;
         for (double c : est) total += c;
         std::vector<int32_t> cut(P + 1, int32_t(sg.size()));
@@ -215,19 +306,49 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
                 if (acc >= total * p / P) cut[p++] = int32_t(k + 1);
             }
         }
-        const int chunks = std::max(1, (nt + TB - 1) / TB);
+        const int chunks = std::max(1, (nt_est + TB - 1) / TB);
         for (int p = 0; p < P; p++) {
             double w = 0;
             for (int32_t k = cut[p]; k < cut[p + 1]; k++) w += est[k];
             out.n_tiles += int64_t(chunks) * (int64_t(w + in.tile - 1) / in.tile);
             // a block's run time follows its source count (its warps run
             // side by side), so the longest source lists go first
-            items.push_back({w * chunks, WorkItem{0, 0, base + cut[p], base + cut[p + 1], p, int32_t(lf)}});
+            items.push_back({w * chunks, WorkItem{t0, nt_item, base + cut[p], base + cut[p + 1], p, leaf}});
         }
+    };
+    auto flush_items = [&]() {
+        std::stable_sort(items.begin(), items.end(), [](const Cost& a, const Cost& b) { return a.cost > b.cost; });
+        for (auto& c : items) out.items.push_back(c.it);
+        items.clear();
+    };
+    for (int64_t lf = 0; lf < nleaf; lf++) {
+        const int32_t nt = in.leaf_start[lf + 1] - in.leaf_start[lf];
+        if (lists[lf].empty() || (nt == 0 && !in.all_leaves)) continue;
+        double npp, npc;
+        make_segments(lists[lf], nt, lf, npp, npc);
+        out.pp_pairs += npp;
+        out.pc_pairs += npc;
+        add_items(0, 0, int32_t(lf), nt);
     }
-    std::stable_sort(items.begin(), items.end(), [](const Cost& a, const Cost& b) { return a.cost > b.cost; });
-    out.items.reserve(items.size());
-    for (auto& c : items) out.items.push_back(c.it);
+    flush_items();
+    out.n_leaf_items = int64_t(out.items.size());
+    // target clusters: their interpolation points are the targets
+    if (!clusters.empty()) out.down_of_face.assign(size_t(g.lev_off[LL + 1]), -1);
+    for (const TList& t : clusters) {
+        const int K = nproxy(t.deg);
+        const int64_t gf = g.lev_off[t.level] + t.node;
+        const int32_t s0 = int32_t(in.n + slot[std::make_pair(gf, t.deg)]);
+        double npp, npc;
+        make_segments(t.src, K, -1, npp, npc);
+        out.cp_pairs += npp;
+        out.cc_pairs += npc;
+        add_items(s0, K, -1, K);
+        out.down_of_face[gf] = int32_t(out.down.size());
+        out.down.push_back(DownJob{t.level, int32_t(gf), t.node, t.deg, s0, int32_t(out.n_coef)});
+        out.n_coef += K;
+        out.max_cluster_k = std::max(out.max_cluster_k, K);
+    }
+    flush_items();
 }
 
 // ---------------------------------------------------------------- interpolation

@@ -40,7 +40,7 @@ class Config(C.Structure):
                 ("theta", C.c_double), ("many_count", C.c_int32), ("assign_mode", C.c_int32),
                 ("list_mode", C.c_int32), ("use_graph", C.c_int32), ("src_parts", C.c_int32),
                 ("block_threads", C.c_int32), ("targets_per_thread", C.c_int32), ("autotune", C.c_int32),
-                ("rebuild", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("rebuild", C.c_int32), ("cluster_targets", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class TreeInfo(C.Structure):
@@ -48,7 +48,8 @@ class TreeInfo(C.Structure):
                 ("n_proxy", C.c_int32), ("n_pairs", C.c_int64), ("n_list_entries", C.c_int64),
                 ("n_items", C.c_int64), ("n_tiles", C.c_int64), ("unassigned", C.c_int64), ("pp_interactions", C.c_double),
                 ("pc_interactions", C.c_double), ("block_threads", C.c_int32),
-                ("targets_per_thread", C.c_int32), ("src_parts", C.c_int32), ("pad", C.c_int32)]
+                ("targets_per_thread", C.c_int32), ("src_parts", C.c_int32), ("target_clusters", C.c_int32),
+                ("cp_interactions", C.c_double), ("cc_interactions", C.c_double)]
 
 
 def build():
@@ -72,7 +73,8 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_vorticity_rh4_ref", "fss_vorticity_rh_vortices", "fss_tree_traverse", "fss_interp_nodes",
            "fss_tree_geometry", "fss_rhs_direct_noalloc", "fss_mlp_create", "fss_mlp_destroy",
            "fss_mlp_param_count", "fss_mlp_init", "fss_mlp_set_params", "fss_mlp_get_params", "fss_mlp_set_data",
-           "fss_mlp_gradient", "fss_mlp_train", "fss_mlp_predict", "fss_selector_features", "fss_select_classes",
+           "fss_mlp_gradient", "fss_mlp_train", "fss_mlp_predict", "fss_selector_class_table", "fss_selector_features",
+           "fss_select_classes",
            "fss_selector_apply", "fss_ensemble_create", "fss_ensemble_destroy", "fss_ensemble_set_stream",
            "fss_ensemble_add", "fss_ensemble_build", "fss_ensemble_rk4_step", "fss_ensemble_get_state",
            "fss_ensemble_info", "fss_version"]

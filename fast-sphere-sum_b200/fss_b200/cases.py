@@ -1,7 +1,7 @@
 """Run one fixed case of the library (for profiling and quick checks).
 
     python -m fss_b200.cases rhs  --level 8 --precision mixed [--repeat 2]
-    python -m fss_b200.cases rk4  --level 8 --precision mixed --steps 2
+    python -m fss_b200.cases rk4  --level 8 --precision mixed --steps 2 [--learned]
     python -m fss_b200.cases direct --level 6 --precision mixed
     python -m fss_b200.cases ensemble --members 64 --steps 20
 
@@ -9,6 +9,9 @@ The ensemble case: members on icosahedral levels drawn uniformly from 5-8,
 each an RH R=4 wave with a seeded +-5% amplitude perturbation and 4-16
 Gaussian vortices; mixed-precision BLTC n=8, theta=0.7; one CUDA graph per
 RK4 step for all members.
+
+--learned: per-leaf interaction lists with the learned per-leaf (degree,
+theta) choice (tolerance 1e-6, safety 2) and the autotuned block shape.
 
 Inputs: icosahedral grid of the given level, RH4 wave + seeded vortices.
 Prints one line with the wall time; exits non-zero on any library error.
@@ -34,6 +37,7 @@ def main(argv=None):
     p.add_argument("--repeat", type=int, default=2)
     p.add_argument("--vortices", type=int, default=32)
     p.add_argument("--no-graph", action="store_true")
+    p.add_argument("--learned", action="store_true")
     a = p.parse_args(argv)
     prec = PREC_MIXED if a.precision == "mixed" else PREC_FP64
     if a.case == "ensemble":
@@ -41,9 +45,13 @@ def main(argv=None):
     s, area = make_state(a.level, "rh_vortices", n_vortex=a.vortices, seed=2)
     method = METHOD_DIRECT if a.case == "direct" else METHOD_TREECODE
     t0 = time.perf_counter()
+    extra = dict(list_mode=1, autotune=1) if a.learned else {}
     with Context(method=method, precision=prec, degree=a.degree, theta=a.theta,
-                 use_graph=0 if a.no_graph else 1) as ctx:
+                 use_graph=0 if a.no_graph else 1, **extra) as ctx:
         ctx.set_particles(s, area)
+        if a.learned:
+            from . import selector
+            selector.apply(ctx, tol=1e-6, safety=2.0)
         if a.case == "rk4":
             ctx.rk4_step(0.01, nsteps=a.steps)
             out = ctx.get_state()

@@ -11,13 +11,17 @@ from the treecode itself: for each class, every leaf runs that class in
 mixed precision, and the result is compared with the FP64 direct sum on the
 GPU.
 
-    python -m fss_b200.selector gen   --out sel_data.npz [--fields 24]
+    python -m fss_b200.selector gen   --out sel_data.npz [--fields 24] [--clusters]
     python -m fss_b200.selector train --data sel_data.npz --out selector_weights.npz
-    python -m fss_b200.selector eval  --weights selector_weights.npz --level 8 --seed 999
+    python -m fss_b200.selector eval  --weights selector_weights.npz --level 8 --seed 999 [--clusters]
 
-The trained weights used by default sit beside this file
-(``selector_weights.npz``); they carry the feature standardisation and the
-training record.
+Two networks: one for target-leaf evaluation (every far source summed at
+the particles, per-leaf traversal) and one for target clusters (the
+reference's cp/cc types; the per-leaf choices are carried up to the faces
+of a dual traversal), each trained on labels of its own mode.  The trained
+weights used by default sit beside this file (``selector_weights.npz``,
+``selector_weights_clusters.npz``); they carry the feature standardisation
+and the training record.
 """
 import argparse
 import ctypes as C
@@ -27,14 +31,24 @@ import time
 
 import numpy as np
 
-from . import (FssError, LIST_LEAF, METHOD_DIRECT, METHOD_TREECODE, PREC_FP64, PREC_MIXED, Context, RH_AMP,
+from . import (FssError, LIST_DUAL, LIST_LEAF, METHOD_DIRECT, METHOD_TREECODE, PREC_FP64, PREC_MIXED, Context, RH_AMP,
                _check, lib, make_state)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "selector_weights.npz")
+WEIGHTS_CLUSTERS = os.path.join(HERE, "selector_weights_clusters.npz")
 NCLS, NFEAT = 12, 16
-DEGREES = [4 + 2 * (c // 3) for c in range(NCLS)]
-THETAS = [0.5 + 0.1 * (c % 3) for c in range(NCLS)]
+
+
+def class_table(clusters=False):
+    """(degrees, thetas) of the 12 classes, c = 3 i + j: n = 4 + 2i, theta =
+    0.5 + 0.1 j for target-leaf evaluation; n = 6 + 2i, theta = 0.7 + 0.1 j
+    with target clusters."""
+    n0, t0 = (6, 0.7) if clusters else (4, 0.5)
+    return [n0 + 2 * (c // 3) for c in range(NCLS)], [t0 + 0.1 * (c % 3) for c in range(NCLS)]
+
+
+DEGREES, THETAS = class_table(False)
 FLOOR = 1e-12  # labels below this relative error carry no information
 _vp = C.c_void_p
 
@@ -57,6 +71,7 @@ def _setup():
     L.fss_mlp_predict.argtypes = [_vp, C.c_int64, _vp, _vp]
     L.fss_selector_features.argtypes = [_vp, _vp, _vp, P(C.c_double)]
     L.fss_select_classes.argtypes = [C.c_int64, C.c_int32, _vp, _vp, C.c_double, _vp]
+    L.fss_selector_class_table.argtypes = [C.c_int32, _vp, _vp]
     L.fss_selector_apply.argtypes = [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp]
     L._sel_ready = True
     return L
@@ -161,17 +176,23 @@ def field(level, seed, n_vortex, amp_scale=1.0):
     return s, a
 
 
-def label_field(s, a, device=0):
-    """Features, costs and per-class log errors of every leaf of one field."""
+def default_weights(clusters):
+    return WEIGHTS_CLUSTERS if clusters else WEIGHTS
+
+
+def label_field(s, a, device=0, clusters=False):
+    """Features, costs and per-class log errors of every leaf of one field
+    (target-leaf evaluation, or target clusters with `clusters`)."""
     with Context(method=METHOD_DIRECT, precision=PREC_FP64, device=device) as d:
         d.set_particles(s, a)
         uref = d.rhs(s, a)[:, :3]
     U = float(np.sqrt(np.mean(np.sum(uref ** 2, 1))))
     y = None
     X = K = None
+    degrees, thetas = class_table(clusters)
     for c in range(NCLS):
-        with Context(method=METHOD_TREECODE, precision=PREC_MIXED, list_mode=LIST_LEAF, degree=DEGREES[c],
-                     theta=THETAS[c], device=device) as ctx:
+        with Context(method=METHOD_TREECODE, precision=PREC_MIXED, list_mode=LIST_DUAL if clusters else LIST_LEAF,
+                     cluster_targets=int(clusters), degree=degrees[c], theta=thetas[c], device=device) as ctx:
             ctx.set_particles(s, a)
             if X is None:
                 X, K, _ = features(ctx)
@@ -185,7 +206,7 @@ def label_field(s, a, device=0):
     return X, y, K, counts
 
 
-def generate(out, fields, seed0=100, levels=(7, 8), device=0, log=print):
+def generate(out, fields, seed0=100, levels=(7, 8), device=0, log=print, clusters=False):
     """Training set from `fields` seeded fields alternating over `levels`."""
     rng = np.random.default_rng(seed0)
     Xs, Ys, Ks, Ns, meta = [], [], [], [], []
@@ -196,10 +217,11 @@ def generate(out, fields, seed0=100, levels=(7, 8), device=0, log=print):
         amp = float(rng.uniform(0.95, 1.05))
         seed = seed0 + i
         s, a = field(level, seed, nv, amp)
-        X, y, K, cnt = label_field(s, a, device)
+        X, y, K, cnt = label_field(s, a, device, clusters)
         keep = cnt > 0
         Xs.append(X[keep]); Ys.append(y[keep]); Ks.append(K[keep]); Ns.append(cnt[keep])
-        meta.append(dict(level=level, seed=seed, n_vortex=nv, amp_scale=amp, leaves=int(keep.sum())))
+        meta.append(dict(level=level, seed=seed, n_vortex=nv, amp_scale=amp, leaves=int(keep.sum()),
+                         clusters=bool(clusters)))
         log(f"field {i}: level {level} seed {seed} vortices {nv} leaves {int(keep.sum())} ({time.time() - t0:.0f}s)")
     np.savez_compressed(out, X=np.concatenate(Xs), Y=np.concatenate(Ys), K=np.concatenate(Ks),
                         N=np.concatenate(Ns), meta=json.dumps(meta))
@@ -235,11 +257,12 @@ def load(path=WEIGHTS):
     return w["params"].astype(np.float32), w["mean"].astype(np.float32), w["std"].astype(np.float32)
 
 
-def apply(ctx, tol=1e-6, safety=2.0, weights=WEIGHTS, device=0):
-    """Choose per-leaf (n, theta) for `ctx` and switch it to per-leaf lists.
-    Returns the class index of every leaf."""
+def apply(ctx, tol=1e-6, safety=2.0, weights=None, device=0):
+    """Choose per-leaf (n, theta) for `ctx` and switch it to per-leaf lists
+    (with target clusters, when the context has them: the network of that
+    mode).  Returns the class index of every leaf."""
     L = _setup()
-    params, mean, std = load(weights)
+    params, mean, std = load(weights or default_weights(bool(ctx.cfg.cluster_targets)))
     m = MLP(device=device, params=params)
     nleaf = ctx.tree_info()["leaf_count"]
     choice = np.zeros(nleaf, dtype=np.int32)
@@ -265,47 +288,52 @@ def main(argv=None):
     g.add_argument("--out", default="sel_data.npz")
     g.add_argument("--fields", type=int, default=24)
     g.add_argument("--seed", type=int, default=100)
+    g.add_argument("--clusters", action="store_true")
     t = sub.add_parser("train")
     t.add_argument("--data", default="sel_data.npz")
     t.add_argument("--out", default=WEIGHTS)
     t.add_argument("--epochs", type=int, default=60)
     t.add_argument("--lr", type=float, default=2e-3)
     e = sub.add_parser("eval")
-    e.add_argument("--weights", default=WEIGHTS)
+    e.add_argument("--weights", default=None)
+    e.add_argument("--clusters", action="store_true")
     e.add_argument("--level", type=int, default=8)
     e.add_argument("--seed", type=int, default=999)
     e.add_argument("--tol", type=float, default=1e-6)
     e.add_argument("--safety", type=float, default=2.0)
     a = ap.parse_args(argv)
     if a.cmd == "gen":
-        generate(a.out, a.fields, a.seed)
+        generate(a.out, a.fields, a.seed, clusters=a.clusters)
     elif a.cmd == "train":
         train(a.data, a.out, epochs=a.epochs, lr=a.lr)
     else:
-        print(json.dumps(evaluate(a.weights, a.level, a.seed, a.tol, a.safety)))
+        print(json.dumps(evaluate(a.weights or default_weights(a.clusters), a.level, a.seed, a.tol, a.safety,
+                                  clusters=a.clusters)))
 
 
-def evaluate(weights, level, seed, tol=1e-6, safety=2.0, n_vortex=32, device=0):
-    """Interactions and error of the selector against fixed n=8, theta=0.7."""
+def evaluate(weights, level, seed, tol=1e-6, safety=2.0, n_vortex=32, device=0, clusters=False):
+    """Interactions and error of the selector against fixed n=8, theta=0.7
+    (both with target clusters when `clusters`)."""
     s, a = field(level, seed, n_vortex)
     with Context(method=METHOD_DIRECT, precision=PREC_FP64, device=device) as d:
         d.set_particles(s, a)
         uref = d.rhs(s, a)[:, :3]
     nref = np.linalg.norm(uref)
     out = {}
-    with Context(method=METHOD_TREECODE, precision=PREC_MIXED, degree=8, theta=0.7, device=device) as c:
+    def work(i):
+        return i["pp_interactions"] + i["pc_interactions"] + i["cp_interactions"] + i["cc_interactions"]
+
+    with Context(method=METHOD_TREECODE, precision=PREC_MIXED, degree=8, theta=0.7, cluster_targets=int(clusters),
+                 device=device) as c:
         c.set_particles(s, a)
         u = c.rhs(s, a)[:, :3]
-        i = c.tree_info()
-        out["fixed"] = dict(rel_l2=float(np.linalg.norm(u - uref) / nref),
-                            interactions=i["pp_interactions"] + i["pc_interactions"])
-    with Context(method=METHOD_TREECODE, precision=PREC_MIXED, list_mode=LIST_LEAF, device=device) as c:
+        out["fixed"] = dict(rel_l2=float(np.linalg.norm(u - uref) / nref), interactions=work(c.tree_info()))
+    with Context(method=METHOD_TREECODE, precision=PREC_MIXED, list_mode=LIST_LEAF, cluster_targets=int(clusters),
+                 device=device) as c:
         c.set_particles(s, a)
         choice = apply(c, tol=tol, safety=safety, weights=weights, device=device)
         u = c.rhs(s, a)[:, :3]
-        i = c.tree_info()
-        out["learned"] = dict(rel_l2=float(np.linalg.norm(u - uref) / nref),
-                              interactions=i["pp_interactions"] + i["pc_interactions"],
+        out["learned"] = dict(rel_l2=float(np.linalg.norm(u - uref) / nref), interactions=work(c.tree_info()),
                               classes=np.bincount(choice, minlength=NCLS).tolist())
     out["interaction_ratio"] = out["fixed"]["interactions"] / out["learned"]["interactions"]
     return out

@@ -102,7 +102,16 @@ typedef struct fss_config {
     int32_t autotune;      /* at fss_set_particles, time every supported block
                               shape on the actual lists and keep the fastest */
     int32_t rebuild;       /* fss_rebuild_policy */
-    int32_t reserved[5];
+    int32_t cluster_targets; /* 1 = the reference's cp/cc interaction types
+                              (fast_rhs.h cp, cc): a well-separated target face
+                              holding more than many_count particles takes its
+                              far sources at its interpolation points,
+                              interpolated down to its particles; 0 = every far
+                              source is summed at the target particles.  With
+                              FSS_LIST_LEAF the per-leaf (n, theta) are carried
+                              up to the faces of a dual traversal (theta = min,
+                              n = max over a face's leaves) */
+    int32_t reserved[4];
 } fss_config;
 
 typedef struct fss_ctx fss_ctx;
@@ -168,7 +177,9 @@ typedef struct fss_tree_info {
     int32_t block_threads;   /* pair-kernel block shape in use */
     int32_t targets_per_thread;
     int32_t src_parts;
-    int32_t pad;
+    int32_t target_clusters; /* faces evaluated at interpolation points (cp/cc) */
+    double cp_interactions;  /* interpolation point-particle pairs per RHS */
+    double cc_interactions;  /* interpolation point-proxy pairs per RHS */
 } fss_tree_info;
 int fss_get_tree_info(fss_ctx* ctx, fss_tree_info* info);
 
@@ -191,8 +202,8 @@ int fss_profile_enable(fss_ctx* ctx, int32_t on);
  * the number of kernels through *count. */
 int fss_profile_read(fss_ctx* ctx, char* names, int32_t names_cap, double* ms, int64_t* launches,
                      int32_t cap, int32_t* count);
-/* Algorithmic work of one RHS evaluation: pair interactions (23 flops each),
- * and bytes of the upward pass. */
+/* Algorithmic work of one RHS evaluation: pair interactions (23 flops each;
+ * pp + pc + cp + cc), and bytes of the upward pass. */
 int fss_work_per_rhs(fss_ctx* ctx, double* interactions, double* upward_bytes);
 
 /* ----------------------------------------------------------------- inputs
@@ -280,8 +291,14 @@ int fss_mlp_gradient(fss_mlp* m, float* grad, double* loss);
  * batch loss per epoch into losses[epochs]. */
 int fss_mlp_train(fss_mlp* m, int32_t epochs, int32_t batch, double lr, uint64_t seed, double* losses);
 int fss_mlp_predict(fss_mlp* m, int64_t n, const float* x, float* y);
+/* The 12 classes (degree, theta) of class c = 3 i + j: with clusters = 0
+ * (far sources summed at the target particles) n = 4 + 2i, theta = 0.5 +
+ * 0.1j; with clusters = 1 (target clusters, cp/cc) n = 6 + 2i, theta = 0.7 +
+ * 0.1j.  Host only. */
+int fss_selector_class_table(int32_t clusters, int32_t* degree, double* theta);
 /* Features (16 per leaf) and exact interaction counts (12 per leaf, one per
- * class) of the current tree and state, and the RMS speed U. */
+ * class of the context's mode) of the current tree and state, and the RMS
+ * speed U. */
 int fss_selector_features(fss_ctx* ctx, float* features, double* costs, double* u_rms);
 /* Per leaf the class minimising cost + mu * 10^(2 y) with mu chosen by
  * bisection so that sum_l 10^(2 y_l) <= budget (host only). */
@@ -289,8 +306,8 @@ int fss_select_classes(int64_t nleaf, int32_t nclass, const double* pred_log_err
                        double budget, int32_t* choice);
 /* Predict with `m` (features standardised with mean/std), choose classes
  * for a relative L2 tolerance tol (budget (tol/safety)^2 N), switch the
- * context to per-leaf lists with those parameters.  choice_out: nleaf ints
- * (nullable). */
+ * context to per-leaf parameters (FSS_LIST_LEAF; with cluster_targets the
+ * per-face dual traversal).  choice_out: nleaf ints (nullable). */
 int fss_selector_apply(fss_ctx* ctx, fss_mlp* m, const float* feat_mean, const float* feat_std, double tol,
                        double safety, int32_t* choice_out);
 

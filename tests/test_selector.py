@@ -90,3 +90,36 @@ def test_selector_gain_over_fixed_degree(fss):
     assert r["learned"]["rel_l2"] <= 1e-6, r
     assert r["fixed"]["rel_l2"] <= 1e-6, r
     assert r["interaction_ratio"] > 1.0, r
+
+
+def test_class_tables_agree_with_library(fss):
+    from fss_b200 import selector as S
+    L = S._setup()
+    for clusters in (0, 1):
+        deg = np.zeros(12, dtype=np.int32)
+        th = np.zeros(12)
+        assert L.fss_selector_class_table(clusters, S._p(deg), S._p(th)) == 0
+        d_py, t_py = S.class_table(bool(clusters))
+        assert deg.tolist() == d_py and th.tolist() == t_py
+
+
+def test_cluster_weights_file_is_consistent(fss):
+    from fss_b200 import selector as S
+    if not os.path.exists(S.WEIGHTS_CLUSTERS):
+        pytest.skip("no trained weights")
+    p, mean, std = S.load(S.WEIGHTS_CLUSTERS)
+    assert p.shape == (6028,) and np.all(np.isfinite(p)) and np.all(std > 0)
+
+
+@pytest.mark.gpu
+def test_selector_gain_with_target_clusters(fss):
+    """Target clusters (cp/cc): the learned per-leaf (n, theta) carried up to
+    the faces keeps rel-L2 <= 1e-6 with fewer interactions than the fixed
+    n = 8, theta = 0.7 evaluation with target clusters, on a field outside
+    the training set."""
+    from fss_b200 import selector as S
+    if not os.path.exists(S.WEIGHTS_CLUSTERS):
+        pytest.skip("no trained weights")
+    r = S.evaluate(S.WEIGHTS_CLUSTERS, level=8, seed=4243, tol=1e-6, safety=2.0, n_vortex=24, clusters=True)
+    assert r["learned"]["rel_l2"] <= 1e-6, r
+    assert r["interaction_ratio"] > 1.0, r
