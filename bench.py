@@ -188,8 +188,9 @@ def time_steps(ctx, stream, steps, flush):
 
 
 def make_arm(fss, state, area, stream, prec, args, dev, clusters=False):
+    """Fixed degree/theta treecode; block shape chosen by the autotuner."""
     ctx = fss.Context(method=fss.METHOD_TREECODE, precision=prec, degree=args.degree, theta=args.theta,
-                      cluster_targets=int(clusters), device=dev)
+                      cluster_targets=int(clusters), device=dev, autotune=1)
     ctx.set_stream(stream.cuda_stream)
     ctx.set_particles(state, area)
     return ctx

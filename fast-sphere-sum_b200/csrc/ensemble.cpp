@@ -78,8 +78,8 @@ int eupload(fss_ensemble* e, DBuf& b, const std::vector<T>& v) {
 // Every member's particles into the leaves they are in now.
 int resort(fss_ensemble* e) {
     const int64_t n = e->ntot;
-    launch_reassign(e->stream, n, e->s0.as<double4>(), e->leaves.as<EnsLeaf>(), 0, e->verts.as<double>(),
-                    e->tri_verts.as<int32_t>(), e->lev_off.as<int64_t>(), e->key.as<uint32_t>());
+    launch_reassign(e->stream, n, e->s0.as<double4>(), e->leaves.as<EnsLeaf>(), 0, e->node.as<NodeGeom>(),
+                    e->lev_off.as<int64_t>(), e->key.as<uint32_t>());
     int bits = 0;
     while ((int64_t(1) << bits) < e->nleaf) bits++;
     launch_sort(e->stream, n, std::max(bits, 1), e->key.as<uint32_t>(), e->key_tmp.as<uint32_t>(),

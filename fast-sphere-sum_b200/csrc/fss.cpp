@@ -134,7 +134,7 @@ int src_size_ensure(fss_ctx* c, int64_t count) {
 int build_direct_lists(fss_ctx* c) {
     const int64_t n = c->n;
     c->shape = pairs_shape(c->fp64, c->cfg.block_threads, c->cfg.targets_per_thread);
-    const int TB = c->shape.threads * c->shape.per_thread;
+    const int TB = c->shape.targets();
     const int64_t tiles = (n + TB - 1) / TB;
     int P = c->cfg.src_parts;
     if (P <= 0) {
@@ -352,14 +352,14 @@ int build_tree(fss_ctx* c) {
 }
 
 // Block shape for the treecode's pair kernel: the configured one, or the
-// smallest supported block whose targets cover the largest leaf (so that
-// no leaf spills a tail block).
+// smallest supported block whose consumer threads cover the largest leaf (so
+// that no leaf needs a second chunk).
 PairShape choose_shape(fss_ctx* c) {
     if (c->cfg.block_threads > 0) return pairs_shape(c->fp64, c->cfg.block_threads, c->cfg.targets_per_thread);
     int maxleaf = 1;
     for (int64_t l = 0; l < c->nleaf; l++) maxleaf = std::max(maxleaf, c->leaf_start_h[l + 1] - c->leaf_start_h[l]);
     for (const PairShape& sh : pair_shapes(c->fp64))
-        if (sh.per_thread == 1 && sh.threads >= maxleaf) return sh;
+        if (sh.per_thread == 1 && sh.targets() >= maxleaf) return sh;
     return pair_shapes(c->fp64).back();
 }
 
@@ -375,8 +375,8 @@ int materialize(fss_ctx* c, PairShape shape) {
     in.n = n;
     in.leaf_start = c->leaf_start_h.data();
     in.tile = shape.tile;
-    in.threads = shape.threads;
-    in.per_thread = shape.per_thread;
+    in.threads = shape.targets();
+    in.per_thread = 1;
     int P = c->cfg.src_parts;
     if (P <= 0) {
         int64_t chunks = 0;
@@ -398,15 +398,23 @@ int materialize(fss_ctx* c, PairShape shape) {
         for (int d = 0; d <= kMaxDegree; d++)
             if ((j.degmask >> d) & 1) c->nmax = std::max(c->nmax, d);
     }
-    std::vector<double> vinv_all;
-    std::vector<int32_t> vinv_off(kMaxDegree + 1, 0);
+    std::vector<double> vinv_all, vinvT_all, bary_all;
+    std::vector<int32_t> vinv_off(kMaxDegree + 1, 0), bary_off(kMaxDegree + 1, 0);
     for (int d = 0; d <= c->nmax; d++) {
         std::vector<double> nodes, vi;
         interp_nodes(d, nodes, vi);
         vinv_off[d] = int32_t(vinv_all.size());
         vinv_all.insert(vinv_all.end(), vi.begin(), vi.end());
+        const int K = nproxy(d);
+        for (int k = 0; k < K; k++)
+            for (int m = 0; m < K; m++) vinvT_all.push_back(vi[size_t(m) * K + k]);
+        bary_off[d] = int32_t(bary_all.size());
+        bary_all.insert(bary_all.end(), nodes.begin(), nodes.end());
     }
     TRY(upload(c, c->vinv, vinv_all));
+    TRY(upload(c, c->vinvT, vinvT_all));
+    TRY(upload(c, c->bary, bary_all));
+    TRY(upload(c, c->bary_off, bary_off));
     TRY(upload(c, c->vinv_off, vinv_off));
     TRY(upload(c, c->segs, L.segs));
     TRY(upload(c, c->items, L.items));
@@ -467,12 +475,30 @@ int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
     }
     const bool down = c->tree && !c->lists.down.empty();
     if (down) {
-        ProfScope ps(c, "downward", 2);
-        launch_down(c->stream, want_psi, int(c->lists.down.size()), c->down_jobs.as<DownJob>(), c->partials.as<double4>(),
-                    c->parts, c->pstride, c->vinv.as<double>(), c->vinv_off.as<int32_t>(), c->down_coef.as<double4>(),
-                    int(c->nleaf), c->xs.as<double4>(), c->leaf_start.as<int32_t>(), c->node.as<NodeGeom>(),
-                    c->lev_off.as<int64_t>(), c->leaf_level, c->down_of_face.as<int32_t>(),
-                    c->partials.as<double4>() + int64_t(c->parts) * c->pstride);
+        DownArgs d;
+        d.njobs = int(c->lists.down.size());
+        d.jobs = c->down_jobs.as<DownJob>();
+        d.level_off = c->lists.down_level_off.data();
+        d.partials = c->partials.as<double4>();
+        d.parts = c->parts;
+        d.pstride = c->pstride;
+        d.vinvT = c->vinvT.as<double>();
+        d.vinv_off = c->vinv_off.as<int32_t>();
+        d.bary = c->bary.as<double>();
+        d.bary_off = c->bary_off.as<int32_t>();
+        d.verts = c->verts.as<double>();
+        d.tri_verts = c->tri_verts.as<int32_t>();
+        d.node = c->node.as<NodeGeom>();
+        d.coef = c->down_coef.as<double4>();
+        d.nleaf = int(c->nleaf);
+        d.leaf_level = c->leaf_level;
+        d.leaf_off = c->geom.lev_off[c->leaf_level];
+        d.xs = c->xs.as<double4>();
+        d.leaf_start = c->leaf_start.as<int32_t>();
+        d.down_of_face = c->down_of_face.as<int32_t>();
+        d.out = c->partials.as<double4>() + int64_t(c->parts) * c->pstride;
+        ProfScope ps(c, "downward", down_launch_count(d));
+        launch_down(c->stream, want_psi, d);
     }
     if (want_psi) launch_wsum(c->stream, c->n, c->xs.as<double4>(), c->area_s.as<double>(), c->wtotal.as<double>());
     ea.n = c->n;
@@ -543,8 +569,8 @@ int resort(fss_ctx* c) {
     // reassign, 3 per 8-bit sort pass, gather + commit, leaf bounds
     ProfScope ps(c, "resort", 1 + 3 * ((bits + 7) / 8) + 2 + 1);
     const int64_t n = c->n;
-    launch_reassign(c->stream, n, c->s0.as<double4>(), nullptr, c->leaf_level, c->verts.as<double>(),
-                    c->tri_verts.as<int32_t>(), c->lev_off.as<int64_t>(), c->key.as<uint32_t>());
+    launch_reassign(c->stream, n, c->s0.as<double4>(), nullptr, c->leaf_level, c->node.as<NodeGeom>(),
+                    c->lev_off.as<int64_t>(), c->key.as<uint32_t>());
     launch_sort(c->stream, n, bits, c->key.as<uint32_t>(), c->key_tmp.as<uint32_t>(),
                 c->sortq.as<int32_t>(), c->vals_tmp.as<int32_t>(), c->hist.as<uint32_t>());
     launch_resort(c->stream, c->fp64, n, c->sortq.as<int32_t>(), c->s0.as<double4>(), c->area_s.as<double>(),

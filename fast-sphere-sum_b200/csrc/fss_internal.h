@@ -66,15 +66,18 @@ struct EnsLeaf {
     int64_t part_base;
 };
 
-// Downward pass of a target cluster: a face that receives far sources at
-// its K = nproxy(deg) interpolation points (fast_rhs.h cp and cc).  The
-// field there (unified indices [slot, slot + K)) becomes coefficients of the
-// Chebyshev product basis (K double4 from `coef`), evaluated at every
-// particle of the face.
+// Downward pass: a face that receives far sources at its K = nproxy(deg)
+// interpolation points (a target cluster, fast_rhs.h cp and cc; slot >= 0:
+// unified indices [slot, slot + K)), or a face below one (slot = -1).  Its
+// field is held as coefficients of the Chebyshev product basis (K double4
+// from `coef`): its own points' values, plus its parent's polynomial
+// re-interpolated at its points (parent = job index, -1 at the top).
 struct DownJob {
     int32_t level, node, local, deg;  // node = global face index
-    int32_t slot;                     // first interpolation point (unified index)
+    int32_t slot;                     // first own interpolation point (unified index), or -1
     int32_t coef;                     // first coefficient (double4 units)
+    int32_t parent;                   // parent's job, or -1
+    int32_t pad;
 };
 
 // Per-node geometry for the upward pass: inverse of [v1 v2 v3] (columns),

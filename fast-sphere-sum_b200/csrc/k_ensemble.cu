@@ -5,65 +5,29 @@
 
 #include "device_common.cuh"
 #include "kernels.h"
+#include "moments.cuh"
 
 namespace fss {
 
 // Upward pass over the leaves of every member.  Leaf g: particles
 // [leaf_start[g], leaf_start[g+1]) of the concatenated arrays (current after
 // each re-sort), leaf level LL, index within its member's leaf level, and
-// the start of its moment slots (LL + 1 levels x KM).
-__global__ void __launch_bounds__(128) k_up_leaf_batch(const float4* __restrict__ src, const EnsLeaf* __restrict__ leaves,
+// the start of its moment slots (LL + 1 levels x KM); moments as for one
+// problem (leaf_moments).
+__global__ void __launch_bounds__(kUpThreads) k_up_leaf_batch(const float4* __restrict__ src, const EnsLeaf* __restrict__ leaves,
                                                        const int32_t* __restrict__ leaf_start,
                                                        const NodeGeom* __restrict__ node,
                                                        const int64_t* __restrict__ lev_off, int nmax,
                                                        double* __restrict__ part) {
-    __shared__ double Tw[128][kMaxDegree + 1];
-    __shared__ double Tv[128][kMaxDegree + 1];
+    __shared__ double W[kUpRows][kUpLd];
+    __shared__ double V[kUpRows][kUpLd];
     const EnsLeaf lf = leaves[blockIdx.x];
     const int a0 = leaf_start[lf.gleaf], a1 = leaf_start[lf.gleaf + 1];
-    const int tid = threadIdx.x;
     const int KM = nproxy(nmax);
-    int ma = 0, mb = 0;
-    if (tid < KM) {
-        int g = 0;
-        while ((g + 1) * (g + 2) / 2 <= tid) g++;
-        mb = tid - g * (g + 1) / 2;
-        ma = g - mb;
-    }
     for (int l = 0; l <= lf.leaf_level; l++) {
-        double* out = part + lf.part_base + int64_t(l) * KM;
         if (!((lf.level_mask >> l) & 1)) continue;
         const NodeGeom ng = node[lev_off[l] + (lf.local >> (2 * (lf.leaf_level - l)))];
-        double acc = 0;
-        for (int c0 = a0; c0 < a1; c0 += 128) {
-            const int j = c0 + tid;
-            if (j < a1) {
-                const float4 q = src[j];
-                const double x = q.x, y = q.y, z = q.z, w = q.w;
-                const double c0_ = ng.minv[0] * x + ng.minv[1] * y + ng.minv[2] * z;
-                const double c1_ = ng.minv[3] * x + ng.minv[4] * y + ng.minv[5] * z;
-                const double c2_ = ng.minv[6] * x + ng.minv[7] * y + ng.minv[8] * z;
-                const double inv = 1.0 / (c0_ + c1_ + c2_);
-                const double u = 2.0 * (c0_ * inv) - 1.0, v = 2.0 * (c1_ * inv) - 1.0;
-                double ta0 = 1.0, ta1 = u, tb0 = 1.0, tb1 = v;
-                Tw[tid][0] = w;
-                Tv[tid][0] = 1.0;
-                if (nmax >= 1) { Tw[tid][1] = w * u; Tv[tid][1] = v; }
-                for (int a = 2; a <= nmax; a++) {
-                    const double ta2 = 2.0 * u * ta1 - ta0, tb2 = 2.0 * v * tb1 - tb0;
-                    Tw[tid][a] = w * ta2;
-                    Tv[tid][a] = tb2;
-                    ta0 = ta1; ta1 = ta2; tb0 = tb1; tb1 = tb2;
-                }
-            }
-            __syncthreads();
-            if (tid < KM) {
-                const int cnt = min(128, a1 - c0);
-                for (int jj = 0; jj < cnt; jj++) acc = fma(Tw[jj][ma], Tv[jj][mb], acc);
-            }
-            __syncthreads();
-        }
-        if (tid < KM) out[tid] = acc;
+        leaf_moments<float>(src, a0, a1, 0.0, 0.0, 0.0, ng, nmax, W, V, part + lf.part_base + int64_t(l) * KM);
     }
 }
 

@@ -4,6 +4,7 @@
 
 #include "device_common.cuh"
 #include "kernels.h"
+#include "moments.cuh"
 
 namespace fss {
 
@@ -13,10 +14,9 @@ namespace fss {
 // with b_j the barycentric coordinates of the central projection of x_j on
 // S's plane and phi_m = T_a(2 b1 - 1) T_b(2 b2 - 1), a + b <= n.  The moments
 // M_m = sum_j w_j phi_m(b_j) are formed per leaf for every ancestor frame
-// (kernel 1, one block per leaf, particles read once per level), summed over
-// the leaves of each face and contracted with Vinv (kernel 2).  FP64.
-
-constexpr int kUpThreads = 128;
+// (kernel 1, one block per leaf, a small FP64 tensor-core contraction per
+// level), summed over the leaves of each face and contracted with Vinv
+// (kernel 2).  FP64.
 
 template <typename T>
 __global__ void __launch_bounds__(kUpThreads) k_up_leaf(const typename Vec4<T>::type* __restrict__ src,
@@ -25,58 +25,21 @@ __global__ void __launch_bounds__(kUpThreads) k_up_leaf(const typename Vec4<T>::
                                                         const NodeGeom* __restrict__ node,
                                                         const int64_t* __restrict__ lev_off, int leaf_level,
                                                         int nmax, int level_mask, double* __restrict__ part) {
-    __shared__ double Tw[kUpThreads][kMaxDegree + 1];
-    __shared__ double Tv[kUpThreads][kMaxDegree + 1];
-    const int leaf = blockIdx.x, tid = threadIdx.x;
+    __shared__ double W[kUpRows][kUpLd];
+    __shared__ double V[kUpRows][kUpLd];
+    const int leaf = blockIdx.x;
     const int KM = nproxy(nmax);
     const int a0 = leaf_start[leaf], a1 = leaf_start[leaf + 1];
-    // basis index m -> (a, b): m = g (g + 1) / 2 + b, a = g - b
-    int ma = 0, mb = 0;
-    if (tid < KM) {
-        int g = 0;
-        while ((g + 1) * (g + 2) / 2 <= tid) g++;
-        mb = tid - g * (g + 1) / 2;
-        ma = g - mb;
-    }
     double fx = 0, fy = 0, fz = 0;
     if (frame) {
         const double4 f = frame[leaf];
         fx = f.x; fy = f.y; fz = f.z;
     }
     for (int l = 0; l <= leaf_level; l++) {
-        double* out = part + (int64_t(leaf) * (leaf_level + 1) + l) * KM;
         if (!((level_mask >> l) & 1)) continue;
         const NodeGeom ng = node[lev_off[l] + (leaf >> (2 * (leaf_level - l)))];
-        double acc = 0;
-        for (int c0 = a0; c0 < a1; c0 += kUpThreads) {
-            const int j = c0 + tid;
-            if (j < a1) {
-                const typename Vec4<T>::type q = src[j];
-                const double x = fx + double(q.x), y = fy + double(q.y), z = fz + double(q.z), w = double(q.w);
-                const double c0_ = ng.minv[0] * x + ng.minv[1] * y + ng.minv[2] * z;
-                const double c1_ = ng.minv[3] * x + ng.minv[4] * y + ng.minv[5] * z;
-                const double c2_ = ng.minv[6] * x + ng.minv[7] * y + ng.minv[8] * z;
-                const double inv = 1.0 / (c0_ + c1_ + c2_);
-                const double u = 2.0 * (c0_ * inv) - 1.0, v = 2.0 * (c1_ * inv) - 1.0;
-                double ta0 = 1.0, ta1 = u, tb0 = 1.0, tb1 = v;
-                Tw[tid][0] = w;
-                Tv[tid][0] = 1.0;
-                if (nmax >= 1) { Tw[tid][1] = w * u; Tv[tid][1] = v; }
-                for (int a = 2; a <= nmax; a++) {
-                    const double ta2 = 2.0 * u * ta1 - ta0, tb2 = 2.0 * v * tb1 - tb0;
-                    Tw[tid][a] = w * ta2;
-                    Tv[tid][a] = tb2;
-                    ta0 = ta1; ta1 = ta2; tb0 = tb1; tb1 = tb2;
-                }
-            }
-            __syncthreads();
-            if (tid < KM) {
-                const int cnt = min(kUpThreads, a1 - c0);
-                for (int jj = 0; jj < cnt; jj++) acc = fma(Tw[jj][ma], Tv[jj][mb], acc);
-            }
-            __syncthreads();
-        }
-        if (tid < KM) out[tid] = acc;
+        leaf_moments<T>(src, a0, a1, fx, fy, fz, ng, nmax, W, V,
+                        part + (int64_t(leaf) * (leaf_level + 1) + l) * KM);
     }
 }
 
@@ -250,109 +213,172 @@ __global__ void k_scatter_state(int64_t n, const int32_t* __restrict__ perm, con
 
 // ---------------------------------------------------------------- downward pass
 // Target clusters (fast_rhs.h cp and cc): the sum A of a face's far
-// sources at its interpolation points y_k is interpolated to its particles,
-//   A(x_i) = sum_k A(y_k) l_k(b_i) = sum_m c_m phi_m(b_i),   c_m = sum_k Vinv[m][k] A(y_k),
-// with b_i the barycentric coordinates of the central projection of x_i on
-// the face's plane and phi_m the Chebyshev product basis of the upward pass.
-// Kernel 1 forms c for every target cluster; kernel 2, one block per leaf,
-// evaluates the polynomials of all the leaf's ancestors that are target
-// clusters at its particles and writes the sum (x, y, z and, when the
-// stream function is wanted, its log term) to the down-pass partial slot of
-// every particle.  FP64.
+// sources at its interpolation points y_k becomes the interpolant
+//   A(x) = sum_k A(y_k) l_k(b(x)) = sum_m c_m phi_m(b(x)),   c_m = sum_k Vinv[m][k] A(y_k),
+// with b(x) the barycentric coordinates of the central projection of x on
+// the face's plane and phi_m the Chebyshev product basis of the upward
+// pass.  Level by level from the top, a face's coefficients interpolate
+// its own far field at its points plus its parent's interpolant there (a
+// face below a target cluster inherits this way); then, one block per
+// leaf, the leaf face's interpolant is evaluated at its particles into the
+// down-pass partial slot.  x, y, z and, when the stream function is wanted,
+// its log term.  FP64.
 
+// Interpolant with coefficients C (degree deg) of face geometry ng at x:
+// sum_a T_a(u) sum_b c_ab T_b(v) (a + b <= deg), both Chebyshev families by
+// their three-term recurrences.
 template <bool PSI>
-__global__ void __launch_bounds__(kUpThreads) k_down_combine(const DownJob* __restrict__ jobs,
+__device__ __forceinline__ double4 eval_interp(const NodeGeom& ng, double x, double y, double z,
+                                               const double4* C, int deg) {
+    const double c0 = ng.minv[0] * x + ng.minv[1] * y + ng.minv[2] * z;
+    const double c1 = ng.minv[3] * x + ng.minv[4] * y + ng.minv[5] * z;
+    const double c2 = ng.minv[6] * x + ng.minv[7] * y + ng.minv[8] * z;
+    const double inv = 1.0 / (c0 + c1 + c2);
+    const double u = 2.0 * (c0 * inv) - 1.0, v = 2.0 * (c1 * inv) - 1.0;
+    const double u2 = 2.0 * u, v2 = 2.0 * v;
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+    double ta = 1.0, ta_prev = u;  // T_a(u), T_{a-1}(u) (T_{-1} = T_1)
+    for (int a = 0; a <= deg; a++) {
+        double4 s = make_double4(0.0, 0.0, 0.0, 0.0);
+        double tb = 1.0, tb_prev = v;
+        int m = a * (a + 1) / 2;  // index of (a, 0): g = a, b = 0
+        for (int b = 0; a + b <= deg; b++) {
+            const double4 cm = C[m];
+            s.x = fma(tb, cm.x, s.x);
+            s.y = fma(tb, cm.y, s.y);
+            s.z = fma(tb, cm.z, s.z);
+            if (PSI) s.w = fma(tb, cm.w, s.w);
+            const double tn = fma(v2, tb, -tb_prev);
+            tb_prev = tb;
+            tb = tn;
+            m += a + b + 2;  // (g, b) -> (g + 1, b + 1)
+        }
+        acc.x = fma(ta, s.x, acc.x);
+        acc.y = fma(ta, s.y, acc.y);
+        acc.z = fma(ta, s.z, acc.z);
+        if (PSI) acc.w = fma(ta, s.w, acc.w);
+        const double tn = fma(u2, ta, -ta_prev);
+        ta_prev = ta;
+        ta = tn;
+    }
+    return acc;
+}
+
+// One level of the downward pass: block b takes the level's jobs [j0 + 4b,
+// j0 + 4b + 4).  A face's values at its points y_k are its own far field
+// (partial slots at [slot, slot + K), when it is a target cluster) plus its
+// parent's interpolant there; c = Vinv values (VT = Vinv transposed, so that
+// consecutive threads read consecutive entries).
+constexpr int kDownGroup = 4;
+constexpr int kDownThreads = 256;
+template <bool PSI>
+__global__ void __launch_bounds__(kDownThreads) k_down_level(const DownJob* __restrict__ jobs, int j0, int nj,
                                                              const double4* __restrict__ partials, int parts,
-                                                             int64_t pstride, const double* __restrict__ vinv,
+                                                             int64_t pstride, const NodeGeom* __restrict__ node,
+                                                             const double* __restrict__ verts,
+                                                             const int32_t* __restrict__ tri_verts,
+                                                             const double* __restrict__ bary,
+                                                             const int32_t* __restrict__ bary_off,
+                                                             const double* __restrict__ vinvT,
                                                              const int32_t* __restrict__ vinv_off,
                                                              double4* __restrict__ coef) {
-    __shared__ double4 A[kMaxK];
-    const DownJob job = jobs[blockIdx.x];
-    const int K = nproxy(job.deg);
-    for (int k = threadIdx.x; k < K; k += kUpThreads) {
-        double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
-        for (int p = 0; p < parts; p++) {
-            const double4 v = partials[int64_t(p) * pstride + job.slot + k];
-            a.x += v.x; a.y += v.y; a.z += v.z; a.w += v.w;
-        }
-        A[k] = a;
+    __shared__ double4 Cp[kDownGroup][kMaxK];
+    __shared__ double4 Y[kDownGroup][kMaxK];
+    __shared__ DownJob J[kDownGroup], P[kDownGroup];
+    const int tid = threadIdx.x;
+    const int jb = j0 + kDownGroup * blockIdx.x;
+    const int nq = min(kDownGroup, j0 + nj - jb);
+    if (tid < nq) {
+        J[tid] = jobs[jb + tid];
+        if (J[tid].parent >= 0) P[tid] = jobs[J[tid].parent];
     }
     __syncthreads();
-    const double* V = vinv + vinv_off[job.deg];
-    for (int m = threadIdx.x; m < K; m += kUpThreads) {
-        double4 c = make_double4(0.0, 0.0, 0.0, 0.0);
-        for (int k = 0; k < K; k++) {
-            const double w = V[m * K + k];
-            const double4 v = A[k];
-            c.x = fma(w, v.x, c.x); c.y = fma(w, v.y, c.y); c.z = fma(w, v.z, c.z);
-            if (PSI) c.w = fma(w, v.w, c.w);
+    for (int idx = tid; idx < nq * kMaxK; idx += kDownThreads) {
+        const int q = idx / kMaxK, m = idx % kMaxK;
+        if (J[q].parent >= 0 && m < nproxy(P[q].deg)) Cp[q][m] = coef[int64_t(P[q].coef) + m];
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nq * kMaxK; idx += kDownThreads) {
+        const int q = idx / kMaxK, k = idx % kMaxK;
+        const DownJob& job = J[q];
+        if (k >= nproxy(job.deg)) continue;
+        double4 val = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (job.slot >= 0)
+            for (int p = 0; p < parts; p++) {
+                const double4 v = partials[int64_t(p) * pstride + job.slot + k];
+                val.x += v.x; val.y += v.y; val.z += v.z; val.w += v.w;
+            }
+        if (job.parent >= 0) {
+            const int32_t* tv = tri_verts + 3 * int64_t(job.node);
+            const double* v0 = verts + 3 * int64_t(tv[0]);
+            const double* v1 = verts + 3 * int64_t(tv[1]);
+            const double* v2 = verts + 3 * int64_t(tv[2]);
+            const double* nd = bary + bary_off[job.deg] + 3 * k;
+            double y[3];
+            for (int c = 0; c < 3; c++) y[c] = nd[0] * v0[c] + nd[1] * v1[c] + nd[2] * v2[c];
+            const double r = 1.0 / sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+            const double4 e = eval_interp<PSI>(node[P[q].node], y[0] * r, y[1] * r, y[2] * r, Cp[q], P[q].deg);
+            val.x += e.x; val.y += e.y; val.z += e.z; val.w += e.w;
         }
-        coef[int64_t(job.coef) + m] = c;
+        Y[q][k] = val;
+    }
+    __syncthreads();
+    // c_m = sum_k Vinv[m][k] Y_k: four threads per output, each a quarter of
+    // the k range (short independent chains), combined by shuffles
+    const int total = nq * kMaxK * 4;
+    for (int base = 0; base < total; base += kDownThreads) {  // same trip count in every lane
+        const int idx = base + tid;
+        const int o = idx >> 2, part = idx & 3;
+        const int q = (idx < total) ? o / kMaxK : 0, m = (idx < total) ? o % kMaxK : kMaxK;
+        const DownJob& job = J[q];
+        const int K = nproxy(job.deg);
+        const double* VT = vinvT + vinv_off[job.deg];
+        double4 c = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (m < K) {
+#pragma unroll 4
+            for (int k = part; k < K; k += 4) {
+                const double w = __ldg(&VT[k * K + m]);
+                const double4 v = Y[q][k];
+                c.x = fma(w, v.x, c.x); c.y = fma(w, v.y, c.y); c.z = fma(w, v.z, c.z);
+                if (PSI) c.w = fma(w, v.w, c.w);
+            }
+        }
+        // the four parts of one output are consecutive lanes of one warp
+        for (int d = 1; d < 4; d <<= 1) {
+            c.x += __shfl_xor_sync(0xffffffffu, c.x, d);
+            c.y += __shfl_xor_sync(0xffffffffu, c.y, d);
+            c.z += __shfl_xor_sync(0xffffffffu, c.z, d);
+            if (PSI) c.w += __shfl_xor_sync(0xffffffffu, c.w, d);
+        }
+        if (part == 0 && m < K) coef[int64_t(job.coef) + m] = c;
     }
 }
 
 template <bool PSI>
 __global__ void __launch_bounds__(kUpThreads) k_down_leaf(const double4* __restrict__ xs,
                                                           const int32_t* __restrict__ leaf_start,
-                                                          const NodeGeom* __restrict__ node,
-                                                          const int64_t* __restrict__ lev_off, int leaf_level,
+                                                          const NodeGeom* __restrict__ node, int64_t leaf_off,
                                                           const int32_t* __restrict__ down_of_face,
                                                           const DownJob* __restrict__ jobs,
                                                           const double4* __restrict__ coef,
                                                           double4* __restrict__ out) {
-    __shared__ double4 C[kMaxLevels][kMaxK];
-    __shared__ int deg_s[kMaxLevels];
+    __shared__ double4 C[kMaxK];
     const int leaf = blockIdx.x, tid = threadIdx.x;
     const int a0 = leaf_start[leaf], a1 = leaf_start[leaf + 1];
     if (a0 == a1) return;
-    for (int l = 0; l <= leaf_level; l++) {
-        const int j = down_of_face[lev_off[l] + (leaf >> (2 * (leaf_level - l)))];
-        if (j < 0) {
-            if (tid == 0) deg_s[l] = -1;
-            continue;
-        }
-        const DownJob job = jobs[j];
-        if (tid == 0) deg_s[l] = job.deg;
-        const int K = nproxy(job.deg);
-        for (int k = tid; k < K; k += kUpThreads) C[l][k] = coef[int64_t(job.coef) + k];
+    const int j = down_of_face[leaf_off + leaf];
+    if (j < 0) {
+        for (int i = a0 + tid; i < a1; i += kUpThreads) out[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+        return;
     }
+    const DownJob job = jobs[j];
+    const int K = nproxy(job.deg);
+    for (int k = tid; k < K; k += kUpThreads) C[k] = coef[int64_t(job.coef) + k];
     __syncthreads();
+    const NodeGeom& ng = node[leaf_off + leaf];
     for (int i = a0 + tid; i < a1; i += kUpThreads) {
         const double4 x = xs[i];
-        double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
-        for (int l = 0; l <= leaf_level; l++) {
-            const int deg = deg_s[l];
-            if (deg < 0) continue;
-            const NodeGeom& ng = node[lev_off[l] + (leaf >> (2 * (leaf_level - l)))];
-            const double c0 = ng.minv[0] * x.x + ng.minv[1] * x.y + ng.minv[2] * x.z;
-            const double c1 = ng.minv[3] * x.x + ng.minv[4] * x.y + ng.minv[5] * x.z;
-            const double c2 = ng.minv[6] * x.x + ng.minv[7] * x.y + ng.minv[8] * x.z;
-            const double inv = 1.0 / (c0 + c1 + c2);
-            const double u = 2.0 * (c0 * inv) - 1.0, v = 2.0 * (c1 * inv) - 1.0;
-            double Tu[kMaxDegree + 1], Tv[kMaxDegree + 1];
-            Tu[0] = 1.0; Tv[0] = 1.0;
-            Tu[1] = u; Tv[1] = v;
-#pragma unroll
-            for (int a = 2; a <= kMaxDegree; a++) {
-                Tu[a] = 2.0 * u * Tu[a - 1] - Tu[a - 2];
-                Tv[a] = 2.0 * v * Tv[a - 1] - Tv[a - 2];
-            }
-            const double4* Cl = C[l];
-#pragma unroll
-            for (int g = 0; g <= kMaxDegree; g++) {
-                if (g > deg) break;
-#pragma unroll
-                for (int b = 0; b <= g; b++) {
-                    const double phi = Tu[g - b] * Tv[b];
-                    const double4 cm = Cl[g * (g + 1) / 2 + b];
-                    acc.x = fma(phi, cm.x, acc.x);
-                    acc.y = fma(phi, cm.y, acc.y);
-                    acc.z = fma(phi, cm.z, acc.z);
-                    if (PSI) acc.w = fma(phi, cm.w, acc.w);
-                }
-            }
-        }
-        out[i] = acc;
+        out[i] = eval_interp<PSI>(ng, x.x, x.y, x.z, C, job.deg);
     }
 }
 
@@ -411,20 +437,34 @@ void launch_scatter_state(cudaStream_t st, int64_t n, const int32_t* perm, const
     k_scatter_state<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, perm, s0, tracer, out5);
 }
 
-void launch_down(cudaStream_t st, bool psi, int njobs, const DownJob* jobs, const double4* partials, int parts,
-                 int64_t pstride, const double* vinv, const int32_t* vinv_off, double4* coef, int nleaf,
-                 const double4* xs, const int32_t* leaf_start, const NodeGeom* node, const int64_t* lev_off,
-                 int leaf_level, const int32_t* down_of_face, double4* out) {
-    if (njobs == 0) return;
-    if (psi) {
-        k_down_combine<true><<<njobs, kUpThreads, 0, st>>>(jobs, partials, parts, pstride, vinv, vinv_off, coef);
-        k_down_leaf<true><<<nleaf, kUpThreads, 0, st>>>(xs, leaf_start, node, lev_off, leaf_level, down_of_face, jobs,
-                                                        coef, out);
-    } else {
-        k_down_combine<false><<<njobs, kUpThreads, 0, st>>>(jobs, partials, parts, pstride, vinv, vinv_off, coef);
-        k_down_leaf<false><<<nleaf, kUpThreads, 0, st>>>(xs, leaf_start, node, lev_off, leaf_level, down_of_face,
-                                                         jobs, coef, out);
+void launch_down(cudaStream_t st, bool psi, const DownArgs& d) {
+    if (d.njobs == 0) return;
+    for (int l = 0; l <= d.leaf_level; l++) {
+        const int j0 = d.level_off[l], nj = d.level_off[l + 1] - j0;
+        if (nj == 0) continue;
+        const int nb = (nj + kDownGroup - 1) / kDownGroup;
+        if (psi)
+            k_down_level<true><<<nb, kDownThreads, 0, st>>>(d.jobs, j0, nj, d.partials, d.parts, d.pstride, d.node,
+                                                            d.verts, d.tri_verts, d.bary, d.bary_off, d.vinvT,
+                                                            d.vinv_off, d.coef);
+        else
+            k_down_level<false><<<nb, kDownThreads, 0, st>>>(d.jobs, j0, nj, d.partials, d.parts, d.pstride, d.node,
+                                                             d.verts, d.tri_verts, d.bary, d.bary_off, d.vinvT,
+                                                             d.vinv_off, d.coef);
     }
+    if (psi)
+        k_down_leaf<true><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_off, d.down_of_face,
+                                                          d.jobs, d.coef, d.out);
+    else
+        k_down_leaf<false><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_off, d.down_of_face,
+                                                           d.jobs, d.coef, d.out);
+}
+
+int down_launch_count(const DownArgs& d) {
+    if (d.njobs == 0) return 0;
+    int n = 1;
+    for (int l = 0; l <= d.leaf_level; l++) n += (d.level_off[l + 1] > d.level_off[l]) ? 1 : 0;
+    return n;
 }
 
 }  // namespace fss

@@ -2,7 +2,7 @@
 // the particle-cluster far field.
 //
 // A block works on one work item: the targets of one leaf (taken in chunks
-// of the block size; the leaf's current particle range is read from
+// of the consumer count; the leaf's current particle range is read from
 // leaf_start on the device, since particles are re-sorted into the leaves
 // they have moved into) or an explicit target range (direct sum).  Its
 // sources are a list of segments -- the particles of a run of leaves (range
@@ -11,7 +11,9 @@
 // TMA copy (cp.async.bulk, no multicast) per piece with completion counted
 // on the tile slot's mbarrier.  Tiles circulate in a ring of kDepth slots
 // released by the consumer warps through a second mbarrier; an empty tile
-// ends a chunk.  One target per thread.  Per pair (23 algorithmic flops):
+// ends a chunk.  Warp 0 only produces (and, in FP32, converts each landed
+// tile to pair-interleaved order for the packed f32x2 pipe); the other warps
+// consume, one target per thread.  Per pair (23 algorithmic flops):
 //
 //   d   = x_j - x_i
 //   r2  = |d|^2           (= 2 (1 - x_i.x_j) on the unit sphere, no cancellation)
@@ -48,6 +50,60 @@ __device__ __forceinline__ void tile_pairs(const typename Vec4<T>::type* __restr
             T lg = lg2_fast(r2);
             if (GUARD) lg = (r2 > T(0)) ? lg : T(0);
             ap = fma(q.w, lg, ap);
+        }
+    }
+}
+
+// FP32 tiles in pair-interleaved order: float4 2p = {x_a, x_b, y_a, y_b},
+// 2p + 1 = {z_a, z_b, w_a, w_b} for sources a = 2p, b = 2p + 1 (an odd tail
+// padded with w = 0 at the origin, |x_i - 0|^2 = 1).  Both sources of a pair
+// go through the packed f32x2 pipe together: per pair of sources 2 shared
+// loads, 9 packed operations and 2 reciprocals.
+template <bool PSI, bool GUARD>
+__device__ __forceinline__ void tile_pairs_packed(const float4* __restrict__ s, int npair, f2 ntx, f2 nty, f2 ntz,
+                                                  f2& ax, f2& ay, f2& az, float& ap) {
+#pragma unroll 4
+    for (int p = 0; p < npair; p++) {
+        const float4 A = s[2 * p], B = s[2 * p + 1];
+        const f2 dx = f2_add(f2_pack(A.x, A.y), ntx);
+        const f2 dy = f2_add(f2_pack(A.z, A.w), nty);
+        const f2 dz = f2_add(f2_pack(B.x, B.y), ntz);
+        const f2 r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+        float r0, r1;
+        f2_unpack(r2, r0, r1);
+        float i0 = rcp_fast(r0), i1 = rcp_fast(r1);
+        if (GUARD) {
+            i0 = (r0 > 0.f) ? i0 : 0.f;
+            i1 = (r1 > 0.f) ? i1 : 0.f;
+        }
+        const f2 sc = f2_mul(f2_pack(B.z, B.w), f2_pack(i0, i1));
+        ax = f2_fma(sc, dx, ax);
+        ay = f2_fma(sc, dy, ay);
+        az = f2_fma(sc, dz, az);
+        if (PSI) {
+            float l0 = lg2_fast(r0), l1 = lg2_fast(r1);
+            if (GUARD) {
+                l0 = (r0 > 0.f) ? l0 : 0.f;
+                l1 = (r1 > 0.f) ? l1 : 0.f;
+            }
+            ap = fmaf(B.z, l0, fmaf(B.w, l1, ap));
+        }
+    }
+}
+
+// In-place conversion of a landed FP32 tile of `cnt` sources to the
+// pair-interleaved order, by one warp: lane L reads sources [8L, 8L + 8) and
+// writes pairs [4L, 4L + 4), i.e. the same 128 bytes, two sources at a time.
+__device__ __forceinline__ void tile_to_pairs(float4* t, int cnt) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int a = 8 * lane + 2 * k;
+        if (a < cnt) {
+            const float4 u = t[a];
+            const float4 v = (a + 1 < cnt) ? t[a + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+            t[a] = make_float4(u.x, v.x, u.y, v.y);
+            t[a + 1] = make_float4(u.z, v.z, u.w, v.w);
         }
     }
 }
@@ -131,106 +187,150 @@ struct SlotHdr {
 };
 
 struct RingState {
-    int64_t issued, consumed;
+    int64_t issued, consumed, converted;
     bool failed;
 };
 
 // One work item: every chunk of targets against every tile of its segments.
+// Warp 0 is the producer: it packs and issues the tiles and (FP32) converts
+// each landed tile to the pair-interleaved order, releasing it through
+// ready_bar; it computes nothing.  Warps 1.. are the consumers, one target
+// per thread (THREADS - 32 targets per chunk); they wait on ready_bar (FP32)
+// or full_bar (FP64) and release a slot through empty_bar.
 template <typename T, int THREADS, int TILE, bool PSI>
 __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4<T>::type* __restrict__ src,
                                          const Segment* __restrict__ segs, const int32_t* __restrict__ leaf_start,
                                          double4* __restrict__ partials, int64_t pstride,
                                          typename Vec4<T>::type* ring, SlotHdr* hdr, uint64_t* full_bar,
-                                         uint64_t* empty_bar, RingState& rs) {
+                                         uint64_t* empty_bar, uint64_t* ready_bar, RingState& rs) {
     using S4 = typename Vec4<T>::type;
-    constexpr bool kKahan = sizeof(T) == 4;
+    constexpr bool kPacked = sizeof(T) == 4;
+    constexpr int kTargets = THREADS - 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ct = tid - 32;  // consumer thread index (warps 1..)
     int t0 = it.t0, nt = it.nt;
     if (it.leaf >= 0) {
         t0 = leaf_start[it.leaf];
         nt = leaf_start[it.leaf + 1] - t0;
     }
-    for (int c0 = 0; c0 < nt && !rs.failed; c0 += THREADS) {
-        const int cn = min(THREADS, nt - c0);
-        const bool active = warp * 32 < cn;
-        const S4 v = src[t0 + c0 + ((tid < cn) ? tid : 0)];
-        const T tx = v.x, ty = v.y, tz = v.z;
-        T ax = 0, ay = 0, az = 0, ap = 0, sx = 0, sy = 0, sz = 0, sp = 0, cx = 0, cy = 0, cz = 0, cp = 0;
-        int pg = it.g0, poff = 0;
-        bool pdone = false;
-        // producer: warp 0; one tile per call, then one empty tile that ends
-        // the chunk
-        auto produce = [&]() {
-            if (pdone || rs.failed) return;
-            const int slot = int(rs.issued % kDepth);
-            bool ok = true;
-            if (rs.issued >= kDepth) ok = mbar_wait_bounded(&empty_bar[slot], uint32_t((rs.issued / kDepth) - 1) & 1);
-            if (!__all_sync(0xffffffffu, ok)) {
-                rs.failed = true;
-                return;
-            }
-            bool gd = false;
-            const int cnt = pack_tile<S4, TILE>(segs, leaf_start, it.g1, pg, poff, t0 + c0, t0 + c0 + cn, src,
-                                                ring + slot * TILE, &full_bar[slot], gd);
-            if (lane == 0) {
-                hdr[slot].count = cnt;
-                hdr[slot].guard = gd ? 1 : 0;
-                mbar_arrive(&full_bar[slot]);
-            }
-            __syncwarp();
-            if (cnt == 0) pdone = true;
-            rs.issued++;
-        };
-        if (warp == 0)
-            for (int d = 0; d < kDepth - 1; d++) produce();
-        for (;;) {
-            if (warp == 0) produce();
-            const int slot = int(rs.consumed % kDepth);
-            if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full_bar[slot], uint32_t(rs.consumed / kDepth) & 1))) {
-                rs.failed = true;
-                break;
-            }
-            const SlotHdr h = hdr[slot];
-            if (active && h.count > 0) {
-                const S4* tile = ring + slot * TILE;
-                if (h.guard)
-                    tile_pairs<T, PSI, true>(tile, h.count, tx, ty, tz, ax, ay, az, ap);
-                else
-                    tile_pairs<T, PSI, false>(tile, h.count, tx, ty, tz, ax, ay, az, ap);
-                if (kKahan) {
-                    kahan_add(sx, cx, ax);
-                    kahan_add(sy, cy, ay);
-                    kahan_add(sz, cz, az);
-                    if (PSI) kahan_add(sp, cp, ap);
-                    ax = ay = az = ap = T(0);
+    for (int c0 = 0; c0 < nt && !rs.failed; c0 += kTargets) {
+        const int cn = min(kTargets, nt - c0);
+        if (warp == 0) {
+            // ------------------------------------------------ producer
+            int pg = it.g0, poff = 0;
+            bool pdone = false;
+            for (;;) {
+                // convert every produced tile (each waits for its copies)
+                while (kPacked && rs.converted < rs.issued && !rs.failed) {
+                    const int slot = int(rs.converted % kDepth);
+                    if (!__all_sync(0xffffffffu,
+                                    mbar_wait_bounded(&full_bar[slot], uint32_t(rs.converted / kDepth) & 1))) {
+                        rs.failed = true;
+                        break;
+                    }
+                    tile_to_pairs(reinterpret_cast<float4*>(ring + slot * TILE), hdr[slot].count);
+                    fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&ready_bar[slot]);
+                    rs.converted++;
                 }
+                if (pdone || rs.failed) break;
+                // the next tile, once its slot is free (then the empty tile
+                // that ends the chunk)
+                const int slot = int(rs.issued % kDepth);
+                bool ok = true;
+                if (rs.issued >= kDepth)
+                    ok = mbar_wait_bounded(&empty_bar[slot], uint32_t((rs.issued / kDepth) - 1) & 1);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    rs.failed = true;
+                    break;
+                }
+                bool gd = false;
+                const int cnt = pack_tile<S4, TILE>(segs, leaf_start, it.g1, pg, poff, t0 + c0, t0 + c0 + cn, src,
+                                                    ring + slot * TILE, &full_bar[slot], gd);
+                if (lane == 0) {
+                    hdr[slot].count = cnt;
+                    hdr[slot].guard = gd ? 1 : 0;
+                    mbar_arrive(&full_bar[slot]);
+                }
+                __syncwarp();
+                if (cnt == 0) pdone = true;
+                rs.issued++;
             }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty_bar[slot]);
-            rs.consumed++;
-            if (h.count == 0) break;
+            rs.consumed = rs.issued;
+        } else {
+            // ------------------------------------------------ consumers
+            const bool active = (warp - 1) * 32 < cn;
+            const S4 v = src[t0 + c0 + ((ct < cn) ? ct : 0)];
+            T ax = 0, ay = 0, az = 0, ap = 0, sx = 0, sy = 0, sz = 0, sp = 0, cx = 0, cy = 0, cz = 0, cp = 0;
+            f2 ntx = 0, nty = 0, ntz = 0;
+            if (kPacked) {
+                ntx = f2_pack(-float(v.x), -float(v.x));
+                nty = f2_pack(-float(v.y), -float(v.y));
+                ntz = f2_pack(-float(v.z), -float(v.z));
+            }
+            for (;;) {
+                const int slot = int(rs.consumed % kDepth);
+                uint64_t* wait_bar = kPacked ? &ready_bar[slot] : &full_bar[slot];
+                if (!__all_sync(0xffffffffu, mbar_wait_bounded(wait_bar, uint32_t(rs.consumed / kDepth) & 1))) {
+                    rs.failed = true;
+                    break;
+                }
+                const SlotHdr h = hdr[slot];
+                if (active && h.count > 0) {
+                    if constexpr (kPacked) {
+                        const float4* tile = reinterpret_cast<const float4*>(ring + slot * TILE);
+                        f2 px = 0, py = 0, pz = 0;
+                        float pw = 0.f;
+                        if (h.guard)
+                            tile_pairs_packed<PSI, true>(tile, (h.count + 1) >> 1, ntx, nty, ntz, px, py, pz, pw);
+                        else
+                            tile_pairs_packed<PSI, false>(tile, (h.count + 1) >> 1, ntx, nty, ntz, px, py, pz, pw);
+                        float a0, a1;
+                        f2_unpack(px, a0, a1);
+                        kahan_add(sx, cx, T(a0 + a1));
+                        f2_unpack(py, a0, a1);
+                        kahan_add(sy, cy, T(a0 + a1));
+                        f2_unpack(pz, a0, a1);
+                        kahan_add(sz, cz, T(a0 + a1));
+                        if (PSI) kahan_add(sp, cp, T(pw));
+                    } else {
+                        const S4* tile = ring + slot * TILE;
+                        if (h.guard)
+                            tile_pairs<T, PSI, true>(tile, h.count, v.x, v.y, v.z, ax, ay, az, ap);
+                        else
+                            tile_pairs<T, PSI, false>(tile, h.count, v.x, v.y, v.z, ax, ay, az, ap);
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty_bar[slot]);
+                rs.consumed++;
+                if (h.count == 0) break;
+            }
+            if (!rs.failed && ct < cn) {
+                double4 o;
+                if (kPacked)
+                    o = make_double4(double(sx) - double(cx), double(sy) - double(cy), double(sz) - double(cz),
+                                     double(sp) - double(cp));
+                else
+                    o = make_double4(double(ax), double(ay), double(az), double(ap));
+                partials[int64_t(it.part) * pstride + t0 + c0 + ct] = o;
+            }
+            rs.issued = rs.consumed;
         }
         // every tile produced for this chunk has been consumed, so the
         // counters agree in every warp unless a wait gave up
         rs.failed = __syncthreads_or(rs.failed) != 0;
         if (rs.failed) return;
-        if (tid < cn) {
-            double4 o;
-            if (kKahan)
-                o = make_double4(double(sx) - double(cx), double(sy) - double(cy), double(sz) - double(cz),
-                                 double(sp) - double(cp));
-            else
-                o = make_double4(double(ax), double(ay), double(az), double(ap));
-            partials[int64_t(it.part) * pstride + t0 + c0 + tid] = o;
-        }
     }
 }
 
-__device__ __forceinline__ void init_ring(uint64_t* full_bar, uint64_t* empty_bar, int warps) {
+__device__ __forceinline__ void init_ring(uint64_t* full_bar, uint64_t* empty_bar, uint64_t* ready_bar, int warps) {
     if (threadIdx.x == 0) {
         for (int d = 0; d < kDepth; d++) {
             mbar_init(&full_bar[d], 1);
-            mbar_init(&empty_bar[d], warps);
+            mbar_init(&empty_bar[d], warps - 1);  // consumer warps
+            mbar_init(&ready_bar[d], 1);
         }
         mbar_init_fence();
     }
@@ -246,13 +346,13 @@ __global__ void __launch_bounds__(THREADS) k_pairs(const typename Vec4<T>::type*
                                                    int64_t pstride, int* __restrict__ err) {
     using S4 = typename Vec4<T>::type;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth];
+    __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth], ready_bar[kDepth];
     __shared__ SlotHdr hdr[kDepth];
-    init_ring(full_bar, empty_bar, THREADS / 32);
-    RingState rs{0, 0, false};
+    init_ring(full_bar, empty_bar, ready_bar, THREADS / 32);
+    RingState rs{0, 0, 0, false};
     const WorkItem it = items[blockIdx.x];
     run_item<T, THREADS, TILE, PSI>(it, src, segs, leaf_start, partials, pstride, reinterpret_cast<S4*>(smem_raw),
-                                    hdr, full_bar, empty_bar, rs);
+                                    hdr, full_bar, empty_bar, ready_bar, rs);
     if (rs.failed && threadIdx.x == 0) set_error(err, kErrTimeout);
 }
 
@@ -267,11 +367,11 @@ __global__ void __launch_bounds__(THREADS) k_pairs_persistent(const typename Vec
                                                               int64_t pstride, int* __restrict__ err) {
     using S4 = typename Vec4<T>::type;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth];
+    __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth], ready_bar[kDepth];
     __shared__ SlotHdr hdr[kDepth];
     __shared__ int next_item;
-    init_ring(full_bar, empty_bar, THREADS / 32);
-    RingState rs{0, 0, false};
+    init_ring(full_bar, empty_bar, ready_bar, THREADS / 32);
+    RingState rs{0, 0, 0, false};
     for (;;) {
         if (threadIdx.x == 0) next_item = atomicAdd(queue, 1);
         __syncthreads();
@@ -280,7 +380,7 @@ __global__ void __launch_bounds__(THREADS) k_pairs_persistent(const typename Vec
         if (item >= nitems) break;
         const WorkItem it = items[item];
         run_item<T, THREADS, TILE, false>(it, src, segs, leaf_start, partials, pstride,
-                                          reinterpret_cast<S4*>(smem_raw), hdr, full_bar, empty_bar, rs);
+                                          reinterpret_cast<S4*>(smem_raw), hdr, full_bar, empty_bar, ready_bar, rs);
         if (rs.failed) break;
     }
     if (rs.failed && threadIdx.x == 0) set_error(err, kErrTimeout);
@@ -303,8 +403,8 @@ static cudaError_t run_pairs(cudaStream_t st, int nitems, const void* src, const
 }
 
 const std::vector<PairShape>& pair_shapes(bool fp64) {
-    static const std::vector<PairShape> f32 = {{128, 1, 256}, {160, 1, 256}, {192, 1, 256}, {256, 1, 256}};
-    static const std::vector<PairShape> f64 = {{128, 1, 128}, {160, 1, 128}, {192, 1, 128}, {256, 1, 128}};
+    static const std::vector<PairShape> f32 = {{160, 1, 256}, {192, 1, 256}, {224, 1, 256}, {288, 1, 256}};
+    static const std::vector<PairShape> f64 = {{160, 1, 128}, {192, 1, 128}, {224, 1, 128}, {288, 1, 128}};
     return fp64 ? f64 : f32;
 }
 
@@ -317,9 +417,10 @@ PairShape pairs_shape(bool fp64, int threads, int per_thread) {
 
 PairShape cluster_shape(bool fp64, int k) {
     const int tile = tile_capacity(fp64);
-    if (k <= 64) return PairShape{64, 1, tile};
-    if (k <= 96) return PairShape{96, 1, tile};
-    return pairs_shape(fp64, 128, 1);
+    if (k <= 32) return PairShape{64, 1, tile};
+    if (k <= 64) return PairShape{96, 1, tile};
+    if (k <= 96) return PairShape{128, 1, tile};
+    return PairShape{160, 1, tile};
 }
 
 template <typename T, bool PSI>
@@ -334,7 +435,8 @@ static cudaError_t dispatch(cudaStream_t st, PairShape sh, int nitems, const voi
     FSS_SHAPE(128)
     FSS_SHAPE(160)
     FSS_SHAPE(192)
-    FSS_SHAPE(256)
+    FSS_SHAPE(224)
+    FSS_SHAPE(288)
 #undef FSS_SHAPE
     return cudaErrorInvalidConfiguration;
 }

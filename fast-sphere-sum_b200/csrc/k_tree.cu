@@ -138,27 +138,58 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(int64_t n, const ui
     hist[int64_t(threadIdx.x) * nblk + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of m entries in one block of 1024 threads.
+// Exclusive scan of m entries in one block of 1024 threads, in chunks of
+// 1024 x kScanPer entries staged through shared memory (coalesced loads and
+// stores; each thread scans kScanPer consecutive entries; warp-shuffle scan
+// of the thread sums; a running carry across chunks).
+constexpr int kScanPer = 8;
 __global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ a, int64_t m) {
-    __shared__ uint32_t part[1024];
-    const int t = threadIdx.x;
-    const int64_t per = (m + 1023) / 1024;
-    const int64_t lo = t * per, hi = (lo + per < m) ? lo + per : m;
-    uint32_t s = 0;
-    for (int64_t i = lo; i < hi; i++) s += a[i];
-    part[t] = s;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        const uint32_t v = (t >= off) ? part[t - off] : 0u;
+    __shared__ uint32_t buf[1024 * kScanPer];
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry_s;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t == 0) carry_s = 0;
+    for (int64_t base = 0; base < m; base += 1024 * kScanPer) {
+        for (int k = 0; k < kScanPer; k++) {
+            const int64_t i = base + int64_t(k) * 1024 + t;
+            buf[k * 1024 + t] = (i < m) ? a[i] : 0u;
+        }
         __syncthreads();
-        part[t] += v;
+        uint32_t v[kScanPer], s = 0;
+        for (int k = 0; k < kScanPer; k++) {
+            v[k] = buf[t * kScanPer + k];
+            s += v[k];
+        }
+        // inclusive scan of the thread sums
+        uint32_t x = s;
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= d) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
         __syncthreads();
-    }
-    uint32_t run = (t > 0) ? part[t - 1] : 0u;
-    for (int64_t i = lo; i < hi; i++) {
-        const uint32_t v = a[i];
-        a[i] = run;
-        run += v;
+        if (w == 0) {
+            uint32_t z = wsum[lane];
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, z, d);
+                if (lane >= d) z += y;
+            }
+            wsum[lane] = z;
+        }
+        __syncthreads();
+        const uint32_t carry = carry_s;
+        uint32_t run = carry + (x - s) + (w > 0 ? wsum[w - 1] : 0u);
+        for (int k = 0; k < kScanPer; k++) {
+            buf[t * kScanPer + k] = run;
+            run += v[k];
+        }
+        __syncthreads();
+        if (t == 1023) carry_s = run;
+        for (int k = 0; k < kScanPer; k++) {
+            const int64_t i = base + int64_t(k) * 1024 + t;
+            if (i < m) a[i] = buf[k * 1024 + t];
+        }
+        __syncthreads();
     }
 }
 
@@ -258,18 +289,27 @@ __global__ void k_gather(int64_t n, const double* __restrict__ in5, const double
 // Particles move between RK4 steps; at the start of a step each is put in
 // the leaf it is in now.  Its previous leaf key[s] is kept when the
 // particle is still inside it (all cone coordinates >= 0), otherwise it
-// descends from the 20 root faces in complete mode (the first child that
-// contains it, else the most-inside one).  With `leaves` the keys are global
-// leaf indices of an ensemble (each member's leaf level and the leaf's
-// index on it from the table; a member's leaves are consecutive); without,
-// leaf indices of one tree with leaves on `leaf_level`.
+// descends from the 20 root faces (the first child that contains it, else
+// the most-inside one).  Cone coordinates c = Minv p come from each face's
+// inverse vertex matrix (FP64); the initial build's exact-rounding LU is
+// only needed for parity with the reference's assignment.  With `leaves`
+// the keys are global leaf indices of an ensemble (each member's leaf level
+// and the leaf's index on it from the table; a member's leaves are
+// consecutive); without, leaf indices of one tree with leaves on
+// `leaf_level`.
+__device__ __forceinline__ double min_cone(const NodeGeom& g, double x, double y, double z) {
+    const double c0 = g.minv[0] * x + g.minv[1] * y + g.minv[2] * z;
+    const double c1 = g.minv[3] * x + g.minv[4] * y + g.minv[5] * z;
+    const double c2 = g.minv[6] * x + g.minv[7] * y + g.minv[8] * z;
+    return fmin(c0, fmin(c1, c2));
+}
+
 __global__ void k_reassign(int64_t n, const double4* __restrict__ pos, const EnsLeaf* __restrict__ leaves,
-                           int leaf_level, const double* __restrict__ verts, const int32_t* __restrict__ tri_verts,
-                           const int64_t* __restrict__ lev_off, uint32_t* __restrict__ key) {
+                           int leaf_level, const NodeGeom* __restrict__ node, const int64_t* __restrict__ lev_off,
+                           uint32_t* __restrict__ key) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double4 q = pos[i];
-    const double p[3] = {q.x, q.y, q.z};
     const uint32_t g = key[i];
     int LL = leaf_level, local = int(g);
     if (leaves) {
@@ -277,25 +317,18 @@ __global__ void k_reassign(int64_t n, const double4* __restrict__ pos, const Ens
         LL = lf.leaf_level;
         local = lf.local;
     }
-    double c[3];
-    {
-        const int32_t* tv = tri_verts + 3 * (lev_off[LL] + local);
-        cone_coords_exact(verts + 3 * int64_t(tv[0]), verts + 3 * int64_t(tv[1]), verts + 3 * int64_t(tv[2]), p, c);
-        if (c[0] >= 0 && c[1] >= 0 && c[2] >= 0) return;
-    }
+    if (min_cone(node[lev_off[LL] + local], q.x, q.y, q.z) >= 0.0) return;
     int prev = 0;
     for (int l = 0; l <= LL; l++) {
         const int lb = (l > 0) ? 4 * prev : 0, ub = (l > 0) ? lb + 4 : 20;
-        int found = -1, best = lb;
+        int best = lb;
         double best_min = -1e300;
         for (int j = lb; j < ub; j++) {
-            const int32_t* tv = tri_verts + 3 * (lev_off[l] + j);
-            cone_coords_exact(verts + 3 * int64_t(tv[0]), verts + 3 * int64_t(tv[1]), verts + 3 * int64_t(tv[2]), p, c);
-            if (c[0] >= 0 && c[1] >= 0 && c[2] >= 0) { found = j; break; }
-            const double m = fmin(c[0], fmin(c[1], c[2]));
+            const double m = min_cone(node[lev_off[l] + j], q.x, q.y, q.z);
+            if (m >= 0.0) { best = j; break; }
             if (m > best_min) { best_min = m; best = j; }
         }
-        prev = (found >= 0) ? found : best;
+        prev = best;
     }
     key[i] = uint32_t(int64_t(g) - local + prev);
 }
@@ -393,9 +426,9 @@ void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, con
 }
 
 void launch_reassign(cudaStream_t st, int64_t n, const double4* pos, const EnsLeaf* leaves, int leaf_level,
-                     const double* verts, const int32_t* tri_verts, const int64_t* lev_off, uint32_t* key) {
+                     const NodeGeom* node, const int64_t* lev_off, uint32_t* key) {
     if (n == 0) return;
-    k_reassign<<<unsigned((n + 127) / 128), 128, 0, st>>>(n, pos, leaves, leaf_level, verts, tri_verts, lev_off, key);
+    k_reassign<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, pos, leaves, leaf_level, node, lev_off, key);
 }
 
 void launch_resort(cudaStream_t st, bool fp64, int64_t n, const int32_t* q, double4* s0, double* area,

@@ -35,10 +35,13 @@ struct EpiArgs {
     const double4* frame = nullptr;
 };
 
+// Pair-kernel block: `threads` = one producer warp + consumer warps with one
+// target each.
 struct PairShape {
-    int threads = 128;
+    int threads = 160;
     int per_thread = 1;
     int tile = 256;
+    int targets() const { return (threads - 32) * per_thread; }
 };
 
 // k_tree.cu
@@ -56,7 +59,7 @@ void launch_leaf_bounds(cudaStream_t st, int64_t n, const uint32_t* skey, int32_
 // (through the free stage buffers xs and acc) and the stage-1 sources
 // rewritten.
 void launch_reassign(cudaStream_t st, int64_t n, const double4* pos, const EnsLeaf* leaves, int leaf_level,
-                     const double* verts, const int32_t* tri_verts, const int64_t* lev_off, uint32_t* key);
+                     const NodeGeom* node, const int64_t* lev_off, uint32_t* key);
 void launch_resort(cudaStream_t st, bool fp64, int64_t n, const int32_t* q, double4* s0, double* area,
                    double* tracer, int32_t* perm, double4* xs, double4* acc, void* src);
 void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, const double* area_in, const int32_t* perm,
@@ -64,12 +67,12 @@ void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, con
                    double* tracer_s, void* src);
 
 // k_pairs.cu
-// Supported block shapes of the pair kernel (threads; one target each).
+// Block shapes of the pair kernel the autotuner tries (threads = 32 + targets).
 const std::vector<PairShape>& pair_shapes(bool fp64);
 // The supported shape with `threads`, or the default (128).
 PairShape pairs_shape(bool fp64, int threads, int per_thread);
 // Block for work items of k targets (target clusters: their interpolation
-// points): the smallest of 64, 96, 128 threads that holds them.
+// points): the smallest of 64, 96, 128, 160 threads whose consumers hold them.
 PairShape cluster_shape(bool fp64, int k);
 cudaError_t launch_pairs(cudaStream_t st, bool fp64, bool psi, PairShape shape, int nitems, const void* src,
                          const Segment* segs, const int32_t* leaf_start, const WorkItem* items, double4* partials,
@@ -87,13 +90,31 @@ void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, cons
 void launch_up_combine(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part, int leaf_level,
                        int nmax, const double* vinv, const int32_t* vinv_off, const double4* proxy_pos,
                        const NodeGeom* node, int local_frames, int64_t n, void* src);
-// Downward pass of the target clusters: coefficients from the field at
-// their interpolation points (parts partial slots of stride pstride), then
-// their sum at every particle into `out` (the down-pass partial slot).
-void launch_down(cudaStream_t st, bool psi, int njobs, const DownJob* jobs, const double4* partials, int parts,
-                 int64_t pstride, const double* vinv, const int32_t* vinv_off, double4* coef, int nleaf,
-                 const double4* xs, const int32_t* leaf_start, const NodeGeom* node, const int64_t* lev_off,
-                 int leaf_level, const int32_t* down_of_face, double4* out);
+// Downward pass of the target clusters and the faces below them.
+struct DownArgs {
+    int njobs = 0;
+    const DownJob* jobs = nullptr;
+    const int32_t* level_off = nullptr;  // host array: first job of each level (leaf_level + 2)
+    const double4* partials = nullptr;   // field at the interpolation points: parts slots of stride pstride
+    int parts = 1;
+    int64_t pstride = 0;
+    const double* vinvT = nullptr;       // inverse Vandermonde matrices transposed, by degree
+    const int32_t* vinv_off = nullptr;
+    const double* bary = nullptr;        // interpolation nodes (barycentric, 3 per point) by degree
+    const int32_t* bary_off = nullptr;
+    const double* verts = nullptr;
+    const int32_t* tri_verts = nullptr;
+    const NodeGeom* node = nullptr;
+    double4* coef = nullptr;
+    int nleaf = 0, leaf_level = 0;
+    int64_t leaf_off = 0;                // global index of the first leaf face
+    const double4* xs = nullptr;
+    const int32_t* leaf_start = nullptr;
+    const int32_t* down_of_face = nullptr;
+    double4* out = nullptr;              // down-pass partial slot, one per particle
+};
+void launch_down(cudaStream_t st, bool psi, const DownArgs& d);
+int down_launch_count(const DownArgs& d);
 void launch_epilogue(cudaStream_t st, bool fp64, const EpiArgs& a);
 void launch_refresh(cudaStream_t st, bool fp64, int64_t n, const double4* s0, const double* area,
                     const uint32_t* leaf_of, const double4* frame, double4* xs, void* src);

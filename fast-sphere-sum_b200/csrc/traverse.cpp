@@ -333,7 +333,12 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
     flush_items();
     out.n_leaf_items = int64_t(out.items.size());
     // target clusters: their interpolation points are the targets
-    if (!clusters.empty()) out.down_of_face.assign(size_t(g.lev_off[LL + 1]), -1);
+    const int64_t nfaces = g.lev_off[LL + 1];
+    std::vector<int32_t> own_slot, own_deg;
+    if (!clusters.empty()) {
+        own_slot.assign(nfaces, -1);
+        own_deg.assign(nfaces, -1);
+    }
     for (const TList& t : clusters) {
         const int K = nproxy(t.deg);
         const int64_t gf = g.lev_off[t.level] + t.node;
@@ -343,12 +348,30 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
         out.cp_pairs += npp;
         out.cc_pairs += npc;
         add_items(s0, K, -1, K);
-        out.down_of_face[gf] = int32_t(out.down.size());
-        out.down.push_back(DownJob{t.level, int32_t(gf), t.node, t.deg, s0, int32_t(out.n_coef)});
-        out.n_coef += K;
+        own_slot[gf] = s0;
+        own_deg[gf] = t.deg;
         out.max_cluster_k = std::max(out.max_cluster_k, K);
     }
     flush_items();
+    // downward pass: every target cluster and every face below one, level by
+    // level (a face below takes its parent's degree unless it has its own)
+    if (!clusters.empty()) {
+        out.down_of_face.assign(nfaces, -1);
+        out.down_level_off.assign(LL + 2, 0);
+        for (int l = 0; l <= LL; l++) {
+            out.down_level_off[l] = int32_t(out.down.size());
+            for (int64_t f = 0; f < g.level_count(l); f++) {
+                const int64_t gf = g.lev_off[l] + f;
+                const int32_t pj = (l > 0) ? out.down_of_face[g.lev_off[l - 1] + f / 4] : -1;
+                const int deg = own_deg[gf] >= 0 ? own_deg[gf] : (pj >= 0 ? out.down[pj].deg : -1);
+                if (deg < 0) continue;
+                out.down_of_face[gf] = int32_t(out.down.size());
+                out.down.push_back(DownJob{l, int32_t(gf), int32_t(f), deg, own_slot[gf], int32_t(out.n_coef), pj, 0});
+                out.n_coef += nproxy(deg);
+            }
+        }
+        out.down_level_off[LL + 1] = int32_t(out.down.size());
+    }
 }
 
 // ---------------------------------------------------------------- interpolation

@@ -56,7 +56,7 @@ struct ListInput {
     int leaf_level = 0;                 // tree_levels - 1
     int64_t n = 0;                      // particles
     const int32_t* leaf_start = nullptr;  // nleaf + 1 (sorted order) at the build; estimates only
-    int threads = 128, per_thread = 1;  // targets per block = threads * per_thread
+    int threads = 128, per_thread = 1;  // targets per block chunk = threads * per_thread
     int tile = 256;                     // sources per shared-memory tile
     int parts = 1;                      // source-list split
     bool all_leaves = false;            // items also for leaves empty at the build
@@ -68,7 +68,8 @@ struct ListOutput {
     int64_t n_leaf_items = 0;
     int max_cluster_k = 0;          // largest interpolation point count of a target cluster
     std::vector<ProxyJob> jobs;
-    std::vector<DownJob> down;      // target clusters
+    std::vector<DownJob> down;      // target clusters and the faces below them, by level
+    std::vector<int32_t> down_level_off;  // first down job of each level (leaf_level + 2 entries)
     std::vector<int32_t> down_of_face;  // global face -> down job, or -1 (empty without target clusters)
     int64_t n_coef = 0;             // down-pass coefficients (double4)
     std::vector<double> proxy_pos;  // 4 doubles per proxy slot: y (on sphere) and pad

@@ -10,8 +10,9 @@ each an RH R=4 wave with a seeded +-5% amplitude perturbation and 4-16
 Gaussian vortices; mixed-precision BLTC n=8, theta=0.7; one CUDA graph per
 RK4 step for all members.
 
---learned: per-leaf interaction lists with the learned per-leaf (degree,
-theta) choice (tolerance 1e-6, safety 2) and the autotuned block shape.
+--learned: the learned per-leaf (degree, theta) choice (tolerance 1e-6,
+safety 2) and the autotuned block shape, with target clusters (the
+reference's cp/cc types) unless --no-clusters.
 
 Inputs: icosahedral grid of the given level, RH4 wave + seeded vortices.
 Prints one line with the wall time; exits non-zero on any library error.
@@ -38,6 +39,8 @@ def main(argv=None):
     p.add_argument("--vortices", type=int, default=32)
     p.add_argument("--no-graph", action="store_true")
     p.add_argument("--learned", action="store_true")
+    p.add_argument("--clusters", action="store_true", help="target clusters with fixed degree/theta")
+    p.add_argument("--no-clusters", action="store_true")
     a = p.parse_args(argv)
     prec = PREC_MIXED if a.precision == "mixed" else PREC_FP64
     if a.case == "ensemble":
@@ -46,6 +49,8 @@ def main(argv=None):
     method = METHOD_DIRECT if a.case == "direct" else METHOD_TREECODE
     t0 = time.perf_counter()
     extra = dict(list_mode=1, autotune=1) if a.learned else {}
+    if (a.learned and not a.no_clusters) or a.clusters:
+        extra["cluster_targets"] = 1
     with Context(method=method, precision=prec, degree=a.degree, theta=a.theta,
                  use_graph=0 if a.no_graph else 1, **extra) as ctx:
         ctx.set_particles(s, area)

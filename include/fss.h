@@ -96,9 +96,11 @@ typedef struct fss_config {
     int32_t use_graph;     /* capture the RK4 step in a CUDA graph */
     int32_t src_parts;     /* split each target's source list in this many parts
                               (0 = automatic) */
-    int32_t block_threads; /* threads per interaction block (0 = automatic: the
-                              smallest block that holds the largest leaf) */
-    int32_t targets_per_thread; /* with block_threads: 1 or 2 */
+    int32_t block_threads; /* threads per interaction block: one producer warp
+                              plus one consumer thread per target, 160, 192,
+                              224 or 288 (0 = automatic: the smallest block
+                              whose consumers hold the largest leaf) */
+    int32_t targets_per_thread; /* 1 */
     int32_t autotune;      /* at fss_set_particles, time every supported block
                               shape on the actual lists and keep the fastest */
     int32_t rebuild;       /* fss_rebuild_policy */

@@ -51,7 +51,7 @@ def test_direct_parts_and_shapes_agree(fss, oracle):
     s, a = fss.make_state(4, "rh4_ref")
     ref = oracle.rhs_direct(s, a)
     for parts in (1, 3, 7):
-        for bt in (0, 64):
+        for bt in (0, 192, 288):
             with fss.Context(method=fss.METHOD_DIRECT, precision=fss.PREC_MIXED, src_parts=parts,
                              block_threads=bt) as ctx:
                 ctx.set_particles(s, a)
