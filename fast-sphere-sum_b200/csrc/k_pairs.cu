@@ -31,6 +31,7 @@
 namespace fss {
 
 constexpr int kDepth = 4;  // ring depth (tiles in flight)
+constexpr int TILE_F32 = tile_capacity(false);
 
 template <typename T, bool PSI, bool GUARD>
 __device__ __forceinline__ void tile_pairs(const typename Vec4<T>::type* __restrict__ s, int cnt, T tx, T ty, T tz,
@@ -54,57 +55,77 @@ __device__ __forceinline__ void tile_pairs(const typename Vec4<T>::type* __restr
     }
 }
 
-// FP32 tiles in pair-interleaved order: float4 2p = {x_a, x_b, y_a, y_b},
-// 2p + 1 = {z_a, z_b, w_a, w_b} for sources a = 2p, b = 2p + 1 (an odd tail
-// padded with w = 0 at the origin, |x_i - 0|^2 = 1).  Both sources of a pair
-// go through the packed f32x2 pipe together: per pair of sources 2 shared
-// loads, 9 packed operations and 2 reciprocals.
+// FP32 tiles in SoA order: x[TILE], y[TILE], z[TILE], w[TILE], padded to a
+// multiple of 4 sources with w = 0 at the origin (|x_i - 0|^2 = 1, no
+// contribution).  One 128-bit shared load brings a component of four
+// sources; each pair of sources goes through the packed f32x2 pipe: per
+// four sources 4 shared loads, 18 packed operations and 4 reciprocals.
 template <bool PSI, bool GUARD>
-__device__ __forceinline__ void tile_pairs_packed(const float4* __restrict__ s, int npair, f2 ntx, f2 nty, f2 ntz,
-                                                  f2& ax, f2& ay, f2& az, float& ap) {
-#pragma unroll 4
-    for (int p = 0; p < npair; p++) {
-        const float4 A = s[2 * p], B = s[2 * p + 1];
-        const f2 dx = f2_add(f2_pack(A.x, A.y), ntx);
-        const f2 dy = f2_add(f2_pack(A.z, A.w), nty);
-        const f2 dz = f2_add(f2_pack(B.x, B.y), ntz);
-        const f2 r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
-        float r0, r1;
-        f2_unpack(r2, r0, r1);
-        float i0 = rcp_fast(r0), i1 = rcp_fast(r1);
-        if (GUARD) {
-            i0 = (r0 > 0.f) ? i0 : 0.f;
-            i1 = (r1 > 0.f) ? i1 : 0.f;
-        }
-        const f2 sc = f2_mul(f2_pack(B.z, B.w), f2_pack(i0, i1));
-        ax = f2_fma(sc, dx, ax);
-        ay = f2_fma(sc, dy, ay);
-        az = f2_fma(sc, dz, az);
-        if (PSI) {
-            float l0 = lg2_fast(r0), l1 = lg2_fast(r1);
+__device__ __forceinline__ void tile_pairs_soa(const float* __restrict__ s, int nquad, f2 ntx, f2 nty, f2 ntz,
+                                               f2& ax, f2& ay, f2& az, float& ap) {
+    constexpr int T = TILE_F32;
+#pragma unroll 2
+    for (int q = 0; q < nquad; q++) {
+        const float4 X = reinterpret_cast<const float4*>(s)[q];
+        const float4 Y = reinterpret_cast<const float4*>(s + T)[q];
+        const float4 Z = reinterpret_cast<const float4*>(s + 2 * T)[q];
+        const float4 W = reinterpret_cast<const float4*>(s + 3 * T)[q];
+        const f2 qx[2] = {f2_pack(X.x, X.y), f2_pack(X.z, X.w)};
+        const f2 qy[2] = {f2_pack(Y.x, Y.y), f2_pack(Y.z, Y.w)};
+        const f2 qz[2] = {f2_pack(Z.x, Z.y), f2_pack(Z.z, Z.w)};
+        const f2 qw[2] = {f2_pack(W.x, W.y), f2_pack(W.z, W.w)};
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const f2 dx = f2_add(qx[h], ntx);
+            const f2 dy = f2_add(qy[h], nty);
+            const f2 dz = f2_add(qz[h], ntz);
+            const f2 r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+            float r0, r1;
+            f2_unpack(r2, r0, r1);
+            float i0 = rcp_fast(r0), i1 = rcp_fast(r1);
             if (GUARD) {
-                l0 = (r0 > 0.f) ? l0 : 0.f;
-                l1 = (r1 > 0.f) ? l1 : 0.f;
+                i0 = (r0 > 0.f) ? i0 : 0.f;
+                i1 = (r1 > 0.f) ? i1 : 0.f;
             }
-            ap = fmaf(B.z, l0, fmaf(B.w, l1, ap));
+            const f2 sc = f2_mul(qw[h], f2_pack(i0, i1));
+            ax = f2_fma(sc, dx, ax);
+            ay = f2_fma(sc, dy, ay);
+            az = f2_fma(sc, dz, az);
+            if (PSI) {
+                float l0 = lg2_fast(r0), l1 = lg2_fast(r1);
+                if (GUARD) {
+                    l0 = (r0 > 0.f) ? l0 : 0.f;
+                    l1 = (r1 > 0.f) ? l1 : 0.f;
+                }
+                float w0, w1;
+                f2_unpack(qw[h], w0, w1);
+                ap = fmaf(w0, l0, fmaf(w1, l1, ap));
+            }
         }
     }
 }
 
-// In-place conversion of a landed FP32 tile of `cnt` sources to the
-// pair-interleaved order, by one warp: lane L reads sources [8L, 8L + 8) and
-// writes pairs [4L, 4L + 4), i.e. the same 128 bytes, two sources at a time.
-__device__ __forceinline__ void tile_to_pairs(float4* t, int cnt) {
+// Transposition of a landed FP32 tile of `cnt` float4 sources into SoA
+// order, by one warp: lane L reads sources [8L, 8L + 8) and writes their 8
+// entries of each component array (padding [cnt, 4 ceil(cnt / 4)) with
+// zeros).
+__device__ __forceinline__ void tile_to_soa(const float4* __restrict__ in, float* __restrict__ out, int cnt) {
+    constexpr int T = TILE_F32;
     const int lane = threadIdx.x & 31;
+    const int j0 = 8 * lane;
+    const int padded = (cnt + 3) & ~3;
+    if (j0 >= padded) return;
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int a = 8 * lane + 2 * k;
-        if (a < cnt) {
-            const float4 u = t[a];
-            const float4 v = (a + 1 < cnt) ? t[a + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
-            t[a] = make_float4(u.x, v.x, u.y, v.y);
-            t[a + 1] = make_float4(u.z, v.z, u.w, v.w);
-        }
+    for (int half = 0; half < 2; half++) {
+        const int j = j0 + 4 * half;
+        if (j >= padded) break;
+        float4 v[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) v[k] = (j + k < cnt) ? in[j + k] : make_float4(0.f, 0.f, 0.f, 0.f);
+        reinterpret_cast<float4*>(out + j)[0] = make_float4(v[0].x, v[1].x, v[2].x, v[3].x);
+        reinterpret_cast<float4*>(out + T + j)[0] = make_float4(v[0].y, v[1].y, v[2].y, v[3].y);
+        reinterpret_cast<float4*>(out + 2 * T + j)[0] = make_float4(v[0].z, v[1].z, v[2].z, v[3].z);
+        reinterpret_cast<float4*>(out + 3 * T + j)[0] = make_float4(v[0].w, v[1].w, v[2].w, v[3].w);
     }
 }
 
@@ -201,7 +222,7 @@ template <typename T, int THREADS, int TILE, bool PSI>
 __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4<T>::type* __restrict__ src,
                                          const Segment* __restrict__ segs, const int32_t* __restrict__ leaf_start,
                                          double4* __restrict__ partials, int64_t pstride,
-                                         typename Vec4<T>::type* ring, SlotHdr* hdr, uint64_t* full_bar,
+                                         typename Vec4<T>::type* ring, float* soa, SlotHdr* hdr, uint64_t* full_bar,
                                          uint64_t* empty_bar, uint64_t* ready_bar, RingState& rs) {
     using S4 = typename Vec4<T>::type;
     constexpr bool kPacked = sizeof(T) == 4;
@@ -228,8 +249,8 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
                         rs.failed = true;
                         break;
                     }
-                    tile_to_pairs(reinterpret_cast<float4*>(ring + slot * TILE), hdr[slot].count);
-                    fence_proxy_async_smem();
+                    tile_to_soa(reinterpret_cast<const float4*>(ring + slot * TILE), soa + slot * 4 * TILE,
+                                hdr[slot].count);
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&ready_bar[slot]);
                     rs.converted++;
@@ -279,13 +300,13 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
                 const SlotHdr h = hdr[slot];
                 if (active && h.count > 0) {
                     if constexpr (kPacked) {
-                        const float4* tile = reinterpret_cast<const float4*>(ring + slot * TILE);
+                        const float* tile = soa + slot * 4 * TILE;
                         f2 px = 0, py = 0, pz = 0;
                         float pw = 0.f;
                         if (h.guard)
-                            tile_pairs_packed<PSI, true>(tile, (h.count + 1) >> 1, ntx, nty, ntz, px, py, pz, pw);
+                            tile_pairs_soa<PSI, true>(tile, (h.count + 3) >> 2, ntx, nty, ntz, px, py, pz, pw);
                         else
-                            tile_pairs_packed<PSI, false>(tile, (h.count + 1) >> 1, ntx, nty, ntz, px, py, pz, pw);
+                            tile_pairs_soa<PSI, false>(tile, (h.count + 3) >> 2, ntx, nty, ntz, px, py, pz, pw);
                         float a0, a1;
                         f2_unpack(px, a0, a1);
                         kahan_add(sx, cx, T(a0 + a1));
@@ -325,6 +346,15 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
     }
 }
 
+// Shared memory of a pair block: the landing ring (kDepth tiles as copied)
+// and, in FP32, the SoA ring the consumers read.
+template <typename T, int TILE>
+FSS_HD constexpr size_t ring_bytes() { return size_t(kDepth) * TILE * sizeof(typename Vec4<T>::type); }
+template <typename T, int TILE>
+FSS_HD constexpr size_t pair_smem_bytes() {
+    return ring_bytes<T, TILE>() + (sizeof(T) == 4 ? size_t(kDepth) * 4 * TILE * sizeof(float) : 0);
+}
+
 __device__ __forceinline__ void init_ring(uint64_t* full_bar, uint64_t* empty_bar, uint64_t* ready_bar, int warps) {
     if (threadIdx.x == 0) {
         for (int d = 0; d < kDepth; d++) {
@@ -352,7 +382,8 @@ __global__ void __launch_bounds__(THREADS) k_pairs(const typename Vec4<T>::type*
     RingState rs{0, 0, 0, false};
     const WorkItem it = items[blockIdx.x];
     run_item<T, THREADS, TILE, PSI>(it, src, segs, leaf_start, partials, pstride, reinterpret_cast<S4*>(smem_raw),
-                                    hdr, full_bar, empty_bar, ready_bar, rs);
+                                    reinterpret_cast<float*>(smem_raw + ring_bytes<T, TILE>()), hdr, full_bar,
+                                    empty_bar, ready_bar, rs);
     if (rs.failed && threadIdx.x == 0) set_error(err, kErrTimeout);
 }
 
@@ -380,7 +411,9 @@ __global__ void __launch_bounds__(THREADS) k_pairs_persistent(const typename Vec
         if (item >= nitems) break;
         const WorkItem it = items[item];
         run_item<T, THREADS, TILE, false>(it, src, segs, leaf_start, partials, pstride,
-                                          reinterpret_cast<S4*>(smem_raw), hdr, full_bar, empty_bar, ready_bar, rs);
+                                          reinterpret_cast<S4*>(smem_raw),
+                                          reinterpret_cast<float*>(smem_raw + ring_bytes<T, TILE>()), hdr, full_bar,
+                                          empty_bar, ready_bar, rs);
         if (rs.failed) break;
     }
     if (rs.failed && threadIdx.x == 0) set_error(err, kErrTimeout);
@@ -393,7 +426,7 @@ static cudaError_t run_pairs(cudaStream_t st, int nitems, const void* src, const
                              const int32_t* leaf_start, const WorkItem* items, double4* partials, int64_t pstride,
                              int* err) {
     constexpr int TILE = tile_capacity(sizeof(T) == 8);
-    constexpr size_t smem = size_t(kDepth) * TILE * sizeof(typename Vec4<T>::type);
+    constexpr size_t smem = pair_smem_bytes<T, TILE>();
     static_assert(smem <= 48 * 1024, "ring must fit the default dynamic shared memory limit");
     if (nitems == 0) return cudaSuccess;
     k_pairs<T, THREADS, PSI, TILE><<<nitems, THREADS, smem, st>>>(static_cast<const typename Vec4<T>::type*>(src),
@@ -455,7 +488,7 @@ cudaError_t launch_pairs_persistent(cudaStream_t st, int nitems, const void* src
                                     const int32_t* leaf_start, const WorkItem* items, int* queue,
                                     double4* partials, int64_t pstride, int* err, int blocks) {
     constexpr int TILE = tile_capacity(false);
-    constexpr size_t smem = size_t(kDepth) * TILE * sizeof(float4);
+    constexpr size_t smem = pair_smem_bytes<float, TILE>();
     if (nitems == 0) return cudaSuccess;
     k_pairs_persistent<float, kPersistentThreads, TILE><<<blocks, kPersistentThreads, smem, st>>>(
         static_cast<const float4*>(src), segs, leaf_start, items, nitems, queue, partials, pstride, err);
@@ -465,8 +498,7 @@ cudaError_t launch_pairs_persistent(cudaStream_t st, int nitems, const void* src
 int persistent_blocks_per_sm() {
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pairs_persistent<float, kPersistentThreads, tile_capacity(false)>,
-                                                  kPersistentThreads,
-                                                  size_t(kDepth) * tile_capacity(false) * sizeof(float4));
+                                                  kPersistentThreads, pair_smem_bytes<float, tile_capacity(false)>());
     return nb > 0 ? nb : 1;
 }
 
