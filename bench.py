@@ -1,14 +1,15 @@
 """Benchmark: RK4 steps/s of the barotropic-vorticity treecode on B200.
 
 Headline workload: 655,362 particles (icosahedral level 8), Rossby-Haurwitz
-R=4 wave + 32 seeded Gaussian vortices, mixed-precision BLTC (FP32
+R=4 wave + 32 seeded Gaussian vortices, mixed-precision treecode (FP32
 interactions with Kahan accumulation, FP64 RK4 / renormalisation /
-interpolation weights), dt = 0.01 day, static tree built once (as the
-reference does before its time loop).  Beside it: the plain FP64 BLTC
-(n = 8, theta = 0.7) on the same GPU, the velocity error of both against the
-FP64 direct sum, an end-to-end number through the C ABI with host buffers,
-the pair kernel's roofline, and the reference's CPU direct sum timed on this
-host's cores.
+interpolation weights) with the learned per-leaf degree/MAC and target
+clusters, particles re-sorted into their current leaves every step,
+dt = 0.01 day.  Beside it: the plain FP64 BLTC (n = 8, theta = 0.7) on the
+same GPU (the ratio's denominator) and the FP64 treecode with the headline's
+algorithm, the velocity error of each against the FP64 direct sum, an
+end-to-end number through the C ABI with host buffers, the pair kernel's
+roofline, and the reference's CPU direct sum timed on this host's cores.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -70,13 +71,22 @@ def dist_setup():
 
 
 def max_over_ranks(x, ws):
+    """The largest x over the ranks (a GPU tensor under NCCL, a CPU one under
+    gloo)."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(steps, seconds, ws):
+    """Whole-job steps/s of ws replicas that each ran `steps` steps, timed by
+    the slowest rank's `seconds` (every rank passes its own time)."""
+    return ws * steps / max_over_ranks(seconds, ws)
 
 
 def barrier(ws):
@@ -307,7 +317,7 @@ def main():
     torch.cuda.synchronize()
     barrier(ws)
     t_max = max_over_ranks(t, ws)
-    value = ws * args.steps / t_max
+    value = replica_value(args.steps, t, ws)
     clocks = clk.summary()
 
     # kernel-level pass (events around every launch, no graph): shares and roofline
