@@ -66,6 +66,11 @@ struct fss_ctx {
     int dev = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
+    // second stream of a treecode RHS with target clusters: the target-leaf
+    // pair launch runs on it beside the upward/downward passes (fork and
+    // join through events, so graph capture records them as edges)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_up = nullptr, ev_join = nullptr;
     bool fp64 = false;
     bool tree = true;
     bool resort = false;  // re-sort particles into their current leaves every RK4 step
@@ -121,6 +126,9 @@ struct fss_ctx {
             cudaEventDestroy(p.b);
         }
         for (auto e : ev_pool) cudaEventDestroy(e);
+        for (cudaEvent_t e : {ev_fork, ev_up, ev_join})
+            if (e) cudaEventDestroy(e);
+        if (side) cudaStreamDestroy(side);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 };

@@ -439,21 +439,43 @@ int materialize(fss_ctx* c, PairShape shape) {
 // The pair kernel over all work items: target leaves with the block shape
 // of the context, target clusters with a block fitted to their
 // interpolation point count.
-int launch_all_pairs(fss_ctx* c, bool want_psi) {
-    const ListOutput& L = c->lists;
-    const int nl = int(L.n_leaf_items), nall = int(L.items.size());
-    CU(launch_pairs(c->stream, c->fp64, want_psi, c->shape, nl, c->src.p, c->segs.as<Segment>(),
+int launch_leaf_pairs(fss_ctx* c, cudaStream_t st, bool want_psi) {
+    CU(launch_pairs(st, c->fp64, want_psi, c->shape, int(c->lists.n_leaf_items), c->src.p, c->segs.as<Segment>(),
                     c->leaf_start.as<int32_t>(), c->items.as<WorkItem>(), c->partials.as<double4>(), c->pstride,
                     c->err_flag.as<int>()));
+    return FSS_OK;
+}
+
+int launch_cluster_pairs(fss_ctx* c, cudaStream_t st, bool want_psi) {
+    const ListOutput& L = c->lists;
+    const int nl = int(L.n_leaf_items), nall = int(L.items.size());
     if (nall > nl)
-        CU(launch_pairs(c->stream, c->fp64, want_psi, cluster_shape(c->fp64, L.max_cluster_k), nall - nl, c->src.p,
+        CU(launch_pairs(st, c->fp64, want_psi, cluster_shape(c->fp64, L.max_cluster_k), nall - nl, c->src.p,
                         c->segs.as<Segment>(), c->leaf_start.as<int32_t>(), c->items.as<WorkItem>() + nl,
                         c->partials.as<double4>(), c->pstride, c->err_flag.as<int>()));
     return FSS_OK;
 }
 
+int launch_all_pairs(fss_ctx* c, bool want_psi) {
+    TRY(launch_leaf_pairs(c, c->stream, want_psi));
+    return launch_cluster_pairs(c, c->stream, want_psi);
+}
+
 // One right-hand side on the current stage state (xs/src).
 int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
+    // With target clusters, the target-leaf pair launch (compute-bound) runs
+    // on the side stream beside the chain upward pass -> target-cluster
+    // pairs -> downward pass (mostly latency-bound); it waits for the upward
+    // pass only when a leaf takes proxies.  Partial slots of the two are
+    // disjoint (particles vs interpolation points).  Sequential while
+    // profiling, so that every range times its own kernels.
+    const bool overlap = c->tree && !c->lists.down.empty() && !c->prof;
+    const bool leaf_needs_up = c->lists.pc_pairs > 0;
+    if (overlap) {
+        CU(cudaEventRecord(c->ev_fork, c->stream));
+        CU(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+        if (!leaf_needs_up) TRY(launch_leaf_pairs(c, c->side, want_psi));
+    }
     if (c->tree && !c->lists.jobs.empty()) {
         {
             ProfScope ps(c, "upward_leaf");
@@ -469,7 +491,14 @@ int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
                               c->n, c->src.p);
         }
     }
-    {
+    if (overlap) {
+        if (leaf_needs_up) {
+            CU(cudaEventRecord(c->ev_up, c->stream));
+            CU(cudaStreamWaitEvent(c->side, c->ev_up, 0));
+            TRY(launch_leaf_pairs(c, c->side, want_psi));
+        }
+        TRY(launch_cluster_pairs(c, c->stream, want_psi));
+    } else {
         ProfScope ps(c, c->fp64 ? "pairs_fp64" : "pairs_mixed", c->lists.n_leaf_items < int64_t(c->lists.items.size()) ? 2 : 1);
         TRY(launch_all_pairs(c, want_psi));
     }
@@ -499,6 +528,10 @@ int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
         d.out = c->partials.as<double4>() + int64_t(c->parts) * c->pstride;
         ProfScope ps(c, "downward", down_launch_count(d));
         launch_down(c->stream, want_psi, d);
+    }
+    if (overlap) {  // join: the epilogue needs the target-leaf partials
+        CU(cudaEventRecord(c->ev_join, c->side));
+        CU(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     }
     if (want_psi) launch_wsum(c->stream, c->n, c->xs.as<double4>(), c->area_s.as<double>(), c->wtotal.as<double>());
     ea.n = c->n;
@@ -743,8 +776,17 @@ int fss_create(const fss_config* cfg, fss_ctx** out) {
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, c->dev));
     if (prop.major < 10) return fail(c, FSS_ERR_UNSUPPORTED, "this build targets sm_100a (Blackwell B200)");
-    CU(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    // the latency-bound chain of an RHS (upward pass, target-cluster pairs,
+    // downward pass) runs on the context's stream at the highest priority;
+    // the compute-bound target-leaf pairs beside it at the lowest
+    int prio_least = 0, prio_greatest = 0;
+    CU(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+    CU(cudaStreamCreateWithPriority(&c->own_stream, cudaStreamNonBlocking, prio_greatest));
     c->stream = c->own_stream;
+    CU(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_least));
+    CU(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&c->ev_up, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     CU(c->err_flag.ensure(sizeof(int)));
     CU(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), c->stream));
     CU(cudaStreamSynchronize(c->stream));
