@@ -238,6 +238,10 @@ int set_particles(fss_ctx* c, int64_t n, const double* state5, const double* are
     TRY(ensure_particle_buffers(c, n));
     CU(cudaMemcpyAsync(c->in5.p, state5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, c->stream));
     CU(cudaMemcpyAsync(c->area_in.p, area, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    // the positions given here are the grid the remesh step returns to
+    CU(c->grid3.ensure(sizeof(double) * 3 * size_t(n)));
+    CU(cudaMemcpy2DAsync(c->grid3.p, 3 * sizeof(double), c->in5.p, 5 * sizeof(double), 3 * sizeof(double), size_t(n),
+                         cudaMemcpyDeviceToDevice, c->stream));
     if (c->tree) {
         TRY(build_tree(c));
     } else {
@@ -1108,5 +1112,92 @@ int fss_tree_geometry(int32_t tree_levels, double* tri_info) {
 }
 
 const char* fss_version(void) { return "fss-b200 0.1 (sm_100a; direct sum + icosahedral BLTC; FP64 and FP32/Kahan)"; }
+
+// ------------------------------------------------------------------ remesh
+
+namespace {
+// Vertex -> triangles adjacency (CSR, increasing triangle order), after
+// checking every vertex index.
+bool remesh_adjacency(int64_t n, int64_t ntri, const int32_t* tris, std::vector<int32_t>& off,
+                      std::vector<int32_t>& adj) {
+    off.assign(size_t(n) + 1, 0);
+    for (int64_t j = 0; j < 3 * ntri; j++) {
+        if (tris[j] < 0 || tris[j] >= n) return false;
+        off[size_t(tris[j]) + 1]++;
+    }
+    for (int64_t i = 0; i < n; i++) off[i + 1] += off[i];
+    adj.assign(size_t(3 * ntri), 0);
+    std::vector<int32_t> fill(off.begin(), off.end() - 1);
+    for (int64_t j = 0; j < ntri; j++)
+        for (int k = 0; k < 3; k++) adj[fill[tris[3 * j + k]]++] = int32_t(j);
+    return true;
+}
+}  // namespace
+
+int fss_remesh(int64_t n, const double* moved5, double* target5, int64_t ntri, const int32_t* tris, double omega,
+               int64_t* n_fallback, int64_t* n_not_found) {
+    fss_ctx* c = nullptr;  // for the error macros: messages go to fss_last_error(NULL)
+    if (n < 3 || ntri < 1 || !moved5 || !target5 || !tris) return fail(c, FSS_ERR_INVALID, "bad remesh arguments");
+    if (n > (int64_t(1) << 30) || 3 * ntri > (int64_t(1) << 31) - 1)
+        return fail(c, FSS_ERR_INVALID, "too many particles or triangles");
+    std::vector<int32_t> off, adj;
+    if (!remesh_adjacency(n, ntri, tris, off, adj)) return fail(c, FSS_ERR_INVALID, "triangle vertex out of range");
+    cudaStream_t st;
+    CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } guard{st};
+    DBuf dm, dt, dtri, doff, dadj, dfail, dcnt;
+    CU(dm.ensure(sizeof(double) * 5 * size_t(n)));
+    CU(dt.ensure(sizeof(double) * 5 * size_t(n)));
+    CU(dtri.ensure(sizeof(int32_t) * 3 * size_t(ntri)));
+    CU(doff.ensure(sizeof(int32_t) * off.size()));
+    CU(dadj.ensure(sizeof(int32_t) * adj.size()));
+    CU(dfail.ensure(sizeof(int32_t) * size_t(n)));
+    CU(dcnt.ensure(2 * sizeof(int32_t)));
+    CU(cudaMemcpyAsync(dm.p, moved5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(dt.p, target5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(dtri.p, tris, sizeof(int32_t) * 3 * ntri, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(doff.p, off.data(), sizeof(int32_t) * off.size(), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(dadj.p, adj.data(), sizeof(int32_t) * adj.size(), cudaMemcpyHostToDevice, st));
+    CU(launch_remesh(st, n, dm.as<double>(), dt.as<double>(), ntri, dtri.as<int32_t>(), doff.as<int32_t>(),
+                     dadj.as<int32_t>(), omega, dfail.as<int32_t>(), dcnt.as<int32_t>(), n_fallback, n_not_found));
+    CU(cudaMemcpyAsync(target5, dt.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    return FSS_OK;
+}
+
+int fss_remesh_current(fss_ctx* c, int64_t ntri, const int32_t* tris, double omega, int64_t* n_fallback,
+                       int64_t* n_not_found) {
+    if (!c || !tris || ntri < 1) return fail(c, FSS_ERR_INVALID, "bad remesh arguments");
+    if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    if (3 * ntri > (int64_t(1) << 31) - 1) return fail(c, FSS_ERR_INVALID, "too many triangles");
+    CU(cudaSetDevice(c->dev));
+    const int64_t n = c->n;
+    std::vector<int32_t> off, adj;
+    if (!remesh_adjacency(n, ntri, tris, off, adj)) return fail(c, FSS_ERR_INVALID, "triangle vertex out of range");
+    TRY(upload(c, c->rm_tris, std::vector<int32_t>(tris, tris + 3 * ntri)));
+    TRY(upload(c, c->rm_off, off));
+    TRY(upload(c, c->rm_adj, adj));
+    CU(c->rm_target.ensure(sizeof(double) * 5 * size_t(n)));
+    CU(c->rm_failed.ensure(sizeof(int32_t) * size_t(n)));
+    CU(c->rm_cnt.ensure(2 * sizeof(int32_t)));
+    TRY(refresh_stage(c));
+    // moved state in the caller's order, targets = grid positions
+    launch_scatter_state(c->stream, n, c->tree ? c->perm.as<int32_t>() : nullptr, c->s0.as<double4>(),
+                         c->tracer_s.as<double>(), c->out5.as<double>());
+    launch_remesh_targets(c->stream, n, c->grid3.as<double>(), c->out5.as<double>(), c->rm_target.as<double>());
+    CU(launch_remesh(c->stream, n, c->out5.as<double>(), c->rm_target.as<double>(), ntri, c->rm_tris.as<int32_t>(),
+                     c->rm_off.as<int32_t>(), c->rm_adj.as<int32_t>(), omega, c->rm_failed.as<int32_t>(),
+                     c->rm_cnt.as<int32_t>(), n_fallback, n_not_found));
+    // the regridded state becomes the step state (sorted order of the
+    // context), then particles go back into the leaves of their grid points
+    CU(cudaMemcpyAsync(c->in5.p, c->rm_target.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToDevice, c->stream));
+    TRY(gather(c, true));
+    c->stage_dirty = false;
+    if (c->tree && c->resort) TRY(resort(c));
+    return check_device_error(c);
+}
 
 }  // extern "C"

@@ -122,6 +122,16 @@ void launch_wsum(cudaStream_t st, int64_t n, const double4* xs, const double* ar
 void launch_scatter_state(cudaStream_t st, int64_t n, const int32_t* perm, const double4* s0, const double* tracer,
                           double* out5);
 
+// k_remesh.cu
+// Remesh targets (grid points, 5 doubles each, zeta and tracer replaced
+// where a moved-mesh triangle contains them); returns the number of points
+// that needed the search over all triangles and the number found nowhere.
+// Synchronises the stream (the fallback search is sized on the host).
+cudaError_t launch_remesh(cudaStream_t st, int64_t n, const double* moved5, double* target5, int64_t ntri,
+                          const int32_t* tris, const int32_t* off, const int32_t* adj, double omega,
+                          int32_t* failed, int32_t* counters, int64_t* n_fallback, int64_t* n_not_found);
+void launch_remesh_targets(cudaStream_t st, int64_t n, const double* grid3, const double* moved5, double* target5);
+
 // k_ensemble.cu
 void launch_up_leaf_batch(cudaStream_t st, int nleaf, const void* src, const EnsLeaf* leaves,
                           const int32_t* leaf_start, const NodeGeom* node, const int64_t* lev_off, int nmax,

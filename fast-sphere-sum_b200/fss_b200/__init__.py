@@ -67,7 +67,7 @@ _i64 = C.c_int64
 # every symbol include/fss.h declares
 SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fss_set_stream",
            "fss_set_particles", "fss_rebuild_tree", "fss_rhs", "fss_rhs_direct", "fss_rhs_treecode",
-           "fss_rk4_step", "fss_rk4_step_host", "fss_get_state", "fss_rhs_current", "fss_get_tree_info",
+           "fss_rk4_step", "fss_rk4_step_host", "fss_get_state", "fss_rhs_current", "fss_remesh", "fss_remesh_current", "fss_get_tree_info",
            "fss_get_tree", "fss_set_leaf_params", "fss_profile_enable", "fss_profile_read",
            "fss_work_per_rhs", "fss_icos_counts", "fss_icos_grid", "fss_area_init",
            "fss_vorticity_rh4_ref", "fss_vorticity_rh_vortices", "fss_tree_traverse", "fss_interp_nodes",
@@ -106,6 +106,9 @@ def lib():
     L.fss_rk4_step_host.argtypes = [_vp, _vp, C.c_double, C.c_double, C.c_int32]
     L.fss_get_state.argtypes = [_vp, _D]
     L.fss_rhs_current.argtypes = [_vp, C.c_double, _D, _vp]
+    _I32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    L.fss_remesh.argtypes = [_i64, _D, _D, _i64, _I32, C.c_double, C.POINTER(_i64), C.POINTER(_i64)]
+    L.fss_remesh_current.argtypes = [_vp, _i64, _I32, C.c_double, C.POINTER(_i64), C.POINTER(_i64)]
     L.fss_get_tree_info.argtypes = [_vp, P(TreeInfo)]
     L.fss_get_tree.argtypes = [_vp, _vp, _vp, _vp, _i64]
     L.fss_set_leaf_params.argtypes = [_vp, C.c_int32, _I, _D]
@@ -162,6 +165,17 @@ def area_init(state5, faces):
 
 
 RH_AMP = 7.848e-6 * 86400.0  # w = K of the Rossby-Haurwitz wave, per day
+
+
+def remesh(moved5, target5, tris, omega=OMEGA):
+    """remesh.h regrid_points2 (fss_remesh): (new target state, fallback
+    count, not-found count)."""
+    m = np.ascontiguousarray(moved5, dtype=np.float64).reshape(-1)
+    t = np.ascontiguousarray(target5, dtype=np.float64).copy().reshape(-1)
+    tr = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1)
+    fb, bad = _i64(), _i64()
+    _check(lib().fss_remesh(m.size // 5, m, t, tr.size // 3, tr, omega, C.byref(fb), C.byref(bad)))
+    return t.reshape(-1, 5), fb.value, bad.value
 
 
 def make_state(level, field="rh4_ref", n_vortex=0, seed=1, amp=RH_AMP, width=0.1):
@@ -282,6 +296,14 @@ class Context:
 
     def rhs_treecode(self, state5, area, omega=OMEGA, psi=False):
         return self._rhs(lib().fss_rhs_treecode, state5, area, omega, psi)
+
+    def remesh_current(self, tris, omega=OMEGA):
+        """remesh.h regrid_points2 on the device state, onto the positions
+        given to set_particles; returns (fallback count, not-found count)."""
+        t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1)
+        fb, bad = _i64(), _i64()
+        self._c(lib().fss_remesh_current(self.h, t.size // 3, t, omega, C.byref(fb), C.byref(bad)))
+        return fb.value, bad.value
 
     def rhs_current(self, omega=OMEGA, psi=False):
         out = np.zeros((self.n, 5))

@@ -163,6 +163,28 @@ int fss_get_state(fss_ctx* ctx, double* state5);
 /* Velocity of the device-resident state into host modify5 (and psi). */
 int fss_rhs_current(fss_ctx* ctx, double omega, double* modify5, double* psi);
 
+/* remesh.h:109-178 regrid_points2 (helpers.h:251-265 tri_interp): particles
+ * that moved with the flow are put back on the grid.  Every target point
+ * keeps its position and takes the absolute vorticity (zeta + 2 omega z) and
+ * tracer interpolated, with normalised barycentric coordinates, from the
+ * first triangle of the moved mesh (vertices moved5, triangles tris: 3
+ * vertex indices each) that contains it: first among the triangles adjacent
+ * to its own vertex, in increasing index order (the reference reads that
+ * adjacency from a file), then among all triangles.  A point found in no
+ * triangle keeps its values.  Host arrays, 5 doubles per particle; target5
+ * is read (positions, kept values) and written.  *n_fallback: points that
+ * needed the search over all triangles; *n_not_found: points found nowhere
+ * (the reference throws).  Either may be NULL. */
+int fss_remesh(int64_t n, const double* moved5, double* target5, int64_t ntri, const int32_t* tris,
+               double omega, int64_t* n_fallback, int64_t* n_not_found);
+/* The same on the context's device-resident state (new_dynamics.cpp:213-216,
+ * use_remesh): the targets are the positions given to fss_set_particles; the
+ * remeshed state becomes the context's state (and, with re-sorting, the
+ * particles go back into the leaves of their grid points).  A point found in
+ * no triangle keeps its current zeta and tracer. */
+int fss_remesh_current(fss_ctx* ctx, int64_t ntri, const int32_t* tris, double omega, int64_t* n_fallback,
+                       int64_t* n_not_found);
+
 /* Tree summary of the last build. */
 typedef struct fss_tree_info {
     int32_t tree_levels;     /* levels 0..tree_levels-1 */

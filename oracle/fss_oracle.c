@@ -560,3 +560,74 @@ int64_t orc_tree_traverse(int tree_levels, double theta, int many_count, const i
     free(q);
     return (nout <= out_cap) ? nout : -nout;
 }
+
+/* ----------------------------------------------------------------- remesh */
+
+/* helpers.h:152-157 norm_barycoords: cone coordinates scaled by the
+ * reciprocal of their sum ((c0 + c1) + c2). */
+static void norm_barycoords(const double *p1, const double *p2, const double *p3, const double *p,
+                            double *c) {
+    orc_barycoords(p1, p2, p3, p, c);
+    const double r = 1.0 / (c[0] + c[1] + c[2]);
+    for (int k = 0; k < 3; k++) c[k] *= r;
+}
+
+/* helpers.h:251-265 tri_interp: absolute vorticity zeta + 2 omega z and the
+ * tracer, interpolated at the target with normalised barycentric
+ * coordinates; zeta = interpolated - 2 omega z_target. */
+static void tri_interp(const int *tv, const double *moved5, double *target5, int64_t i, double omega) {
+    const double *v1 = moved5 + 5 * (int64_t)tv[0], *v2 = moved5 + 5 * (int64_t)tv[1],
+                 *v3 = moved5 + 5 * (int64_t)tv[2];
+    double *t = target5 + 5 * i;
+    double b[3];
+    norm_barycoords(v1, v2, v3, t, b);
+    const double a1 = v1[3] + 2 * omega * v1[2];
+    const double a2 = v2[3] + 2 * omega * v2[2];
+    const double a3 = v3[3] + 2 * omega * v3[2];
+    const double av = b[0] * a1 + b[1] * a2 + b[2] * a3;
+    t[3] = av - 2 * omega * t[2];
+    t[4] = b[0] * v1[4] + b[1] * v2[4] + b[2] * v3[4];
+}
+
+/* remesh.h:109-178 regrid_points2: every target point (its position kept)
+ * takes the zeta and tracer interpolated from the first triangle of the
+ * moved mesh that contains it, searched among the triangles adjacent to its
+ * own vertex in increasing index order, then among all triangles in index
+ * order.  The reference reads that adjacency from a CSV file it does not
+ * contain; here it is built from `tris` in increasing index order.  Returns
+ * the number of targets found in no triangle (left unchanged); *fallback
+ * receives the number that needed the search over all triangles. */
+int64_t orc_remesh(int64_t n, const double *moved5, double *target5, int64_t ntri, const int *tris,
+                   double omega, int64_t *fallback) {
+    int64_t *off = calloc((size_t)n + 1, sizeof(int64_t));
+    int64_t *adj = malloc(sizeof(int64_t) * (size_t)(3 * ntri + 1));
+    for (int64_t j = 0; j < 3 * ntri; j++) off[tris[j] + 1]++;
+    for (int64_t i = 0; i < n; i++) off[i + 1] += off[i];
+    int64_t *fill = malloc(sizeof(int64_t) * (size_t)(n + 1));
+    memcpy(fill, off, sizeof(int64_t) * (size_t)(n + 1));
+    for (int64_t j = 0; j < ntri; j++)
+        for (int k = 0; k < 3; k++) adj[fill[tris[3 * j + k]]++] = j;
+    int64_t bad = 0, fb = 0;
+    for (int64_t i = 0; i < n; i++) {
+        const double *p = target5 + 5 * i;
+        int64_t found = -1;
+        for (int64_t a = off[i]; a < off[i + 1] && found < 0; a++) {
+            const int *tv = tris + 3 * adj[a];
+            if (check_in_tri(moved5 + 5 * (int64_t)tv[0], moved5 + 5 * (int64_t)tv[1], moved5 + 5 * (int64_t)tv[2], p))
+                found = adj[a];
+        }
+        if (found < 0) {
+            fb++;
+            for (int64_t j = 0; j < ntri && found < 0; j++) {
+                const int *tv = tris + 3 * j;
+                if (check_in_tri(moved5 + 5 * (int64_t)tv[0], moved5 + 5 * (int64_t)tv[1], moved5 + 5 * (int64_t)tv[2], p))
+                    found = j;
+            }
+        }
+        if (found < 0) { bad++; continue; }
+        tri_interp(tris + 3 * found, moved5, target5, i, omega);
+    }
+    free(off); free(adj); free(fill);
+    if (fallback) *fallback = fb;
+    return bad;
+}

@@ -63,6 +63,8 @@ def _setup(L):
     L.orc_tree_traverse.argtypes = [C.c_int, C.c_double, C.c_int, _I, _D, C.c_double, _I, i64]
     L.orc_tree_traverse.restype = i64
     L.orc_barycoords.argtypes = [_D, _D, _D, _D, _D]
+    L.orc_remesh.argtypes = [i64, _D, _D, i64, _I, C.c_double, C.POINTER(i64)]
+    L.orc_remesh.restype = i64
 
 
 def _setup_ref(R):
@@ -83,6 +85,8 @@ def _setup_ref(R):
     R.ref_tree_members.restype = i64
     R.ref_rhs_fast.argtypes = [i64, _D, _D, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, _D]
     R.ref_rhs_fast.restype = C.c_int
+    R.ref_regrid.argtypes = [i64, _D, _D, i64, _I, C.c_double]
+    R.ref_regrid.restype = C.c_int
 
 
 _setup(_lib)
@@ -222,3 +226,18 @@ def ref_tree(tree_levels, theta, many_count, state5):
         if np_ >= 0:
             return loc.reshape(tree_levels, n), counts, pairs[:7 * np_].reshape(np_, 7)
         cap = -np_
+
+
+def remesh(moved5, target5, tris, omega=OMEGA, use_ref=False):
+    """remesh.h regrid_points2: (new target state, fallback count, not-found
+    count); adjacency in increasing triangle order."""
+    m = np.ascontiguousarray(moved5, dtype=np.float64).reshape(-1)
+    t = np.ascontiguousarray(target5, dtype=np.float64).copy().reshape(-1)
+    tr = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1)
+    n, ntri = m.size // 5, tr.size // 3
+    if use_ref:
+        rc = ref().ref_regrid(n, m, t, ntri, tr, omega)
+        return t.reshape(n, 5), None, (0 if rc == 0 else -1)
+    fb = C.c_int64()
+    bad = lib().orc_remesh(n, m, t, ntri, tr, omega, C.byref(fb))
+    return t.reshape(n, 5), fb.value, bad

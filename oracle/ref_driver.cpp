@@ -22,6 +22,7 @@
 #include "icos_utils.h"
 #include "fast_rhs.h"
 #include "interp_utils.h"
+#include "remesh.h"
 
 using std::vector;
 
@@ -232,6 +233,30 @@ int ref_rhs_fast(int64_t n, const double* state5, const double* area, double ome
     rhs_func(m, s, a, omega, c);
     std::memcpy(modify5, m.data(), sizeof(double) * 5 * n);
     return c.info;
+}
+
+// remesh.h:109-178 regrid_points2 on the reference's own code, with the
+// vertex -> triangles adjacency built from `tris` in increasing index order
+// (the reference reads it from a CSV file it does not contain).  Returns 0,
+// or -1 when a target lies in no triangle (the reference throws).
+int ref_regrid(int64_t n, const double* moved5, double* target5, int64_t ntri, const int* tris, double omega) {
+    vector<double> moved(moved5, moved5 + 5 * n), target(target5, target5 + 5 * n);
+    vector<vector<int>> triangles(ntri, vector<int>(3)), vert_tris(n);
+    for (int64_t j = 0; j < ntri; j++)
+        for (int k = 0; k < 3; k++) {
+            triangles[j][k] = tris[3 * j + k];
+            vert_tris[tris[3 * j + k]].push_back(int(j));
+        }
+    std::streambuf* old = std::cout.rdbuf(nullptr);  // the reference prints its counts
+    int rc = 0;
+    try {
+        regrid_points2(moved, target, triangles, vert_tris, int(n), int(ntri), omega, 0, int(n), 0);
+    } catch (...) {
+        rc = -1;
+    }
+    std::cout.rdbuf(old);
+    std::memcpy(target5, target.data(), sizeof(double) * 5 * n);
+    return rc;
 }
 
 }  // extern "C"

@@ -134,3 +134,43 @@ def test_reference_drops_edge_particles(oracle):
     g = gold("tree_l3.npz")
     assert (g["loc"][-1] < 0).sum() > 0
     assert (g["loc"][0] >= 0).sum() == g["state"].shape[0]
+
+
+def _moved_grid(oracle, level, scale, seed, far=0):
+    """The level's grid state and the same particles moved by a seeded
+    random displacement of `scale` x the mean spacing (plus `far` of them
+    moved a further 3 spacings), projected back onto the sphere."""
+    s, area, tris = oracle.icos_state(level)
+    h = np.sqrt(4 * np.pi / s.shape[0])
+    rng = np.random.default_rng(seed)
+    m = s.copy()
+    d = scale * h * rng.standard_normal((s.shape[0], 3))
+    if far:
+        d[rng.choice(s.shape[0], far, replace=False)] *= 3.0 / max(scale, 1e-12)
+    m[:, :3] += d
+    m[:, :3] /= np.linalg.norm(m[:, :3], axis=1, keepdims=True)
+    return m, s, tris
+
+
+@need_ref
+@pytest.mark.parametrize("scale,far", [(0.05, 0), (0.3, 8)])
+def test_remesh_bit_exact_vs_reference(oracle, scale, far):
+    """remesh.h regrid_points2: oracle == the reference's own code, including
+    targets found only by the search over all triangles."""
+    m, s, tris = _moved_grid(oracle, 4, scale, seed=21, far=far)
+    got, fb, bad = oracle.remesh(m, s, tris)
+    ref, _, rc = oracle.remesh(m, s, tris, use_ref=True)
+    assert bad == 0 and rc == 0
+    if far:
+        assert fb > 0
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
+    assert np.array_equal(got[:, :3], s[:, :3])        # positions stay on the grid
+
+
+def test_remesh_of_unmoved_grid_is_identity(oracle):
+    """A grid point that is a vertex of its triangle takes that vertex's
+    values (barycentric (1, 0, 0) up to rounding)."""
+    s, area, tris = oracle.icos_state(3)
+    got, fb, bad = oracle.remesh(s, s, tris)
+    assert bad == 0 and fb == 0
+    assert np.allclose(got[:, 3:], s[:, 3:], rtol=0, atol=1e-12 * np.abs(s[:, 3:]).max())
