@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-remesh", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=2048, help="targets in one CPU-baseline sample")
     p.add_argument("--tol", type=float, default=1e-6, help="selector: relative L2 velocity error target")
     p.add_argument("--safety", type=float, default=2.0, help="selector: predicted-error safety factor")
@@ -244,6 +245,65 @@ def cpu_reference_sample(state, area, sample, seed=7):
                       f"{n} sources, {threads} threads, {dt:.2f} s; scaled by N/sample to one RHS, x4 per RK4 step"}
 
 
+def remesh_measure(fss, ctx, state, area, level, stream, reps=5):
+    """The remesh step as the reference's time loop uses it (new_dynamics.cpp
+    213-217: after every RK4 step the moved particles are regridded onto the
+    grid with remesh.h regrid_points2).  From the grid state: one RK4 step,
+    then fss_remesh (host buffers, the drop-in; host wall clock, copies
+    included) and fss_remesh_current (device-resident), both checked bit for
+    bit against the reference's own regrid_points2 on the same input
+    (oracle/_ref, one thread, timed), and `reps` RK4 steps each followed by
+    fss_remesh_current (steps/s with remeshing every step)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    _, tris = fss.icos_grid(level)
+    ctx.set_particles(state, area)
+    ctx.rk4_step(DT, nsteps=1)
+    moved = ctx.get_state()
+    target = moved.copy()
+    target[:, :3] = state[:, :3]
+    fss.remesh(moved, target, tris)              # warm
+    t0 = time.perf_counter()
+    got, fb, bad = fss.remesh(moved, target, tris)
+    wall_ms = 1e3 * (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    ctx.remesh_current(tris)
+    cur_ms = 1e3 * (time.perf_counter() - t0)
+    got_dev = ctx.get_state()
+    stream.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ctx.rk4_step(DT, nsteps=1)
+        ctx.remesh_current(tris)
+    stream.synchronize()
+    loop_s = time.perf_counter() - t0
+    out = {"workload": "one RK4 step from the grid, then regrid onto the grid (the reference's use_remesh loop)",
+           "points": int(moved.shape[0]), "triangles": int(tris.shape[0]), "fallback": fb, "not_found": bad,
+           "wall_ms_host_buffers": wall_ms, "h2d_d2h_bytes": int(2 * moved.nbytes + target.nbytes),
+           "wall_ms_device_resident": cur_ms, "rk4_plus_remesh_steps_per_s": reps / loop_s}
+    if O.ref() is not None:
+        # the reference is O(triangles) per point outside its adjacent
+        # triangles: time it on a contiguous row range from a seeded start,
+        # doubled until it runs ~2 s, and scale by N / rows
+        n = moved.shape[0]
+        lb, k, el = int(np.random.default_rng(11).integers(0, n // 2)), 1, 0.0
+        while True:
+            t0 = time.perf_counter()
+            ref, _, rc = O.remesh(moved, target, tris, use_ref=True, rows=(lb, min(n, lb + k)))
+            el = time.perf_counter() - t0
+            if el >= 2.0 or lb + k >= n or rc != 0:
+                break
+            k *= 2
+        ub = min(n, lb + k)
+        out["cpu_reference_ms"] = 1e3 * el * n / (ub - lb)
+        out["cpu_reference"] = (f"remesh.h regrid_points2 (oracle/_ref), 1 thread, rows {lb}..{ub} "
+                                f"({el:.2f} s), scaled by N/rows")
+        out["bit_exact_vs_reference_rows"] = bool(
+            rc == 0 and np.array_equal(got[lb:ub].view(np.uint64), ref[lb:ub].view(np.uint64))
+            and np.array_equal(got_dev[lb:ub].view(np.uint64), ref[lb:ub].view(np.uint64)))
+    return out
+
+
 def main_reference(args, ws, rank):
     if rank != 0:
         return
@@ -387,6 +447,14 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_reference_sample(state, area, args.cpu_sample)
 
+    # the remesh step: one RK4 step from the grid, regridded back onto it
+    remesh = None
+    if rank == 0 and ws == 1 and not args.no_remesh:
+        try:
+            remesh = remesh_measure(fss, ctx, state, area, args.level, stream)
+        except fss.FssError as e:  # too many points left their triangles in one step
+            remesh = {"error": str(e)}
+
     ctx.close()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -414,7 +482,7 @@ def main():
                 "fp64_same_algorithm": fp64c,
                 "ratio_vs_fp64_same_algorithm": (value / fp64c["value"]) if fp64c else None,
                 "interactions_per_rhs": inter, "tree": info,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "remesh": remesh,
                 "gpu_launches": int(round(launches_per_step * args.steps)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)

@@ -9,8 +9,9 @@ namespace fss {
 // system [v1 v2 v3] c = p solved by LU with partial pivoting in LAPACK
 // dgetf2/dgetrs order (helpers.h:137-150 barycoords via dgesv_).  Every
 // operation is an explicitly rounded intrinsic, so no multiply-add is fused
-// and the result is bit-identical to the host FP64 arithmetic.
-__device__ __forceinline__ void cone_coords_exact(const double* v1, const double* v2, const double* v3,
+// and the result is bit-identical to the host FP64 arithmetic.  Returns true
+// when a pivot is exactly zero (then b = p, as dgesv_ leaves it).
+__device__ __forceinline__ bool cone_coords_exact(const double* v1, const double* v2, const double* v3,
                                                   const double* p, double* b) {
     double a[9] = {v1[0], v1[1], v1[2], v2[0], v2[1], v2[2], v3[0], v3[1], v3[2]};  // a[i + 3j]
     b[0] = p[0]; b[1] = p[1]; b[2] = p[2];
@@ -37,7 +38,7 @@ __device__ __forceinline__ void cone_coords_exact(const double* v1, const double
 #pragma unroll
             for (int i = k + 1; i < 3; i++) a[i + 3 * j] = __dsub_rn(a[i + 3 * j], __dmul_rn(a[i + 3 * k], a[k + 3 * j]));
     }
-    if (singular) return;  // dgesv_ leaves b = p
+    if (singular) return true;  // dgesv_ leaves b = p
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const int pr = ipiv[k];
@@ -54,6 +55,7 @@ __device__ __forceinline__ void cone_coords_exact(const double* v1, const double
         for (int i = 0; i < 2; i++)
             if (i < k) b[i] = __dsub_rn(b[i], __dmul_rn(a[i + 3 * k], b[k]));
     }
+    return false;
 }
 
 }  // namespace fss

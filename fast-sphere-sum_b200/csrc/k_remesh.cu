@@ -62,8 +62,8 @@ __global__ void k_remesh_adjacent(int64_t n, const double* __restrict__ moved5, 
 }
 
 // One block per listed point: the first triangle (lowest index) of the whole
-// moved mesh that contains it.  Points in no triangle keep their values and
-// are counted in `bad`.
+// moved mesh that contains it (few listed points).  Points in no triangle
+// keep their values and are counted in `bad`.
 constexpr int kSearchThreads = 256;
 __global__ void __launch_bounds__(kSearchThreads) k_remesh_search(int32_t nfail, const int32_t* __restrict__ failed,
                                                                   const double* __restrict__ moved5,
@@ -98,6 +98,232 @@ __global__ void __launch_bounds__(kSearchThreads) k_remesh_search(int32_t nfail,
     }
 }
 
+// ---- search over all triangles on a cell grid (many listed points)
+//
+// Cap of a triangle: with u_k = v_k/|v_k|, c = (u_1+u_2+u_3)/|u_1+u_2+u_3|
+// and m = min_k u_k.c, every point p of the cone {sum a_k v_k, a_k >= 0}
+// satisfies (p/|p|).c >= m, since |sum b_k u_k| <= sum b_k.  The LU test is
+// backward stable (partial pivoting: it decides for vertices perturbed by
+// ~1e-15), so a point it places inside still has (p/|p|).c >= m - 1e-13 when
+// m >= 1/2 (then |u_1+u_2+u_3| >= 3/2).  Such a cap, widened by 1e-10, lies
+// in the ball of chord radius sqrt(2 - 2 cos r) about c, so the triangle can
+// contain only points whose unit vector falls in the cells that ball's box
+// covers on a G^3 grid over [-1, 1]^3.  Triangles with m < 1/2, a zero pivot
+// (tested for every point, as the LU then returns b = p), non-finite values,
+// or a box of more than kMaxCells cells go to a list tested for every point.
+// A point takes the lowest index that passes the exact test among its
+// cell's triangles and that list: the same triangle as a scan in index
+// order.  Points whose direction is undefined (zero or non-finite) scan all
+// triangles.
+constexpr int kMaxCells = 64;
+constexpr double kCapSlack = 1e-10;
+
+__device__ __forceinline__ int cell_of(double x, int G) {
+    const double f = floor(__dmul_rn(__dadd_rn(x, 1.0), 0.5 * G));  // G a power of two: 0.5 * G exact
+    return f < 0 ? 0 : (f > G - 1 ? G - 1 : int(f));
+}
+
+// Cap (c, cos r) of triangle j and its cell box; false when the triangle
+// belongs to the list tested for every point.
+__device__ __forceinline__ bool tri_cap(const double* __restrict__ moved5, const int32_t* tv, int G, double4* cap,
+                                        int lo[3], int hi[3]) {
+    const double* v[3] = {moved5 + 5 * int64_t(tv[0]), moved5 + 5 * int64_t(tv[1]), moved5 + 5 * int64_t(tv[2])};
+    double u[3][3], c[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const double r = sqrt(v[k][0] * v[k][0] + v[k][1] * v[k][1] + v[k][2] * v[k][2]);
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            u[k][d] = v[k][d] / r;
+            c[d] += u[k][d];
+        }
+    }
+    const double cn = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+#pragma unroll
+    for (int d = 0; d < 3; d++) c[d] /= cn;
+    double m = 1.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) m = fmin(m, u[k][0] * c[0] + u[k][1] * c[1] + u[k][2] * c[2]);
+    const double cosr = m - kCapSlack;
+    *cap = make_double4(c[0], c[1], c[2], cosr);
+    if (!(m >= 0.5) || !isfinite(c[0]) || !isfinite(c[1]) || !isfinite(c[2])) return false;
+    double b[3];
+    const double q[3] = {c[0], c[1], c[2]};
+    if (cone_coords_exact(v[0], v[1], v[2], q, b)) return false;  // zero pivot
+    const double rho = __dadd_rn(__dsqrt_rn(__dsub_rn(2.0, __dmul_rn(2.0, cosr))), 1e-9);
+    int ncell = 1;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        lo[d] = cell_of(__dsub_rn(c[d], rho), G);
+        hi[d] = cell_of(__dadd_rn(c[d], rho), G);
+        ncell *= hi[d] - lo[d] + 1;
+    }
+    return ncell <= kMaxCells;
+}
+
+// Cell box packed 8 bits per bound (G <= 128); kNoBox marks the list
+// tested for every point.
+constexpr uint64_t kNoBox = ~uint64_t(0);
+__device__ __forceinline__ void unpack_box(uint64_t b, int lo[3], int hi[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        lo[d] = int((b >> (16 * d)) & 255u);
+        hi[d] = int((b >> (16 * d + 8)) & 255u);
+    }
+}
+
+// Caps, cell boxes, per-cell counts, the list tested for every point and
+// the entry total.
+__global__ void k_grid_count(int64_t ntri, const double* __restrict__ moved5, const int32_t* __restrict__ tris, int G,
+                             double4* __restrict__ caps, uint64_t* __restrict__ box, uint32_t* __restrict__ cnt,
+                             int32_t* __restrict__ glist, uint32_t* __restrict__ scal) {
+    const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= ntri) return;
+    double4 cap;
+    int lo[3], hi[3];
+    if (!tri_cap(moved5, tris + 3 * j, G, &cap, lo, hi)) {
+        caps[j] = make_double4(0.0, 0.0, 0.0, -2.0);  // passes every cap test
+        box[j] = kNoBox;
+        glist[atomicAdd(scal + 1, 1u)] = int32_t(j);
+        return;
+    }
+    caps[j] = cap;
+    uint64_t b = 0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) b |= (uint64_t(lo[d]) | (uint64_t(hi[d]) << 8)) << (16 * d);
+    box[j] = b;
+    uint32_t k = 0;
+    for (int x = lo[0]; x <= hi[0]; x++)
+        for (int y = lo[1]; y <= hi[1]; y++)
+            for (int z = lo[2]; z <= hi[2]; z++, k++) atomicAdd(cnt + (int64_t(x) * G + y) * G + z, 1u);
+    atomicAdd(scal, k);
+}
+
+// After the exclusive scan cnt[cell] = start of the cell; each entry takes
+// cnt[cell]++, leaving cnt[cell] = end of the cell (= start of cell + 1).
+__global__ void k_grid_fill(int64_t ntri, const uint64_t* __restrict__ box, int G, uint32_t* __restrict__ cnt,
+                            int32_t* __restrict__ ent) {
+    const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= ntri) return;
+    const uint64_t b = box[j];
+    if (b == kNoBox) return;
+    int lo[3], hi[3];
+    unpack_box(b, lo, hi);
+    for (int x = lo[0]; x <= hi[0]; x++)
+        for (int y = lo[1]; y <= hi[1]; y++)
+            for (int z = lo[2]; z <= hi[2]; z++) ent[atomicAdd(cnt + (int64_t(x) * G + y) * G + z, 1u)] = int32_t(j);
+}
+
+// One warp per listed point.
+constexpr int kGridWarps = 8;
+__global__ void __launch_bounds__(32 * kGridWarps)
+    k_remesh_grid_search(int32_t nfail, const int32_t* __restrict__ failed, const double* __restrict__ moved5,
+                         double* __restrict__ target5, int64_t ntri, const int32_t* __restrict__ tris,
+                         const double4* __restrict__ caps, int G, const uint32_t* __restrict__ cend,
+                         const int32_t* __restrict__ ent, const int32_t* __restrict__ glist, int32_t nglob,
+                         double omega, int32_t* __restrict__ bad) {
+    const int lane = threadIdx.x & 31;
+    const int32_t nwarp = gridDim.x * kGridWarps;
+    for (int32_t f = blockIdx.x * kGridWarps + (threadIdx.x >> 5); f < nfail; f += nwarp) {
+        const int64_t i = failed[f];
+        double* t = target5 + 5 * i;
+        const double p[3] = {t[0], t[1], t[2]};
+        uint32_t best = uint32_t(ntri);
+        double c[3];
+        const double r = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+        if (!(r > 0) || !isfinite(r)) {
+            for (int64_t j = lane; j < ntri; j += 32)
+                if (tri_contains(moved5, tris + 3 * j, p, c)) {
+                    best = uint32_t(j);
+                    break;
+                }
+        } else {
+            const double q[3] = {p[0] / r, p[1] / r, p[2] / r};
+            const int64_t cell = (int64_t(cell_of(q[0], G)) * G + cell_of(q[1], G)) * G + cell_of(q[2], G);
+            const uint32_t e0 = cell ? cend[cell - 1] : 0u, e1 = cend[cell];
+            for (uint32_t k = e0 + lane; k < e1; k += 32) {
+                const int32_t j = ent[k];
+                if (uint32_t(j) >= best) continue;
+                const double4 cp = caps[j];
+                if (q[0] * cp.x + q[1] * cp.y + q[2] * cp.z < cp.w) continue;
+                if (tri_contains(moved5, tris + 3 * int64_t(j), p, c)) best = uint32_t(j);
+            }
+            for (int32_t k = lane; k < nglob; k += 32) {
+                const int32_t j = glist[k];
+                if (uint32_t(j) < best && tri_contains(moved5, tris + 3 * int64_t(j), p, c)) best = uint32_t(j);
+            }
+        }
+        best = __reduce_min_sync(0xffffffffu, best);
+        if (lane == 0) {
+            if (best < uint32_t(ntri)) {
+                const int32_t* tv = tris + 3 * int64_t(best);
+                tri_contains(moved5, tv, p, c);
+                tri_interp_exact(moved5, tv, t, omega, c);
+            } else {
+                atomicAdd(bad, 1);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Power-of-two grid side with cells about three mean triangle edges wide.
+static int grid_side(int64_t ntri) {
+    const double edge = sqrt(4.0 * (4.0 * 3.141592653589793 / double(ntri)) / sqrt(3.0));
+    int G = 4;
+    while (G < 128 && 2.0 / (2 * G) > 3.0 * edge) G *= 2;
+    return G;
+}
+
+// Stream-ordered scratch for the cell-grid search.
+struct GridScratch {
+    cudaStream_t st;
+    void* p[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    explicit GridScratch(cudaStream_t s) : st(s) {}
+    ~GridScratch() {
+        for (void* q : p)
+            if (q) cudaFreeAsync(q, st);
+    }
+};
+
+static cudaError_t grid_search(cudaStream_t st, int32_t nfail, const int32_t* failed, const double* moved5,
+                               double* target5, int64_t ntri, const int32_t* tris, double omega, int32_t* bad) {
+    const int G = grid_side(ntri);
+    const int64_t ncell = int64_t(G) * G * G;
+    GridScratch g(st);
+    cudaError_t e;
+    if ((e = cudaMallocAsync(&g.p[0], size_t(ntri) * sizeof(double4), st)) != cudaSuccess ||
+        (e = cudaMallocAsync(&g.p[1], size_t(ncell) * sizeof(uint32_t), st)) != cudaSuccess ||
+        (e = cudaMallocAsync(&g.p[2], size_t(ntri) * sizeof(int32_t), st)) != cudaSuccess ||
+        (e = cudaMallocAsync(&g.p[3], 2 * sizeof(uint32_t), st)) != cudaSuccess ||
+        (e = cudaMallocAsync(&g.p[5], size_t(ntri) * sizeof(uint64_t), st)) != cudaSuccess)
+        return e;
+    double4* caps = static_cast<double4*>(g.p[0]);
+    uint32_t* cnt = static_cast<uint32_t*>(g.p[1]);
+    int32_t* glist = static_cast<int32_t*>(g.p[2]);
+    uint32_t* scal = static_cast<uint32_t*>(g.p[3]);
+    uint64_t* box = static_cast<uint64_t*>(g.p[5]);
+    if ((e = cudaMemsetAsync(cnt, 0, size_t(ncell) * sizeof(uint32_t), st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(scal, 0, 2 * sizeof(uint32_t), st)) != cudaSuccess)
+        return e;
+    const unsigned tb = unsigned((ntri + 255) / 256);
+    k_grid_count<<<tb, 256, 0, st>>>(ntri, moved5, tris, G, caps, box, cnt, glist, scal);
+    launch_scan_u32(st, cnt, ncell);
+    uint32_t hs[2];
+    if ((e = cudaMemcpyAsync(hs, scal, sizeof(hs), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return e;
+    // every triangle adds at most kMaxCells entries: the total fits 32 bits
+    if ((e = cudaMallocAsync(&g.p[4], size_t(hs[0] ? hs[0] : 1) * sizeof(int32_t), st)) != cudaSuccess) return e;
+    int32_t* ent = static_cast<int32_t*>(g.p[4]);
+    k_grid_fill<<<tb, 256, 0, st>>>(ntri, box, G, cnt, ent);
+    const int32_t blocks = (nfail + kGridWarps - 1) / kGridWarps < 8 * 148 ? (nfail + kGridWarps - 1) / kGridWarps
+                                                                           : 8 * 148;
+    k_remesh_grid_search<<<blocks, 32 * kGridWarps, 0, st>>>(nfail, failed, moved5, target5, ntri, tris, caps, G, cnt,
+                                                             ent, glist, int32_t(hs[1]), omega, bad);
+    return cudaGetLastError();
+}
+
 // Grid positions with the moved state's zeta and tracer (the values kept by
 // a point found in no triangle).
 __global__ void k_remesh_targets(int64_t n, const double* __restrict__ grid3, const double* __restrict__ moved5,
@@ -111,6 +337,9 @@ __global__ void k_remesh_targets(int64_t n, const double* __restrict__ grid3, co
     t[3] = moved5[5 * i + 3];
     t[4] = moved5[5 * i + 4];
 }
+
+// Up to this many listed points a block scans all triangles per point.
+constexpr int32_t kDirectSearchMax = 64;
 
 cudaError_t launch_remesh(cudaStream_t st, int64_t n, const double* moved5, double* target5, int64_t ntri,
                           const int32_t* tris, const int32_t* off, const int32_t* adj, double omega,
@@ -126,9 +355,13 @@ cudaError_t launch_remesh(cudaStream_t st, int64_t n, const double* moved5, doub
         return e;
     int32_t nbad = 0;
     if (nfail > 0) {
-        const int blocks = nfail < 4 * 148 ? nfail : 4 * 148;
-        k_remesh_search<<<blocks, kSearchThreads, 0, st>>>(nfail, failed, moved5, target5, ntri, tris, omega,
-                                                           counters + 1);
+        if (nfail <= kDirectSearchMax || ntri == 0) {
+            k_remesh_search<<<nfail, kSearchThreads, 0, st>>>(nfail, failed, moved5, target5, ntri, tris, omega,
+                                                              counters + 1);
+        } else if ((e = grid_search(st, nfail, failed, moved5, target5, ntri, tris, omega, counters + 1)) !=
+                   cudaSuccess) {
+            return e;
+        }
         if ((e = cudaMemcpyAsync(&nbad, counters + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
             (e = cudaStreamSynchronize(st)) != cudaSuccess)
             return e;

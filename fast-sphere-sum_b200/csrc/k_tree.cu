@@ -333,6 +333,10 @@ void launch_level_hist(cudaStream_t st, int64_t n, int tree_levels, const int32_
     k_level_hist<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, tree_levels, loc, lev_off, counts);
 }
 
+void launch_scan_u32(cudaStream_t st, uint32_t* a, int64_t m) {
+    if (m > 0) k_scan_exclusive<<<1, 1024, 0, st>>>(a, m);
+}
+
 int64_t sort_scratch_words(int64_t n) {
     const int64_t nblk = (n + kSortTile - 1) / kSortTile;
     return 256 * nblk;

@@ -131,6 +131,8 @@ cudaError_t launch_remesh(cudaStream_t st, int64_t n, const double* moved5, doub
                           const int32_t* tris, const int32_t* off, const int32_t* adj, double omega,
                           int32_t* failed, int32_t* counters, int64_t* n_fallback, int64_t* n_not_found);
 void launch_remesh_targets(cudaStream_t st, int64_t n, const double* grid3, const double* moved5, double* target5);
+// In-place exclusive prefix sum of m 32-bit counts (one block).
+void launch_scan_u32(cudaStream_t st, uint32_t* a, int64_t m);
 
 // k_ensemble.cu
 void launch_up_leaf_batch(cudaStream_t st, int nleaf, const void* src, const EnsLeaf* leaves,

@@ -87,6 +87,8 @@ def _setup_ref(R):
     R.ref_rhs_fast.restype = C.c_int
     R.ref_regrid.argtypes = [i64, _D, _D, i64, _I, C.c_double]
     R.ref_regrid.restype = C.c_int
+    R.ref_regrid_range.argtypes = [i64, _D, _D, i64, _I, C.c_double, i64, i64]
+    R.ref_regrid_range.restype = C.c_int
 
 
 _setup(_lib)
@@ -228,15 +230,17 @@ def ref_tree(tree_levels, theta, many_count, state5):
         cap = -np_
 
 
-def remesh(moved5, target5, tris, omega=OMEGA, use_ref=False):
+def remesh(moved5, target5, tris, omega=OMEGA, use_ref=False, rows=None):
     """remesh.h regrid_points2: (new target state, fallback count, not-found
-    count); adjacency in increasing triangle order."""
+    count); adjacency in increasing triangle order.  With use_ref, `rows` =
+    (lb, ub) regrids only those targets (the reference's lb/ub)."""
     m = np.ascontiguousarray(moved5, dtype=np.float64).reshape(-1)
     t = np.ascontiguousarray(target5, dtype=np.float64).copy().reshape(-1)
     tr = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1)
     n, ntri = m.size // 5, tr.size // 3
     if use_ref:
-        rc = ref().ref_regrid(n, m, t, ntri, tr, omega)
+        lb, ub = rows if rows is not None else (0, n)
+        rc = ref().ref_regrid_range(n, m, t, ntri, tr, omega, lb, ub)
         return t.reshape(n, 5), None, (0 if rc == 0 else -1)
     fb = C.c_int64()
     bad = lib().orc_remesh(n, m, t, ntri, tr, omega, C.byref(fb))

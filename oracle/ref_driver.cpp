@@ -238,8 +238,10 @@ int ref_rhs_fast(int64_t n, const double* state5, const double* area, double ome
 // remesh.h:109-178 regrid_points2 on the reference's own code, with the
 // vertex -> triangles adjacency built from `tris` in increasing index order
 // (the reference reads it from a CSV file it does not contain).  Returns 0,
-// or -1 when a target lies in no triangle (the reference throws).
-int ref_regrid(int64_t n, const double* moved5, double* target5, int64_t ntri, const int* tris, double omega) {
+// or -1 when a target lies in no triangle (the reference throws).  Only
+// targets lb <= i < ub are regridded (the reference's own lb/ub arguments).
+int ref_regrid_range(int64_t n, const double* moved5, double* target5, int64_t ntri, const int* tris, double omega,
+                     int64_t lb, int64_t ub) {
     vector<double> moved(moved5, moved5 + 5 * n), target(target5, target5 + 5 * n);
     vector<vector<int>> triangles(ntri, vector<int>(3)), vert_tris(n);
     for (int64_t j = 0; j < ntri; j++)
@@ -250,13 +252,17 @@ int ref_regrid(int64_t n, const double* moved5, double* target5, int64_t ntri, c
     std::streambuf* old = std::cout.rdbuf(nullptr);  // the reference prints its counts
     int rc = 0;
     try {
-        regrid_points2(moved, target, triangles, vert_tris, int(n), int(ntri), omega, 0, int(n), 0);
+        regrid_points2(moved, target, triangles, vert_tris, int(n), int(ntri), omega, int(lb), int(ub), 0);
     } catch (...) {
         rc = -1;
     }
     std::cout.rdbuf(old);
     std::memcpy(target5, target.data(), sizeof(double) * 5 * n);
     return rc;
+}
+
+int ref_regrid(int64_t n, const double* moved5, double* target5, int64_t ntri, const int* tris, double omega) {
+    return ref_regrid_range(n, moved5, target5, ntri, tris, omega, 0, n);
 }
 
 }  // extern "C"

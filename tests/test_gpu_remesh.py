@@ -21,7 +21,7 @@ def _moved(oracle, level, scale, seed, far=0):
     return m, s, tris
 
 
-@pytest.mark.parametrize("level,scale,far", [(4, 0.05, 0), (4, 0.3, 12), (6, 0.2, 40)])
+@pytest.mark.parametrize("level,scale,far", [(4, 0.05, 0), (4, 0.3, 12), (6, 0.2, 40), (6, 0.2, 400)])
 def test_remesh_bit_exact_vs_oracle(fss, oracle, level, scale, far):
     m, s, tris = _moved(oracle, level, scale, seed=level + far, far=far)
     ref, fb_ref, bad_ref = oracle.remesh(m, s, tris)
@@ -60,3 +60,15 @@ def test_remesh_rejects_bad_triangles(fss, oracle):
     bad[0, 0] = s.shape[0]
     with pytest.raises(fss.FssError):
         fss.remesh(s, s, bad)
+
+
+
+def test_remesh_many_fallbacks_cell_grid(fss, oracle):
+    """Hundreds of points outside their adjacent triangles, on a mesh
+    tangled enough that some triangles go to the always-tested list: the
+    cell-grid search picks the same (first) triangle as the oracle's scan."""
+    m, s, tris = _moved(oracle, 5, 1.5, seed=1)
+    ref, fb_ref, bad_ref = oracle.remesh(m, s, tris)
+    got, fb, bad = fss.remesh(m, s, tris)
+    assert fb == fb_ref and fb > 64 and bad == bad_ref
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
