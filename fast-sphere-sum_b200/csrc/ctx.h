@@ -14,30 +14,6 @@
 
 namespace fss {
 
-struct DBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    ~DBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    cudaError_t ensure(size_t b) {
-        if (b <= bytes && p) return cudaSuccess;
-        release();
-        if (b == 0) b = 16;
-        cudaError_t e = cudaMalloc(&p, b);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return e;
-        }
-        bytes = b;
-        return cudaSuccess;
-    }
-    template <typename T> T* as() const { return static_cast<T*>(p); }
-};
-
 struct ProfEntry {
     double ms = 0;
     int64_t launches = 0;
@@ -103,7 +79,7 @@ struct fss_ctx {
     // device
     DBuf in5, area_in, perm, key, key_tmp, vals_tmp, hist, leaf_start, s0, xs, acc, area_s, tracer_s, src, partials,
         segs, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
-        wtotal, err_flag, loc, sortq, grid3, rm_target, rm_tris, rm_off, rm_adj, rm_failed, rm_cnt, down_jobs, down_of_face, down_coef, bary, bary_off, vinvT;
+        wtotal, err_flag, loc, sortq, grid3, rm_target, rm_tris, rm_off, rm_adj, down_jobs, down_of_face, down_coef, bary, bary_off, vinvT;
     int64_t src_count = 0;
 
     // graph
@@ -118,6 +94,11 @@ struct fss_ctx {
     std::vector<std::string> prof_order;
 
     std::unique_ptr<fss_ctx> alt;  // the other method, created on demand
+    // remesh: device triangles and adjacency of the last call, kept while
+    // the caller's triangles (host copy) and the particle count are unchanged
+    fss::RemeshScratch rm;
+    std::vector<int32_t> rm_tris_host;
+    int64_t rm_n = -1;
 
     ~fss_ctx() {
         if (graph) cudaGraphExecDestroy(graph);

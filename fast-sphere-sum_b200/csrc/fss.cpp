@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1115,22 +1116,25 @@ const char* fss_version(void) { return "fss-b200 0.1 (sm_100a; direct sum + icos
 
 // ------------------------------------------------------------------ remesh
 
+
 namespace {
-// Vertex -> triangles adjacency (CSR, increasing triangle order), after
-// checking every vertex index.
-bool remesh_adjacency(int64_t n, int64_t ntri, const int32_t* tris, std::vector<int32_t>& off,
-                      std::vector<int32_t>& adj) {
-    off.assign(size_t(n) + 1, 0);
-    for (int64_t j = 0; j < 3 * ntri; j++) {
-        if (tris[j] < 0 || tris[j] >= n) return false;
-        off[size_t(tris[j]) + 1]++;
-    }
-    for (int64_t i = 0; i < n; i++) off[i + 1] += off[i];
-    adj.assign(size_t(3 * ntri), 0);
-    std::vector<int32_t> fill(off.begin(), off.end() - 1);
-    for (int64_t j = 0; j < ntri; j++)
-        for (int k = 0; k < 3; k++) adj[fill[tris[3 * j + k]]++] = int32_t(j);
-    return true;
+// fss_remesh's device buffers, kept per device between calls (never freed:
+// they live until the process ends) and used under a lock.
+struct RemeshHost {
+    std::mutex mu;
+    cudaStream_t st = nullptr;
+    DBuf dm, dt, dtri, doff, dadj;
+    fss::RemeshScratch rs;
+    std::vector<int32_t> tris_host;
+    int64_t n = -1;
+};
+constexpr int kMaxDevices = 64;
+RemeshHost* remesh_host(int dev) {
+    static std::mutex mu;
+    static RemeshHost* h[kMaxDevices] = {};
+    std::lock_guard<std::mutex> g(mu);
+    if (!h[dev]) h[dev] = new RemeshHost;
+    return h[dev];
 }
 }  // namespace
 
@@ -1140,30 +1144,38 @@ int fss_remesh(int64_t n, const double* moved5, double* target5, int64_t ntri, c
     if (n < 3 || ntri < 1 || !moved5 || !target5 || !tris) return fail(c, FSS_ERR_INVALID, "bad remesh arguments");
     if (n > (int64_t(1) << 30) || 3 * ntri > (int64_t(1) << 31) - 1)
         return fail(c, FSS_ERR_INVALID, "too many particles or triangles");
-    std::vector<int32_t> off, adj;
-    if (!remesh_adjacency(n, ntri, tris, off, adj)) return fail(c, FSS_ERR_INVALID, "triangle vertex out of range");
-    cudaStream_t st;
-    CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    struct StreamGuard {
-        cudaStream_t s;
-        ~StreamGuard() { cudaStreamDestroy(s); }
-    } guard{st};
-    DBuf dm, dt, dtri, doff, dadj, dfail, dcnt;
-    CU(dm.ensure(sizeof(double) * 5 * size_t(n)));
-    CU(dt.ensure(sizeof(double) * 5 * size_t(n)));
-    CU(dtri.ensure(sizeof(int32_t) * 3 * size_t(ntri)));
-    CU(doff.ensure(sizeof(int32_t) * off.size()));
-    CU(dadj.ensure(sizeof(int32_t) * adj.size()));
-    CU(dfail.ensure(sizeof(int32_t) * size_t(n)));
-    CU(dcnt.ensure(2 * sizeof(int32_t)));
-    CU(cudaMemcpyAsync(dm.p, moved5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(dt.p, target5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(dtri.p, tris, sizeof(int32_t) * 3 * ntri, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(doff.p, off.data(), sizeof(int32_t) * off.size(), cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(dadj.p, adj.data(), sizeof(int32_t) * adj.size(), cudaMemcpyHostToDevice, st));
-    CU(launch_remesh(st, n, dm.as<double>(), dt.as<double>(), ntri, dtri.as<int32_t>(), doff.as<int32_t>(),
-                     dadj.as<int32_t>(), omega, dfail.as<int32_t>(), dcnt.as<int32_t>(), n_fallback, n_not_found));
-    CU(cudaMemcpyAsync(target5, dt.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, st));
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(c, FSS_ERR_UNSUPPORTED, "device index out of range");
+    RemeshHost& h = *remesh_host(dev);
+    std::lock_guard<std::mutex> lock(h.mu);
+    if (!h.st) CU(cudaStreamCreateWithFlags(&h.st, cudaStreamNonBlocking));
+    cudaStream_t st = h.st;
+    CU(h.dm.ensure(sizeof(double) * 5 * size_t(n)));
+    CU(h.dt.ensure(sizeof(double) * 5 * size_t(n)));
+    CU(cudaMemcpyAsync(h.dm.p, moved5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(h.dt.p, target5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, st));
+    const bool same = h.n == n && h.tris_host.size() == size_t(3 * ntri) &&
+                      std::memcmp(h.tris_host.data(), tris, sizeof(int32_t) * 3 * ntri) == 0;
+    if (!same) {
+        h.n = -1;
+        h.tris_host.assign(tris, tris + 3 * ntri);
+        CU(h.dtri.ensure(sizeof(int32_t) * 3 * size_t(ntri)));
+        CU(h.doff.ensure(sizeof(uint32_t) * size_t(n + 1)));
+        CU(h.dadj.ensure(sizeof(int32_t) * 3 * size_t(ntri)));
+        CU(cudaMemcpyAsync(h.dtri.p, h.tris_host.data(), sizeof(int32_t) * 3 * ntri, cudaMemcpyHostToDevice, st));
+        bool valid = false;
+        CU(launch_remesh_adjacency(st, n, ntri, h.dtri.as<int32_t>(), h.doff.as<uint32_t>(), h.dadj.as<int32_t>(),
+                                   h.rs, &valid));
+        if (!valid) {
+            h.tris_host.clear();
+            return fail(c, FSS_ERR_INVALID, "triangle vertex out of range");
+        }
+        h.n = n;
+    }
+    CU(launch_remesh(st, n, h.dm.as<double>(), h.dt.as<double>(), ntri, h.dtri.as<int32_t>(), h.doff.as<uint32_t>(),
+                     h.dadj.as<int32_t>(), omega, h.rs, n_fallback, n_not_found));
+    CU(cudaMemcpyAsync(target5, h.dt.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
     return FSS_OK;
 }
@@ -1175,22 +1187,34 @@ int fss_remesh_current(fss_ctx* c, int64_t ntri, const int32_t* tris, double ome
     if (3 * ntri > (int64_t(1) << 31) - 1) return fail(c, FSS_ERR_INVALID, "too many triangles");
     CU(cudaSetDevice(c->dev));
     const int64_t n = c->n;
-    std::vector<int32_t> off, adj;
-    if (!remesh_adjacency(n, ntri, tris, off, adj)) return fail(c, FSS_ERR_INVALID, "triangle vertex out of range");
-    TRY(upload(c, c->rm_tris, std::vector<int32_t>(tris, tris + 3 * ntri)));
-    TRY(upload(c, c->rm_off, off));
-    TRY(upload(c, c->rm_adj, adj));
+    // triangles and adjacency: rebuilt on the device only when they changed
+    const bool same = c->rm_n == n && c->rm_tris_host.size() == size_t(3 * ntri) &&
+                      std::memcmp(c->rm_tris_host.data(), tris, sizeof(int32_t) * 3 * ntri) == 0;
+    if (!same) {
+        c->rm_n = -1;
+        c->rm_tris_host.assign(tris, tris + 3 * ntri);
+        CU(c->rm_tris.ensure(sizeof(int32_t) * 3 * size_t(ntri)));
+        CU(c->rm_off.ensure(sizeof(uint32_t) * size_t(n + 1)));
+        CU(c->rm_adj.ensure(sizeof(int32_t) * 3 * size_t(ntri)));
+        CU(cudaMemcpyAsync(c->rm_tris.p, c->rm_tris_host.data(), sizeof(int32_t) * 3 * ntri, cudaMemcpyHostToDevice,
+                           c->stream));
+        bool valid = false;
+        CU(launch_remesh_adjacency(c->stream, n, ntri, c->rm_tris.as<int32_t>(), c->rm_off.as<uint32_t>(),
+                                   c->rm_adj.as<int32_t>(), c->rm, &valid));
+        if (!valid) {
+            c->rm_tris_host.clear();
+            return fail(c, FSS_ERR_INVALID, "triangle vertex out of range");
+        }
+        c->rm_n = n;
+    }
     CU(c->rm_target.ensure(sizeof(double) * 5 * size_t(n)));
-    CU(c->rm_failed.ensure(sizeof(int32_t) * size_t(n)));
-    CU(c->rm_cnt.ensure(2 * sizeof(int32_t)));
     TRY(refresh_stage(c));
     // moved state in the caller's order, targets = grid positions
     launch_scatter_state(c->stream, n, c->tree ? c->perm.as<int32_t>() : nullptr, c->s0.as<double4>(),
                          c->tracer_s.as<double>(), c->out5.as<double>());
     launch_remesh_targets(c->stream, n, c->grid3.as<double>(), c->out5.as<double>(), c->rm_target.as<double>());
     CU(launch_remesh(c->stream, n, c->out5.as<double>(), c->rm_target.as<double>(), ntri, c->rm_tris.as<int32_t>(),
-                     c->rm_off.as<int32_t>(), c->rm_adj.as<int32_t>(), omega, c->rm_failed.as<int32_t>(),
-                     c->rm_cnt.as<int32_t>(), n_fallback, n_not_found));
+                     c->rm_off.as<uint32_t>(), c->rm_adj.as<int32_t>(), omega, c->rm, n_fallback, n_not_found));
     // the regridded state becomes the step state (sorted order of the
     // context), then particles go back into the leaves of their grid points
     CU(cudaMemcpyAsync(c->in5.p, c->rm_target.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToDevice, c->stream));

@@ -43,7 +43,7 @@ __device__ __forceinline__ void tri_interp_exact(const double* __restrict__ move
 // (adjacency adj[off[i] .. off[i+1]) in increasing triangle order).  Points
 // found in none are listed in `failed`.
 __global__ void k_remesh_adjacent(int64_t n, const double* __restrict__ moved5, double* __restrict__ target5,
-                                  const int32_t* __restrict__ tris, const int32_t* __restrict__ off,
+                                  const int32_t* __restrict__ tris, const uint32_t* __restrict__ off,
                                   const int32_t* __restrict__ adj, double omega, int32_t* __restrict__ failed,
                                   int32_t* __restrict__ nfailed) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -51,7 +51,7 @@ __global__ void k_remesh_adjacent(int64_t n, const double* __restrict__ moved5, 
     double* t = target5 + 5 * i;
     const double p[3] = {t[0], t[1], t[2]};
     double c[3];
-    for (int32_t a = off[i]; a < off[i + 1]; a++) {
+    for (uint32_t a = off[i]; a < off[i + 1]; a++) {
         const int32_t* tv = tris + 3 * int64_t(adj[a]);
         if (tri_contains(moved5, tv, p, c)) {
             tri_interp_exact(moved5, tv, t, omega, c);
@@ -59,6 +59,73 @@ __global__ void k_remesh_adjacent(int64_t n, const double* __restrict__ moved5, 
         }
     }
     failed[atomicAdd(nfailed, 1)] = int32_t(i);
+}
+
+// ---- vertex -> triangles adjacency (count, scan, fill, per-vertex sort)
+__global__ void k_adj_count(int64_t n, int64_t ntri, const int32_t* __restrict__ tris, uint32_t* __restrict__ cnt,
+                            uint32_t* __restrict__ bad) {
+    const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= 3 * ntri) return;
+    const int32_t v = tris[j];
+    if (v < 0 || int64_t(v) >= n)
+        atomicOr(bad, 1u);
+    else
+        atomicAdd(cnt + v, 1u);
+}
+
+__global__ void k_adj_fill(int64_t n, int64_t ntri, const int32_t* __restrict__ tris, uint32_t* __restrict__ cur,
+                           int32_t* __restrict__ adj) {
+    const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= 3 * ntri) return;
+    const int32_t v = tris[j];
+    if (v >= 0 && int64_t(v) < n) adj[atomicAdd(cur + v, 1u)] = int32_t(j / 3);
+}
+
+// Each vertex's list into increasing triangle order (insertion sort: a few
+// entries per vertex on a triangulated sphere).
+__global__ void k_adj_sort(int64_t n, const uint32_t* __restrict__ off, int32_t* __restrict__ adj) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t a = off[i], b = off[i + 1];
+    for (uint32_t k = a + 1; k < b; k++) {
+        const int32_t x = adj[k];
+        uint32_t q = k;
+        while (q > a && adj[q - 1] > x) {
+            adj[q] = adj[q - 1];
+            q--;
+        }
+        adj[q] = x;
+    }
+}
+
+cudaError_t launch_remesh_adjacency(cudaStream_t st, int64_t n, int64_t ntri, const int32_t* tris, uint32_t* off,
+                                    int32_t* adj, RemeshScratch& s, bool* valid) {
+    cudaError_t e;
+    *valid = false;
+    if ((e = s.scal.ensure(2 * sizeof(uint32_t))) != cudaSuccess ||
+        (e = s.adj_cur.ensure(size_t(n + 1) * sizeof(uint32_t))) != cudaSuccess ||
+        (e = s.part.ensure(size_t(scan_part_words(n + 1)) * sizeof(uint32_t))) != cudaSuccess)
+        return e;
+    uint32_t* flag = s.scal.as<uint32_t>();
+    uint32_t* cur = s.adj_cur.as<uint32_t>();
+    if ((e = cudaMemsetAsync(off, 0, size_t(n + 1) * sizeof(uint32_t), st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(flag, 0, sizeof(uint32_t), st)) != cudaSuccess)
+        return e;
+    const unsigned g3 = unsigned((3 * ntri + 255) / 256);
+    k_adj_count<<<g3, 256, 0, st>>>(n, ntri, tris, off, flag);
+    uint32_t hbad = 1;
+    if ((e = cudaMemcpyAsync(&hbad, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return e;
+    if (hbad) return cudaGetLastError();
+    launch_scan_u32(st, off, n + 1, s.part.as<uint32_t>());
+    if ((e = cudaMemcpyAsync(cur, off, size_t(n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st)) !=
+        cudaSuccess)
+        return e;
+    k_adj_fill<<<g3, 256, 0, st>>>(n, ntri, tris, cur, adj);
+    k_adj_sort<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, off, adj);
+    *valid = true;
+    return cudaGetLastError();
 }
 
 // One block per listed point: the first triangle (lowest index) of the whole
@@ -275,47 +342,37 @@ static int grid_side(int64_t ntri) {
     return G;
 }
 
-// Stream-ordered scratch for the cell-grid search.
-struct GridScratch {
-    cudaStream_t st;
-    void* p[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    explicit GridScratch(cudaStream_t s) : st(s) {}
-    ~GridScratch() {
-        for (void* q : p)
-            if (q) cudaFreeAsync(q, st);
-    }
-};
-
 static cudaError_t grid_search(cudaStream_t st, int32_t nfail, const int32_t* failed, const double* moved5,
-                               double* target5, int64_t ntri, const int32_t* tris, double omega, int32_t* bad) {
+                               double* target5, int64_t ntri, const int32_t* tris, double omega, int32_t* bad,
+                               RemeshScratch& s) {
     const int G = grid_side(ntri);
     const int64_t ncell = int64_t(G) * G * G;
-    GridScratch g(st);
     cudaError_t e;
-    if ((e = cudaMallocAsync(&g.p[0], size_t(ntri) * sizeof(double4), st)) != cudaSuccess ||
-        (e = cudaMallocAsync(&g.p[1], size_t(ncell) * sizeof(uint32_t), st)) != cudaSuccess ||
-        (e = cudaMallocAsync(&g.p[2], size_t(ntri) * sizeof(int32_t), st)) != cudaSuccess ||
-        (e = cudaMallocAsync(&g.p[3], 2 * sizeof(uint32_t), st)) != cudaSuccess ||
-        (e = cudaMallocAsync(&g.p[5], size_t(ntri) * sizeof(uint64_t), st)) != cudaSuccess)
+    if ((e = s.caps.ensure(size_t(ntri) * sizeof(double4))) != cudaSuccess ||
+        (e = s.box.ensure(size_t(ntri) * sizeof(uint64_t))) != cudaSuccess ||
+        (e = s.cells.ensure(size_t(ncell) * sizeof(uint32_t))) != cudaSuccess ||
+        (e = s.glist.ensure(size_t(ntri) * sizeof(int32_t))) != cudaSuccess ||
+        (e = s.scal.ensure(2 * sizeof(uint32_t))) != cudaSuccess ||
+        (e = s.part.ensure(size_t(scan_part_words(ncell)) * sizeof(uint32_t))) != cudaSuccess)
         return e;
-    double4* caps = static_cast<double4*>(g.p[0]);
-    uint32_t* cnt = static_cast<uint32_t*>(g.p[1]);
-    int32_t* glist = static_cast<int32_t*>(g.p[2]);
-    uint32_t* scal = static_cast<uint32_t*>(g.p[3]);
-    uint64_t* box = static_cast<uint64_t*>(g.p[5]);
+    double4* caps = s.caps.as<double4>();
+    uint64_t* box = s.box.as<uint64_t>();
+    uint32_t* cnt = s.cells.as<uint32_t>();
+    int32_t* glist = s.glist.as<int32_t>();
+    uint32_t* scal = s.scal.as<uint32_t>();
     if ((e = cudaMemsetAsync(cnt, 0, size_t(ncell) * sizeof(uint32_t), st)) != cudaSuccess ||
         (e = cudaMemsetAsync(scal, 0, 2 * sizeof(uint32_t), st)) != cudaSuccess)
         return e;
     const unsigned tb = unsigned((ntri + 255) / 256);
     k_grid_count<<<tb, 256, 0, st>>>(ntri, moved5, tris, G, caps, box, cnt, glist, scal);
-    launch_scan_u32(st, cnt, ncell);
+    launch_scan_u32(st, cnt, ncell, s.part.as<uint32_t>());
     uint32_t hs[2];
     if ((e = cudaMemcpyAsync(hs, scal, sizeof(hs), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return e;
     // every triangle adds at most kMaxCells entries: the total fits 32 bits
-    if ((e = cudaMallocAsync(&g.p[4], size_t(hs[0] ? hs[0] : 1) * sizeof(int32_t), st)) != cudaSuccess) return e;
-    int32_t* ent = static_cast<int32_t*>(g.p[4]);
+    if ((e = s.ent.ensure(size_t(hs[0] ? hs[0] : 1) * sizeof(int32_t))) != cudaSuccess) return e;
+    int32_t* ent = s.ent.as<int32_t>();
     k_grid_fill<<<tb, 256, 0, st>>>(ntri, box, G, cnt, ent);
     const int32_t blocks = (nfail + kGridWarps - 1) / kGridWarps < 8 * 148 ? (nfail + kGridWarps - 1) / kGridWarps
                                                                            : 8 * 148;
@@ -342,11 +399,16 @@ __global__ void k_remesh_targets(int64_t n, const double* __restrict__ grid3, co
 constexpr int32_t kDirectSearchMax = 64;
 
 cudaError_t launch_remesh(cudaStream_t st, int64_t n, const double* moved5, double* target5, int64_t ntri,
-                          const int32_t* tris, const int32_t* off, const int32_t* adj, double omega,
-                          int32_t* failed, int32_t* counters, int64_t* n_fallback, int64_t* n_not_found) {
+                          const int32_t* tris, const uint32_t* off, const int32_t* adj, double omega,
+                          RemeshScratch& s, int64_t* n_fallback, int64_t* n_not_found) {
     if (n == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), st);
-    if (e != cudaSuccess) return e;
+    cudaError_t e;
+    if ((e = s.failed.ensure(size_t(n) * sizeof(int32_t))) != cudaSuccess ||
+        (e = s.counters.ensure(2 * sizeof(int32_t))) != cudaSuccess)
+        return e;
+    int32_t* failed = s.failed.as<int32_t>();
+    int32_t* counters = s.counters.as<int32_t>();
+    if ((e = cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), st)) != cudaSuccess) return e;
     k_remesh_adjacent<<<unsigned((n + 127) / 128), 128, 0, st>>>(n, moved5, target5, tris, off, adj, omega, failed,
                                                                  counters);
     int32_t nfail = 0;
@@ -358,7 +420,7 @@ cudaError_t launch_remesh(cudaStream_t st, int64_t n, const double* moved5, doub
         if (nfail <= kDirectSearchMax || ntri == 0) {
             k_remesh_search<<<nfail, kSearchThreads, 0, st>>>(nfail, failed, moved5, target5, ntri, tris, omega,
                                                               counters + 1);
-        } else if ((e = grid_search(st, nfail, failed, moved5, target5, ntri, tris, omega, counters + 1)) !=
+        } else if ((e = grid_search(st, nfail, failed, moved5, target5, ntri, tris, omega, counters + 1, s)) !=
                    cudaSuccess) {
             return e;
         }

@@ -88,59 +88,97 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(int64_t n, const ui
     hist[int64_t(threadIdx.x) * nblk + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of m entries in one block of 1024 threads, in chunks of
+// Exclusive scan of 32-bit counts by blocks of 1024 threads, in chunks of
 // 1024 x kScanPer entries staged through shared memory (coalesced loads and
 // stores; each thread scans kScanPer consecutive entries; warp-shuffle scan
-// of the thread sums; a running carry across chunks).
+// of the thread sums).  scan_chunk scans one chunk from a carry and returns
+// the carry after it (all threads).
 constexpr int kScanPer = 8;
-__global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ a, int64_t m) {
-    __shared__ uint32_t buf[1024 * kScanPer];
-    __shared__ uint32_t wsum[32];
-    __shared__ uint32_t carry_s;
+constexpr int64_t kScanChunk = 1024 * kScanPer;
+
+struct ScanSmem {
+    uint32_t buf[kScanChunk];
+    uint32_t wsum[32];
+    uint32_t carry;
+};
+
+__device__ __forceinline__ uint32_t scan_chunk(uint32_t* __restrict__ a, int64_t m, int64_t base, uint32_t carry,
+                                               ScanSmem& sm) {
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    if (t == 0) carry_s = 0;
-    for (int64_t base = 0; base < m; base += 1024 * kScanPer) {
-        for (int k = 0; k < kScanPer; k++) {
-            const int64_t i = base + int64_t(k) * 1024 + t;
-            buf[k * 1024 + t] = (i < m) ? a[i] : 0u;
-        }
-        __syncthreads();
-        uint32_t v[kScanPer], s = 0;
-        for (int k = 0; k < kScanPer; k++) {
-            v[k] = buf[t * kScanPer + k];
-            s += v[k];
-        }
-        // inclusive scan of the thread sums
-        uint32_t x = s;
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
-            if (lane >= d) x += y;
-        }
-        if (lane == 31) wsum[w] = x;
-        __syncthreads();
-        if (w == 0) {
-            uint32_t z = wsum[lane];
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, z, d);
-                if (lane >= d) z += y;
-            }
-            wsum[lane] = z;
-        }
-        __syncthreads();
-        const uint32_t carry = carry_s;
-        uint32_t run = carry + (x - s) + (w > 0 ? wsum[w - 1] : 0u);
-        for (int k = 0; k < kScanPer; k++) {
-            buf[t * kScanPer + k] = run;
-            run += v[k];
-        }
-        __syncthreads();
-        if (t == 1023) carry_s = run;
-        for (int k = 0; k < kScanPer; k++) {
-            const int64_t i = base + int64_t(k) * 1024 + t;
-            if (i < m) a[i] = buf[k * 1024 + t];
-        }
-        __syncthreads();
+    for (int k = 0; k < kScanPer; k++) {
+        const int64_t i = base + int64_t(k) * 1024 + t;
+        sm.buf[k * 1024 + t] = (i < m) ? a[i] : 0u;
     }
+    __syncthreads();
+    uint32_t v[kScanPer], s = 0;
+    for (int k = 0; k < kScanPer; k++) {
+        v[k] = sm.buf[t * kScanPer + k];
+        s += v[k];
+    }
+    // inclusive scan of the thread sums
+    uint32_t x = s;
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) sm.wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t z = sm.wsum[lane];
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, z, d);
+            if (lane >= d) z += y;
+        }
+        sm.wsum[lane] = z;
+    }
+    __syncthreads();
+    uint32_t run = carry + (x - s) + (w > 0 ? sm.wsum[w - 1] : 0u);
+    for (int k = 0; k < kScanPer; k++) {
+        sm.buf[t * kScanPer + k] = run;
+        run += v[k];
+    }
+    __syncthreads();
+    if (t == 1023) sm.carry = run;
+    for (int k = 0; k < kScanPer; k++) {
+        const int64_t i = base + int64_t(k) * 1024 + t;
+        if (i < m) a[i] = sm.buf[k * 1024 + t];
+    }
+    __syncthreads();
+    return sm.carry;
+}
+
+// One block, all chunks in turn.
+__global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ a, int64_t m) {
+    __shared__ ScanSmem sm;
+    uint32_t carry = 0;
+    for (int64_t base = 0; base < m; base += kScanChunk) carry = scan_chunk(a, m, base, carry, sm);
+}
+
+// Large scans: chunk totals, one-block scan of the totals, then every chunk
+// scanned from its offset by its own block.
+__global__ void __launch_bounds__(1024) k_chunk_totals(const uint32_t* __restrict__ a, int64_t m,
+                                                       uint32_t* __restrict__ tot) {
+    __shared__ uint32_t wsum[32];
+    const int64_t base = int64_t(blockIdx.x) * kScanChunk;
+    uint32_t s = 0;
+    for (int k = 0; k < kScanPer; k++) {
+        const int64_t i = base + int64_t(k) * 1024 + threadIdx.x;
+        if (i < m) s += a[i];
+    }
+    for (int d = 16; d > 0; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = wsum[threadIdx.x];
+        for (int d = 16; d > 0; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
+        if (threadIdx.x == 0) tot[blockIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_chunk_scan(uint32_t* __restrict__ a, int64_t m,
+                                                     const uint32_t* __restrict__ off) {
+    __shared__ ScanSmem sm;
+    scan_chunk(a, m, int64_t(blockIdx.x) * kScanChunk, off[blockIdx.x], sm);
 }
 
 __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(int64_t n, const uint32_t* __restrict__ kin,
@@ -333,8 +371,18 @@ void launch_level_hist(cudaStream_t st, int64_t n, int tree_levels, const int32_
     k_level_hist<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, tree_levels, loc, lev_off, counts);
 }
 
-void launch_scan_u32(cudaStream_t st, uint32_t* a, int64_t m) {
-    if (m > 0) k_scan_exclusive<<<1, 1024, 0, st>>>(a, m);
+int64_t scan_part_words(int64_t m) { return (m + kScanChunk - 1) / kScanChunk; }
+
+void launch_scan_u32(cudaStream_t st, uint32_t* a, int64_t m, uint32_t* part) {
+    if (m <= 0) return;
+    const int64_t nchunk = scan_part_words(m);
+    if (nchunk <= 4 || !part) {
+        k_scan_exclusive<<<1, 1024, 0, st>>>(a, m);
+        return;
+    }
+    k_chunk_totals<<<unsigned(nchunk), 1024, 0, st>>>(a, m, part);
+    k_scan_exclusive<<<1, 1024, 0, st>>>(part, nchunk);
+    k_chunk_scan<<<unsigned(nchunk), 1024, 0, st>>>(a, m, part);
 }
 
 int64_t sort_scratch_words(int64_t n) {

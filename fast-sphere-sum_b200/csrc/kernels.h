@@ -4,6 +4,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 
+#include "dbuf.h"
 #include "fss_internal.h"
 
 namespace fss {
@@ -123,16 +124,28 @@ void launch_scatter_state(cudaStream_t st, int64_t n, const int32_t* perm, const
                           double* out5);
 
 // k_remesh.cu
+// Device scratch of the remesh step, grown on demand and kept by its owner
+// between calls.
+struct RemeshScratch {
+    DBuf failed, counters, adj_cur, caps, box, cells, glist, scal, ent, part;
+};
+// Vertex -> triangles adjacency of `tris` in increasing triangle order:
+// off[n + 1] (32-bit), adj[3 ntri].  *valid = false (nothing else usable)
+// when a vertex index is outside [0, n).  Synchronises the stream.
+cudaError_t launch_remesh_adjacency(cudaStream_t st, int64_t n, int64_t ntri, const int32_t* tris, uint32_t* off,
+                                    int32_t* adj, RemeshScratch& s, bool* valid);
 // Remesh targets (grid points, 5 doubles each, zeta and tracer replaced
 // where a moved-mesh triangle contains them); returns the number of points
 // that needed the search over all triangles and the number found nowhere.
 // Synchronises the stream (the fallback search is sized on the host).
 cudaError_t launch_remesh(cudaStream_t st, int64_t n, const double* moved5, double* target5, int64_t ntri,
-                          const int32_t* tris, const int32_t* off, const int32_t* adj, double omega,
-                          int32_t* failed, int32_t* counters, int64_t* n_fallback, int64_t* n_not_found);
+                          const int32_t* tris, const uint32_t* off, const int32_t* adj, double omega,
+                          RemeshScratch& s, int64_t* n_fallback, int64_t* n_not_found);
 void launch_remesh_targets(cudaStream_t st, int64_t n, const double* grid3, const double* moved5, double* target5);
-// In-place exclusive prefix sum of m 32-bit counts (one block).
-void launch_scan_u32(cudaStream_t st, uint32_t* a, int64_t m);
+// In-place exclusive prefix sum of m 32-bit counts; `part` holds
+// scan_part_words(m) words of scratch (NULL: one block scans all).
+int64_t scan_part_words(int64_t m);
+void launch_scan_u32(cudaStream_t st, uint32_t* a, int64_t m, uint32_t* part);
 
 // k_ensemble.cu
 void launch_up_leaf_batch(cudaStream_t st, int nleaf, const void* src, const EnsLeaf* leaves,

@@ -176,7 +176,9 @@ int fss_rhs_current(fss_ctx* ctx, double omega, double* modify5, double* psi);
  * needed the search over all triangles; *n_not_found: points found nowhere
  * (the reference throws).  Either may be NULL.  The search over all
  * triangles runs on a cell grid of triangle caps (same first triangle as the
- * reference's linear scan), so its cost stays near linear in the points. */
+ * reference's linear scan), so its cost stays near linear in the points.
+ * Device buffers and the triangles' adjacency are kept per device between
+ * calls (until the process ends); calls on one device are serialised. */
 int fss_remesh(int64_t n, const double* moved5, double* target5, int64_t ntri, const int32_t* tris,
                double omega, int64_t* n_fallback, int64_t* n_not_found);
 /* The same on the context's device-resident state (new_dynamics.cpp:213-216,

@@ -72,3 +72,27 @@ def test_remesh_many_fallbacks_cell_grid(fss, oracle):
     got, fb, bad = fss.remesh(m, s, tris)
     assert fb == fb_ref and fb > 64 and bad == bad_ref
     assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
+
+
+def test_remesh_current_cached_adjacency(fss, oracle):
+    """Repeated regrids with the same triangles reuse the device adjacency;
+    a bad triangle list in between is refused and the next call rebuilds."""
+    level = 5
+    s, a = fss.make_state(level, "rh_vortices", n_vortex=8, seed=9)
+    _, tris = fss.icos_grid(level)
+    bad = tris.copy()
+    bad[7, 1] = -1
+    with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as ctx:
+        ctx.set_particles(s, a)
+        for k in range(3):
+            ctx.rk4_step(0.02, nsteps=2)
+            moved = ctx.get_state()
+            target = moved.copy()
+            target[:, :3] = s[:, :3]
+            ref, fb_ref, _ = oracle.remesh(moved, target, tris)
+            if k == 1:
+                with pytest.raises(fss.FssError):
+                    ctx.remesh_current(bad)
+            fb, nf = ctx.remesh_current(tris)
+            assert fb == fb_ref and nf == 0
+            assert np.array_equal(ctx.get_state().view(np.uint64), ref.view(np.uint64))
