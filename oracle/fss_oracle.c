@@ -597,24 +597,34 @@ static void tri_interp(const int *tv, const double *moved5, double *target5, int
  * contain; here it is built from `tris` in increasing index order.  Returns
  * the number of targets found in no triangle (left unchanged); *fallback
  * receives the number that needed the search over all triangles. */
-int64_t orc_remesh(int64_t n, const double *moved5, double *target5, int64_t ntri, const int *tris,
-                   double omega, int64_t *fallback) {
+/* Adjacency order: by corner key (keys[3 j + c] for corner c of triangle j),
+ * or by triangle index when keys is NULL. */
+static const uint64_t *g_sort_keys;
+static int cmp_corner(const void *x, const void *y) {
+    const int64_t a = *(const int64_t *)x, b = *(const int64_t *)y;
+    const uint64_t ka = g_sort_keys ? g_sort_keys[a] : (uint64_t)a, kb = g_sort_keys ? g_sort_keys[b] : (uint64_t)b;
+    return ka < kb ? -1 : (ka > kb ? 1 : 0);
+}
+
+int64_t orc_remesh_keyed(int64_t n, const double *moved5, double *target5, int64_t ntri, const int *tris,
+                         const uint64_t *keys, double omega, int64_t *fallback) {
     int64_t *off = calloc((size_t)n + 1, sizeof(int64_t));
-    int64_t *adj = malloc(sizeof(int64_t) * (size_t)(3 * ntri + 1));
+    int64_t *adj = malloc(sizeof(int64_t) * (size_t)(3 * ntri + 1));  /* corner ids 3 j + c */
     for (int64_t j = 0; j < 3 * ntri; j++) off[tris[j] + 1]++;
     for (int64_t i = 0; i < n; i++) off[i + 1] += off[i];
     int64_t *fill = malloc(sizeof(int64_t) * (size_t)(n + 1));
     memcpy(fill, off, sizeof(int64_t) * (size_t)(n + 1));
-    for (int64_t j = 0; j < ntri; j++)
-        for (int k = 0; k < 3; k++) adj[fill[tris[3 * j + k]]++] = j;
+    for (int64_t j = 0; j < 3 * ntri; j++) adj[fill[tris[j]]++] = j;
+    g_sort_keys = keys;
+    for (int64_t i = 0; i < n; i++) qsort(adj + off[i], (size_t)(off[i + 1] - off[i]), sizeof(int64_t), cmp_corner);
     int64_t bad = 0, fb = 0;
     for (int64_t i = 0; i < n; i++) {
         const double *p = target5 + 5 * i;
         int64_t found = -1;
         for (int64_t a = off[i]; a < off[i + 1] && found < 0; a++) {
-            const int *tv = tris + 3 * adj[a];
+            const int *tv = tris + 3 * (adj[a] / 3);
             if (check_in_tri(moved5 + 5 * (int64_t)tv[0], moved5 + 5 * (int64_t)tv[1], moved5 + 5 * (int64_t)tv[2], p))
-                found = adj[a];
+                found = adj[a] / 3;
         }
         if (found < 0) {
             fb++;
@@ -630,4 +640,103 @@ int64_t orc_remesh(int64_t n, const double *moved5, double *target5, int64_t ntr
     free(off); free(adj); free(fill);
     if (fallback) *fallback = fb;
     return bad;
+}
+
+int64_t orc_remesh(int64_t n, const double *moved5, double *target5, int64_t ntri, const int *tris,
+                   double omega, int64_t *fallback) {
+    return orc_remesh_keyed(n, moved5, target5, ntri, tris, NULL, omega, fallback);
+}
+
+/* ------------------------------------------------------------------ AMR */
+
+/* amr.h:13-178 amr on flat arrays.  Triangles are visited in index order
+ * while the count grows (children appended during the pass are visited in
+ * the same pass; the first child keeps the parent's index and is not).  A
+ * triangle is split in four when its vorticity range exceeds vtol or its
+ * circulation A |z1 + z2 + z3| / 3 exceeds ctol (the reference hard-codes
+ * 0.2 and 0.0025).  Edge midpoints (unprojected averages of all five state
+ * components) are shared through the parent pairs (check_in_vec3: the first
+ * point whose pair is (min, max)); areas move A/6 from each corner to each
+ * midpoint.  The reference's vert_tris lists are kept as one key per
+ * triangle corner: a list is its triangles in increasing key order (initial
+ * lists by triangle index; appended entries 2^40 + 9 s + slot, s the
+ * refinement's running number).  parent has two ints per point, (0, 0) for
+ * primitive points.  Returns 0, or -1 when max_points or max_tris would be
+ * exceeded (undefined behaviour in the reference; arrays then partly
+ * updated).  Nothing happens when *n >= max_points (as the reference). */
+#define AMR_KEY_APPEND ((uint64_t)1 << 40)
+static int amr_find_parent(const int *parent, int64_t n, int a, int b) {
+    for (int64_t i = 0; i < n; i++)
+        if (parent[2 * i] == a && parent[2 * i + 1] == b) return (int)i;
+    return -1;
+}
+
+int orc_amr(int64_t *n_io, int64_t max_points, double *state5, double *area, int64_t *ntri_io, int64_t max_tris,
+            int *tris, uint64_t *keys, int *parent, uint64_t *seq_io, double vtol, double ctol) {
+    int64_t n = *n_io, ntri = *ntri_io;
+    uint64_t seq = *seq_io;
+    int rc = 0;
+    if (n >= max_points) return 0;
+    for (int64_t i = 0; i < ntri; i++) {
+        const int iv1 = tris[3 * i], iv2 = tris[3 * i + 1], iv3 = tris[3 * i + 2];
+        const double vor1 = state5[5 * (int64_t)iv1 + 3], vor2 = state5[5 * (int64_t)iv2 + 3],
+                     vor3 = state5[5 * (int64_t)iv3 + 3];
+        double mx = (vor2 < vor3) ? vor3 : vor2; /* std::max(vor1, std::max(vor2, vor3)) */
+        mx = (vor1 < mx) ? mx : vor1;
+        double mn = (vor3 < vor2) ? vor3 : vor2; /* std::min */
+        mn = (mn < vor1) ? mn : vor1;
+        const double A = orc_sphere_tri_area(state5 + 5 * (int64_t)iv1, state5 + 5 * (int64_t)iv2,
+                                             state5 + 5 * (int64_t)iv3, 1.0);
+        const double circ = A * fabs(vor1 + vor2 + vor3) / 3.0;
+        if (!((mx - mn) > vtol || circ > ctol)) continue;
+        area[iv1] -= A / 6.0;
+        area[iv2] -= A / 6.0;
+        area[iv3] -= A / 6.0;
+        const int ea[3] = {iv1, iv2, iv3}, eb[3] = {iv2, iv3, iv1}; /* v12 = v1 + v2, v23 = v2 + v3, v31 = v3 + v1 */
+        int m[3];
+        for (int k = 0; k < 3; k++) {
+            const int lo = ea[k] < eb[k] ? ea[k] : eb[k], hi = ea[k] < eb[k] ? eb[k] : ea[k];
+            m[k] = amr_find_parent(parent, n, lo, hi);
+        }
+        for (int k = 0; k < 3; k++) {
+            const int lo = ea[k] < eb[k] ? ea[k] : eb[k], hi = ea[k] < eb[k] ? eb[k] : ea[k];
+            if (m[k] == -1) {
+                if (n >= max_points) { rc = -1; goto done; }
+                m[k] = (int)n;
+                for (int c = 0; c < 5; c++) {
+                    double v = state5[5 * (int64_t)ea[k] + c];
+                    v += state5[5 * (int64_t)eb[k] + c];
+                    state5[5 * n + c] = v * 0.5;
+                }
+                area[n] = A / 6.0;
+                parent[2 * n] = lo;
+                parent[2 * n + 1] = hi;
+                n++;
+            } else {
+                area[m[k]] += A / 6.0;
+            }
+        }
+        if (ntri + 3 > max_tris) { rc = -1; goto done; }
+        {
+            const int m12 = m[0], m23 = m[1], m31 = m[2];
+            const uint64_t k1 = keys[3 * i], k2 = keys[3 * i + 1], k3 = keys[3 * i + 2];
+            const uint64_t b = AMR_KEY_APPEND + 9 * seq;
+            const int64_t t2 = ntri, t3 = ntri + 1, t4 = ntri + 2;
+            tris[3 * i] = iv1; tris[3 * i + 1] = m12; tris[3 * i + 2] = m31;
+            keys[3 * i] = k1; keys[3 * i + 1] = b + 0; keys[3 * i + 2] = b + 6;
+            tris[3 * t2] = iv2; tris[3 * t2 + 1] = m12; tris[3 * t2 + 2] = m23;
+            keys[3 * t2] = k2; keys[3 * t2 + 1] = b + 1; keys[3 * t2 + 2] = b + 3;
+            tris[3 * t3] = iv3; tris[3 * t3 + 1] = m31; tris[3 * t3 + 2] = m23;
+            keys[3 * t3] = k3; keys[3 * t3 + 1] = b + 7; keys[3 * t3 + 2] = b + 4;
+            tris[3 * t4] = m12; tris[3 * t4 + 1] = m23; tris[3 * t4 + 2] = m31;
+            keys[3 * t4] = b + 2; keys[3 * t4 + 1] = b + 5; keys[3 * t4 + 2] = b + 8;
+            ntri += 3;
+            seq++;
+        }
+    }
+done:
+    *n_io = n;
+    *ntri_io = ntri;
+    *seq_io = seq;
+    return rc;
 }

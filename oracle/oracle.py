@@ -65,6 +65,12 @@ def _setup(L):
     L.orc_barycoords.argtypes = [_D, _D, _D, _D, _D]
     L.orc_remesh.argtypes = [i64, _D, _D, i64, _I, C.c_double, C.POINTER(i64)]
     L.orc_remesh.restype = i64
+    _U = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+    L.orc_remesh_keyed.argtypes = [i64, _D, _D, i64, _I, C.c_void_p, C.c_double, C.POINTER(i64)]
+    L.orc_remesh_keyed.restype = i64
+    L.orc_amr.argtypes = [C.POINTER(i64), i64, _D, _D, C.POINTER(i64), i64, _I, _U, _I, C.POINTER(C.c_uint64),
+                          C.c_double, C.c_double]
+    L.orc_amr.restype = C.c_int
 
 
 def _setup_ref(R):
@@ -89,6 +95,11 @@ def _setup_ref(R):
     R.ref_regrid.restype = C.c_int
     R.ref_regrid_range.argtypes = [i64, _D, _D, i64, _I, C.c_double, i64, i64]
     R.ref_regrid_range.restype = C.c_int
+    R.ref_amr.argtypes = [i64, i64, i64, _D, _D, _I, C.c_void_p, i64, i64, C.POINTER(i64), C.POINTER(i64), _D, _D, _I,
+                          _I, _I, _I]
+    R.ref_amr.restype = C.c_int
+    R.ref_regrid_csr.argtypes = [i64, _D, _D, i64, _I, _I, _I, C.c_double]
+    R.ref_regrid_csr.restype = C.c_int
 
 
 _setup(_lib)
@@ -230,7 +241,7 @@ def ref_tree(tree_levels, theta, many_count, state5):
         cap = -np_
 
 
-def remesh(moved5, target5, tris, omega=OMEGA, use_ref=False, rows=None):
+def remesh(moved5, target5, tris, omega=OMEGA, use_ref=False, rows=None, keys=None):
     """remesh.h regrid_points2: (new target state, fallback count, not-found
     count); adjacency in increasing triangle order.  With use_ref, `rows` =
     (lb, ub) regrids only those targets (the reference's lb/ub)."""
@@ -243,5 +254,77 @@ def remesh(moved5, target5, tris, omega=OMEGA, use_ref=False, rows=None):
         rc = ref().ref_regrid_range(n, m, t, ntri, tr, omega, lb, ub)
         return t.reshape(n, 5), None, (0 if rc == 0 else -1)
     fb = C.c_int64()
-    bad = lib().orc_remesh(n, m, t, ntri, tr, omega, C.byref(fb))
+    if keys is not None:
+        k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1)
+        bad = lib().orc_remesh_keyed(n, m, t, ntri, tr, k.ctypes.data_as(C.c_void_p), omega, C.byref(fb))
+    else:
+        bad = lib().orc_remesh(n, m, t, ntri, tr, omega, C.byref(fb))
     return t.reshape(n, 5), fb.value, bad
+
+
+AMR_VTOL, AMR_CTOL = 0.2, 0.0025  # amr.h:14-15
+
+
+def amr(state5, area, tris, max_points, max_tris, parent=None, keys=None, seq=0, vtol=AMR_VTOL, ctol=AMR_CTOL):
+    """amr.h amr (oracle restatement): dict of n, ntri, state5, area, tris,
+    keys (adjacency order per corner), parent, seq, rc."""
+    n, ntri = state5.shape[0], tris.shape[0]
+    st = np.zeros((max_points, 5)); st[:n] = state5
+    ar = np.zeros(max_points); ar[:n] = area
+    tr = np.zeros((max_tris, 3), dtype=np.int32); tr[:ntri] = tris
+    ky = np.zeros((max_tris, 3), dtype=np.uint64)
+    ky[:ntri] = np.arange(ntri, dtype=np.uint64)[:, None] if keys is None else keys
+    pa = np.zeros((max_points, 2), dtype=np.int32)
+    if parent is not None:
+        pa[:n] = parent
+    nn, nt, sq = i64(n), i64(ntri), C.c_uint64(seq)
+    rc = lib().orc_amr(C.byref(nn), max_points, st.reshape(-1), ar, C.byref(nt), max_tris, tr.reshape(-1),
+                       ky.reshape(-1), pa.reshape(-1), C.byref(sq), vtol, ctol)
+    n, ntri = nn.value, nt.value
+    return dict(n=n, ntri=ntri, state5=st[:n], area=ar[:n], tris=tr[:ntri], keys=ky[:ntri], parent=pa[:n],
+                seq=sq.value, rc=rc)
+
+
+def vert_tris(n, tris, keys=None):
+    """Each vertex's triangles in adjacency order (by corner key, else by index)."""
+    tris = np.asarray(tris)
+    corners = np.arange(tris.size)
+    order = np.lexsort((corners if keys is None else np.asarray(keys, dtype=np.uint64).reshape(-1),
+                        tris.reshape(-1)))
+    v = tris.reshape(-1)[order]
+    cut = np.searchsorted(v, np.arange(n + 1))
+    t = order // 3
+    return [t[cut[i]:cut[i + 1]] for i in range(n)]
+
+
+def ref_amr(state5, area, tris, max_count, parent=None, cap_points=None, cap_tris=None):
+    """The reference's own amr() (oracle/_ref): dict of n, ntri, state5, area,
+    tris, parent, vert_tris (list of arrays)."""
+    n, ntri = state5.shape[0], tris.shape[0]
+    cap_points = cap_points or max_count
+    cap_tris = cap_tris or 4 * max_count
+    st = np.zeros((cap_points, 5)); ar = np.zeros(cap_points)
+    tr = np.zeros((cap_tris, 3), dtype=np.int32); pa = np.zeros((cap_points, 2), dtype=np.int32)
+    off = np.zeros(cap_points + 1, dtype=np.int32); adj = np.zeros(3 * cap_tris, dtype=np.int32)
+    pin = None if parent is None else np.ascontiguousarray(parent, dtype=np.int32)
+    nn, nt = i64(), i64()
+    rc = ref().ref_amr(n, max_count, ntri, np.ascontiguousarray(state5, dtype=np.float64).reshape(-1),
+                       np.ascontiguousarray(area, dtype=np.float64), np.ascontiguousarray(tris, dtype=np.int32).reshape(-1),
+                       None if pin is None else pin.ctypes.data_as(C.c_void_p), cap_points, cap_tris,
+                       C.byref(nn), C.byref(nt), st.reshape(-1), ar, tr.reshape(-1), pa.reshape(-1), off, adj)
+    assert rc == 0, "output capacity"
+    n, ntri = nn.value, nt.value
+    return dict(n=n, ntri=ntri, state5=st[:n], area=ar[:n], tris=tr[:ntri], parent=pa[:n],
+                vert_tris=[adj[off[i]:off[i + 1]] for i in range(n)])
+
+
+def ref_remesh_lists(moved5, target5, tris, vert_tris, omega=OMEGA):
+    """The reference's regrid_points2 with explicit vert_tris lists."""
+    m = np.ascontiguousarray(moved5, dtype=np.float64).reshape(-1)
+    t = np.ascontiguousarray(target5, dtype=np.float64).copy().reshape(-1)
+    tr = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1)
+    off = np.zeros(len(vert_tris) + 1, dtype=np.int32)
+    off[1:] = np.cumsum([len(v) for v in vert_tris])
+    adj = np.ascontiguousarray(np.concatenate(vert_tris) if len(vert_tris) else np.zeros(0), dtype=np.int32)
+    rc = ref().ref_regrid_csr(m.size // 5, m, t, tr.size // 3, tr, off, adj, omega)
+    return t.reshape(-1, 5), rc

@@ -23,6 +23,7 @@
 #include "fast_rhs.h"
 #include "interp_utils.h"
 #include "remesh.h"
+#include "amr.h"
 
 using std::vector;
 
@@ -261,8 +262,75 @@ int ref_regrid_range(int64_t n, const double* moved5, double* target5, int64_t n
     return rc;
 }
 
+// regrid_points2 with explicit vert_tris lists (CSR), e.g. those amr() kept.
+int ref_regrid_csr(int64_t n, const double* moved5, double* target5, int64_t ntri, const int* tris, const int* vt_off,
+                   const int* vt_adj, double omega) {
+    vector<double> moved(moved5, moved5 + 5 * n), target(target5, target5 + 5 * n);
+    vector<vector<int>> triangles(ntri, vector<int>(3)), vert_tris(n);
+    for (int64_t j = 0; j < ntri; j++)
+        for (int k = 0; k < 3; k++) triangles[j][k] = tris[3 * j + k];
+    for (int64_t i = 0; i < n; i++) vert_tris[i].assign(vt_adj + vt_off[i], vt_adj + vt_off[i + 1]);
+    std::streambuf* old = std::cout.rdbuf(nullptr);
+    int rc = 0;
+    try {
+        regrid_points2(moved, target, triangles, vert_tris, int(n), int(ntri), omega, 0, int(n), 0);
+    } catch (...) {
+        rc = -1;
+    }
+    std::cout.rdbuf(old);
+    std::memcpy(target5, target.data(), sizeof(double) * 5 * n);
+    return rc;
+}
+
 int ref_regrid(int64_t n, const double* moved5, double* target5, int64_t ntri, const int* tris, double omega) {
     return ref_regrid_range(n, moved5, target5, ntri, tris, omega, 0, n);
+}
+
+// amr.h:13 amr on the reference's own structures built from flat arrays:
+// dynamics_tris from `tris`, amr_vert_tris in increasing triangle order,
+// amr_parent_verts of max_count pairs ((0, 0), or parent_in for the first n
+// points).  Writes the new counts, state, areas, triangles, parents (for the
+// n_out points) and the vert_tris lists as CSR (vt_off[n_out + 1], vt_adj).
+// Returns 0, or -2 when an output capacity is too small.
+int ref_amr(int64_t n, int64_t max_count, int64_t ntri, const double* state5, const double* area, const int* tris,
+            const int* parent_in, int64_t cap_points, int64_t cap_tris, int64_t* n_out, int64_t* ntri_out,
+            double* state5_out, double* area_out, int* tris_out, int* parent_out, int* vt_off, int* vt_adj) {
+    run_information config1;
+    config1.point_count = int(n);
+    config1.tri_count = int(ntri);
+    config1.max_count = int(max_count);
+    config1.dynamics_tris.assign(ntri, vector<int>(3));
+    config1.amr_vert_tris.assign(n, vector<int>());
+    for (int64_t j = 0; j < ntri; j++)
+        for (int k = 0; k < 3; k++) {
+            config1.dynamics_tris[j][k] = tris[3 * j + k];
+            config1.amr_vert_tris[tris[3 * j + k]].push_back(int(j));
+        }
+    config1.amr_parent_verts.assign(max_count, vector<int>(2, 0));
+    if (parent_in)
+        for (int64_t i = 0; i < n; i++) {
+            config1.amr_parent_verts[i][0] = parent_in[2 * i];
+            config1.amr_parent_verts[i][1] = parent_in[2 * i + 1];
+        }
+    vector<double> st(state5, state5 + 5 * n), ar(area, area + n);
+    amr(st, ar, config1);
+    const int64_t np = config1.point_count, nt = config1.tri_count;
+    *n_out = np;
+    *ntri_out = nt;
+    if (np > cap_points || nt > cap_tris) return -2;
+    std::memcpy(state5_out, st.data(), sizeof(double) * 5 * np);
+    std::memcpy(area_out, ar.data(), sizeof(double) * np);
+    for (int64_t j = 0; j < nt; j++)
+        for (int k = 0; k < 3; k++) tris_out[3 * j + k] = config1.dynamics_tris[j][k];
+    int64_t a = 0;
+    for (int64_t i = 0; i < np; i++) {
+        parent_out[2 * i] = config1.amr_parent_verts[i][0];
+        parent_out[2 * i + 1] = config1.amr_parent_verts[i][1];
+        vt_off[i] = int(a);
+        for (int t : config1.amr_vert_tris[i]) vt_adj[a++] = t;
+    }
+    vt_off[np] = int(a);
+    return 0;
 }
 
 }  // extern "C"

@@ -34,6 +34,26 @@ def main():
     loc, counts, pairs = O.ref_tree(3, 0.7, 10, s3)
     np.savez_compressed(os.path.join(HERE, "tree_l3.npz"), state=s3, loc=loc, counts=counts, pairs=pairs,
                         theta=0.7, many_count=10)
+    # amr.h amr on the 162-point grid with a weakened Gaussian vortex
+    # (vorticity_functions.h:26 gauss_vortex, zeta x 0.1), then
+    # regrid_points2 with the vert_tris lists amr() left, on that mesh
+    # rotated by 0.005 rad about z
+    g, ga, gt = O.icos_state(2, use_ref=True)
+    O.ref().ref_gauss_vortex(g.shape[0], g.reshape(-1), ga)
+    g[:, 3] *= 0.1
+    R = O.ref_amr(g, ga, gt, 10 * 4 ** 7 + 2)
+    grid = R["state5"].copy()
+    grid[:, :3] /= np.linalg.norm(grid[:, :3], axis=1, keepdims=True)
+    c, sn = np.cos(0.005), np.sin(0.005)
+    moved = grid.copy()
+    moved[:, :3] = grid[:, :3] @ np.array([[c, -sn, 0], [sn, c, 0], [0, 0, 1]]).T
+    out, rc = O.ref_remesh_lists(moved, grid, R["tris"], R["vert_tris"])
+    assert rc == 0
+    vt_off = np.concatenate([[0], np.cumsum([len(v) for v in R["vert_tris"]])]).astype(np.int32)
+    np.savez_compressed(os.path.join(HERE, "amr_l2.npz"), state=g, area=ga, faces=gt, max_count=10 * 4 ** 7 + 2,
+                        out_state=R["state5"], out_area=R["area"], out_tris=R["tris"], out_parent=R["parent"],
+                        vt_off=vt_off, vt_adj=np.concatenate(R["vert_tris"]).astype(np.int32),
+                        remesh_moved=moved, remesh_target=grid, remesh_out=out)
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 

@@ -174,3 +174,66 @@ def test_remesh_of_unmoved_grid_is_identity(oracle):
     got, fb, bad = oracle.remesh(s, s, tris)
     assert bad == 0 and fb == 0
     assert np.allclose(got[:, 3:], s[:, 3:], rtol=0, atol=1e-12 * np.abs(s[:, 3:]).max())
+
+
+def _csr(lists):
+    off = np.concatenate([[0], np.cumsum([len(v) for v in lists])]).astype(np.int32)
+    return off, (np.concatenate(lists) if len(lists) else np.zeros(0)).astype(np.int32)
+
+
+def test_amr_matches_golden(oracle):
+    """amr.h amr: points, areas, triangles, parent pairs and the vert_tris
+    lists (as corner keys) equal the reference's, bit for bit; so does
+    regrid_points2 on the refined mesh with those lists."""
+    g = gold("amr_l2.npz")
+    mc = int(g["max_count"])
+    M = oracle.amr(g["state"], g["area"], g["faces"], mc, 4 * mc)
+    assert M["rc"] == 0 and M["n"] == g["out_state"].shape[0] and M["ntri"] == g["out_tris"].shape[0]
+    assert np.array_equal(bits(M["state5"]), bits(g["out_state"]))
+    assert np.array_equal(bits(M["area"]), bits(g["out_area"]))
+    assert np.array_equal(M["tris"], g["out_tris"])
+    assert np.array_equal(M["parent"], g["out_parent"])
+    off, adj = _csr(oracle.vert_tris(M["n"], M["tris"], M["keys"]))
+    assert np.array_equal(off, g["vt_off"]) and np.array_equal(adj, g["vt_adj"])
+    out, fb, bad = oracle.remesh(g["remesh_moved"], g["remesh_target"], M["tris"], keys=M["keys"])
+    assert bad == 0 and np.array_equal(bits(out), bits(g["remesh_out"]))
+
+
+def _gauss_grid(oracle, level):
+    s, a, tris = oracle.icos_state(level, use_ref=True)
+    oracle.ref().ref_gauss_vortex(s.shape[0], s.reshape(-1), a)
+    return s, a, tris
+
+
+@need_ref
+@pytest.mark.parametrize("level", [3, 4])
+def test_amr_bit_exact_vs_reference(oracle, level):
+    """The full Gaussian vortex at the reference's tolerances (2,562 points
+    grow to 16,734 in one call at level 4)."""
+    s, a, tris = _gauss_grid(oracle, level)
+    mc = 10 * 4 ** (level + 3) + 2
+    R = oracle.ref_amr(s, a, tris, mc)
+    M = oracle.amr(s, a, tris, mc, 4 * mc)
+    assert M["rc"] == 0 and (M["n"], M["ntri"]) == (R["n"], R["ntri"]) and M["n"] > 4 * s.shape[0]
+    for k in ("state5", "area"):
+        assert np.array_equal(bits(M[k]), bits(R[k]))
+    assert np.array_equal(M["tris"], R["tris"]) and np.array_equal(M["parent"], R["parent"])
+    vt = oracle.vert_tris(M["n"], M["tris"], M["keys"])
+    assert all(np.array_equal(x, y) for x, y in zip(vt, R["vert_tris"]))
+
+
+@need_ref
+def test_amr_remesh_vs_reference(oracle):
+    """regrid_points2 on the refined mesh with the lists amr() left."""
+    s, a, tris = _gauss_grid(oracle, 4)
+    mc = 10 * 4 ** 7 + 2
+    M = oracle.amr(s, a, tris, mc, 4 * mc)
+    grid = M["state5"].copy()
+    grid[:, :3] /= np.linalg.norm(grid[:, :3], axis=1, keepdims=True)
+    c, sn = np.cos(0.005), np.sin(0.005)
+    moved = grid.copy()
+    moved[:, :3] = grid[:, :3] @ np.array([[c, -sn, 0], [sn, c, 0], [0, 0, 1]]).T
+    ref, rc = oracle.ref_remesh_lists(moved, grid, M["tris"], oracle.vert_tris(M["n"], M["tris"], M["keys"]))
+    got, fb, bad = oracle.remesh(moved, grid, M["tris"], keys=M["keys"])
+    assert rc == 0 and bad == 0 and fb > 1000
+    assert np.array_equal(bits(got), bits(ref))
