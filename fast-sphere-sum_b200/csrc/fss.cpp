@@ -1165,8 +1165,8 @@ int fss_remesh(int64_t n, const double* moved5, double* target5, int64_t ntri, c
         CU(h.dadj.ensure(sizeof(int32_t) * 3 * size_t(ntri)));
         CU(cudaMemcpyAsync(h.dtri.p, h.tris_host.data(), sizeof(int32_t) * 3 * ntri, cudaMemcpyHostToDevice, st));
         bool valid = false;
-        CU(launch_remesh_adjacency(st, n, ntri, h.dtri.as<int32_t>(), h.doff.as<uint32_t>(), h.dadj.as<int32_t>(),
-                                   h.rs, &valid));
+        CU(launch_remesh_adjacency(st, n, ntri, h.dtri.as<int32_t>(), nullptr, h.doff.as<uint32_t>(),
+                                   h.dadj.as<int32_t>(), h.rs, &valid));
         if (!valid) {
             h.tris_host.clear();
             return fail(c, FSS_ERR_INVALID, "triangle vertex out of range");
@@ -1199,7 +1199,7 @@ int fss_remesh_current(fss_ctx* c, int64_t ntri, const int32_t* tris, double ome
         CU(cudaMemcpyAsync(c->rm_tris.p, c->rm_tris_host.data(), sizeof(int32_t) * 3 * ntri, cudaMemcpyHostToDevice,
                            c->stream));
         bool valid = false;
-        CU(launch_remesh_adjacency(c->stream, n, ntri, c->rm_tris.as<int32_t>(), c->rm_off.as<uint32_t>(),
+        CU(launch_remesh_adjacency(c->stream, n, ntri, c->rm_tris.as<int32_t>(), nullptr, c->rm_off.as<uint32_t>(),
                                    c->rm_adj.as<int32_t>(), c->rm, &valid));
         if (!valid) {
             c->rm_tris_host.clear();

@@ -40,8 +40,8 @@ __device__ __forceinline__ void tri_interp_exact(const double* __restrict__ move
 }
 
 // One thread per grid point: the triangles adjacent to its vertex
-// (adjacency adj[off[i] .. off[i+1]) in increasing triangle order).  Points
-// found in none are listed in `failed`.
+// (adjacency adj[off[i] .. off[i+1]): corner ids 3 t + c in list order).
+// Points found in none are listed in `failed`.
 __global__ void k_remesh_adjacent(int64_t n, const double* __restrict__ moved5, double* __restrict__ target5,
                                   const int32_t* __restrict__ tris, const uint32_t* __restrict__ off,
                                   const int32_t* __restrict__ adj, double omega, int32_t* __restrict__ failed,
@@ -52,7 +52,7 @@ __global__ void k_remesh_adjacent(int64_t n, const double* __restrict__ moved5, 
     const double p[3] = {t[0], t[1], t[2]};
     double c[3];
     for (uint32_t a = off[i]; a < off[i + 1]; a++) {
-        const int32_t* tv = tris + 3 * int64_t(adj[a]);
+        const int32_t* tv = tris + 3 * int64_t(adj[a] / 3);
         if (tri_contains(moved5, tv, p, c)) {
             tri_interp_exact(moved5, tv, t, omega, c);
             return;
@@ -78,19 +78,22 @@ __global__ void k_adj_fill(int64_t n, int64_t ntri, const int32_t* __restrict__ 
     const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (j >= 3 * ntri) return;
     const int32_t v = tris[j];
-    if (v >= 0 && int64_t(v) < n) adj[atomicAdd(cur + v, 1u)] = int32_t(j / 3);
+    if (v >= 0 && int64_t(v) < n) adj[atomicAdd(cur + v, 1u)] = int32_t(j);
 }
 
-// Each vertex's list into increasing triangle order (insertion sort: a few
-// entries per vertex on a triangulated sphere).
-__global__ void k_adj_sort(int64_t n, const uint32_t* __restrict__ off, int32_t* __restrict__ adj) {
+// Each vertex's list into list order: increasing corner key, or increasing
+// corner id (= triangle order) without keys (insertion sort: a few entries
+// per vertex on a triangulated sphere).
+__global__ void k_adj_sort(int64_t n, const uint32_t* __restrict__ off, const uint64_t* __restrict__ keys,
+                           int32_t* __restrict__ adj) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t a = off[i], b = off[i + 1];
     for (uint32_t k = a + 1; k < b; k++) {
         const int32_t x = adj[k];
+        const uint64_t kx = keys ? keys[x] : uint64_t(x);
         uint32_t q = k;
-        while (q > a && adj[q - 1] > x) {
+        while (q > a && (keys ? keys[adj[q - 1]] : uint64_t(adj[q - 1])) > kx) {
             adj[q] = adj[q - 1];
             q--;
         }
@@ -98,8 +101,9 @@ __global__ void k_adj_sort(int64_t n, const uint32_t* __restrict__ off, int32_t*
     }
 }
 
-cudaError_t launch_remesh_adjacency(cudaStream_t st, int64_t n, int64_t ntri, const int32_t* tris, uint32_t* off,
-                                    int32_t* adj, RemeshScratch& s, bool* valid) {
+cudaError_t launch_remesh_adjacency(cudaStream_t st, int64_t n, int64_t ntri, const int32_t* tris,
+                                    const uint64_t* keys, uint32_t* off, int32_t* adj, RemeshScratch& s,
+                                    bool* valid) {
     cudaError_t e;
     *valid = false;
     if ((e = s.scal.ensure(2 * sizeof(uint32_t))) != cudaSuccess ||
@@ -123,7 +127,7 @@ cudaError_t launch_remesh_adjacency(cudaStream_t st, int64_t n, int64_t ntri, co
         cudaSuccess)
         return e;
     k_adj_fill<<<g3, 256, 0, st>>>(n, ntri, tris, cur, adj);
-    k_adj_sort<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, off, adj);
+    k_adj_sort<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, off, keys, adj);
     *valid = true;
     return cudaGetLastError();
 }

@@ -129,11 +129,14 @@ void launch_scatter_state(cudaStream_t st, int64_t n, const int32_t* perm, const
 struct RemeshScratch {
     DBuf failed, counters, adj_cur, caps, box, cells, glist, scal, ent, part;
 };
-// Vertex -> triangles adjacency of `tris` in increasing triangle order:
-// off[n + 1] (32-bit), adj[3 ntri].  *valid = false (nothing else usable)
-// when a vertex index is outside [0, n).  Synchronises the stream.
-cudaError_t launch_remesh_adjacency(cudaStream_t st, int64_t n, int64_t ntri, const int32_t* tris, uint32_t* off,
-                                    int32_t* adj, RemeshScratch& s, bool* valid);
+// Vertex -> triangles adjacency of `tris`: off[n + 1] (32-bit), adj[3 ntri]
+// holding corner ids 3 t + c, each vertex's list in increasing key order
+// (keys[3 t + c]; NULL: increasing triangle order).  *valid = false (nothing
+// else usable) when a vertex index is outside [0, n).  Synchronises the
+// stream.
+cudaError_t launch_remesh_adjacency(cudaStream_t st, int64_t n, int64_t ntri, const int32_t* tris,
+                                    const uint64_t* keys, uint32_t* off, int32_t* adj, RemeshScratch& s,
+                                    bool* valid);
 // Remesh targets (grid points, 5 doubles each, zeta and tracer replaced
 // where a moved-mesh triangle contains them); returns the number of points
 // that needed the search over all triangles and the number found nowhere.
@@ -142,6 +145,25 @@ cudaError_t launch_remesh(cudaStream_t st, int64_t n, const double* moved5, doub
                           const int32_t* tris, const uint32_t* off, const int32_t* adj, double omega,
                           RemeshScratch& s, int64_t* n_fallback, int64_t* n_not_found);
 void launch_remesh_targets(cudaStream_t st, int64_t n, const double* grid3, const double* moved5, double* target5);
+// k_amr.cu: one generation of the AMR pass at a time (see k_amr.cu).
+cudaError_t amr_seed_parents(cudaStream_t st, int64_t n, const int32_t* parent, unsigned long long* hkeys,
+                             long long* hvals, int64_t hmask, int* err);
+void amr_test(cudaStream_t st, int64_t q0, int64_t m, const int32_t* tris, const double* state5, double vtol,
+              double ctol, uint32_t* flag, uint32_t* rank, double* tarea);
+void amr_edges(cudaStream_t st, int64_t q0, int64_t m, const uint32_t* flag, const uint32_t* rank,
+               const int32_t* tris, int32_t* refined, int64_t* occ_slot, unsigned long long* hkeys, long long* hvals,
+               int64_t hmask, int* err);
+void amr_creators(cudaStream_t st, int64_t nocc, const int64_t* occ_slot, const long long* hvals, uint32_t* cflag,
+                  uint32_t* crank);
+void amr_newpts(cudaStream_t st, int64_t nocc, int64_t n, const int32_t* refined, const int32_t* tris,
+                const int64_t* occ_slot, const uint32_t* cflag, const uint32_t* crank, long long* hvals,
+                double* state5, int32_t* parent);
+void amr_split(cudaStream_t st, int64_t nref, int64_t q0, int64_t q1, uint64_t seq0, const int32_t* refined,
+               const int64_t* occ_slot, const long long* hvals, const uint32_t* cflag, const double* tarea,
+               int32_t* tris, uint64_t* keys, uint32_t* rec_v, double* rec_d, uint8_t* rec_k);
+void amr_areas(cudaStream_t st, int64_t nrec, const uint32_t* sv, const int32_t* perm, const double* rec_d,
+               const uint8_t* rec_k, double* area);
+
 // In-place exclusive prefix sum of m 32-bit counts; `part` holds
 // scan_part_words(m) words of scratch (NULL: one block scans all).
 int64_t scan_part_words(int64_t m);

@@ -77,7 +77,8 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_select_classes",
            "fss_selector_apply", "fss_ensemble_create", "fss_ensemble_destroy", "fss_ensemble_set_stream",
            "fss_ensemble_add", "fss_ensemble_build", "fss_ensemble_rk4_step", "fss_ensemble_get_state",
-           "fss_ensemble_info", "fss_version"]
+           "fss_ensemble_info", "fss_amr_create", "fss_amr_destroy", "fss_amr_counts", "fss_amr_refine",
+           "fss_amr_get_mesh", "fss_amr_remesh", "fss_version"]
 
 NOALLOC_MAX_PARTICLES = 262144  # FSS_NOALLOC_MAX_PARTICLES in include/fss.h
 
@@ -133,6 +134,13 @@ def lib():
     L.fss_ensemble_rk4_step.argtypes = [_vp, C.c_double, C.c_double, C.c_int32]
     L.fss_ensemble_get_state.argtypes = [_vp, C.c_int32, _D]
     L.fss_ensemble_info.argtypes = [_vp, P(C.c_int32), P(_i64), P(C.c_double), P(_i64)]
+    L.fss_amr_create.argtypes = [_i64, _i64, _I32, _vp, _i64, _i64, C.c_int32, P(_vp)]
+    L.fss_amr_destroy.argtypes = [_vp]
+    L.fss_amr_destroy.restype = None
+    L.fss_amr_counts.argtypes = [_vp, P(_i64), P(_i64)]
+    L.fss_amr_refine.argtypes = [_vp, P(_i64), _D, _D, C.c_double, C.c_double]
+    L.fss_amr_get_mesh.argtypes = [_vp, _vp, _vp, _vp]
+    L.fss_amr_remesh.argtypes = [_vp, _D, _D, C.c_double, P(_i64), P(_i64)]
     L.fss_version.restype = C.c_char_p
     _lib = L
     return L
@@ -373,6 +381,71 @@ def rhs_direct_noalloc(n, state5_dev_ptr, area_dev_ptr, out5_dev_ptr, stream_han
     """fss_rhs_direct_noalloc on caller-owned device buffers (raw pointers);
     asynchronous on the given stream.  Raises FssError on a bad size."""
     _check(lib().fss_rhs_direct_noalloc(n, state5_dev_ptr, area_dev_ptr, omega, out5_dev_ptr, stream_handle))
+
+
+AMR_VORTICITY_TOL, AMR_CIRCULATION_TOL = 0.2, 0.0025  # amr.h:14-15
+
+
+class Amr:
+    """amr.h amr on a device-resident triangle mesh (fss_amr_*): refine()
+    appends points to host arrays with room for max_count points; mesh()
+    returns (tris, corner_keys, parent_verts); remesh() is regrid_points2 on
+    this mesh with the vert_tris lists amr() leaves."""
+
+    def __init__(self, tris, n, max_count, max_tris, parent_verts=None, device=0):
+        t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1)
+        pv = None if parent_verts is None else np.ascontiguousarray(parent_verts, dtype=np.int32).reshape(-1)
+        self.h = _vp()
+        self.max_count = max_count
+        _check(lib().fss_amr_create(n, t.size // 3, t, None if pv is None else pv.ctypes.data_as(_vp), max_count,
+                                    max_tris, device, C.byref(self.h)))
+
+    def counts(self):
+        n, nt = _i64(), _i64()
+        _check(lib().fss_amr_counts(self.h, C.byref(n), C.byref(nt)))
+        return n.value, nt.value
+
+    def refine(self, state5, area, vorticity_tol=AMR_VORTICITY_TOL, circulation_tol=AMR_CIRCULATION_TOL):
+        """(state5, area) of the current points -> (new state5, new area)."""
+        n = state5.shape[0]
+        st = np.zeros((self.max_count, 5)); st[:n] = state5
+        ar = np.zeros(self.max_count); ar[:n] = area
+        pc = _i64(n)
+        _check(lib().fss_amr_refine(self.h, C.byref(pc), st.reshape(-1), ar, vorticity_tol, circulation_tol))
+        return st[:pc.value].copy(), ar[:pc.value].copy()
+
+    def mesh(self):
+        n, nt = self.counts()
+        tris = np.zeros((nt, 3), dtype=np.int32)
+        keys = np.zeros((nt, 3), dtype=np.uint64)
+        par = np.zeros((n, 2), dtype=np.int32)
+        _check(lib().fss_amr_get_mesh(self.h, tris.ctypes.data_as(_vp), keys.ctypes.data_as(_vp),
+                                      par.ctypes.data_as(_vp)))
+        return tris, keys, par
+
+    def remesh(self, moved5, target5, omega=OMEGA):
+        m = np.ascontiguousarray(moved5, dtype=np.float64)
+        t = np.ascontiguousarray(target5, dtype=np.float64).copy()
+        fb, bad = _i64(), _i64()
+        _check(lib().fss_amr_remesh(self.h, m.reshape(-1), t.reshape(-1), omega, C.byref(fb), C.byref(bad)))
+        return t, fb.value, bad.value
+
+    def close(self):
+        if self.h:
+            lib().fss_amr_destroy(self.h)
+            self.h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Ensemble:

@@ -189,6 +189,39 @@ int fss_remesh(int64_t n, const double* moved5, double* target5, int64_t ntri, c
 int fss_remesh_current(fss_ctx* ctx, int64_t ntri, const int32_t* tris, double omega, int64_t* n_fallback,
                        int64_t* n_not_found);
 
+/* ------------------------------------------------------------- AMR
+ * amr.h:13-178 amr.  The handle holds the triangle mesh, the reference's
+ * vert_tris lists (one ordering key per triangle corner: a vertex's list is
+ * its triangles in increasing key order; initial lists in increasing
+ * triangle order) and the parent pairs (amr_parent_verts: (0, 0) for a
+ * primitive point), on the device.  max_count is the reference's point
+ * limit; max_tris bounds the triangle count. */
+typedef struct fss_amr fss_amr;
+int fss_amr_create(int64_t n, int64_t ntri, const int32_t* tris, const int32_t* parent_verts, int64_t max_count,
+                   int64_t max_tris, int device, fss_amr** out);
+void fss_amr_destroy(fss_amr* a);
+int fss_amr_counts(const fss_amr* a, int64_t* point_count, int64_t* tri_count);
+/* One amr() call.  state5 and area are host arrays with room for max_count
+ * points; *point_count must be the mesh's count and becomes the new one.
+ * Triangles are visited in index order while their count grows; a triangle
+ * whose vorticity range exceeds vorticity_tol or whose circulation
+ * A |z1 + z2 + z3| / 3 exceeds circulation_tol (the reference: 0.2 and
+ * 0.0025) is split in four; new edge midpoints (unprojected averages of all
+ * five components) are appended; areas move A/6 from corners to midpoints.
+ * Nothing happens when *point_count >= max_count (as the reference).  More
+ * points than max_count or triangles than max_tris within the call (the
+ * reference: undefined) returns FSS_ERR_CAPACITY, leaves the host arrays
+ * unchanged and the handle unusable. */
+int fss_amr_refine(fss_amr* a, int64_t* point_count, double* state5, double* area, double vorticity_tol,
+                   double circulation_tol);
+/* The mesh: tris (3 per triangle), corner_keys (3 per triangle), parent
+ * pairs (2 per point); any may be NULL. */
+int fss_amr_get_mesh(const fss_amr* a, int32_t* tris, uint64_t* corner_keys, int32_t* parent_verts);
+/* regrid_points2 on the handle's mesh with its vert_tris lists (the order
+ * amr() leaves them in); as fss_remesh otherwise. */
+int fss_amr_remesh(fss_amr* a, const double* moved5, double* target5, double omega, int64_t* n_fallback,
+                   int64_t* n_not_found);
+
 /* Tree summary of the last build. */
 typedef struct fss_tree_info {
     int32_t tree_levels;     /* levels 0..tree_levels-1 */
