@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-remesh", action="store_true")
+    p.add_argument("--no-amr", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=2048, help="targets in one CPU-baseline sample")
     p.add_argument("--tol", type=float, default=1e-6, help="selector: relative L2 velocity error target")
     p.add_argument("--safety", type=float, default=2.0, help="selector: predicted-error safety factor")
@@ -280,7 +281,7 @@ def remesh_measure(fss, ctx, state, area, level, stream, reps=5):
     out = {"workload": "one RK4 step from the grid, then regrid onto the grid (the reference's use_remesh loop)",
            "points": int(moved.shape[0]), "triangles": int(tris.shape[0]), "fallback": fb, "not_found": bad,
            "wall_ms_host_buffers": wall_ms, "h2d_d2h_bytes": int(2 * moved.nbytes + target.nbytes),
-           "wall_ms_device_resident": cur_ms, "rk4_plus_remesh_steps_per_s": reps / loop_s}
+           "wall_ms_device_resident_first_call": cur_ms, "rk4_plus_remesh_steps_per_s": reps / loop_s}
     if O.ref() is not None:
         # the reference is O(triangles) per point outside its adjacent
         # triangles: time it on a contiguous row range from a seeded start,
@@ -301,6 +302,52 @@ def remesh_measure(fss, ctx, state, area, level, stream, reps=5):
         out["bit_exact_vs_reference_rows"] = bool(
             rc == 0 and np.array_equal(got[lb:ub].view(np.uint64), ref[lb:ub].view(np.uint64))
             and np.array_equal(got_dev[lb:ub].view(np.uint64), ref[lb:ub].view(np.uint64)))
+    return out
+
+
+def amr_measure(fss, level=5, reps=3):
+    """amr.h amr as the reference's -a loop calls it, on the reference's
+    Gaussian vortex (level-`level` grid, the reference's tolerances 0.2 and
+    0.0025; max_count of level + 2): fss_amr_refine (host buffers, host wall
+    clock with the copies, a fresh mesh per repetition), then
+    fss_amr_remesh on the refined mesh rotated by 0.005 rad; beside it the
+    reference's own amr() on the same input (oracle/_ref, one thread, timed)
+    and a bit-for-bit comparison of points and triangles."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    state, area = fss.make_state(level, "gauss_ref")
+    _, tris = fss.icos_grid(level)
+    n = state.shape[0]
+    mc = 10 * 4 ** (level + 2) + 2
+    times = []
+    for r in range(reps + 1):
+        with fss.Amr(tris, n, mc, 4 * mc) as amr:
+            t0 = time.perf_counter()
+            st, ar = amr.refine(state, area)
+            if r:
+                times.append(1e3 * (time.perf_counter() - t0))
+            if r == reps:
+                t_new, _, _ = amr.mesh()
+                grid = st.copy()
+                grid[:, :3] /= np.linalg.norm(grid[:, :3], axis=1, keepdims=True)
+                c, sn = np.cos(0.005), np.sin(0.005)
+                moved = grid.copy()
+                moved[:, :3] = grid[:, :3] @ np.array([[c, -sn, 0], [sn, c, 0], [0, 0, 1]]).T
+                amr.remesh(moved, grid)  # builds the adjacency
+                t0 = time.perf_counter()
+                _, fb, nf = amr.remesh(moved, grid)
+                rm_ms = 1e3 * (time.perf_counter() - t0)
+    out = {"workload": f"amr() on the Gaussian vortex, level {level} grid, tolerances 0.2 / 0.0025",
+           "points_in": int(n), "points_out": int(st.shape[0]), "triangles_out": int(t_new.shape[0]),
+           "wall_ms_host_buffers": float(np.median(times)),
+           "remesh_after_amr_ms_host_buffers": rm_ms, "remesh_fallback": fb, "remesh_not_found": nf}
+    if O.ref() is not None:
+        t0 = time.perf_counter()
+        R = O.ref_amr(state, area, tris, mc)
+        out["cpu_reference_ms"] = 1e3 * (time.perf_counter() - t0)
+        out["cpu_reference"] = "amr.h amr (oracle/_ref), 1 thread"
+        out["bit_exact_vs_reference"] = bool(R["n"] == st.shape[0] and np.array_equal(R["tris"], t_new)
+                                             and np.array_equal(R["state5"].view(np.uint64), st.view(np.uint64)))
     return out
 
 
@@ -455,6 +502,10 @@ def main():
         except fss.FssError as e:  # too many points left their triangles in one step
             remesh = {"error": str(e)}
 
+    amr = None
+    if rank == 0 and ws == 1 and not args.no_amr:
+        amr = amr_measure(fss)
+
     ctx.close()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -482,7 +533,7 @@ def main():
                 "fp64_same_algorithm": fp64c,
                 "ratio_vs_fp64_same_algorithm": (value / fp64c["value"]) if fp64c else None,
                 "interactions_per_rhs": inter, "tree": info,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "remesh": remesh,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "remesh": remesh, "amr": amr,
                 "gpu_launches": int(round(launches_per_step * args.steps)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)

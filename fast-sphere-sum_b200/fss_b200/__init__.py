@@ -191,6 +191,9 @@ def make_state(level, field="rh4_ref", n_vortex=0, seed=1, amp=RH_AMP, width=0.1
 
     field 'rh4_ref': the reference's rossby_haurwitz_4 (vorticity_functions.h:13).
     field 'rh_vortices': RH R=4 wave (w = K = amp) + n_vortex seeded Gaussian vortices.
+    field 'gauss_ref': the reference's gauss_vortex (vorticity_functions.h:26-45:
+    4 pi exp(-16 |c - x|^2) about colatitude pi/2 - pi/20, mean removed;
+    tracer 2 + latitude), in numpy (not bit-exact with the reference).
     """
     xyz, faces = icos_grid(level)
     s = np.zeros((xyz.shape[0], 5))
@@ -198,6 +201,12 @@ def make_state(level, field="rh4_ref", n_vortex=0, seed=1, amp=RH_AMP, width=0.1
     area = area_init(s, faces)
     if field == "rh4_ref":
         _check(lib().fss_vorticity_rh4_ref(s.shape[0], s.reshape(-1)))
+    elif field == "gauss_ref":
+        xyz = s[:, :3]
+        c = np.array([np.cos(np.pi / 20), 0.0, np.sin(np.pi / 20)])
+        z = 4 * np.pi * np.exp(-16 * np.sum((c - xyz) ** 2, axis=1))
+        s[:, 3] = z - np.sum(z * area) / (4 * np.pi)
+        s[:, 4] = 2 + (np.pi / 2 - np.arctan2(np.hypot(xyz[:, 0], xyz[:, 1]), xyz[:, 2]))
     elif field == "rh_vortices":
         _check(lib().fss_vorticity_rh_vortices(s.shape[0], s.reshape(-1), area.ctypes.data_as(_vp), amp,
                                                n_vortex, width, seed))

@@ -13,18 +13,9 @@ pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-def gauss_state(fss, level, scale=1.0):
-    """Gaussian vortex on the level-`level` grid (the shape of the
-    reference's gauss_vortex initial condition), in numpy."""
-    xyz, tris = fss.icos_grid(level)
-    s = np.zeros((xyz.shape[0], 5))
-    s[:, :3] = xyz
-    area = fss.area_init(s, tris)
-    c = np.array([np.cos(np.pi / 20) * 1.0, 0.0, np.sin(np.pi / 20)])
-    z = 4 * np.pi * np.exp(-16 * np.sum((c - xyz) ** 2, axis=1))
-    s[:, 3] = scale * (z - np.sum(z * area) / (4 * np.pi))
-    s[:, 4] = 2 + np.arcsin(np.clip(xyz[:, 2], -1, 1))
-    return s, area, tris
+def gauss_state(fss, level):
+    s, area = fss.make_state(level, "gauss_ref")
+    return s, area, fss.icos_grid(level)[1]
 
 
 def check(M, st, ar, amr):
