@@ -193,6 +193,25 @@ int fss_amr_create(int64_t n, int64_t ntri, const int32_t* tris, const int32_t* 
     ACU(a->hkeys.ensure(sizeof(unsigned long long) * size_t(hcap)));
     ACU(a->hvals.ensure(sizeof(long long) * size_t(hcap)));
     ACU(a->err.ensure(sizeof(int)));
+    // per-pass scratch at its largest (a generation holds at most max_tris
+    // triangles; refinements are bounded by the free triangle slots), so
+    // that refining allocates nothing
+    const size_t mt = size_t(max_tris), mref = size_t(std::max<int64_t>((max_tris - ntri) / 3, 1));
+    ACU(a->flag.ensure(sizeof(uint32_t) * mt));
+    ACU(a->rank.ensure(sizeof(uint32_t) * mt));
+    ACU(a->tarea.ensure(sizeof(double) * mt));
+    ACU(a->part.ensure(sizeof(uint32_t) * size_t(scan_part_words(3 * max_tris))));
+    ACU(a->refined.ensure(sizeof(int32_t) * mref));
+    ACU(a->occ_slot.ensure(sizeof(int64_t) * 3 * mref));
+    ACU(a->cflag.ensure(sizeof(uint32_t) * 3 * mref));
+    ACU(a->crank.ensure(sizeof(uint32_t) * 3 * mref));
+    ACU(a->rec_v.ensure(sizeof(uint32_t) * 6 * mref));
+    ACU(a->rec_d.ensure(sizeof(double) * 6 * mref));
+    ACU(a->rec_k.ensure(sizeof(uint8_t) * 6 * mref));
+    ACU(a->sort_tmp.ensure(sizeof(uint32_t) * 6 * mref));
+    ACU(a->sort_perm.ensure(sizeof(int32_t) * 6 * mref));
+    ACU(a->sort_perm_tmp.ensure(sizeof(int32_t) * 6 * mref));
+    ACU(a->sort_hist.ensure(sizeof(uint32_t) * size_t(sort_scratch_words(int64_t(6 * mref)))));
     // initial lists in increasing triangle order: key = triangle index
     std::vector<uint64_t> keys(3 * size_t(ntri));
     for (int64_t j = 0; j < ntri; j++) keys[3 * j] = keys[3 * j + 1] = keys[3 * j + 2] = uint64_t(j);
