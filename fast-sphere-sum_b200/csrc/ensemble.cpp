@@ -79,7 +79,7 @@ int eupload(fss_ensemble* e, DBuf& b, const std::vector<T>& v) {
 int resort(fss_ensemble* e) {
     const int64_t n = e->ntot;
     launch_reassign(e->stream, n, e->s0.as<double4>(), e->leaves.as<EnsLeaf>(), 0, e->node.as<NodeGeom>(),
-                    e->lev_off.as<int64_t>(), e->key.as<uint32_t>());
+                    e->lev_off.as<int64_t>(), e->key.as<uint32_t>(), e->err.as<int>());
     int bits = 0;
     while ((int64_t(1) << bits) < e->nleaf) bits++;
     launch_sort(e->stream, n, std::max(bits, 1), e->key.as<uint32_t>(), e->key_tmp.as<uint32_t>(),
@@ -387,6 +387,7 @@ int fss_ensemble_get_state(fss_ensemble* e, int32_t member, double* state5) {
                         e->stream));
     ECU(cudaMemcpyAsync(&err, e->err.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
     ECU(cudaStreamSynchronize(e->stream));
+    if (err == kErrNonFinite) return efail(FSS_ERR_INVALID, "non-finite particle position (diverged state?)");
     if (err) return efail(FSS_ERR_TIMEOUT, "a kernel's bounded wait timed out");
     for (int64_t k = 0; k < n; k++) {
         double* o = state5 + 5 * int64_t(perm[k]);

@@ -101,6 +101,7 @@ int check_device_error(fss_ctx* c) {
     prof_resolve(c);
     if (h != 0) {
         cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), c->stream);
+        if (h == kErrNonFinite) return fail(c, FSS_ERR_INVALID, "non-finite particle position (diverged state?)");
         return fail(c, h == kErrTimeout ? FSS_ERR_TIMEOUT : FSS_ERR_TREE,
                     h == kErrTimeout ? "a kernel's bounded wait timed out" : "tree build error");
     }
@@ -332,6 +333,8 @@ int build_tree(fss_ctx* c) {
     CU(cudaMemcpyAsync(c->leaf_start_h.data(), c->leaf_start.p, sizeof(int32_t) * (c->nleaf + 1),
                        cudaMemcpyDeviceToHost, c->stream));
     CU(cudaStreamSynchronize(c->stream));
+    // stop here on non-finite input positions (before lists and autotuning)
+    TRY(check_device_error(c));
     // per-face counts on every level from the leaf ranges
     c->counts_h.assign(nfaces, 0);
     for (int l = 0; l <= LL; l++) {
@@ -608,7 +611,7 @@ int resort(fss_ctx* c) {
     ProfScope ps(c, "resort", 1 + 3 * ((bits + 7) / 8) + 2 + 1);
     const int64_t n = c->n;
     launch_reassign(c->stream, n, c->s0.as<double4>(), nullptr, c->leaf_level, c->node.as<NodeGeom>(),
-                    c->lev_off.as<int64_t>(), c->key.as<uint32_t>());
+                    c->lev_off.as<int64_t>(), c->key.as<uint32_t>(), c->err_flag.as<int>());
     launch_sort(c->stream, n, bits, c->key.as<uint32_t>(), c->key_tmp.as<uint32_t>(),
                 c->sortq.as<int32_t>(), c->vals_tmp.as<int32_t>(), c->hist.as<uint32_t>());
     launch_resort(c->stream, c->fp64, n, c->sortq.as<int32_t>(), c->s0.as<double4>(), c->area_s.as<double>(),

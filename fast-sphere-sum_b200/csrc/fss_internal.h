@@ -13,7 +13,7 @@
 namespace fss {
 
 // Error codes a kernel records in the context's device error word.
-enum : int { kErrNone = 0, kErrTimeout = 1, kErrTree = 2 };
+enum : int { kErrNone = 0, kErrTimeout = 1, kErrTree = 2, kErrNonFinite = 3 };
 
 // One run of sources of a work item.  The pair kernel resolves it to a
 // range [lo, hi) of the unified source array (particles [0, n), proxies

@@ -26,6 +26,7 @@ __global__ void k_assign(int64_t n, const double* __restrict__ in5, const double
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double p[3] = {in5[5 * i], in5[5 * i + 1], in5[5 * i + 2]};
+    if (!isfinite(p[0]) || !isfinite(p[1]) || !isfinite(p[2])) set_error(err, kErrNonFinite);
     int prev = 0;
     for (int l = 0; l < tree_levels; l++) {
         const int lb = (l > 0) ? 4 * prev : 0, ub = (l > 0) ? lb + 4 : 20;
@@ -49,7 +50,6 @@ __global__ void k_assign(int64_t n, const double* __restrict__ in5, const double
         }
     }
     if (key) key[i] = uint32_t(prev);
-    (void)err;
 }
 
 // Per-face member counts of every level from loc (reference-mode parity).
@@ -294,10 +294,18 @@ __device__ __forceinline__ double min_cone(const NodeGeom& g, double x, double y
 
 __global__ void k_reassign(int64_t n, const double4* __restrict__ pos, const EnsLeaf* __restrict__ leaves,
                            int leaf_level, const NodeGeom* __restrict__ node, const int64_t* __restrict__ lev_off,
-                           uint32_t* __restrict__ key) {
+                           uint32_t* __restrict__ key, int* __restrict__ err) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double4 q = pos[i];
+    // a non-finite position (a diverged state) fails every cone test and
+    // would send the particle down the first-child chain: all such particles
+    // would pile into one leaf and one block.  It keeps its leaf instead,
+    // and the call reports the error.
+    if (!isfinite(q.x) || !isfinite(q.y) || !isfinite(q.z)) {
+        set_error(err, kErrNonFinite);
+        return;
+    }
     const uint32_t g = key[i];
     int LL = leaf_level, local = int(g);
     if (leaves) {
@@ -428,9 +436,9 @@ void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, con
 }
 
 void launch_reassign(cudaStream_t st, int64_t n, const double4* pos, const EnsLeaf* leaves, int leaf_level,
-                     const NodeGeom* node, const int64_t* lev_off, uint32_t* key) {
+                     const NodeGeom* node, const int64_t* lev_off, uint32_t* key, int* err) {
     if (n == 0) return;
-    k_reassign<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, pos, leaves, leaf_level, node, lev_off, key);
+    k_reassign<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, pos, leaves, leaf_level, node, lev_off, key, err);
 }
 
 void launch_resort(cudaStream_t st, bool fp64, int64_t n, const int32_t* q, double4* s0, double* area,

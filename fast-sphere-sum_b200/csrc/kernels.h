@@ -60,7 +60,7 @@ void launch_leaf_bounds(cudaStream_t st, int64_t n, const uint32_t* skey, int32_
 // (through the free stage buffers xs and acc) and the stage-1 sources
 // rewritten.
 void launch_reassign(cudaStream_t st, int64_t n, const double4* pos, const EnsLeaf* leaves, int leaf_level,
-                     const NodeGeom* node, const int64_t* lev_off, uint32_t* key);
+                     const NodeGeom* node, const int64_t* lev_off, uint32_t* key, int* err);
 void launch_resort(cudaStream_t st, bool fp64, int64_t n, const int32_t* q, double4* s0, double* area,
                    double* tracer, int32_t* perm, double4* xs, double4* acc, void* src);
 void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, const double* area_in, const int32_t* perm,

@@ -89,3 +89,26 @@ def test_rhs_current_matches_rhs(fss):
         m1 = ctx.rhs_current()
         m2 = ctx.rhs(s, a)
     assert np.array_equal(m1, m2)
+
+
+def test_non_finite_positions_are_reported(fss):
+    """A NaN position fails every point-in-face test; the tree assignment
+    and the per-step re-sort report it (FSS_ERR_INVALID) instead of piling
+    such particles into one leaf, and a diverged state costs no more than a
+    normal step."""
+    import time
+    s, a = fss.make_state(5, "rh_vortices", n_vortex=4, seed=1)
+    bad = s.copy()
+    bad[7, 0] = np.nan
+    with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as ctx:
+        with pytest.raises(fss.FssError):
+            ctx.set_particles(bad, a)
+    with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as ctx:
+        ctx.set_particles(s, a)
+        ctx.rk4_step(0.01, nsteps=1)
+        diverged = np.ascontiguousarray(s.copy())
+        diverged[:, :3] = np.nan
+        t0 = time.perf_counter()
+        with pytest.raises(fss.FssError):
+            ctx.rk4_step_host(diverged, 0.01)
+        assert time.perf_counter() - t0 < 5.0
