@@ -140,3 +140,27 @@ def test_context_needs_gpu_or_reports(fss):
     with pytest.raises(fss.FssError) as e:
         fss.Context()
     assert e.value.code == 7
+
+
+def test_amr_and_remesh_need_gpu_or_report(fss):
+    """The AMR handle and the remesh step refuse loudly without a GPU, after
+    validating their arguments on the host."""
+    from conftest import gpu_available
+    if gpu_available():
+        pytest.skip("GPU present")
+    xyz, tris = fss.icos_grid(2)
+    with pytest.raises(fss.FssError) as e:
+        fss.Amr(tris, xyz.shape[0], 4 * xyz.shape[0], 4 * tris.shape[0])
+    assert e.value.code == 7
+    bad = tris.copy()
+    bad[0, 0] = xyz.shape[0]
+    with pytest.raises(fss.FssError) as e:
+        fss.Amr(bad, xyz.shape[0], 4 * xyz.shape[0], 4 * tris.shape[0])
+    assert e.value.code == 1  # checked before any device call
+    with pytest.raises(fss.FssError) as e:
+        fss.Amr(tris, xyz.shape[0], xyz.shape[0] - 1, 4 * tris.shape[0])
+    assert e.value.code == 1
+    s = np.zeros((xyz.shape[0], 5))
+    s[:, :3] = xyz
+    with pytest.raises(fss.FssError):
+        fss.remesh(s, s, tris)
