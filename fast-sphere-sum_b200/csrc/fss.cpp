@@ -1183,6 +1183,53 @@ int fss_remesh(int64_t n, const double* moved5, double* target5, int64_t ntri, c
     return FSS_OK;
 }
 
+int fss_remesh_lists(int64_t n, const double* moved5, double* target5, int64_t ntri, const int32_t* tris,
+                     const int32_t* vt_off, const int32_t* vt_adj, double omega, int64_t* n_fallback,
+                     int64_t* n_not_found) {
+    fss_ctx* c = nullptr;  // for the error macros: messages go to fss_last_error(NULL)
+    if (n < 3 || ntri < 1 || !moved5 || !target5 || !tris || !vt_off || !vt_adj)
+        return fail(c, FSS_ERR_INVALID, "bad remesh arguments");
+    if (n > (int64_t(1) << 30) || 3 * ntri > (int64_t(1) << 31) - 1)
+        return fail(c, FSS_ERR_INVALID, "too many particles or triangles");
+    for (int64_t j = 0; j < 3 * ntri; j++)
+        if (tris[j] < 0 || tris[j] >= n) return fail(c, FSS_ERR_INVALID, "triangle vertex out of range");
+    if (vt_off[0] != 0) return fail(c, FSS_ERR_INVALID, "vert_tris offsets must start at 0");
+    for (int64_t i = 0; i < n; i++)
+        if (vt_off[i + 1] < vt_off[i]) return fail(c, FSS_ERR_INVALID, "vert_tris offsets must not decrease");
+    const int64_t na = vt_off[n];
+    // the remesh kernels read corner ids (3 t + c) and use the triangle t
+    std::vector<uint32_t> off(size_t(n) + 1);
+    std::vector<int32_t> adj(size_t(std::max<int64_t>(na, 1)));
+    for (int64_t i = 0; i <= n; i++) off[i] = uint32_t(vt_off[i]);
+    for (int64_t a = 0; a < na; a++) {
+        if (vt_adj[a] < 0 || vt_adj[a] >= ntri) return fail(c, FSS_ERR_INVALID, "vert_tris triangle out of range");
+        adj[a] = 3 * vt_adj[a];
+    }
+    cudaStream_t st;
+    CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } guard{st};
+    DBuf dm, dt, dtri, doff, dadj;
+    RemeshScratch rs;
+    CU(dm.ensure(sizeof(double) * 5 * size_t(n)));
+    CU(dt.ensure(sizeof(double) * 5 * size_t(n)));
+    CU(dtri.ensure(sizeof(int32_t) * 3 * size_t(ntri)));
+    CU(doff.ensure(sizeof(uint32_t) * off.size()));
+    CU(dadj.ensure(sizeof(int32_t) * adj.size()));
+    CU(cudaMemcpyAsync(dm.p, moved5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(dt.p, target5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(dtri.p, tris, sizeof(int32_t) * 3 * ntri, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(doff.p, off.data(), sizeof(uint32_t) * off.size(), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(dadj.p, adj.data(), sizeof(int32_t) * adj.size(), cudaMemcpyHostToDevice, st));
+    CU(launch_remesh(st, n, dm.as<double>(), dt.as<double>(), ntri, dtri.as<int32_t>(), doff.as<uint32_t>(),
+                     dadj.as<int32_t>(), omega, rs, n_fallback, n_not_found));
+    CU(cudaMemcpyAsync(target5, dt.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    return FSS_OK;
+}
+
 int fss_remesh_current(fss_ctx* c, int64_t ntri, const int32_t* tris, double omega, int64_t* n_fallback,
                        int64_t* n_not_found) {
     if (!c || !tris || ntri < 1) return fail(c, FSS_ERR_INVALID, "bad remesh arguments");

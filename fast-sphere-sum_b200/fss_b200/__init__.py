@@ -78,7 +78,9 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_selector_apply", "fss_ensemble_create", "fss_ensemble_destroy", "fss_ensemble_set_stream",
            "fss_ensemble_add", "fss_ensemble_build", "fss_ensemble_rk4_step", "fss_ensemble_get_state",
            "fss_ensemble_info", "fss_amr_create", "fss_amr_destroy", "fss_amr_counts", "fss_amr_refine",
-           "fss_amr_get_mesh", "fss_amr_remesh", "fss_version"]
+           "fss_amr_get_mesh", "fss_amr_remesh", "fss_remesh_lists", "fss_state_csv_append",
+           "fss_point_count_append", "fss_output_name", "fss_state_bin_append", "fss_state_bin_read",
+           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_version"]
 
 NOALLOC_MAX_PARTICLES = 262144  # FSS_NOALLOC_MAX_PARTICLES in include/fss.h
 
@@ -141,6 +143,16 @@ def lib():
     L.fss_amr_refine.argtypes = [_vp, P(_i64), _D, _D, C.c_double, C.c_double]
     L.fss_amr_get_mesh.argtypes = [_vp, _vp, _vp, _vp]
     L.fss_amr_remesh.argtypes = [_vp, _D, _D, C.c_double, P(_i64), P(_i64)]
+    L.fss_remesh_lists.argtypes = [_i64, _D, _D, _i64, _I32, _I32, _I32, C.c_double, P(_i64), P(_i64)]
+    L.fss_state_csv_append.argtypes = [C.c_char_p, _i64, _D, _D]
+    L.fss_point_count_append.argtypes = [C.c_char_p, _i64]
+    L.fss_output_name.argtypes = [C.c_char_p, _i64, _i64, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                  _i64]
+    L.fss_state_bin_append.argtypes = [C.c_char_p, _i64, _D, _D]
+    L.fss_state_bin_read.argtypes = [C.c_char_p, _i64, _i64, _vp, _vp, P(_i64)]
+    L.fss_read_points_csv.argtypes = [C.c_char_p, _i64, _D]
+    L.fss_read_tris_csv.argtypes = [C.c_char_p, _i64, _I32]
+    L.fss_read_vert_tris_csv.argtypes = [C.c_char_p, C.c_char_p, _i64, _I32, _I32, _i64]
     L.fss_version.restype = C.c_char_p
     _lib = L
     return L
@@ -390,6 +402,81 @@ def rhs_direct_noalloc(n, state5_dev_ptr, area_dev_ptr, out5_dev_ptr, stream_han
     """fss_rhs_direct_noalloc on caller-owned device buffers (raw pointers);
     asynchronous on the given stream.  Raises FssError on a bad size."""
     _check(lib().fss_rhs_direct_noalloc(n, state5_dev_ptr, area_dev_ptr, omega, out5_dev_ptr, stream_handle))
+
+
+def remesh_lists(moved5, target5, tris, vt_off, vt_adj, omega=OMEGA):
+    """regrid_points2 with explicit vert_tris lists (CSR), tried in list
+    order (fss_remesh_lists): (new target state, fallback count, not-found
+    count)."""
+    m = np.ascontiguousarray(moved5, dtype=np.float64).reshape(-1)
+    t = np.ascontiguousarray(target5, dtype=np.float64).copy().reshape(-1)
+    tr = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1)
+    off = np.ascontiguousarray(vt_off, dtype=np.int32)
+    adj = np.ascontiguousarray(vt_adj if len(vt_adj) else np.zeros(1), dtype=np.int32)
+    fb, bad = _i64(), _i64()
+    _check(lib().fss_remesh_lists(m.size // 5, m, t, tr.size // 3, tr, off, adj, omega, C.byref(fb), C.byref(bad)))
+    return t.reshape(-1, 5), fb.value, bad.value
+
+
+# ------------------------------------------------------------------ files
+
+def output_name(point_count, init_cond, use_fast, tree_levels=1, use_amr=False, use_mpi=False, use_remesh=False,
+                time_steps=1):
+    """The reference's <name> of output_<name>.csv / point_counts_<name>.csv."""
+    buf = C.create_string_buffer(256)
+    _check(lib().fss_output_name(buf, 256, point_count, init_cond.encode(), int(use_fast), tree_levels,
+                                 int(use_amr), int(use_mpi), int(use_remesh), time_steps))
+    return buf.value.decode()
+
+
+def state_csv_append(path, state5, area):
+    s = np.ascontiguousarray(state5, dtype=np.float64)
+    _check(lib().fss_state_csv_append(str(path).encode(), s.shape[0], s.reshape(-1),
+                                      np.ascontiguousarray(area, dtype=np.float64)))
+
+
+def point_count_append(path, n):
+    _check(lib().fss_point_count_append(str(path).encode(), n))
+
+
+def state_bin_append(path, state5, area):
+    s = np.ascontiguousarray(state5, dtype=np.float64)
+    _check(lib().fss_state_bin_append(str(path).encode(), s.shape[0], s.reshape(-1),
+                                      np.ascontiguousarray(area, dtype=np.float64)))
+
+
+def state_bin_read(path, step):
+    """(state5, area) of step `step` of a binary state file."""
+    n = _i64()
+    rc = lib().fss_state_bin_read(str(path).encode(), step, 0, None, None, C.byref(n))
+    if rc not in (0, 8):
+        _check(rc)
+    s = np.zeros((n.value, 5))
+    a = np.zeros(n.value)
+    _check(lib().fss_state_bin_read(str(path).encode(), step, n.value, s.ctypes.data_as(_vp), a.ctypes.data_as(_vp),
+                                    C.byref(n)))
+    return s, a
+
+
+def read_points_csv(path, n):
+    """x, y, z, zeta of the reference's <N>points_rh4.csv (tracer left 0)."""
+    s = np.zeros((n, 5))
+    _check(lib().fss_read_points_csv(str(path).encode(), n, s.reshape(-1)))
+    return s
+
+
+def read_tris_csv(path, ntri):
+    t = np.zeros((ntri, 3), dtype=np.int32)
+    _check(lib().fss_read_tris_csv(str(path).encode(), ntri, t.reshape(-1)))
+    return t
+
+
+def read_vert_tris_csv(lists_path, counts_path, n, cap):
+    """The reference's vert_tris lists as CSR (off[n + 1], adj)."""
+    off = np.zeros(n + 1, dtype=np.int32)
+    adj = np.zeros(max(cap, 1), dtype=np.int32)
+    _check(lib().fss_read_vert_tris_csv(str(lists_path).encode(), str(counts_path).encode(), n, off, adj, cap))
+    return off, adj[:off[-1]].copy()
 
 
 AMR_VORTICITY_TOL, AMR_CIRCULATION_TOL = 0.2, 0.0025  # amr.h:14-15

@@ -189,6 +189,40 @@ int fss_remesh(int64_t n, const double* moved5, double* target5, int64_t ntri, c
 int fss_remesh_current(fss_ctx* ctx, int64_t ntri, const int32_t* tris, double omega, int64_t* n_fallback,
                        int64_t* n_not_found);
 
+/* regrid_points2 with the vertex -> triangles lists given explicitly (CSR:
+ * vert_tris of vertex i = vt_adj[vt_off[i] .. vt_off[i + 1]), e.g. as read
+ * from the reference's <N>vert_tris.csv by fss_read_vert_tris_csv); the
+ * adjacent triangles are tried in list order.  Otherwise as fss_remesh. */
+int fss_remesh_lists(int64_t n, const double* moved5, double* target5, int64_t ntri, const int32_t* tris,
+                     const int32_t* vt_off, const int32_t* vt_adj, double omega, int64_t* n_fallback,
+                     int64_t* n_not_found);
+
+/* ------------------------------------------------------------- state files
+ * The reference's output (new_dynamics.cpp:123-139, 228-236): per step, one
+ * line "x,y,z,zeta,tracer,area" per particle, each number as a default C++
+ * stream writes a double (%g, 6 significant digits), appended to
+ * output_<name>.csv; the particle count appended to point_counts_<name>.csv;
+ * <name> as fss_output_name builds it from the run's flags.  The binary
+ * equivalent appends per step the 8 bytes "FSSSTAT1", the count (int64)
+ * and count x 6 float64 (x, y, z, zeta, tracer, area), little-endian. */
+int fss_state_csv_append(const char* path, int64_t n, const double* state5, const double* area);
+int fss_point_count_append(const char* path, int64_t n);
+int fss_output_name(char* buf, int64_t cap, int64_t point_count, const char* init_cond, int use_fast,
+                    int tree_levels, int use_amr, int use_mpi, int use_remesh, int64_t time_steps);
+int fss_state_bin_append(const char* path, int64_t n, const double* state5, const double* area);
+/* Step `step` (from 0) of a binary state file: *n_out = its count;
+ * FSS_ERR_CAPACITY when that exceeds cap (state5/area may be NULL). */
+int fss_state_bin_read(const char* path, int64_t step, int64_t cap, double* state5, double* area, int64_t* n_out);
+/* The reference's inputs (helpers.h:299-340 read_points): <N>points_rh4.csv
+ * (x, y, z, zeta: the first 4 fields of each of n lines; the tracer is not
+ * read), <N>tris.csv (3 vertex indices per line), <N>vert_tris.csv with
+ * <N>vert_tri_count.csv (each vertex's triangles; CSR into off[n + 1] and
+ * adj[cap]).  Fields are parsed as stod does, then truncated for indices. */
+int fss_read_points_csv(const char* path, int64_t n, double* state5);
+int fss_read_tris_csv(const char* path, int64_t ntri, int32_t* tris);
+int fss_read_vert_tris_csv(const char* lists_path, const char* counts_path, int64_t n, int32_t* off, int32_t* adj,
+                           int64_t cap);
+
 /* ------------------------------------------------------------- AMR
  * amr.h:13-178 amr.  The handle holds the triangle mesh, the reference's
  * vert_tris lists (one ordering key per triangle corner: a vertex's list is

@@ -100,6 +100,8 @@ def _setup_ref(R):
     R.ref_amr.restype = C.c_int
     R.ref_regrid_csr.argtypes = [i64, _D, _D, i64, _I, _I, _I, C.c_double]
     R.ref_regrid_csr.restype = C.c_int
+    R.ref_read_points.argtypes = [C.c_char_p, i64, i64, _D, _I, _I, _I, i64]
+    R.ref_read_points.restype = C.c_int
 
 
 _setup(_lib)
@@ -328,3 +330,33 @@ def ref_remesh_lists(moved5, target5, tris, vert_tris, omega=OMEGA):
     adj = np.ascontiguousarray(np.concatenate(vert_tris) if len(vert_tris) else np.zeros(0), dtype=np.int32)
     rc = ref().ref_regrid_csr(m.size // 5, m, t, tr.size // 3, tr, off, adj, omega)
     return t.reshape(-1, 5), rc
+
+
+def ref_write_state(path, state5, area):
+    """The reference's per-step state lines appended to `path`, written by
+    oracle/_ref/ref_write_state (its stream statement restated in a small
+    program of its own); None when that program was not built."""
+    import subprocess, tempfile
+    exe = os.path.join(HERE, "_ref", "ref_write_state")
+    if not os.path.exists(exe):
+        return None
+    s = np.ascontiguousarray(state5, dtype=np.float64).reshape(-1, 5)
+    rows = np.concatenate([s, np.ascontiguousarray(area, dtype=np.float64)[:, None]], axis=1)
+    with tempfile.NamedTemporaryFile(suffix=".f64", delete=False) as f:
+        f.write(np.ascontiguousarray(rows).tobytes())
+        raw = f.name
+    try:
+        return subprocess.run([exe, raw, str(path)], check=False).returncode
+    finally:
+        os.unlink(raw)
+
+
+def ref_read_points(run_dir, n, ntri, cap):
+    """The reference's read_points run from `run_dir`: (state5, tris, off, adj)."""
+    s = np.zeros((n, 5))
+    t = np.zeros((ntri, 3), dtype=np.int32)
+    off = np.zeros(n + 1, dtype=np.int32)
+    adj = np.zeros(cap, dtype=np.int32)
+    rc = ref().ref_read_points(str(run_dir).encode(), n, ntri, s.reshape(-1), t.reshape(-1), off, adj, cap)
+    assert rc == 0, rc
+    return s, t, off, adj[:off[-1]].copy()

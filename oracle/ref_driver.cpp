@@ -14,6 +14,7 @@
 #include <string>
 #include <thread>
 #include <vector>
+#include <unistd.h>
 
 #include "helpers.h"
 #include "struct_list.h"
@@ -284,6 +285,38 @@ int ref_regrid_csr(int64_t n, const double* moved5, double* target5, int64_t ntr
 
 int ref_regrid(int64_t n, const double* moved5, double* target5, int64_t ntri, const int* tris, double omega) {
     return ref_regrid_range(n, moved5, target5, ntri, tris, omega, 0, n);
+}
+
+// helpers.h:299 read_points itself: it opens ../<N>points_rh4.csv,
+// ../<N>tris.csv, ../<N>vert_tris.csv and ../<N>vert_tri_count.csv relative
+// to the working directory, so it runs from `run_dir` (a directory below
+// the files) and the working directory is restored after.  Outputs: state
+// (x, y, z, zeta; tracer 0), triangles, vert_tris as CSR.
+int ref_read_points(const char* run_dir, int64_t n, int64_t ntri, double* state5, int* tris, int* vt_off, int* vt_adj,
+                    int64_t cap) {
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof(cwd)) || chdir(run_dir) != 0) return -1;
+    run_information config1;
+    config1.point_count = int(n);
+    config1.tri_count = int(ntri);
+    config1.amr_vert_tris.assign(n, vector<int>());
+    config1.dynamics_tris.assign(ntri, vector<int>(3));
+    vector<double> curr_state(5 * n, 0.0);
+    read_points(config1, curr_state);
+    if (chdir(cwd) != 0) return -1;
+    std::memcpy(state5, curr_state.data(), sizeof(double) * 5 * n);
+    for (int64_t j = 0; j < ntri; j++)
+        for (int k = 0; k < 3; k++) tris[3 * j + k] = config1.dynamics_tris[j][k];
+    int64_t a = 0;
+    for (int64_t i = 0; i < n; i++) {
+        vt_off[i] = int(a);
+        for (int t : config1.amr_vert_tris[i]) {
+            if (a >= cap) return -2;
+            vt_adj[a++] = t;
+        }
+    }
+    vt_off[n] = int(a);
+    return 0;
 }
 
 // amr.h:13 amr on the reference's own structures built from flat arrays:

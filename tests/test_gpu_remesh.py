@@ -96,3 +96,26 @@ def test_remesh_current_cached_adjacency(fss, oracle):
             fb, nf = ctx.remesh_current(tris)
             assert fb == fb_ref and nf == 0
             assert np.array_equal(ctx.get_state().view(np.uint64), ref.view(np.uint64))
+
+
+def test_remesh_lists_follow_list_order(fss, oracle):
+    """fss_remesh_lists tries each vertex's triangles in the order of its
+    vert_tris list (here shuffled), as regrid_points2 does with the lists it
+    reads; bit-exact with the oracle ordered by the same lists."""
+    from test_state_files import list_keys
+    m, s, tris = _moved(oracle, 5, 0.4, seed=8, far=25)
+    n = s.shape[0]
+    lists = [[] for _ in range(n)]
+    for j, t in enumerate(tris):
+        for v in t:
+            lists[v].append(j)
+    rng = np.random.default_rng(1)
+    lists = [list(rng.permutation(l)) for l in lists]
+    off = np.concatenate([[0], np.cumsum([len(l) for l in lists])]).astype(np.int32)
+    adj = np.concatenate(lists).astype(np.int32)
+    ref, fb_ref, bad_ref = oracle.remesh(m, s, tris, keys=list_keys(tris, off, adj))
+    got, fb, bad = fss.remesh_lists(m, s, tris, off, adj)
+    assert (fb, bad) == (fb_ref, bad_ref) and fb > 0
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
+    with pytest.raises(fss.FssError):
+        fss.remesh_lists(m, s, tris, off[::-1].copy(), adj)  # offsets must not decrease
