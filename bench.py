@@ -51,7 +51,7 @@ def parse():
     p.add_argument("--no-amr", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=2048, help="targets in one CPU-baseline sample")
     p.add_argument("--tol", type=float, default=1e-6, help="selector: relative L2 velocity error target")
-    p.add_argument("--safety", type=float, default=2.0, help="selector: predicted-error safety factor")
+    p.add_argument("--safety", type=float, default=1.5, help="selector: predicted-error safety factor")
     p.add_argument("--fixed", action="store_true", help="headline arm without the learned selector")
     p.add_argument("--no-clusters", action="store_true",
                    help="headline arm without target clusters (far sources summed at the target particles)")
