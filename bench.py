@@ -275,7 +275,7 @@ def remesh_measure(fss, ctx, state, area, level, stream, reps=5):
     t0 = time.perf_counter()
     for _ in range(reps):
         ctx.rk4_step(DT, nsteps=1)
-        ctx.remesh_current(tris)
+        ctx.remesh_current()  # the triangles of the previous call
     stream.synchronize()
     loop_s = time.perf_counter() - t0
     out = {"workload": "one RK4 step from the grid, then regrid onto the grid (the reference's use_remesh loop)",

@@ -1232,14 +1232,22 @@ int fss_remesh_lists(int64_t n, const double* moved5, double* target5, int64_t n
 
 int fss_remesh_current(fss_ctx* c, int64_t ntri, const int32_t* tris, double omega, int64_t* n_fallback,
                        int64_t* n_not_found) {
-    if (!c || !tris || ntri < 1) return fail(c, FSS_ERR_INVALID, "bad remesh arguments");
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
     if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    const int64_t n = c->n;
+    if (!tris) {  // the triangles of the previous call
+        if (ntri != 0 || c->rm_n != n || c->rm_tris_host.empty())
+            return fail(c, FSS_ERR_STATE, "no triangles from a previous remesh to reuse");
+        ntri = int64_t(c->rm_tris_host.size() / 3);
+        tris = c->rm_tris_host.data();
+    }
+    if (ntri < 1) return fail(c, FSS_ERR_INVALID, "bad remesh arguments");
     if (3 * ntri > (int64_t(1) << 31) - 1) return fail(c, FSS_ERR_INVALID, "too many triangles");
     CU(cudaSetDevice(c->dev));
-    const int64_t n = c->n;
     // triangles and adjacency: rebuilt on the device only when they changed
     const bool same = c->rm_n == n && c->rm_tris_host.size() == size_t(3 * ntri) &&
-                      std::memcmp(c->rm_tris_host.data(), tris, sizeof(int32_t) * 3 * ntri) == 0;
+                      (tris == c->rm_tris_host.data() ||
+                       std::memcmp(c->rm_tris_host.data(), tris, sizeof(int32_t) * 3 * ntri) == 0);
     if (!same) {
         c->rm_n = -1;
         c->rm_tris_host.assign(tris, tris + 3 * ntri);

@@ -111,7 +111,7 @@ def lib():
     L.fss_rhs_current.argtypes = [_vp, C.c_double, _D, _vp]
     _I32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
     L.fss_remesh.argtypes = [_i64, _D, _D, _i64, _I32, C.c_double, C.POINTER(_i64), C.POINTER(_i64)]
-    L.fss_remesh_current.argtypes = [_vp, _i64, _I32, C.c_double, C.POINTER(_i64), C.POINTER(_i64)]
+    L.fss_remesh_current.argtypes = [_vp, _i64, _vp, C.c_double, C.POINTER(_i64), C.POINTER(_i64)]
     L.fss_get_tree_info.argtypes = [_vp, P(TreeInfo)]
     L.fss_get_tree.argtypes = [_vp, _vp, _vp, _vp, _i64]
     L.fss_set_leaf_params.argtypes = [_vp, C.c_int32, _I, _D]
@@ -326,12 +326,17 @@ class Context:
     def rhs_treecode(self, state5, area, omega=OMEGA, psi=False):
         return self._rhs(lib().fss_rhs_treecode, state5, area, omega, psi)
 
-    def remesh_current(self, tris, omega=OMEGA):
+    def remesh_current(self, tris=None, omega=OMEGA):
         """remesh.h regrid_points2 on the device state, onto the positions
-        given to set_particles; returns (fallback count, not-found count)."""
-        t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1)
+        given to set_particles; returns (fallback count, not-found count).
+        tris=None reuses the triangles of the previous call."""
         fb, bad = _i64(), _i64()
-        self._c(lib().fss_remesh_current(self.h, t.size // 3, t, omega, C.byref(fb), C.byref(bad)))
+        if tris is None:
+            self._c(lib().fss_remesh_current(self.h, 0, None, omega, C.byref(fb), C.byref(bad)))
+            return fb.value, bad.value
+        t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1)
+        self._c(lib().fss_remesh_current(self.h, t.size // 3, t.ctypes.data_as(_vp), omega, C.byref(fb),
+                                         C.byref(bad)))
         return fb.value, bad.value
 
     def rhs_current(self, omega=OMEGA, psi=False):

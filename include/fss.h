@@ -185,7 +185,9 @@ int fss_remesh(int64_t n, const double* moved5, double* target5, int64_t ntri, c
  * use_remesh): the targets are the positions given to fss_set_particles; the
  * remeshed state becomes the context's state (and, with re-sorting, the
  * particles go back into the leaves of their grid points).  A point found in
- * no triangle keeps its current zeta and tracer. */
+ * no triangle keeps its current zeta and tracer.  tris = NULL with ntri = 0
+ * reuses the triangles of the previous call (skipping the comparison with
+ * them that a repeated array costs). */
 int fss_remesh_current(fss_ctx* ctx, int64_t ntri, const int32_t* tris, double omega, int64_t* n_fallback,
                        int64_t* n_not_found);
 

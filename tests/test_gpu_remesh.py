@@ -76,7 +76,8 @@ def test_remesh_many_fallbacks_cell_grid(fss, oracle):
 
 def test_remesh_current_cached_adjacency(fss, oracle):
     """Repeated regrids with the same triangles reuse the device adjacency;
-    a bad triangle list in between is refused and the next call rebuilds."""
+    a bad triangle list in between is refused and the next call rebuilds; a
+    call without triangles uses those of the previous call."""
     level = 5
     s, a = fss.make_state(level, "rh_vortices", n_vortex=8, seed=9)
     _, tris = fss.icos_grid(level)
@@ -84,6 +85,8 @@ def test_remesh_current_cached_adjacency(fss, oracle):
     bad[7, 1] = -1
     with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as ctx:
         ctx.set_particles(s, a)
+        with pytest.raises(fss.FssError):
+            ctx.remesh_current()  # nothing to reuse yet
         for k in range(3):
             ctx.rk4_step(0.02, nsteps=2)
             moved = ctx.get_state()
@@ -93,7 +96,8 @@ def test_remesh_current_cached_adjacency(fss, oracle):
             if k == 1:
                 with pytest.raises(fss.FssError):
                     ctx.remesh_current(bad)
-            fb, nf = ctx.remesh_current(tris)
+            # the last call passes no triangles: those of the previous call
+            fb, nf = ctx.remesh_current(None if k == 2 else tris)
             assert fb == fb_ref and nf == 0
             assert np.array_equal(ctx.get_state().view(np.uint64), ref.view(np.uint64))
 
