@@ -351,6 +351,40 @@ def amr_measure(fss, level=5, reps=3):
     return out
 
 
+def kernel_rooflines(prof, steps, n, info, up_bytes, peaks):
+    """HBM roofline of the memory-bound ranges with the algorithmic byte
+    units of the scope table: upward pass = N 16 B read per level + K (4 +
+    12) B per proxy (per RHS, from fss_work_per_rhs); tree build (the
+    per-step re-sort) = N (24 + 8 + 16) B + 2 N 12 B per 8-bit radix pass;
+    RK4 combine = N (5 x 8 x (1 + 4) + 5 x 8 + 16) B per step.  The
+    downward pass has no byte unit (FP64, latency-bound): time only.  Times
+    from the kernel-level pass (events around every launch)."""
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    src = "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
+    leaves = max(int(info.get("leaf_count", 1)), 2)
+    passes = (max((leaves - 1).bit_length(), 1) + 7) // 8
+    out = []
+
+    def add(name, ms, nbytes, per):
+        gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
+        out.append({"kernel": name, "bound": "hbm", "bytes": nbytes, "per": per, "ms": ms, "achieved": gbs,
+                    "peak": hbm, "unit": "GB/s", "frac": (gbs / hbm) if gbs else None, "peak_source": src})
+
+    up_ms = sum(prof[k][0] for k in ("upward_leaf", "upward_combine") if k in prof) / (4 * steps)
+    if up_ms > 0:
+        add("upward pass (k_up_leaf + k_up_combine)", up_ms, float(up_bytes), "RHS")
+    if "resort" in prof:
+        add("tree build: per-step re-sort (k_reassign, radix sort, k_resort_*, k_leaf_bounds)",
+            prof["resort"][0] / steps, float(n) * (24 + 8 + 16) + 2.0 * n * 12 * passes, "step")
+    if "epilogue" in prof:
+        add("RK4 combine (k_epilogue, 4 per step)", prof["epilogue"][0] / steps,
+            float(n) * (5 * 8 * 5 + 5 * 8 + 16), "step")
+    if "downward" in prof:
+        out.append({"kernel": "downward pass (k_down_level, k_down_leaf)", "bound": "latency",
+                    "ms": prof["downward"][0] / (4 * steps), "per": "RHS"})
+    return out
+
+
 def main_reference(args, ws, rank):
     if rank != 0:
         return
@@ -450,7 +484,8 @@ def main():
                 "peak_source": f"nominal FP32 148 SM x 128 lanes x 2 x {sm_max:.0f} MHz (MEASURED_PEAKS.json has no FP32 figure)",
                 "frac_at_sampled_clock": (achieved / (fp32_peak * clocks["sm_mhz"] / sm_max)) if clocks.get("sm_mhz") else None,
                 "kernel_shares": {k: round(v[0] / total_ms, 4) for k, v in prof.items()},
-                "upward_bytes_per_rhs": up_bytes}
+                "upward_bytes_per_rhs": up_bytes,
+                "kernels": kernel_rooflines(prof, args.steps, n, ctx.tree_info(), up_bytes, peaks)}
     info = ctx.tree_info()
 
     # ---------------- FP64 arms: plain BLTC (the ratio's denominator: fixed n, theta,
