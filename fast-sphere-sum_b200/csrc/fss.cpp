@@ -608,7 +608,7 @@ int resort(fss_ctx* c) {
     while ((int64_t(1) << bits) < c->nleaf) bits++;
     bits = std::max(bits, 1);
     // reassign, 3 per 8-bit sort pass, gather + commit, leaf bounds
-    ProfScope ps(c, "resort", 1 + 3 * ((bits + 7) / 8) + 2 + 1);
+    ProfScope ps(c, "resort", 1 + sort_launch_count(c->n, bits) + 2 + 1);
     const int64_t n = c->n;
     launch_reassign(c->stream, n, c->s0.as<double4>(), nullptr, c->leaf_level, c->node.as<NodeGeom>(),
                     c->lev_off.as<int64_t>(), c->key.as<uint32_t>(), c->err_flag.as<int>());

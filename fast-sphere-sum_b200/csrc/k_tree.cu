@@ -393,9 +393,17 @@ void launch_scan_u32(cudaStream_t st, uint32_t* a, int64_t m, uint32_t* part) {
     k_chunk_scan<<<unsigned(nchunk), 1024, 0, st>>>(a, m, part);
 }
 
+// Digit histograms (256 per block), then the scan's chunk totals.
 int64_t sort_scratch_words(int64_t n) {
     const int64_t nblk = (n + kSortTile - 1) / kSortTile;
-    return 256 * nblk;
+    return 256 * nblk + scan_part_words(256 * nblk);
+}
+
+int sort_launch_count(int64_t n, int bits) {
+    if (n == 0) return 0;
+    const int64_t nblk = (n + kSortTile - 1) / kSortTile;
+    const int scan = scan_part_words(256 * nblk) <= 4 ? 1 : 3;
+    return ((bits + 7) / 8) * (2 + scan);
 }
 
 void launch_sort(cudaStream_t st, int64_t n, int bits, uint32_t* keys, uint32_t* keys_tmp, int32_t* vals,
@@ -407,7 +415,7 @@ void launch_sort(cudaStream_t st, int64_t n, int bits, uint32_t* keys, uint32_t*
     int pass = 0;
     for (int shift = 0; shift < bits; shift += 8, pass++) {
         k_radix_hist<<<nblk, kSortThreads, 0, st>>>(n, ki, shift, hist, nblk);
-        k_scan_exclusive<<<1, 1024, 0, st>>>(hist, int64_t(256) * nblk);
+        launch_scan_u32(st, hist, int64_t(256) * nblk, hist + int64_t(256) * nblk);
         k_radix_scatter<<<nblk, kSortThreads, 0, st>>>(n, ki, vi, ko, vo, shift, hist, nblk);
         std::swap(ki, ko);
         vi = vo;

@@ -51,6 +51,8 @@ void launch_assign(cudaStream_t st, int64_t n, const double* in5, const double* 
 void launch_level_hist(cudaStream_t st, int64_t n, int tree_levels, const int32_t* loc, const int64_t* lev_off,
                        int32_t* counts);
 int64_t sort_scratch_words(int64_t n);
+// Kernel launches of one launch_sort call.
+int sort_launch_count(int64_t n, int bits);
 void launch_sort(cudaStream_t st, int64_t n, int bits, uint32_t* keys, uint32_t* keys_tmp, int32_t* vals,
                  int32_t* vals_tmp, uint32_t* hist);
 void launch_leaf_bounds(cudaStream_t st, int64_t n, const uint32_t* skey, int32_t nleaf, int32_t* leaf_start);
