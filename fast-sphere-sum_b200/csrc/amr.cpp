@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "amr_internal.h"
 #include "fss.h"
 #include "kernels.h"
 
@@ -18,27 +19,6 @@ void set_last_error(const std::string& msg);
 }
 
 using namespace fss;
-
-struct fss_amr {
-    int dev = 0;
-    cudaStream_t st = nullptr;
-    int64_t n = 0, ntri = 0, max_points = 0, max_tris = 0;
-    uint64_t seq = 0;  // refinements so far (append keys)
-    bool broken = false;
-    // mesh
-    DBuf state5, area, tris, keys, parent, hkeys, hvals, err;
-    int64_t hmask = 0;
-    // one pass
-    DBuf flag, rank, tarea, refined, occ_slot, cflag, crank, part;
-    DBuf rec_v, rec_d, rec_k, sort_tmp, sort_perm, sort_perm_tmp, sort_hist;
-    // remesh on the current mesh
-    DBuf moved, target, off, adj;
-    bool adj_ok = false;
-    RemeshScratch rs;
-    ~fss_amr() {
-        if (st) cudaStreamDestroy(st);
-    }
-};
 
 namespace {
 
@@ -77,8 +57,10 @@ int scan_total(fss_amr* a, const uint32_t* rank, const uint32_t* flag, int64_t m
     return FSS_OK;
 }
 
+}  // namespace
+
 // The whole pass on the device state; host buffers are not touched.
-int refine_device(fss_amr* a, double vtol, double ctol) {
+int fss::amr_refine_device(fss_amr* a, double vtol, double ctol) {
     cudaStream_t st = a->st;
     int64_t n = a->n, q0 = 0, q1 = a->ntri, nrec = 0;
     uint64_t seq = a->seq;
@@ -152,7 +134,6 @@ int refine_device(fss_amr* a, double vtol, double ctol) {
     return FSS_OK;
 }
 
-}  // namespace
 
 extern "C" {
 
@@ -259,7 +240,7 @@ int fss_amr_refine(fss_amr* a, int64_t* point_count, double* state5, double* are
     const int64_t n0 = a->n;
     ACU(cudaMemcpyAsync(a->state5.p, state5, sizeof(double) * 5 * n0, cudaMemcpyHostToDevice, a->st));
     ACU(cudaMemcpyAsync(a->area.p, area, sizeof(double) * n0, cudaMemcpyHostToDevice, a->st));
-    if (int rc = refine_device(a, vorticity_tol, circulation_tol)) {
+    if (int rc = amr_refine_device(a, vorticity_tol, circulation_tol)) {
         a->broken = true;
         return rc;
     }

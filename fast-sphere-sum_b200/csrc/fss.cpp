@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "amr_internal.h"
 #include "ctx.h"
 #include "geometry.h"
 #include "kernels.h"
@@ -238,8 +239,9 @@ int set_particles(fss_ctx* c, int64_t n, const double* state5, const double* are
     invalidate_graph(c);
     c->n = n;
     TRY(ensure_particle_buffers(c, n));
-    CU(cudaMemcpyAsync(c->in5.p, state5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, c->stream));
-    CU(cudaMemcpyAsync(c->area_in.p, area, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    // host or device arrays (unified addressing)
+    CU(cudaMemcpyAsync(c->in5.p, state5, sizeof(double) * 5 * n, cudaMemcpyDefault, c->stream));
+    CU(cudaMemcpyAsync(c->area_in.p, area, sizeof(double) * n, cudaMemcpyDefault, c->stream));
     // the positions given here are the grid the remesh step returns to
     CU(c->grid3.ensure(sizeof(double) * 3 * size_t(n)));
     CU(cudaMemcpy2DAsync(c->grid3.p, 3 * sizeof(double), c->in5.p, 5 * sizeof(double), 3 * sizeof(double), size_t(n),
@@ -1280,6 +1282,37 @@ int fss_remesh_current(fss_ctx* c, int64_t ntri, const int32_t* tris, double ome
     c->stage_dirty = false;
     if (c->tree && c->resort) TRY(resort(c));
     return check_device_error(c);
+}
+
+int fss_amr_refine_current(fss_ctx* c, fss_amr* a, double vorticity_tol, double circulation_tol, double omega,
+                           int64_t* point_count) {
+    if (!c || !a) return fail(c, FSS_ERR_INVALID, "null argument");
+    if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    if (a->broken) return fail(c, FSS_ERR_STATE, "amr handle unusable after a capacity error");
+    if (a->n != c->n) return fail(c, FSS_ERR_INVALID, "the context's particles are not the mesh's points");
+    if (a->dev != c->dev) return fail(c, FSS_ERR_INVALID, "the context and the mesh are on different devices");
+    CU(cudaSetDevice(c->dev));
+    const int64_t n0 = c->n;
+    if (n0 < a->max_points) {  // config1.point_count >= config1.max_count: amr() does nothing
+        // the current state in the caller's order, and its areas, into the mesh
+        TRY(refresh_stage(c));
+        launch_scatter_state(c->stream, n0, c->tree ? c->perm.as<int32_t>() : nullptr, c->s0.as<double4>(),
+                             c->tracer_s.as<double>(), c->out5.as<double>());
+        CU(cudaMemcpyAsync(a->state5.p, c->out5.p, sizeof(double) * 5 * n0, cudaMemcpyDeviceToDevice, c->stream));
+        CU(cudaMemcpyAsync(a->area.p, c->area_in.p, sizeof(double) * n0, cudaMemcpyDeviceToDevice, c->stream));
+        CU(cudaStreamSynchronize(c->stream));
+        if (int rc = amr_refine_device(a, vorticity_tol, circulation_tol)) {
+            a->broken = true;
+            return fail(c, rc, fss_last_error(nullptr));
+        }
+        // the new midpoints onto the sphere (the step's own projection placed
+        // the others there), then the new particle set
+        amr_project(a->st, n0, a->n, a->state5.as<double>(), omega);
+        CU(cudaStreamSynchronize(a->st));
+        if (a->n > n0) TRY(set_particles(c, a->n, a->state5.as<double>(), a->area.as<double>()));
+    }
+    if (point_count) *point_count = c->n;
+    return FSS_OK;
 }
 
 }  // extern "C"

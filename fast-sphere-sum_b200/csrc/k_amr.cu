@@ -230,7 +230,25 @@ __global__ void k_amr_areas(int64_t nrec, const uint32_t* __restrict__ sv, const
     area[v] = a;
 }
 
+// helpers.h:362-372 project_points on points [i0, i1): x *= 1/|x| (|x|
+// summed from 0, helpers.h:82-85 project_to_sphere), zeta += -2 omega dz.
+__global__ void k_amr_project(int64_t i0, int64_t i1, double* __restrict__ state5, double omega) {
+    const int64_t i = i0 + int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= i1) return;
+    double* s = state5 + 5 * i;
+    const double z_old = s[2];
+    const double r = __ddiv_rn(1.0, __dsqrt_rn(dot_self(s)));
+    s[0] = __dmul_rn(s[0], r);
+    s[1] = __dmul_rn(s[1], r);
+    s[2] = __dmul_rn(s[2], r);
+    s[3] = __dadd_rn(s[3], __dmul_rn(__dmul_rn(-2.0, omega), __dsub_rn(s[2], z_old)));
+}
+
 // ---------------------------------------------------------------- launchers
+
+void amr_project(cudaStream_t st, int64_t i0, int64_t i1, double* state5, double omega) {
+    if (i1 > i0) k_amr_project<<<unsigned((i1 - i0 + 255) / 256), 256, 0, st>>>(i0, i1, state5, omega);
+}
 
 cudaError_t amr_seed_parents(cudaStream_t st, int64_t n, const int32_t* parent, unsigned long long* hkeys,
                              long long* hvals, int64_t hmask, int* err) {

@@ -165,6 +165,7 @@ void amr_split(cudaStream_t st, int64_t nref, int64_t q0, int64_t q1, uint64_t s
                int32_t* tris, uint64_t* keys, uint32_t* rec_v, double* rec_d, uint8_t* rec_k);
 void amr_areas(cudaStream_t st, int64_t nrec, const uint32_t* sv, const int32_t* perm, const double* rec_d,
                const uint8_t* rec_k, double* area);
+void amr_project(cudaStream_t st, int64_t i0, int64_t i1, double* state5, double omega);
 
 // In-place exclusive prefix sum of m 32-bit counts; `part` holds
 // scan_part_words(m) words of scratch (NULL: one block scans all).

@@ -78,7 +78,7 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_selector_apply", "fss_ensemble_create", "fss_ensemble_destroy", "fss_ensemble_set_stream",
            "fss_ensemble_add", "fss_ensemble_build", "fss_ensemble_rk4_step", "fss_ensemble_get_state",
            "fss_ensemble_info", "fss_amr_create", "fss_amr_destroy", "fss_amr_counts", "fss_amr_refine",
-           "fss_amr_get_mesh", "fss_amr_remesh", "fss_remesh_lists", "fss_state_csv_append",
+           "fss_amr_get_mesh", "fss_amr_remesh", "fss_amr_refine_current", "fss_remesh_lists", "fss_state_csv_append",
            "fss_point_count_append", "fss_output_name", "fss_state_bin_append", "fss_state_bin_read",
            "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_version"]
 
@@ -143,6 +143,7 @@ def lib():
     L.fss_amr_refine.argtypes = [_vp, P(_i64), _D, _D, C.c_double, C.c_double]
     L.fss_amr_get_mesh.argtypes = [_vp, _vp, _vp, _vp]
     L.fss_amr_remesh.argtypes = [_vp, _D, _D, C.c_double, P(_i64), P(_i64)]
+    L.fss_amr_refine_current.argtypes = [_vp, _vp, C.c_double, C.c_double, C.c_double, P(_i64)]
     L.fss_remesh_lists.argtypes = [_i64, _D, _D, _i64, _I32, _I32, _I32, C.c_double, P(_i64), P(_i64)]
     L.fss_state_csv_append.argtypes = [C.c_char_p, _i64, _D, _D]
     L.fss_point_count_append.argtypes = [C.c_char_p, _i64]
@@ -338,6 +339,14 @@ class Context:
         self._c(lib().fss_remesh_current(self.h, t.size // 3, t.ctypes.data_as(_vp), omega, C.byref(fb),
                                          C.byref(bad)))
         return fb.value, bad.value
+
+    def amr_refine_current(self, amr, vorticity_tol=0.2, circulation_tol=0.0025, omega=OMEGA):
+        """amr() on the context's particles (they must be the mesh's points),
+        new midpoints projected, the new set taken; returns the new count."""
+        pc = _i64()
+        self._c(lib().fss_amr_refine_current(self.h, amr.h, vorticity_tol, circulation_tol, omega, C.byref(pc)))
+        self.n = pc.value
+        return pc.value
 
     def rhs_current(self, omega=OMEGA, psi=False):
         out = np.zeros((self.n, 5))

@@ -250,6 +250,14 @@ int fss_amr_counts(const fss_amr* a, int64_t* point_count, int64_t* tri_count);
  * unchanged and the handle unusable. */
 int fss_amr_refine(fss_amr* a, int64_t* point_count, double* state5, double* area, double vorticity_tol,
                    double circulation_tol);
+/* amr() on the context's current particles, device-resident
+ * (new_dynamics.cpp:219-228): the context's particles must be the mesh's
+ * points (same count, same order); the new midpoints are projected onto the
+ * sphere (zeta += -2 omega dz, as project_points) and the context takes the
+ * new particle set (tree and lists rebuilt; the remesh grid becomes the new
+ * positions).  *point_count receives the new count. */
+int fss_amr_refine_current(fss_ctx* ctx, fss_amr* a, double vorticity_tol, double circulation_tol, double omega,
+                           int64_t* point_count);
 /* The mesh: tris (3 per triangle), corner_keys (3 per triangle), parent
  * pairs (2 per point); any may be NULL. */
 int fss_amr_get_mesh(const fss_amr* a, int32_t* tris, uint64_t* corner_keys, int32_t* parent_verts);

@@ -89,3 +89,36 @@ def test_amr_limits(fss):
             amr.refine(s, a)
         with pytest.raises(fss.FssError):
             amr.refine(s, a)
+
+
+def test_amr_refine_current_matches_host_path(fss, oracle):
+    """The device-resident AMR step (new_dynamics.cpp:219-228: amr, then the
+    new points projected, then the new particle set) gives the context the
+    same state as the host path: refine on host arrays, project the new
+    points (oracle project_points), set_particles."""
+    s, a, tris = gauss_state(fss, 4)
+    mc = 10 * 4 ** 7 + 2
+    with fss.Amr(tris, s.shape[0], mc, 4 * mc) as amr:
+        st, ar = amr.refine(s, a)
+    proj = st.copy()
+    tail = np.ascontiguousarray(proj[s.shape[0]:])
+    oracle.lib().orc_project_points(tail.shape[0], tail.reshape(-1), oracle.OMEGA)
+    proj[s.shape[0]:] = tail
+    with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as ctx:
+        ctx.set_particles(proj, ar)
+        want = ctx.get_state()
+    with fss.Amr(tris, s.shape[0], mc, 4 * mc) as amr, \
+            fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as ctx:
+        ctx.set_particles(s, a)
+        n = ctx.amr_refine_current(amr)
+        assert n == st.shape[0] > s.shape[0]
+        got = ctx.get_state()
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+        ctx.rk4_step(0.01, nsteps=2)  # the context steps on with the new set
+        assert np.all(np.isfinite(ctx.get_state()))
+    # a context whose particles are not the mesh's points is refused
+    with fss.Amr(tris, s.shape[0], mc, 4 * mc) as amr, \
+            fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as ctx:
+        ctx.set_particles(proj, ar)
+        with pytest.raises(fss.FssError):
+            ctx.amr_refine_current(amr)
