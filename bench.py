@@ -337,7 +337,19 @@ def amr_measure(fss, level=5, reps=3):
                 t0 = time.perf_counter()
                 _, fb, nf = amr.remesh(moved, grid)
                 rm_ms = 1e3 * (time.perf_counter() - t0)
+    # the reference's -a loop on the device: RK4 step, then amr() on the
+    # context's particles (new points projected, tree and lists rebuilt)
+    loop_steps = 5
+    with fss.Amr(tris, n, mc, 4 * mc) as amr2, \
+            fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, autotune=0) as ctx2:
+        ctx2.set_particles(state, area)
+        t0 = time.perf_counter()
+        for _ in range(loop_steps):
+            ctx2.rk4_step(DT, nsteps=1)
+            n_loop = ctx2.amr_refine_current(amr2)
+        loop_s = time.perf_counter() - t0
     out = {"workload": f"amr() on the Gaussian vortex, level {level} grid, tolerances 0.2 / 0.0025",
+           "rk4_plus_amr_steps_per_s": loop_steps / loop_s, "rk4_plus_amr_points_after": int(n_loop),
            "points_in": int(n), "points_out": int(st.shape[0]), "triangles_out": int(t_new.shape[0]),
            "wall_ms_host_buffers": float(np.median(times)),
            "remesh_after_amr_ms_host_buffers": rm_ms, "remesh_fallback": fb, "remesh_not_found": nf}
