@@ -305,6 +305,31 @@ def remesh_measure(fss, ctx, state, area, level, stream, reps=5):
     return out
 
 
+def cpu_reference_fast(fss, level=6):
+    """The reference's own fast sum (rhs_eval.h:34 rhs_fast_sum, oracle/_ref,
+    one thread) at its only working setting (degree 2, theta 0.7,
+    many_count 10, 4 tree levels) on the level-`level` grid of the headline
+    field, timed per RHS, with its relative L2 velocity error against the
+    FP64 direct sum (the oracle, all host threads).  Level 8 is out of reach
+    on the host in minutes (its pair traversal is quadratic in the queue)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if O.ref() is None:
+        return None
+    s, a = fss.make_state(level, "rh_vortices", n_vortex=32, seed=2)
+    n = s.shape[0]
+    out = np.zeros(5 * n)
+    t0 = time.perf_counter()
+    rc = O.ref().ref_rhs_fast(n, s.reshape(-1), a, O.OMEGA, 4, 0.7, 10, 2, out)
+    dt = time.perf_counter() - t0
+    ref = O.rhs_direct(s, a)
+    u = out.reshape(n, 5)[:, :3]
+    return {"kind": "reference", "function": "rhs_fast_sum (oracle/_ref)", "level": level, "n": int(n),
+            "tree_levels": 4, "degree": 2, "theta": 0.7, "many_count": 10, "threads": 1, "rc": int(rc),
+            "ms_per_rhs": 1e3 * dt, "steps_per_s": 1.0 / (4 * dt),
+            "rel_l2": float(np.linalg.norm(u - ref[:, :3]) / np.linalg.norm(ref[:, :3]))}
+
+
 def amr_measure(fss, level=5, reps=3):
     """amr.h amr as the reference's -a loop calls it, on the reference's
     Gaussian vortex (level-`level` grid, the reference's tolerances 0.2 and
@@ -549,6 +574,10 @@ def main():
         except fss.FssError as e:  # too many points left their triangles in one step
             remesh = {"error": str(e)}
 
+    cpu_fast = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu_fast = cpu_reference_fast(fss)
+
     amr = None
     if rank == 0 and ws == 1 and not args.no_amr:
         amr = amr_measure(fss)
@@ -580,7 +609,8 @@ def main():
                 "fp64_same_algorithm": fp64c,
                 "ratio_vs_fp64_same_algorithm": (value / fp64c["value"]) if fp64c else None,
                 "interactions_per_rhs": inter, "tree": info,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "remesh": remesh, "amr": amr,
+                "roofline": roofline, "cpu_baseline": cpu, "cpu_reference_fast": cpu_fast, "e2e": e2e,
+                "remesh": remesh, "amr": amr, "interactions_per_s": inter * 4 * value,
                 "gpu_launches": int(round(launches_per_step * args.steps)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
