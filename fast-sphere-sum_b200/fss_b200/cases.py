@@ -4,6 +4,11 @@
     python -m fss_b200.cases rk4  --level 8 --precision mixed --steps 2 [--learned]
     python -m fss_b200.cases direct --level 6 --precision mixed
     python -m fss_b200.cases ensemble --members 64 --steps 20
+    python -m fss_b200.cases mlp --samples 2097152 --epochs 2
+
+The mlp case: the selector network (16 -> 64 -> 64 -> 12) trained by the
+library's own kernels on seeded synthetic rows (about the size of the
+per-leaf error label set, 2M rows), then run forward on all rows.
 
 The ensemble case: members on icosahedral levels drawn uniformly from 5-8,
 each an RH R=4 wave with a seeded +-5% amplitude perturbation and 4-16
@@ -27,7 +32,9 @@ from . import (METHOD_DIRECT, METHOD_TREECODE, PREC_FP64, PREC_MIXED, RH_AMP, Co
 
 def main(argv=None):
     p = argparse.ArgumentParser()
-    p.add_argument("case", choices=["rhs", "rk4", "direct", "ensemble"])
+    p.add_argument("case", choices=["rhs", "rk4", "direct", "ensemble", "mlp"])
+    p.add_argument("--samples", type=int, default=2097152)
+    p.add_argument("--epochs", type=int, default=2)
     p.add_argument("--members", type=int, default=64)
     p.add_argument("--seed", type=int, default=100)
     p.add_argument("--level", type=int, default=8)
@@ -45,6 +52,8 @@ def main(argv=None):
     prec = PREC_MIXED if a.precision == "mixed" else PREC_FP64
     if a.case == "ensemble":
         return ensemble_case(a)
+    if a.case == "mlp":
+        return mlp_case(a)
     s, area = make_state(a.level, "rh_vortices", n_vortex=a.vortices, seed=2)
     method = METHOD_DIRECT if a.case == "direct" else METHOD_TREECODE
     t0 = time.perf_counter()
@@ -97,6 +106,24 @@ def ensemble_case(a):
                           interactions_per_rhs=info["interactions_per_rhs"], steps=a.steps,
                           wall_s=dt, steps_per_s=a.steps / dt,
                           pairs_per_s=4 * a.steps * info["interactions_per_rhs"] / dt, build_s=t_build)))
+
+
+def mlp_case(a):
+    from . import selector
+    rng = np.random.default_rng(a.seed)
+    x = rng.standard_normal((a.samples, 16)).astype(np.float32)
+    t = np.tanh(x[:, :12] * x[:, 4:]).astype(np.float32)
+    net = selector.MLP(params=None, seed=a.seed)
+    try:
+        t0 = time.perf_counter()
+        net.set_data(x, t)
+        losses = net.train(a.epochs, batch=4096, lr=1e-3, seed=a.seed)
+        y = net.predict(x)
+        dt = time.perf_counter() - t0
+    finally:
+        net.close()
+    assert np.all(np.isfinite(losses)) and np.all(np.isfinite(y))
+    print(f"case=mlp samples={a.samples} epochs={a.epochs} loss={losses[-1]:.4e} wall={dt:.3f}s")
 
 
 if __name__ == "__main__":
