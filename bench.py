@@ -55,6 +55,9 @@ def parse():
     p.add_argument("--fixed", action="store_true", help="headline arm without the learned selector")
     p.add_argument("--no-clusters", action="store_true",
                    help="headline arm without target clusters (far sources summed at the target particles)")
+    p.add_argument("--sweep", action="store_true",
+                   help="instead of the headline line: mixed-precision BLTC at fixed n in {6,8,10} x theta in "
+                        "{0.5,0.7}, one JSON line each (errors vs the FP64 direct sum, steps/s)")
     return p.parse_args()
 
 
@@ -219,6 +222,45 @@ def make_learned_arm(fss, state, area, stream, args, dev, clusters=True):
     ctx.set_particles(state, area)
     choice = selector.apply(ctx, tol=args.tol, safety=args.safety, device=dev)
     return ctx, np.bincount(choice, minlength=selector.NCLS).tolist()
+
+
+def run_sweep(fss, state, area, stream, flush, dev, args, u_ref):
+    """Mixed-precision BLTC (FP32 interactions, Kahan sums, FP64 RK4 and
+    renormalisation; far sources summed at the target particles) at each
+    fixed (degree, theta): relative L2 and max velocity error against the
+    FP64 direct sum over all targets and over 4,096 seeded sample targets
+    (seed 7), and RK4 steps/s timed like the headline arm.  One JSON line
+    per setting."""
+    import copy
+    n = state.shape[0]
+    rows = np.sort(np.random.default_rng(7).choice(n, min(4096, n), replace=False))
+
+    def errs(u, v):
+        return (float(np.linalg.norm(u - v) / np.linalg.norm(v)),
+                float(np.max(np.linalg.norm(u - v, axis=1)) / np.max(np.linalg.norm(v, axis=1))))
+
+    for degree in (6, 8, 10):
+        for theta in (0.5, 0.7):
+            a = copy.copy(args)
+            a.degree, a.theta = degree, theta
+            ctx = make_arm(fss, state, area, stream, fss.PREC_MIXED, a, dev)
+            try:
+                u = ctx.rhs(state, area)[:, :3]
+                l2, mx = errs(u, u_ref)
+                l2s, mxs = errs(u[rows], u_ref[rows])
+                warm(ctx, stream, args.warmup)
+                t = time_steps(ctx, stream, args.steps, flush)
+                inter, _ = ctx.work_per_rhs()
+                info = ctx.tree_info()
+            finally:
+                ctx.close()
+            print(json.dumps({"sweep": "mixed-precision BLTC, fixed degree/theta", "level": args.level,
+                              "n_particles": n, "degree": degree, "theta": theta,
+                              "tree_levels": info["tree_levels"], "rel_l2": l2, "rel_max": mx,
+                              "rel_l2_sample4096": l2s, "rel_max_sample4096": mxs,
+                              "steps_per_s": args.steps / t, "ms_per_step": 1e3 * t / args.steps,
+                              "interactions_per_rhs": inter, "interactions_per_s": 4 * inter * args.steps / t,
+                              "reference": "FP64 direct sum on the GPU, all targets"}), flush=True)
 
 
 def warm(ctx, stream, w):
@@ -471,6 +513,14 @@ def main():
         dctx.set_stream(stream.cuda_stream)
         dctx.set_particles(state, area)
         u_ref = dctx.rhs(state, area)[:, :3]
+
+    if args.sweep:
+        if rank == 0:
+            run_sweep(fss, state, area, stream, flush, dev, args, u_ref)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
 
     def rel_err(ctx):
         u = ctx.rhs(state, area)[:, :3]

@@ -25,10 +25,16 @@ __device__ __forceinline__ bool cone_coords_exact(const double* v1, const double
         for (int i = k + 1; i < 3; i++)
             if (fabs(a[i + 3 * k]) > mx) { mx = fabs(a[i + 3 * k]); pr = i; }
         ipiv[k] = pr;
-        if (a[pr + 3 * k] == 0.0) { singular = true; continue; }
-        if (pr != k) {
+        // mx is |a[pr + 3k]|, so this is the test a[pr + 3k] == 0 (NaN fails both)
+        if (mx == 0.0) { singular = true; continue; }
+        // row swap written with compile-time indices only, so a[] stays in
+        // registers (a run-time row index would put the matrix in local memory)
 #pragma unroll
-            for (int j = 0; j < 3; j++) { double t = a[k + 3 * j]; a[k + 3 * j] = a[pr + 3 * j]; a[pr + 3 * j] = t; }
+        for (int i = k + 1; i < 3; i++) {
+            if (pr == i) {
+#pragma unroll
+                for (int j = 0; j < 3; j++) { double t = a[k + 3 * j]; a[k + 3 * j] = a[i + 3 * j]; a[i + 3 * j] = t; }
+            }
         }
         const double r = __drcp_rn(a[k + 3 * k]);
 #pragma unroll
@@ -42,7 +48,9 @@ __device__ __forceinline__ bool cone_coords_exact(const double* v1, const double
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const int pr = ipiv[k];
-        if (pr != k) { double t = b[k]; b[k] = b[pr]; b[pr] = t; }
+#pragma unroll
+        for (int i = k + 1; i < 3; i++)
+            if (pr == i) { double t = b[k]; b[k] = b[i]; b[i] = t; }
     }
 #pragma unroll
     for (int k = 0; k < 3; k++)

@@ -41,7 +41,8 @@ __global__ void __launch_bounds__(128) k_up_combine_batch(const ProxyJob* __rest
                                                           const double4* __restrict__ proxy_pos, int64_t n,
                                                           float4* __restrict__ src) {
     __shared__ double M[kMaxK];
-    const ProxyJob job = jobs[blockIdx.x];
+    // read in place: a copy indexed by a run-time degree (job.off[d]) would sit in local memory
+    const ProxyJob& job = jobs[blockIdx.x];
     const int tid = threadIdx.x;
     const int KM = nproxy(nmax);
     if (tid < KM) {

@@ -51,7 +51,8 @@ __global__ void __launch_bounds__(kUpThreads) k_up_combine(const ProxyJob* __res
                                                            const NodeGeom* __restrict__ node, int local_frames,
                                                            int64_t n, typename Vec4<T>::type* __restrict__ src) {
     __shared__ double M[kMaxK];
-    const ProxyJob job = jobs[blockIdx.x];
+    // read in place: a copy indexed by a run-time degree (job.off[d]) would sit in local memory
+    const ProxyJob& job = jobs[blockIdx.x];
     const int tid = threadIdx.x;
     const int KM = nproxy(nmax);
     if (tid < KM) {
