@@ -123,6 +123,25 @@ def test_tree_moved_particles_vs_reference(oracle):
 
 
 @need_ref
+@pytest.mark.parametrize("threads", [3, 8])
+def test_reference_fast_sum_split_over_threads(oracle, threads):
+    """The CPU baseline's split of the reference's fast sum (top-level target
+    faces per thread, as fast_sum_mpi.cpp splits them per rank) gives the
+    single-thread rhs_func result bit for bit."""
+    s, a, _ = oracle.icos_state(3)
+    n = s.shape[0]
+    one, split, whole = np.zeros(5 * n), np.zeros(5 * n), np.zeros(5 * n)
+    t1, t2 = np.zeros(2), np.zeros(2)
+    R = oracle.ref()
+    assert R.ref_rhs_fast(n, s.reshape(-1), a, oracle.OMEGA, 3, 0.7, 10, 2, whole) == 0
+    assert R.ref_rhs_fast_timed(n, s.reshape(-1), a, oracle.OMEGA, 3, 0.7, 10, 2, 1, one, t1) == 0
+    assert R.ref_rhs_fast_timed(n, s.reshape(-1), a, oracle.OMEGA, 3, 0.7, 10, 2, threads, split, t2) == 0
+    assert np.array_equal(bits(one), bits(whole))
+    assert np.array_equal(bits(split), bits(whole))
+    assert np.all(t1 >= 0) and np.all(t2 >= 0)
+
+
+@need_ref
 def test_rk4_bit_exact_vs_reference(oracle):
     s, a, _ = oracle.icos_state(3)
     assert np.array_equal(bits(oracle.rk4_step(s, a, 0.01)), bits(oracle.rk4_step(s, a, 0.01, use_ref=True)))
