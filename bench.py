@@ -365,17 +365,15 @@ def cpu_reference_fast(fss, level=6):
     s, a = fss.make_state(level, "rh_vortices", n_vortex=32, seed=2)
     n = s.shape[0]
     threads = max(1, min(20, os.cpu_count() or 1))
-    out1, outp = np.zeros(5 * n), np.zeros(5 * n)
-    t1, tp = np.zeros(2), np.zeros(2)
-    rc = O.ref().ref_rhs_fast_timed(n, s.reshape(-1), a, O.OMEGA, 4, 0.7, 10, 2, 1, out1, t1)
-    O.ref().ref_rhs_fast_timed(n, s.reshape(-1), a, O.OMEGA, 4, 0.7, 10, 2, threads, outp, tp)
+    out1, outp, t = np.zeros(5 * n), np.zeros(5 * n), np.zeros(3)
+    rc = O.ref().ref_rhs_fast_timed(n, s.reshape(-1), a, O.OMEGA, 4, 0.7, 10, 2, threads, out1, outp.ctypes.data, t)
     ref = O.rhs_direct(s, a)
     u = out1.reshape(n, 5)[:, :3]
     return {"kind": "reference", "function": "rhs_fast_sum (oracle/_ref)", "level": level, "n": int(n),
             "tree_levels": 4, "degree": 2, "theta": 0.7, "many_count": 10, "rc": int(rc),
-            "setup_ms": 1e3 * t1[0], "ms_per_rhs_1_thread": 1e3 * t1[1],
+            "setup_ms": 1e3 * float(t[0]), "ms_per_rhs_1_thread": 1e3 * float(t[1]),
             "threads": threads, "partition": "fast_sum_mpi.cpp top-level target faces per rank, ranks as threads",
-            "ms_per_rhs": 1e3 * tp[1], "steps_per_s": 1.0 / (4 * tp[1]),
+            "ms_per_rhs": 1e3 * float(t[2]), "steps_per_s": 1.0 / (4 * float(t[2])),
             "threads_equal_1_thread": bool(np.array_equal(out1, outp)),
             "rel_l2": float(np.linalg.norm(u - ref[:, :3]) / np.linalg.norm(ref[:, :3]))}
 

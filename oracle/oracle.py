@@ -91,7 +91,8 @@ def _setup_ref(R):
     R.ref_tree_members.restype = i64
     R.ref_rhs_fast.argtypes = [i64, _D, _D, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, _D]
     R.ref_rhs_fast.restype = C.c_int
-    R.ref_rhs_fast_timed.argtypes = [i64, _D, _D, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _D, _D]
+    R.ref_rhs_fast_timed.argtypes = [i64, _D, _D, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _D,
+                                     C.c_void_p, _D]
     R.ref_rhs_fast_timed.restype = C.c_int
     R.ref_regrid.argtypes = [i64, _D, _D, i64, _I, C.c_double]
     R.ref_regrid.restype = C.c_int

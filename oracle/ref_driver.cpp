@@ -242,17 +242,21 @@ int ref_rhs_fast(int64_t n, const double* state5, const double* area, double ome
 // The reference's fast sum with its set-up and its evaluation timed apart
 // (set-up: icosahedron_init, interp_init, points_assign, tree_traverse, as
 // new_dynamics.cpp:87-88 runs once before the time loop; evaluation: what
-// rhs_func does per call).  With threads > 1 the evaluation is split the way
-// fast_sum_mpi.cpp:324-338 splits it over MPI ranks: rank r owns the top-level
-// target faces [r * (20 / P), (r + 1) * (20 / P)), the last rank the rest, and
-// evaluates the interactions whose target face descends from its own; here
-// the ranks are threads with private modify buffers, summed afterwards (every
-// target gets its contributions from one thread only, in the single-thread
-// order), then scaled as rhs_func scales.  times[0] = set-up s, times[1] =
-// evaluation s.  Returns dgetrf's info.
+// rhs_func does per call), after one set-up: the evaluation on one thread
+// (rhs_func itself, into modify1), and, when modifyp is given, split over
+// `threads` threads the way fast_sum_mpi.cpp:324-338 splits it over MPI
+// ranks: rank r owns the top-level target faces [r * (20 / P), (r + 1) *
+// (20 / P)), the last rank the rest, and evaluates the interactions whose
+// target face descends from its own.  Here the ranks are threads with
+// private modify buffers, summed afterwards (every target gets its
+// contributions from one thread only, in the single-thread order), then
+// scaled as rhs_func scales.  times[0] = set-up s, times[1] = one-thread
+// evaluation s, times[2] = split evaluation s.  Returns dgetrf's info.
 int ref_rhs_fast_timed(int64_t n, const double* state5, const double* area, double omega, int tree_levels,
-                       double theta, int many_count, int degree, int threads, double* modify5, double* times) {
+                       double theta, int many_count, int degree, int threads, double* modify1, double* modifyp,
+                       double* times) {
     using clk = std::chrono::steady_clock;
+    auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
     if (threads < 1) threads = 1;
     if (threads > 20) threads = 20;
     vector<double> s = to_state(n, state5), a(area, area + n), m(5 * n, 0.0);
@@ -269,38 +273,38 @@ int ref_rhs_fast_timed(int64_t n, const double* state5, const double* area, doub
     points_assign(c, s);
     tree_traverse(c);
     const auto t1 = clk::now();
-    // per-thread copies of the configuration, each with its share of the
-    // interactions (made before the timed evaluation)
-    vector<run_information> part;
-    if (threads > 1) {
+    rhs_func(m, s, a, omega, c);
+    const auto t2 = clk::now();
+    std::memcpy(modify1, m.data(), sizeof(double) * 5 * n);
+    double t_split = 0.0;
+    if (modifyp) {
+        // per-thread copies of the configuration, each with its share of the
+        // interactions (made before the timed evaluation)
         const int per = 20 / threads;
-        part.assign(threads, c);
+        vector<run_information> part(threads, c);
         for (auto& p : part) p.tree_interactions.clear();
         for (const interaction_pair& ip : c.tree_interactions) {
             const int top = ip.curr_target >> (2 * ip.lev_target);
-            const int r = std::min(top / per, threads - 1);
-            part[r].tree_interactions.push_back(ip);
+            part[std::min(top / per, threads - 1)].tree_interactions.push_back(ip);
         }
-    }
-    const auto t2 = clk::now();
-    if (threads == 1) {
-        rhs_func(m, s, a, omega, c);
-    } else {
         vector<vector<double>> mt(threads, vector<double>(5 * n, 0.0));
+        const auto t3 = clk::now();
         vector<std::thread> th;
         for (int r = 0; r < threads; r++)
             th.emplace_back([&, r] { rhs_fast_sum(mt[r], s, a, part[r], omega); });
         for (auto& x : th) x.join();
+        std::fill(m.begin(), m.end(), 0.0);
         for (int r = 0; r < threads; r++)
             for (int64_t k = 0; k < 5 * n; k++) m[k] += mt[r][k];
         scalar_mult(m, -1.0 / (4.0 * M_PI));
         for (int64_t i = 0; i < n; i++) m[5 * i + 3] = -2 * omega * m[5 * i + 2];
+        t_split = secs(t3, clk::now());
+        std::memcpy(modifyp, m.data(), sizeof(double) * 5 * n);
     }
-    const auto t3 = clk::now();
-    std::memcpy(modify5, m.data(), sizeof(double) * 5 * n);
     if (times) {
-        times[0] = std::chrono::duration<double>(t1 - t0).count();
-        times[1] = std::chrono::duration<double>(t3 - t2).count();
+        times[0] = secs(t0, t1);
+        times[1] = secs(t1, t2);
+        times[2] = t_split;
     }
     return c.info;
 }
