@@ -79,6 +79,32 @@ def test_solid_body_known_answer(oracle):
     assert errs[1] < errs[0] < 5e-2, errs
 
 
+def test_harmonic_fields_known_answers(oracle):
+    """For a spherical harmonic field zeta of degree l (zero mean), the
+    stream function -(1/4pi) sum zeta_j A_j log(1 - x.x_j) tends to
+    zeta / (l (l + 1)) and the velocity to grad(psi) x x.  Degree 1: zeta =
+    2z, psi = z.  Degree 4: zeta = P = Re((x + iy)^4) (harmonic in R^3, so its
+    surface gradient is grad P - 4 P x), psi = P / 20, u = (grad P x x) / 20.
+    The stream function has no counterpart in the reference, so this is its
+    analytic pin; both converge at about second order as the grid refines."""
+    e1, e4, eu = [], [], []
+    for L in (2, 3, 4):
+        s, a, _ = oracle.icos_state(L)
+        x, y, z = s[:, 0], s[:, 1], s[:, 2]
+        rows = np.arange(s.shape[0])
+        s[:, 3] = 2 * z
+        e1.append(np.linalg.norm(oracle.stream_rows(s, a, rows) - z) / np.linalg.norm(z))
+        P = x ** 4 - 6 * x ** 2 * y ** 2 + y ** 4
+        s[:, 3] = P
+        e4.append(np.linalg.norm(oracle.stream_rows(s, a, rows) - P / 20) / np.linalg.norm(P / 20))
+        grad = np.stack([4 * x ** 3 - 12 * x * y ** 2, 4 * y ** 3 - 12 * x ** 2 * y, np.zeros_like(z)], 1)
+        u = np.cross(grad, s[:, :3]) / 20
+        eu.append(np.linalg.norm(oracle.rhs_direct(s, a)[:, :3] - u) / np.linalg.norm(u))
+    for e in (e1, e4, eu):
+        assert e[1] < e[0] / 3 and e[2] < e[1] / 3, e
+    assert e1[-1] < 1e-2 and e4[-1] < 0.1 and eu[-1] < 2e-2, (e1, e4, eu)
+
+
 need_ref = pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLD), "..", "oracle", "_ref",
                                                               "libref.so")), reason="reference not built here")
 
