@@ -337,6 +337,99 @@ void orc_rossby_haurwitz_4(int64_t n, double *state5) {
     }
 }
 
+/* ------------------------------------------- seeded RH wave + Gaussian vortices
+ *
+ * The benchmark's input field, restated from its definition (no reference
+ * counterpart: the reference hard-codes the RH constants and has one vortex):
+ *
+ *   zeta(x) = 2 w sin(lat) - K (R + 1)(R + 2) cos^R(lat) sin(lat) cos(R lon)
+ *             + sum_v a_v exp(-(d(x, c_v) / width)^2),   R = 4, w = K = amp,
+ *
+ * d the great-circle distance; vortex centres uniform on the sphere (z and
+ * longitude uniform), amplitudes normal with variance 2 pi^2; the
+ * area-weighted mean is removed; tracer = 2 + lat.  Random numbers: the
+ * 64-bit Mersenne twister MT19937-64 (Matsumoto and Nishimura, 2000; the
+ * generator C++ names std::mt19937_64), uniform doubles from its top 53
+ * bits, normals by the Box-Muller transform.  Per vortex the draws are
+ * z, lon, u1, u2 in that order. */
+
+typedef struct {
+    uint64_t mt[312];
+    int i;
+} mt64;
+
+static void mt64_seed(mt64 *g, uint64_t seed) {
+    g->mt[0] = seed;
+    for (int i = 1; i < 312; i++) g->mt[i] = 6364136223846793005ULL * (g->mt[i - 1] ^ (g->mt[i - 1] >> 62)) + (uint64_t)i;
+    g->i = 312;
+}
+
+static uint64_t mt64_next(mt64 *g) {
+    const uint64_t upper = 0xFFFFFFFF80000000ULL, lower = 0x7FFFFFFFULL, a = 0xB5026F5AA96619E9ULL;
+    if (g->i >= 312) {
+        for (int k = 0; k < 312; k++) {
+            const uint64_t x = (g->mt[k] & upper) | (g->mt[(k + 1) % 312] & lower);
+            g->mt[k] = g->mt[(k + 156) % 312] ^ (x >> 1) ^ ((x & 1ULL) ? a : 0ULL);
+        }
+        g->i = 0;
+    }
+    uint64_t x = g->mt[g->i++];
+    x ^= (x >> 29) & 0x5555555555555555ULL;
+    x ^= (x << 17) & 0x71D67FFFEDA60000ULL;
+    x ^= (x << 37) & 0xFFF7EEE000000000ULL;
+    x ^= x >> 43;
+    return x;
+}
+
+static double mt64_uniform(mt64 *g) { return (double)(mt64_next(g) >> 11) * (1.0 / 9007199254740992.0); }
+
+/* Raw generator output, for pinning the generator itself. */
+void orc_mt64_draws(uint64_t seed, int64_t count, uint64_t *out) {
+    mt64 g;
+    mt64_seed(&g, seed);
+    for (int64_t k = 0; k < count; k++) out[k] = mt64_next(&g);
+}
+
+void orc_rh_vortices(int64_t n, double *state5, const double *area, double amp, int nvort, double width,
+                     uint64_t seed) {
+    mt64 g;
+    mt64_seed(&g, seed);
+    double *cen = (double *)malloc(sizeof(double) * 4 * (size_t)(nvort > 0 ? nvort : 1));
+    for (int v = 0; v < nvort; v++) {
+        const double z = 2 * mt64_uniform(&g) - 1;
+        const double lon = 2 * M_PI * mt64_uniform(&g);
+        const double rho = sqrt(fmax(0.0, 1 - z * z));
+        const double u1 = 1.0 - mt64_uniform(&g), u2 = mt64_uniform(&g);
+        cen[4 * v + 0] = rho * cos(lon);
+        cen[4 * v + 1] = rho * sin(lon);
+        cen[4 * v + 2] = z;
+        cen[4 * v + 3] = sqrt(2 * M_PI * M_PI) * sqrt(-2 * log(u1)) * cos(2 * M_PI * u2);
+    }
+    const double w = amp, K = amp;
+    double num = 0, den = 0;
+    for (int64_t i = 0; i < n; i++) {
+        double *p = state5 + 5 * i;
+        double lat, lon;
+        lat_lon(p, &lat, &lon);
+        double zeta = 2 * w * sin(lat) - K * (4 + 1) * (4 + 2) * pow(cos(lat), 4) * sin(lat) * cos(4 * lon);
+        for (int v = 0; v < nvort; v++) {
+            const double *c = cen + 4 * v;
+            const double cosd = fmin(1.0, fmax(-1.0, p[0] * c[0] + p[1] * c[1] + p[2] * c[2]));
+            const double d = acos(cosd) / width;
+            zeta += c[3] * exp(-(d * d));
+        }
+        p[3] = zeta;
+        p[4] = 2 + lat;
+        if (area) {
+            num += zeta * area[i];
+            den += area[i];
+        }
+    }
+    if (area && den > 0)
+        for (int64_t i = 0; i < n; i++) state5[5 * i + 3] -= num / den;
+    free(cen);
+}
+
 /* ------------------------------------------------------------ direct sum */
 
 /* rhs_eval.h:15-32 rhs_direct_sum, one target row (sequential j order). */

@@ -54,6 +54,8 @@ def _setup(L):
     L.orc_icos_init.restype = i64
     L.orc_area_init.argtypes = [i64, _D, i64, _I, _D]
     L.orc_rossby_haurwitz_4.argtypes = [i64, _D]
+    L.orc_rh_vortices.argtypes = [i64, _D, C.c_void_p, C.c_double, C.c_int, C.c_double, C.c_uint64]
+    L.orc_mt64_draws.argtypes = [C.c_uint64, i64, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")]
     L.orc_rhs_direct.argtypes = [i64, _D, _D, C.c_double, _D, C.c_int]
     L.orc_rhs_direct_rows.argtypes = [i64, _D, _D, i64, C.c_void_p, _D, C.c_int]
     L.orc_stream_rows.argtypes = [i64, _D, _D, i64, C.c_void_p, _D]
@@ -156,6 +158,33 @@ def icos_state(level, use_ref=False):
     (L.ref_area_init if use_ref else L.orc_area_init)(n, s.reshape(-1), tris.shape[0], tris.reshape(-1), area)
     (L.ref_rossby_haurwitz_4 if use_ref else L.orc_rossby_haurwitz_4)(n, s.reshape(-1))
     return s, area, tris
+
+
+RH_AMP = 7.848e-6 * 86400.0  # w = K of the benchmark's Rossby-Haurwitz wave, per day
+
+
+def mt64_draws(seed, count):
+    """First `count` outputs of MT19937-64 seeded with `seed`."""
+    out = np.zeros(count, dtype=np.uint64)
+    lib().orc_mt64_draws(seed, count, out)
+    return out
+
+
+def rh_vortices(state5, area, n_vortex, seed, amp=RH_AMP, width=0.1):
+    """The benchmark's seeded RH R=4 wave + Gaussian vortices on the
+    positions of state5 (zeta and tracer overwritten; returns a copy)."""
+    s = np.array(state5, dtype=np.float64)
+    a = np.ascontiguousarray(area, dtype=np.float64)
+    lib().orc_rh_vortices(s.shape[0], s.reshape(-1), a.ctypes.data_as(C.c_void_p), amp, n_vortex, width, seed)
+    return s
+
+
+def rh_vortices_state(level, n_vortex, seed, amp=RH_AMP, width=0.1):
+    """(state5, area) of the benchmark field on the level-`level`
+    icosahedral grid, built by the oracle alone (icos_init, area_init and the
+    field restated above), without the product library."""
+    s, area, _ = icos_state(level)
+    return rh_vortices(s, area, n_vortex, seed, amp, width), area
 
 
 def rhs_direct(state5, area, omega=OMEGA, threads=None, use_ref=False):
