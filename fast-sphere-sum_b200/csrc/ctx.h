@@ -50,6 +50,8 @@ struct fss_ctx {
     bool fp64 = false;
     bool tree = true;
     bool resort = false;  // re-sort particles into their current leaves every RK4 step
+    uint64_t wait_ns = 0;  // limit of the pair kernel's bounded waits
+    int hold_block = -1;   // test hook: block of the next target-leaf launch that withholds a tile
 
     int64_t n = 0;
     bool have = false;

@@ -46,6 +46,9 @@ struct fss_ensemble {
     int64_t nitems = 0, njobs = 0;
     cudaGraphExec_t graph = nullptr;
     double gdt = 0, gomega = 0;
+    fss::PairCtl ctl() const {
+        return fss::PairCtl{cfg.wait_limit_us > 0 ? uint64_t(cfg.wait_limit_us) * 1000ull : fss::kWaitLimitNs, -1, 0};
+    }
     ~fss_ensemble() {
         if (graph) cudaGraphExecDestroy(graph);
         for (fss_ctx* m : members) fss_destroy(m);
@@ -104,7 +107,7 @@ int stage(fss_ensemble* e, int st, double dt, double omega) {
     ECU(cudaMemsetAsync(e->queue.p, 0, sizeof(int), e->stream));
     ECU(launch_pairs_persistent(e->stream, int(e->nitems), e->src.p, e->segs.as<Segment>(),
                                 e->leaf_start.as<int32_t>(), e->items.as<WorkItem>(), e->queue.as<int>(),
-                                e->partials.as<double4>(), e->ntot, e->err.as<int>(), e->blocks));
+                                e->partials.as<double4>(), e->ntot, e->err.as<int>(), e->blocks, e->ctl()));
     EpiArgs a;
     a.n = e->ntot;
     a.parts = 1;
@@ -368,6 +371,37 @@ int fss_ensemble_rk4_step(fss_ensemble* e, double dt, double omega, int32_t nste
         e->gomega = omega;
     }
     for (int s = 0; s < nsteps; s++) ECU(cudaGraphLaunch(e->graph, e->stream));
+    return FSS_OK;
+}
+
+int fss_ensemble_time_pairs(fss_ensemble* e, int32_t reps, double* ms) {
+    if (!e || !e->built || !ms) return efail(FSS_ERR_STATE, "ensemble not built");
+    if (reps < 1) return efail(FSS_ERR_INVALID, "reps < 1");
+    ECU(cudaSetDevice(e->dev));
+    cudaEvent_t a, b;
+    ECU(cudaEventCreate(&a));
+    ECU(cudaEventCreate(&b));
+    struct Ev {
+        cudaEvent_t a, b;
+        ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } guard{a, b};
+    float total = 0;
+    for (int r = 0; r <= reps; r++) {  // launch 0 untimed
+        ECU(cudaMemsetAsync(e->queue.p, 0, sizeof(int), e->stream));
+        ECU(cudaEventRecord(a, e->stream));
+        ECU(launch_pairs_persistent(e->stream, int(e->nitems), e->src.p, e->segs.as<Segment>(),
+                                    e->leaf_start.as<int32_t>(), e->items.as<WorkItem>(), e->queue.as<int>(),
+                                    e->partials.as<double4>(), e->ntot, e->err.as<int>(), e->blocks, e->ctl()));
+        ECU(cudaEventRecord(b, e->stream));
+        ECU(cudaEventSynchronize(b));
+        float t = 0;
+        ECU(cudaEventElapsedTime(&t, a, b));
+        if (r) total += t;
+    }
+    int err = 0;
+    ECU(cudaMemcpy(&err, e->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return efail(FSS_ERR_TIMEOUT, "a kernel's bounded wait timed out");
+    *ms = double(total) / reps;
     return FSS_OK;
 }
 

@@ -450,9 +450,11 @@ int materialize(fss_ctx* c, PairShape shape) {
 // of the context, target clusters with a block fitted to their
 // interpolation point count.
 int launch_leaf_pairs(fss_ctx* c, cudaStream_t st, bool want_psi) {
+    const PairCtl ctl{c->wait_ns, c->hold_block, 0};
+    c->hold_block = -1;  // the test hook holds one launch only
     CU(launch_pairs(st, c->fp64, want_psi, c->shape, int(c->lists.n_leaf_items), c->src.p, c->segs.as<Segment>(),
                     c->leaf_start.as<int32_t>(), c->items.as<WorkItem>(), c->partials.as<double4>(), c->pstride,
-                    c->err_flag.as<int>()));
+                    c->err_flag.as<int>(), ctl));
     return FSS_OK;
 }
 
@@ -462,7 +464,7 @@ int launch_cluster_pairs(fss_ctx* c, cudaStream_t st, bool want_psi) {
     if (nall > nl)
         CU(launch_pairs(st, c->fp64, want_psi, cluster_shape(c->fp64, L.max_cluster_k), nall - nl, c->src.p,
                         c->segs.as<Segment>(), c->leaf_start.as<int32_t>(), c->items.as<WorkItem>() + nl,
-                        c->partials.as<double4>(), c->pstride, c->err_flag.as<int>()));
+                        c->partials.as<double4>(), c->pstride, c->err_flag.as<int>(), PairCtl{c->wait_ns, -1, 0}));
     return FSS_OK;
 }
 
@@ -652,7 +654,8 @@ int rk4_steps(fss_ctx* c, double dt, double omega, int nsteps) {
     if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
     if (nsteps < 0) return fail(c, FSS_ERR_INVALID, "nsteps < 0");
     TRY(refresh_stage(c));
-    const bool use_graph = c->cfg.use_graph && !c->prof;
+    // a held tile (test hook) is taken by one eager step, never baked into a graph
+    const bool use_graph = c->cfg.use_graph && !c->prof && c->hold_block < 0;
     if (!use_graph) {
         for (int s = 0; s < nsteps; s++) TRY(rk4_once(c, dt, omega));
         return FSS_OK;
@@ -770,6 +773,7 @@ int fss_create(const fss_config* cfg, fss_ctx** out) {
     if (cfg->degree < 0 || cfg->degree > kMaxDegree) return fail(c, FSS_ERR_INVALID, "degree must be in 0..12");
     if (!(cfg->theta > 0)) return fail(c, FSS_ERR_INVALID, "theta must be positive");
     if (cfg->tree_levels < 0 || cfg->tree_levels > kMaxLevels) return fail(c, FSS_ERR_INVALID, "tree_levels out of range");
+    if (cfg->wait_limit_us < 0) return fail(c, FSS_ERR_INVALID, "wait_limit_us < 0");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -782,6 +786,7 @@ int fss_create(const fss_config* cfg, fss_ctx** out) {
     c->dev = cfg->device;
     c->fp64 = cfg->precision == FSS_PREC_FP64;
     c->tree = cfg->method == FSS_METHOD_TREECODE;
+    c->wait_ns = cfg->wait_limit_us > 0 ? uint64_t(cfg->wait_limit_us) * 1000ull : kWaitLimitNs;
     CU(cudaSetDevice(c->dev));
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, c->dev));
@@ -1114,6 +1119,13 @@ int fss_tree_geometry(int32_t tree_levels, double* tri_info) {
         return fail(nullptr, FSS_ERR_INVALID, "bad tree_levels");
     TreeGeometry g = build_tree_geometry(tree_levels);
     std::memcpy(tri_info, g.tri_info.data(), sizeof(double) * 4 * g.lev_off[tree_levels]);
+    return FSS_OK;
+}
+
+int fss_test_hold_tile(fss_ctx* c, int32_t block) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    invalidate_graph(c);
+    c->hold_block = block < 0 ? -1 : block;
     return FSS_OK;
 }
 

@@ -41,6 +41,20 @@ struct WorkItem {
     int32_t leaf;
 };
 
+// Default limit of a bounded wait, in nanoseconds of %globaltimer (a context
+// can set its own).
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+
+// Run-time controls of a pair launch: the limit of every bounded wait
+// (nanoseconds of %globaltimer) and a test hook, hold_block >= 0: that block
+// never issues its first source tile nor signals its arrival, so that its
+// waits run out (the launch then reports kErrTimeout).
+struct PairCtl {
+    uint64_t wait_ns;
+    int32_t hold_block;
+    int32_t pad;
+};
+
 // Sources per shared-memory tile: 256 float4 (4 KB) or 128 double4 (4 KB).
 FSS_HD constexpr int tile_capacity(bool fp64) { return fp64 ? 128 : 256; }
 

@@ -223,7 +223,8 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
                                          const Segment* __restrict__ segs, const int32_t* __restrict__ leaf_start,
                                          double4* __restrict__ partials, int64_t pstride,
                                          typename Vec4<T>::type* ring, float* soa, SlotHdr* hdr, uint64_t* full_bar,
-                                         uint64_t* empty_bar, uint64_t* ready_bar, RingState& rs) {
+                                         uint64_t* empty_bar, uint64_t* ready_bar, RingState& rs,
+                                         const PairCtl& ctl, bool hold) {
     using S4 = typename Vec4<T>::type;
     constexpr bool kPacked = sizeof(T) == 4;
     constexpr int kTargets = THREADS - 32;
@@ -244,8 +245,8 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
                 // convert every produced tile (each waits for its copies)
                 while (kPacked && rs.converted < rs.issued && !rs.failed) {
                     const int slot = int(rs.converted % kDepth);
-                    if (!__all_sync(0xffffffffu,
-                                    mbar_wait_bounded(&full_bar[slot], uint32_t(rs.converted / kDepth) & 1))) {
+                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full_bar[slot], uint32_t(rs.converted / kDepth) & 1,
+                                                                   ctl.wait_ns))) {
                         rs.failed = true;
                         break;
                     }
@@ -261,18 +262,24 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
                 const int slot = int(rs.issued % kDepth);
                 bool ok = true;
                 if (rs.issued >= kDepth)
-                    ok = mbar_wait_bounded(&empty_bar[slot], uint32_t((rs.issued / kDepth) - 1) & 1);
+                    ok = mbar_wait_bounded(&empty_bar[slot], uint32_t((rs.issued / kDepth) - 1) & 1, ctl.wait_ns);
                 if (!__all_sync(0xffffffffu, ok)) {
                     rs.failed = true;
                     break;
                 }
                 bool gd = false;
-                const int cnt = pack_tile<S4, TILE>(segs, leaf_start, it.g1, pg, poff, t0 + c0, t0 + c0 + cn, src,
-                                                    ring + slot * TILE, &full_bar[slot], gd);
-                if (lane == 0) {
-                    hdr[slot].count = cnt;
-                    hdr[slot].guard = gd ? 1 : 0;
-                    mbar_arrive(&full_bar[slot]);
+                int cnt = 1;
+                if (hold && rs.issued == 0) {
+                    // test hook: the first tile is neither copied nor signalled
+                    if (lane == 0) hdr[slot].count = cnt;
+                } else {
+                    cnt = pack_tile<S4, TILE>(segs, leaf_start, it.g1, pg, poff, t0 + c0, t0 + c0 + cn, src,
+                                              ring + slot * TILE, &full_bar[slot], gd);
+                    if (lane == 0) {
+                        hdr[slot].count = cnt;
+                        hdr[slot].guard = gd ? 1 : 0;
+                        mbar_arrive(&full_bar[slot]);
+                    }
                 }
                 __syncwarp();
                 if (cnt == 0) pdone = true;
@@ -293,7 +300,8 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
             for (;;) {
                 const int slot = int(rs.consumed % kDepth);
                 uint64_t* wait_bar = kPacked ? &ready_bar[slot] : &full_bar[slot];
-                if (!__all_sync(0xffffffffu, mbar_wait_bounded(wait_bar, uint32_t(rs.consumed / kDepth) & 1))) {
+                if (!__all_sync(0xffffffffu,
+                                mbar_wait_bounded(wait_bar, uint32_t(rs.consumed / kDepth) & 1, ctl.wait_ns))) {
                     rs.failed = true;
                     break;
                 }
@@ -342,7 +350,18 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
         // every tile produced for this chunk has been consumed, so the
         // counters agree in every warp unless a wait gave up
         rs.failed = __syncthreads_or(rs.failed) != 0;
-        if (rs.failed) return;
+        if (rs.failed) {
+            // no bulk copy may still be landing in this block's shared memory
+            // when it exits: the producer waits (bounded) for the tiles not
+            // known to have landed -- at most the last kDepth it issued
+            if (warp == 0) {
+                int64_t t = rs.issued - kDepth;
+                if (kPacked && rs.converted > t) t = rs.converted;
+                for (t = (t < 0) ? 0 : t; t < rs.issued; t++)
+                    mbar_wait_bounded(&full_bar[t % kDepth], uint32_t(t / kDepth) & 1, ctl.wait_ns);
+            }
+            return;
+        }
     }
 }
 
@@ -373,7 +392,7 @@ __global__ void __launch_bounds__(THREADS) k_pairs(const typename Vec4<T>::type*
                                                    const Segment* __restrict__ segs,
                                                    const int32_t* __restrict__ leaf_start,
                                                    const WorkItem* __restrict__ items, double4* __restrict__ partials,
-                                                   int64_t pstride, int* __restrict__ err) {
+                                                   int64_t pstride, int* __restrict__ err, const PairCtl ctl) {
     using S4 = typename Vec4<T>::type;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth], ready_bar[kDepth];
@@ -383,7 +402,7 @@ __global__ void __launch_bounds__(THREADS) k_pairs(const typename Vec4<T>::type*
     const WorkItem it = items[blockIdx.x];
     run_item<T, THREADS, TILE, PSI>(it, src, segs, leaf_start, partials, pstride, reinterpret_cast<S4*>(smem_raw),
                                     reinterpret_cast<float*>(smem_raw + ring_bytes<T, TILE>()), hdr, full_bar,
-                                    empty_bar, ready_bar, rs);
+                                    empty_bar, ready_bar, rs, ctl, int(blockIdx.x) == ctl.hold_block);
     if (rs.failed && threadIdx.x == 0) set_error(err, kErrTimeout);
 }
 
@@ -395,7 +414,8 @@ __global__ void __launch_bounds__(THREADS) k_pairs_persistent(const typename Vec
                                                               const int32_t* __restrict__ leaf_start,
                                                               const WorkItem* __restrict__ items, int nitems,
                                                               int* __restrict__ queue, double4* __restrict__ partials,
-                                                              int64_t pstride, int* __restrict__ err) {
+                                                              int64_t pstride, int* __restrict__ err,
+                                                              const PairCtl ctl) {
     using S4 = typename Vec4<T>::type;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth], ready_bar[kDepth];
@@ -413,7 +433,7 @@ __global__ void __launch_bounds__(THREADS) k_pairs_persistent(const typename Vec
         run_item<T, THREADS, TILE, false>(it, src, segs, leaf_start, partials, pstride,
                                           reinterpret_cast<S4*>(smem_raw),
                                           reinterpret_cast<float*>(smem_raw + ring_bytes<T, TILE>()), hdr, full_bar,
-                                          empty_bar, ready_bar, rs);
+                                          empty_bar, ready_bar, rs, ctl, false);
         if (rs.failed) break;
     }
     if (rs.failed && threadIdx.x == 0) set_error(err, kErrTimeout);
@@ -424,14 +444,14 @@ __global__ void __launch_bounds__(THREADS) k_pairs_persistent(const typename Vec
 template <typename T, int THREADS, bool PSI>
 static cudaError_t run_pairs(cudaStream_t st, int nitems, const void* src, const Segment* segs,
                              const int32_t* leaf_start, const WorkItem* items, double4* partials, int64_t pstride,
-                             int* err) {
+                             int* err, PairCtl ctl) {
     constexpr int TILE = tile_capacity(sizeof(T) == 8);
     constexpr size_t smem = pair_smem_bytes<T, TILE>();
     static_assert(smem <= 48 * 1024, "ring must fit the default dynamic shared memory limit");
     if (nitems == 0) return cudaSuccess;
     k_pairs<T, THREADS, PSI, TILE><<<nitems, THREADS, smem, st>>>(static_cast<const typename Vec4<T>::type*>(src),
                                                                    segs, leaf_start, items, partials,
-                                                                   pstride, err);
+                                                                   pstride, err, ctl);
     return cudaGetLastError();
 }
 
@@ -459,10 +479,10 @@ PairShape cluster_shape(bool fp64, int k) {
 template <typename T, bool PSI>
 static cudaError_t dispatch(cudaStream_t st, PairShape sh, int nitems, const void* src, const Segment* segs,
                             const int32_t* leaf_start, const WorkItem* items, double4* partials,
-                            int64_t pstride, int* err) {
+                            int64_t pstride, int* err, PairCtl ctl) {
 #define FSS_SHAPE(TH)                                                                                            \
     if (sh.threads == TH)                                                                                        \
-        return run_pairs<T, TH, PSI>(st, nitems, src, segs, leaf_start, items, partials, pstride, err);
+        return run_pairs<T, TH, PSI>(st, nitems, src, segs, leaf_start, items, partials, pstride, err, ctl);
     FSS_SHAPE(64)
     FSS_SHAPE(96)
     FSS_SHAPE(128)
@@ -476,22 +496,23 @@ static cudaError_t dispatch(cudaStream_t st, PairShape sh, int nitems, const voi
 
 cudaError_t launch_pairs(cudaStream_t st, bool fp64, bool psi, PairShape shape, int nitems, const void* src,
                          const Segment* segs, const int32_t* leaf_start, const WorkItem* items,
-                         double4* partials, int64_t pstride, int* err) {
+                         double4* partials, int64_t pstride, int* err, PairCtl ctl) {
     if (fp64)
-        return psi ? dispatch<double, true>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err)
-                   : dispatch<double, false>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err);
-    return psi ? dispatch<float, true>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err)
-               : dispatch<float, false>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err);
+        return psi ? dispatch<double, true>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err, ctl)
+                   : dispatch<double, false>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err,
+                                             ctl);
+    return psi ? dispatch<float, true>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err, ctl)
+               : dispatch<float, false>(st, shape, nitems, src, segs, leaf_start, items, partials, pstride, err, ctl);
 }
 
 cudaError_t launch_pairs_persistent(cudaStream_t st, int nitems, const void* src, const Segment* segs,
                                     const int32_t* leaf_start, const WorkItem* items, int* queue,
-                                    double4* partials, int64_t pstride, int* err, int blocks) {
+                                    double4* partials, int64_t pstride, int* err, int blocks, PairCtl ctl) {
     constexpr int TILE = tile_capacity(false);
     constexpr size_t smem = pair_smem_bytes<float, TILE>();
     if (nitems == 0) return cudaSuccess;
     k_pairs_persistent<float, kPersistentThreads, TILE><<<blocks, kPersistentThreads, smem, st>>>(
-        static_cast<const float4*>(src), segs, leaf_start, items, nitems, queue, partials, pstride, err);
+        static_cast<const float4*>(src), segs, leaf_start, items, nitems, queue, partials, pstride, err, ctl);
     return cudaGetLastError();
 }
 

@@ -79,11 +79,11 @@ PairShape pairs_shape(bool fp64, int threads, int per_thread);
 PairShape cluster_shape(bool fp64, int k);
 cudaError_t launch_pairs(cudaStream_t st, bool fp64, bool psi, PairShape shape, int nitems, const void* src,
                          const Segment* segs, const int32_t* leaf_start, const WorkItem* items, double4* partials,
-                         int64_t pstride, int* err);
+                         int64_t pstride, int* err, PairCtl ctl);
 constexpr int kPersistentThreads = 160;
 cudaError_t launch_pairs_persistent(cudaStream_t st, int nitems, const void* src, const Segment* segs,
                                     const int32_t* leaf_start, const WorkItem* items, int* queue, double4* partials,
-                                    int64_t pstride, int* err, int blocks);
+                                    int64_t pstride, int* err, int blocks, PairCtl ctl);
 int persistent_blocks_per_sm();
 
 // k_epi.cu

@@ -40,7 +40,8 @@ class Config(C.Structure):
                 ("theta", C.c_double), ("many_count", C.c_int32), ("assign_mode", C.c_int32),
                 ("list_mode", C.c_int32), ("use_graph", C.c_int32), ("src_parts", C.c_int32),
                 ("block_threads", C.c_int32), ("targets_per_thread", C.c_int32), ("autotune", C.c_int32),
-                ("rebuild", C.c_int32), ("cluster_targets", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("rebuild", C.c_int32), ("cluster_targets", C.c_int32), ("wait_limit_us", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 class TreeInfo(C.Structure):
@@ -77,10 +78,10 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_select_classes",
            "fss_selector_apply", "fss_ensemble_create", "fss_ensemble_destroy", "fss_ensemble_set_stream",
            "fss_ensemble_add", "fss_ensemble_build", "fss_ensemble_rk4_step", "fss_ensemble_get_state",
-           "fss_ensemble_info", "fss_amr_create", "fss_amr_destroy", "fss_amr_counts", "fss_amr_refine",
+           "fss_ensemble_info", "fss_ensemble_time_pairs", "fss_amr_create", "fss_amr_destroy", "fss_amr_counts", "fss_amr_refine",
            "fss_amr_get_mesh", "fss_amr_remesh", "fss_amr_refine_current", "fss_remesh_lists", "fss_state_csv_append",
            "fss_point_count_append", "fss_output_name", "fss_state_bin_append", "fss_state_bin_read",
-           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_version"]
+           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_test_hold_tile", "fss_version"]
 
 NOALLOC_MAX_PARTICLES = 262144  # FSS_NOALLOC_MAX_PARTICLES in include/fss.h
 
@@ -136,6 +137,7 @@ def lib():
     L.fss_ensemble_rk4_step.argtypes = [_vp, C.c_double, C.c_double, C.c_int32]
     L.fss_ensemble_get_state.argtypes = [_vp, C.c_int32, _D]
     L.fss_ensemble_info.argtypes = [_vp, P(C.c_int32), P(_i64), P(C.c_double), P(_i64)]
+    L.fss_ensemble_time_pairs.argtypes = [_vp, C.c_int32, P(C.c_double)]
     L.fss_amr_create.argtypes = [_i64, _i64, _I32, _vp, _i64, _i64, C.c_int32, P(_vp)]
     L.fss_amr_destroy.argtypes = [_vp]
     L.fss_amr_destroy.restype = None
@@ -155,6 +157,7 @@ def lib():
     L.fss_read_tris_csv.argtypes = [C.c_char_p, _i64, _I32]
     L.fss_read_vert_tris_csv.argtypes = [C.c_char_p, C.c_char_p, _i64, _I32, _I32, _i64]
     L.fss_version.restype = C.c_char_p
+    L.fss_test_hold_tile.argtypes = [_vp, C.c_int32]
     _lib = L
     return L
 
@@ -411,6 +414,12 @@ class Context:
         self._c(lib().fss_work_per_rhs(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def test_hold_tile(self, block=0):
+        """Test hook: the next evaluation's target-leaf pair block `block`
+        withholds its first source tile, so that its bounded waits run out
+        (fss_test_hold_tile)."""
+        self._c(lib().fss_test_hold_tile(self.h, block))
+
 
 def rhs_direct_noalloc(n, state5_dev_ptr, area_dev_ptr, out5_dev_ptr, stream_handle=None, omega=OMEGA):
     """fss_rhs_direct_noalloc on caller-owned device buffers (raw pointers);
@@ -614,6 +623,12 @@ class Ensemble:
         out = np.zeros((self.sizes[member], 5))
         _check(lib().fss_ensemble_get_state(self.h, member, out.reshape(-1)))
         return out
+
+    def time_pairs(self, reps=3):
+        """Device ms of one persistent pair launch (mean of `reps`)."""
+        ms = C.c_double()
+        _check(lib().fss_ensemble_time_pairs(self.h, reps, C.byref(ms)))
+        return ms.value
 
     def info(self):
         m, n, w = C.c_int32(), _i64(), _i64()

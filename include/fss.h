@@ -113,7 +113,11 @@ typedef struct fss_config {
                               FSS_LIST_LEAF the per-leaf (n, theta) are carried
                               up to the faces of a dual traversal (theta = min,
                               n = max over a face's leaves) */
-    int32_t reserved[4];
+    int32_t wait_limit_us; /* every wait of the pair kernel on its tile ring
+                              gives up after this many microseconds and the
+                              call returns FSS_ERR_TIMEOUT, the context staying
+                              usable (0 = 2 s) */
+    int32_t reserved[3];
 } fss_config;
 
 typedef struct fss_ctx fss_ctx;
@@ -369,6 +373,11 @@ int fss_ensemble_rk4_step(fss_ensemble* e, double dt, double omega, int32_t nste
 int fss_ensemble_get_state(fss_ensemble* e, int32_t member, double* state5);
 int fss_ensemble_info(fss_ensemble* e, int32_t* members, int64_t* particles, double* interactions_per_rhs,
                       int64_t* work_items);
+/* Device time (ms) of one persistent pair launch on the current stage
+ * sources, the mean of `reps` launches after an untimed one (CUDA events on
+ * the ensemble's stream); the launches only rewrite the partial sums that
+ * the next stage rewrites anyway, so the state is unchanged. */
+int fss_ensemble_time_pairs(fss_ensemble* e, int32_t reps, double* ms);
 
 /* ------------------------------------------------------------ selector
  * Learned per-leaf interpolation degree and MAC (no counterpart in the
@@ -437,6 +446,16 @@ int fss_selector_apply(fss_ctx* ctx, fss_mlp* m, const float* feat_mean, const f
 #define FSS_NOALLOC_MAX_PARTICLES 262144
 int fss_rhs_direct_noalloc(int64_t n, const double* state5, const double* area, double omega, double* modify5,
                            void* stream);
+
+/* Test hook for the failure path (no counterpart in the reference, which has
+ * no error path): in the next right-hand-side evaluation of this context,
+ * block `block` of the target-leaf pair launch neither copies its first
+ * source tile nor signals its arrival, so that the block's bounded waits run
+ * out.  That call returns FSS_ERR_TIMEOUT; the hook is then cleared and the
+ * context stays usable.  No copy is left in flight: the withheld tile was
+ * never issued, and a block whose waits ran out waits (bounded) for the
+ * copies it did issue before it exits.  block < 0 clears the hook. */
+int fss_test_hold_tile(fss_ctx* ctx, int32_t block);
 
 /* Library build string (architecture, features). */
 const char* fss_version(void);

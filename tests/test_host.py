@@ -140,6 +140,10 @@ def test_context_needs_gpu_or_reports(fss):
     with pytest.raises(fss.FssError) as e:
         fss.Context()
     assert e.value.code == 7
+    # settings are validated on the host first
+    with pytest.raises(fss.FssError) as e:
+        fss.Context(wait_limit_us=-1)
+    assert e.value.code == 1
 
 
 def test_amr_and_remesh_need_gpu_or_report(fss):
