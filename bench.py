@@ -13,8 +13,15 @@ roofline, and the reference's CPU direct sum timed on this host's cores.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-With N > 1 (torchrun) every rank runs an independent replica (the path does
-not shard: replicas only); value = all ranks' steps / max-over-ranks time.
+Output: one JSON line of details (tree, per-kernel rooflines, every arm, the
+reference's CPU fast sum, remesh, AMR, the 64-member ensemble), then the
+headline JSON line, short and last (value, rel-L2 against the FP64 direct
+sum, the ratio to the plain FP64 BLTC, e2e, roofline, clocks).
+
+With N > 1 (torchrun) every rank runs an independent replica;
+value = all ranks' steps / max-over-ranks time.  The reference arm
+(--impl reference) builds its inputs with the oracle alone and never loads
+the product library.
 """
 import argparse
 import json
@@ -49,6 +56,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-remesh", action="store_true")
     p.add_argument("--no-amr", action="store_true")
+    p.add_argument("--no-ensemble", action="store_true")
+    p.add_argument("--members", type=int, default=64, help="ensemble members (levels 5-8)")
     p.add_argument("--cpu-sample", type=int, default=2048, help="targets in one CPU-baseline sample")
     p.add_argument("--tol", type=float, default=1e-6, help="selector: relative L2 velocity error target")
     p.add_argument("--safety", type=float, default=1.5, help="selector: predicted-error safety factor")
@@ -471,29 +480,149 @@ def kernel_rooflines(prof, steps, n, info, up_bytes, peaks):
 
 
 def main_reference(args, ws, rank):
+    """The reference's own CPU implementation of the path, timed on this
+    host's cores.  Its fast sum (rhs_fast_sum) cannot be set up at 655,362
+    particles in minutes (its pair traversal is quadratic in the queue) and
+    never reaches 1e-6, so the arm times its FP64 direct sum (rhs_direct_sum /
+    BVE_gfunc, oracle/_ref) on a bounded sample per step: `cpu_sample` seeded
+    target rows against all sources, scaled by N / rows to one RHS, x4 per RK4
+    step.  The inputs are built by the oracle alone (icos_init, area_init and
+    the seeded field), so the product library is never loaded here."""
     if rank != 0:
         return
-    import fss_b200 as fss
-    state, area = fss.make_state(args.level, "rh_vortices", n_vortex=args.vortices, seed=args.seed)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    state, area = O.rh_vortices_state(args.level, args.vortices, args.seed)
+    n = state.shape[0]
     for _ in range(args.warmup):
         cpu_reference_sample(state, area, max(64, args.cpu_sample // 8))
-    vals, secs = [], 0.0
+    secs_extrapolated, timed = 0.0, 0.0
     cb = None
     for k in range(args.steps):
+        t0 = time.perf_counter()
         cb = cpu_reference_sample(state, area, args.cpu_sample, seed=100 + k)
-        vals.append(cb["value"])
-        secs += 1.0 / cb["value"]
-    value = args.steps / secs
+        timed += time.perf_counter() - t0
+        secs_extrapolated += 1.0 / cb["value"]
+    value = args.steps / secs_extrapolated
     cb["value"] = value
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"BVE RHS RK4 step, {state.shape[0]} particles (icosahedral level {args.level}), "
+            "extrapolated": True,
+            "samples": {"count": args.steps, "targets_per_sample": args.cpu_sample, "sources": int(n),
+                        "timed_s": timed, "s_per_rhs_extrapolated": secs_extrapolated / (4 * args.steps),
+                        "note": f"each 'step' is one sample of {args.cpu_sample} targets x {n} sources; "
+                                f"ms_per_step is that sample scaled by N/rows x 4 RHS, not a step that ran"},
+            "config": {"workload": f"BVE RHS RK4 step, {n} particles (icosahedral level {args.level}), "
                                    f"RH4 + {args.vortices} vortices; reference FP64 direct sum on host cores",
-                       "n_particles": int(state.shape[0])},
+                       "n_particles": int(n),
+                       "same_algorithm": False,
+                       "why_direct": "the reference's treecode cannot be set up at this N in minutes and its "
+                                     "degree-2 interpolation stays near 2e-1 rel-L2"},
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def time_arm(ctx, stream, flush, args, ws):
+    """(steps/s over all ranks, ms per step of the slowest rank) of an arm."""
+    warm(ctx, stream, args.warmup)
+    t = max_over_ranks(time_steps(ctx, stream, args.steps, flush), ws)
+    return ws * args.steps / t, 1e3 * t / args.steps
+
+
+def e2e_rhs_func(ctx, state, area, steps):
+    """The reference's own call pattern (new_dynamics.cpp:170-229): per RK4
+    step four fss_rhs calls with host buffers (state in, modify out) and the
+    stage states combined and projected on the host, as rhs_func's caller
+    does.  Host wall clock per step, after a synchronisation."""
+    s = state.copy()
+    dt, om = DT, 2 * np.pi
+
+    def project(x, old_z):
+        x[:, :3] /= np.linalg.norm(x[:, :3], axis=1, keepdims=True)
+        x[:, 3] += -2 * om * (x[:, 2] - old_z)
+        return x
+
+    def step(s):
+        k1 = ctx.rhs(s, area)
+        i1 = s + dt / 2 * k1
+        k2 = ctx.rhs(project(i1, i1[:, 2].copy()), area)
+        i2 = s + dt / 2 * k2
+        k3 = ctx.rhs(project(i2, i2[:, 2].copy()), area)
+        i3 = s + dt * k3
+        k4 = ctx.rhs(project(i3, i3[:, 2].copy()), area)
+        out = s + dt / 6 * (k1 + 2 * k2 + 2 * k3 + k4)
+        return project(out, out[:, 2].copy())
+
+    s = step(s)  # warm
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s = step(s)
+    wall = time.perf_counter() - t0
+    return {"value": steps / wall, "unit": UNIT, "calls_per_step": 4,
+            "h2d_bytes_per_step": int(4 * (state.nbytes + area.nbytes)), "d2h_bytes_per_step": int(4 * state.nbytes),
+            "how": "four fss_rhs calls per RK4 step with host buffers (the reference's rhs_func call pattern, "
+                   "new_dynamics.cpp:170-229), stage combine and projection on the host in NumPy; host wall clock"}
+
+
+def ensemble_measure(fss, args, dev, stream, members=64, steps=20, seed=100):
+    """The ensemble configuration: `members` problems on icosahedral levels
+    drawn uniformly from 5-8 (10,242 - 655,362 particles each), each an RH R=4
+    wave with a seeded +-5% amplitude perturbation and 4-16 Gaussian vortices;
+    mixed-precision BLTC n = 8, theta = 0.7; one persistent pair launch per RK
+    stage over the global (member, target leaf, source run) queue, one CUDA
+    graph per RK4 step.  Device time of `steps` steps (CUDA events, L2 not
+    flushed: the ensemble's working set is far larger than L2); the persistent
+    launch timed alone for its FP32 fraction; member 0 against its own run."""
+    rng = np.random.default_rng(seed)
+    fields, levels = [], []
+    for m in range(members):
+        level = int(rng.integers(5, 9))
+        nv = int(rng.integers(4, 17))
+        amp = float(rng.uniform(0.95, 1.05))
+        fields.append(fss.make_state(level, "rh_vortices", n_vortex=nv, seed=seed + m, amp=fss.RH_AMP * amp))
+        levels.append(level)
+    import torch
+    t0 = time.perf_counter()
+    with fss.Ensemble(degree=8, theta=0.7, device=dev) as ens:
+        ens.set_stream(stream.cuda_stream)
+        for s, a in fields:
+            ens.add(s, a)
+        ens.build()
+        build_s = time.perf_counter() - t0
+        info = ens.info()
+        ens.rk4_step(DT, nsteps=1)  # capture + warm
+        stream.synchronize()
+        a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a_ev.record(stream)
+            ens.rk4_step(DT, nsteps=steps)
+            b_ev.record(stream)
+        stream.synchronize()
+        secs = a_ev.elapsed_time(b_ev) / 1e3
+        pair_ms = ens.time_pairs(3)
+        got0 = ens.get_state(0)
+    s0, a0 = fields[0]
+    with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, degree=8, theta=0.7,
+                     block_threads=160, src_parts=1, device=dev) as ctx:
+        ctx.set_particles(s0, a0)
+        ctx.rk4_step(DT, nsteps=1 + steps)
+        ref0 = ctx.get_state()
+    disp = ref0[:, :3] - s0[:, :3]
+    inter = info["interactions_per_rhs"]
+    peaks = load_peaks()
+    fp32_peak = 148 * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    pair_tflops = FLOPS_PER_PAIR * inter / (pair_ms * 1e-3) / 1e12
+    return {"workload": f"{members} members, icosahedral levels 5-8 drawn uniformly (seed {seed}), RH4 +-5% + 4-16 "
+                        f"vortices, mixed-precision BLTC n=8 theta=0.7, {steps} RK4 steps",
+            "members": members, "levels_5_6_7_8": np.bincount(levels, minlength=9)[5:].tolist(),
+            "particles": info["particles"], "work_items": info["work_items"], "interactions_per_rhs": inter,
+            "steps": steps, "device_s": secs, "steps_per_s": steps / secs,
+            "interactions_per_s": 4 * steps * inter / secs, "build_s": build_s,
+            "pair_launch_ms": pair_ms, "pair_launch_tflops": pair_tflops, "pair_launch_fp32_frac": pair_tflops / fp32_peak,
+            "member0_vs_alone_rel_l2": float(np.linalg.norm(got0[:, :3] - ref0[:, :3]) / np.linalg.norm(disp)),
+            "member0_bit_exact_vs_alone": bool(np.array_equal(got0, ref0))}
 
 
 def main():
@@ -514,7 +643,8 @@ def main():
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")  # 256 MB > L2
 
-    # accuracy reference: the FP64 direct sum on the GPU (parity-tested against the oracle)
+    # accuracy reference: the FP64 direct sum on the GPU (checked against the
+    # CPU oracle on 4,096 seeded targets at this size in tests/test_gpu_fullsize.py)
     with fss.Context(method=fss.METHOD_DIRECT, precision=fss.PREC_FP64, device=dev) as dctx:
         dctx.set_stream(stream.cuda_stream)
         dctx.set_particles(state, area)
@@ -569,35 +699,37 @@ def main():
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s, nominal at max SM clock
     achieved = FLOPS_PER_PAIR * inter / (pairs_ms * 1e-3) / 1e12
     traffic = profiled_traffic("pairs_mixed_level8")
+    info = ctx.tree_info()
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp32_peak, "traffic": traffic,
                 "kernel": "k_pairs (target-leaf + target-cluster launches of one RHS)", "kernel_ms": pairs_ms,
-                "interactions_per_launch": inter,
-                "flops_per_interaction": FLOPS_PER_PAIR,
-                "peak_source": f"nominal FP32 148 SM x 128 lanes x 2 x {sm_max:.0f} MHz (MEASURED_PEAKS.json has no FP32 figure)",
-                "frac_at_sampled_clock": (achieved / (fp32_peak * clocks["sm_mhz"] / sm_max)) if clocks.get("sm_mhz") else None,
-                "kernel_shares": {k: round(v[0] / total_ms, 4) for k, v in prof.items()},
-                "upward_bytes_per_rhs": up_bytes,
-                "kernels": kernel_rooflines(prof, args.steps, n, ctx.tree_info(), up_bytes, peaks)}
-    info = ctx.tree_info()
+                "interactions_per_launch": inter, "flops_per_interaction": FLOPS_PER_PAIR,
+                "peak_source": f"nominal FP32 148 SM x 128 lanes x 2 x {sm_max:.0f} MHz (MEASURED_PEAKS.json has no FP32 figure)"}
+    roofline_detail = {"frac_at_sampled_clock": (achieved / (fp32_peak * clocks["sm_mhz"] / sm_max)) if clocks.get("sm_mhz") else None,
+                       "kernel_shares": {k: round(v[0] / total_ms, 4) for k, v in prof.items()},
+                       "upward_bytes_per_rhs": up_bytes,
+                       "kernels": kernel_rooflines(prof, args.steps, n, info, up_bytes, peaks)}
 
-    # ---------------- FP64 arms: plain BLTC (the ratio's denominator: fixed n, theta,
-    # far sources summed at the target particles) and the same algorithm as the
-    # headline arm's (target clusters) in FP64, for reference
-    fp64 = fp64c = None
+    # ---------------- the other arms on the same GPU: the plain FP64 BLTC (the
+    # ratio's denominator: fixed n, theta, far sources summed at the target
+    # particles), the FP64 treecode with the headline's algorithm (target
+    # clusters), and the mixed-precision treecode with target clusters at
+    # fixed n = 8, theta = 0.7 (what the learned choice alone adds)
+    fp64 = fp64c = fixc = None
+    arms = []
     if not args.no_fp64:
-        for cl in (False, True):
-            c64 = make_arm(fss, state, area, stream, fss.PREC_FP64, args, dev, clusters=cl)
-            e64 = rel_err(c64)
-            warm(c64, stream, args.warmup)
-            t64 = max_over_ranks(time_steps(c64, stream, args.steps, flush), ws)
-            r = {"value": ws * args.steps / t64, "ms_per_step": 1e3 * t64 / args.steps, "rel_l2": e64[0],
-                 "rel_max": e64[1], "degree": args.degree, "theta": args.theta, "target_clusters": cl}
-            c64.close()
-            if cl:
-                fp64c = r
-            else:
-                fp64 = r
+        arms += [("fp64_plain", fss.PREC_FP64, False), ("fp64_same_algorithm", fss.PREC_FP64, True)]
+    if learned:
+        arms += [("mixed_fixed_clusters", fss.PREC_MIXED, clusters)]
+    res = {}
+    for name, prec, cl in arms:
+        c2 = make_arm(fss, state, area, stream, prec, args, dev, clusters=cl)
+        e2 = rel_err(c2)
+        v2, ms2 = time_arm(c2, stream, flush, args, ws)
+        res[name] = {"value": v2, "ms_per_step": ms2, "rel_l2": e2[0], "rel_max": e2[1], "degree": args.degree,
+                     "theta": args.theta, "target_clusters": cl, "precision": "fp64" if prec == fss.PREC_FP64 else "mixed"}
+        c2.close()
+    fp64, fp64c, fixc = res.get("fp64_plain"), res.get("fp64_same_algorithm"), res.get("mixed_fixed_clusters")
 
     # ---------------- end to end through the C ABI with pinned host buffers
     e2e = None
@@ -618,6 +750,10 @@ def main():
         e2e = {"value": ws * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": int(state.nbytes),
                "d2h_bytes_per_step": int(state.nbytes)}
 
+    e2e_rf = None
+    if rank == 0 and ws == 1 and not args.no_e2e:
+        e2e_rf = e2e_rhs_func(ctx, state, area, max(3, args.steps // 4))
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_reference_sample(state, area, args.cpu_sample)
@@ -629,6 +765,7 @@ def main():
             remesh = remesh_measure(fss, ctx, state, area, args.level, stream)
         except fss.FssError as e:  # too many points left their triangles in one step
             remesh = {"error": str(e)}
+    ctx.close()
 
     cpu_fast = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -641,35 +778,48 @@ def main():
     if rank == 0 and ws == 1 and not args.no_amr:
         amr = amr_measure(fss)
 
-    ctx.close()
+    ens = None
+    if rank == 0 and ws == 1 and not args.no_ensemble:
+        try:
+            ens = ensemble_measure(fss, args, dev, stream, members=args.members)
+        except fss.FssError as e:
+            ens = {"error": str(e)}
+
     if rank == 0:
+        workload = (f"BVE RK4 step (4 RHS), {n} particles (icosahedral level {args.level}), RH4 wave + "
+                    f"{args.vortices} seeded vortices, mixed-precision BLTC "
+                    f"({'learned per-leaf degree/theta' if learned else f'n={args.degree} theta={args.theta}'}"
+                    f"{', target clusters' if clusters else ''}), particles re-sorted every step")
+        # everything bulky first, on a line of its own ...
+        detail = {"detail": "bench details (the headline is the next line)", "metric": METRIC,
+                  "selector": (f"learned per-leaf (n, theta), tol {args.tol}, safety {args.safety}, "
+                               f"classes (n, theta) {list(zip(*_sel.class_table(clusters)))}, "
+                               f"class counts {classes}") if learned else "none (fixed degree/theta)",
+                  "tree": info, "roofline_detail": roofline_detail, "arms": res,
+                  "e2e_rhs_func": e2e_rf, "cpu_baseline": cpu, "cpu_reference_fast": cpu_fast,
+                  "remesh": remesh, "amr": amr, "ensemble": ens}
+        print(json.dumps(detail), flush=True)
+        # ... then the headline, short and last
+        short = lambda r: None if r is None else {k: r[k] for k in ("value", "ms_per_step", "rel_l2", "rel_max")}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": f"BVE RK4 step (4 RHS), {n} particles (icosahedral level {args.level}), "
-                                       f"RH4 wave + {args.vortices} seeded vortices, mixed-precision BLTC "
-                                       f"({'learned per-leaf degree/theta' if learned else f'n={args.degree} theta={args.theta}'}"
-                                       f"{', target clusters (reference cp/cc types)' if clusters else ''}), "
-                                       f"tree_levels={info['tree_levels']}, particles re-sorted into their current leaves every step",
-                           "n_particles": n, "degree": args.degree, "theta": args.theta,
-                           "precision": "FP32 interactions + Kahan; FP64 RK4, renormalisation, interpolation",
-                           "selector": (f"learned per-leaf (n, theta), tol {args.tol}, safety {args.safety}, "
-                                        f"classes (n, theta) {list(zip(*_sel.class_table(clusters)))}, "
-                                        f"class counts {classes}") if learned else "none (fixed degree/theta)",
-                           "lists": ("dual traversal with per-face parameters from the per-leaf choice" if learned
-                                     else "dual (reference traversal)") if clusters else
-                                    ("per-leaf" if learned else "dual (reference traversal)"),
-                           "target_clusters": clusters,
+                "rel_l2": err_l2, "rel_max": err_max, "tol": args.tol,
+                "ratio_vs_fp64_plain": (value / fp64["value"]) if fp64 else None,
+                "fp64_plain": short(fp64),
+                "ratio_vs_fp64_same_algorithm": (value / fp64c["value"]) if fp64c else None,
+                "ratio_learned_vs_fixed_clusters": (value / fixc["value"]) if fixc else None,
+                "mixed_fixed_clusters": short(fixc),
+                "config": {"workload": workload, "n_particles": n, "tree_levels": info["tree_levels"],
+                           "error_reference": "FP64 direct sum on the GPU, all targets",
                            "l2": "flushed between timed steps (256 MB write)",
                            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
-                "rel_l2": err_l2, "rel_max": err_max,
-                "fp64_plain": fp64,
-                "ratio_vs_fp64_plain": (value / fp64["value"]) if fp64 else None,
-                "fp64_same_algorithm": fp64c,
-                "ratio_vs_fp64_same_algorithm": (value / fp64c["value"]) if fp64c else None,
-                "interactions_per_rhs": inter, "tree": info,
-                "roofline": roofline, "cpu_baseline": cpu, "cpu_reference_fast": cpu_fast, "e2e": e2e,
-                "remesh": remesh, "amr": amr, "interactions_per_s": inter * 4 * value,
+                "e2e": e2e,
+                "e2e_rhs_func": None if e2e_rf is None else {"value": e2e_rf["value"], "unit": UNIT},
+                "roofline": roofline,
+                "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind")},
+                "ensemble_steps_per_s": None if not ens or "error" in ens else ens["steps_per_s"],
+                "interactions_per_s": inter * 4 * value,
                 "gpu_launches": int(round(launches_per_step * args.steps)),
                 "clocks": clocks}
         print(json.dumps(line), flush=True)

@@ -10,13 +10,16 @@
 //
 // Costs and limits: every GPU that loads the library holds that array
 // (kNoAllocMaxParticles x 16 bytes = 4 MiB) until the process exits; larger
-// particle counts are rejected.  All calls share the array, and each call
-// overwrites the entries it uses before reading them, so no clearing is
-// needed; but two calls whose kernels overlap on the GPU (different streams,
-// or different host threads) race on it.
+// particle counts are rejected.  With CUDA's lazy module loading (the
+// default), the module holding the array -- and so the 4 MiB -- is loaded on
+// a device by the first call there; a caller that must not see that happen
+// inside its loop makes one call at start-up (before any stream capture).
+// All calls share the array, and each call overwrites the entries it uses
+// before reading them, so no clearing is needed; but two calls whose kernels
+// overlap on the GPU (different streams, or different host threads) race on
+// it.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "device_common.cuh"
@@ -34,10 +37,10 @@ constexpr int kNaTile = 256;
 static __device__ __align__(256) float4 g_noalloc_src[kNoAllocMaxParticles];
 
 // Host code must not pass g_noalloc_src itself (on the host it is only a
-// stand-in, not a device address): the device address of the array is
-// looked up once per device with cudaGetSymbolAddress and kept here.
-static std::mutex g_na_mutex;
-static void* g_na_addr[64] = {nullptr};
+// stand-in, not a device address): every call looks up the array's device
+// address on the current device with cudaGetSymbolAddress (cheap once the
+// module is loaded), so no address outlives a device reset or a re-created
+// context.
 
 __global__ void k_na_pack(int64_t n, const double* __restrict__ state5, const double* __restrict__ area,
                           float4* __restrict__ src) {
@@ -115,26 +118,19 @@ extern "C" int fss_rhs_direct_noalloc(int64_t n, const double* state5, const dou
         return FSS_ERR_CAPACITY;
     }
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         set_last_error("fss_rhs_direct_noalloc: no current CUDA device");
         return FSS_ERR_CUDA;
     }
+    // the array's address on the current device (its module is loaded there
+    // by the first call under lazy loading)
     void* scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_na_mutex);
-        if (!g_na_addr[dev]) {
-            // first call on this device (with it current): look the array up
-            void* p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_src);
-            if (e != cudaSuccess || !p) {
-                cudaGetLastError();
-                set_last_error(std::string("fss_rhs_direct_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-                return FSS_ERR_CUDA;
-            }
-            g_na_addr[dev] = p;
-        }
-        scratch = g_na_addr[dev];
+    const cudaError_t ge = cudaGetSymbolAddress(&scratch, g_noalloc_src);
+    if (ge != cudaSuccess || !scratch) {
+        cudaGetLastError();
+        set_last_error(std::string("fss_rhs_direct_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(ge));
+        return FSS_ERR_CUDA;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     float4* src = static_cast<float4*>(scratch);

@@ -439,10 +439,13 @@ int fss_selector_apply(fss_ctx* ctx, fss_mlp* m, const float* feat_mean, const f
  * Limit: n <= FSS_NOALLOC_MAX_PARTICLES; larger n returns FSS_ERR_CAPACITY
  * with a message in fss_last_error(NULL).  The scratch is a fixed device
  * array of FSS_NOALLOC_MAX_PARTICLES x 16 bytes (4 MiB) that every GPU
- * loading the library holds until the process exits.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress, with the
- * device current); make that first call before any stream capture.  All
- * calls share the array: two calls whose kernels overlap on the GPU race. */
+ * loading the library holds until the process exits.  Every call looks up
+ * that array's device address on the current device (cudaGetSymbolAddress).
+ * Under CUDA's lazy module loading (the default) the first call on a device
+ * loads the library's module there, 4 MiB array included: make that first
+ * call at start-up, before any stream capture (or load modules eagerly with
+ * CUDA_MODULE_LOADING=EAGER).  All calls share the array: two calls whose
+ * kernels overlap on the GPU race. */
 #define FSS_NOALLOC_MAX_PARTICLES 262144
 int fss_rhs_direct_noalloc(int64_t n, const double* state5, const double* area, double omega, double* modify5,
                            void* stream);

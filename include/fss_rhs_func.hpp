@@ -7,11 +7,17 @@
 // Include this header in place of rhs_eval.h and link libfss.so.  It reads the
 // fields the reference's evaluators read from run_information -- use_fast,
 // point_count, tree_levels, theta, many_count, degree -- and evaluates on the
-// GPU through the C ABI of fss.h.  As in the reference (new_dynamics.cpp:187-199),
+// GPU through the C ABI of fss.h.  As in the reference (new_dynamics.cpp:87-88),
 // the tree is built from the particles of the first call and kept for later
 // calls with the same settings; a change of any setting or of point_count
 // rebuilds it.  Errors throw std::runtime_error (the reference has no error
 // path; it prints LAPACK info and continues).
+//
+// Precision: FP64 throughout by default, as the reference's rhs_func.  A
+// caller that wants the mixed-precision evaluator (FP32 interactions with
+// Kahan-compensated sums, about 1e-7 relative error) selects it with
+// fss_dropin::set_precision(FSS_PREC_MIXED) before the call, or compiles with
+// -DFSS_DROPIN_PRECISION=FSS_PREC_MIXED.
 #pragma once
 
 #include <memory>
@@ -21,17 +27,32 @@
 
 #include "fss.h"
 
+#ifndef FSS_DROPIN_PRECISION
+#define FSS_DROPIN_PRECISION FSS_PREC_FP64
+#endif
+
 namespace fss_dropin {
 
 struct Settings {
     bool use_fast = false;
     int point_count = 0, tree_levels = 0, many_count = -1, degree = 8;
     double theta = 0.7;
+    int precision = FSS_DROPIN_PRECISION;
     bool operator==(const Settings& o) const {
         return use_fast == o.use_fast && point_count == o.point_count && tree_levels == o.tree_levels &&
-               many_count == o.many_count && degree == o.degree && theta == o.theta;
+               many_count == o.many_count && degree == o.degree && theta == o.theta && precision == o.precision;
     }
 };
+
+// Precision of later rhs_func calls on this thread (fss_precision).
+inline int& precision_setting() {
+    thread_local int p = FSS_DROPIN_PRECISION;
+    return p;
+}
+inline void set_precision(int p) {
+    if (p != FSS_PREC_FP64 && p != FSS_PREC_MIXED) throw std::invalid_argument("fss: unknown precision");
+    precision_setting() = p;
+}
 
 struct Ctx {
     fss_ctx* h = nullptr;
@@ -50,7 +71,7 @@ inline Ctx& context(const Settings& s, const double* state5, const double* area)
         ctx.reset(new Ctx());
         fss_config cfg;
         fss_config_init(&cfg);
-        cfg.precision = FSS_PREC_MIXED;
+        cfg.precision = s.precision;
         cfg.method = s.use_fast ? FSS_METHOD_TREECODE : FSS_METHOD_DIRECT;
         cfg.tree_levels = s.tree_levels;
         cfg.theta = s.theta;
@@ -77,6 +98,7 @@ void rhs_func(std::vector<double>& modify, std::vector<double>& curr_state, std:
     s.theta = config1.theta;
     s.many_count = config1.use_fast ? config1.many_count : -1;
     s.degree = (config1.use_fast && config1.degree > 0) ? config1.degree : 8;
+    s.precision = fss_dropin::precision_setting();
     if ((int64_t)curr_state.size() < 5 * (int64_t)s.point_count || (int64_t)area.size() < s.point_count)
         throw std::runtime_error("fss: state/area shorter than point_count");
     modify.resize(curr_state.size());

@@ -6,7 +6,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("level,tree_levels", [(3, 2), (4, 3), (5, 3), (5, 4)])
+@pytest.mark.parametrize("level,tree_levels", [(3, 2), (4, 3), (5, 3), (5, 4), (6, 4)])
 def test_reference_membership_and_pairs_bit_exact(fss, oracle, level, tree_levels):
     s, a = fss.make_state(level, "rh4_ref")
     loc_o = oracle.points_assign(tree_levels, s)

@@ -138,6 +138,20 @@ def test_tree_bit_exact_vs_reference(oracle, level, tree_levels, theta, many):
 
 
 @need_ref
+def test_tree_level7_bit_exact_vs_reference(oracle):
+    """The C2 tree: 163,842 grid particles, tree depth 4 (1,280 leaves), theta
+    0.7 -- the reference's own points_assign and tree_traverse (~10 s)."""
+    s, a, _ = oracle.icos_state(7)
+    loc_r, cnt_r, pairs_r = oracle.ref_tree(4, 0.7, 10, s)
+    loc_o = oracle.points_assign(4, s)
+    cnt_o = oracle.level_counts(loc_o, 4)
+    assert np.array_equal(loc_o, loc_r)
+    assert np.array_equal(cnt_o, cnt_r)
+    assert np.array_equal(oracle.tree_traverse(4, 0.7, 10, cnt_o), pairs_r)
+    assert (loc_r[-1] < 0).sum() > 0  # the reference drops particles on tree edges
+
+
+@need_ref
 def test_tree_moved_particles_vs_reference(oracle):
     """Off-grid particles (as after time steps), including edge cases."""
     s, a, _ = oracle.icos_state(4)

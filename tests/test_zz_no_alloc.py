@@ -3,13 +3,12 @@ device memory (real-time loops where cudaMalloc/cudaFree could stall the
 device; plugins whose host application owns the device memory budget).
 
 The caller owns every buffer (here torch tensors stand in for the caller's
-memory); the entry point must agree with the allocating fss_rhs_direct to the
-mixed-precision tolerance used throughout the tests, on two calls in a row
-that share its fixed scratch array, and refuse sizes beyond its limit.
-This file is collected last on purpose.
+memory).  The entry point must agree with the FP64 oracle (rhs_eval.h:15-56)
+and with the allocating fss_rhs_direct to the mixed-precision tolerance used
+throughout the tests, on two calls in a row that share its fixed scratch
+array; it must take no device memory once its module is loaded; and it must
+refuse sizes beyond its limit.  This file is collected last on purpose.
 """
-import ctypes
-
 import numpy as np
 import pytest
 
@@ -42,6 +41,29 @@ def test_noalloc_matches_allocating_entry_on_two_calls(fss):
         assert rel_l2(got[:, :3], expect[:, :3]) < 1e-6
         assert rel_l2(got[:, 3], expect[:, 3]) < 1e-6
         assert np.all(got[:, 4] == 0.0)
+
+
+def test_noalloc_matches_oracle_and_takes_no_memory(fss, oracle):
+    import torch
+    dev = torch.device("cuda", 0)
+    state, area = fss.make_state(4, "rh_vortices", n_vortex=8, seed=5)
+    n = state.shape[0]
+    want = oracle.rhs_direct(state, area)
+    s_d = torch.from_numpy(state).to(dev)
+    a_d = torch.from_numpy(area).to(dev)
+    outs = [torch.full((n, 5), float("nan"), dtype=torch.float64, device=dev) for _ in range(2)]
+    torch.cuda.synchronize()
+    fss.rhs_direct_noalloc(n, s_d.data_ptr(), a_d.data_ptr(), outs[0].data_ptr(), None)  # loads the module
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    fss.rhs_direct_noalloc(n, s_d.data_ptr(), a_d.data_ptr(), outs[1].data_ptr(), None)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(dev)[0] == free0
+    for o in outs:
+        got = o.cpu().numpy()
+        assert rel_l2(got[:, :3], want[:, :3]) < 1e-6
+        assert rel_l2(got[:, 3], want[:, 3]) < 1e-6
+    assert np.array_equal(outs[0].cpu().numpy(), outs[1].cpu().numpy())
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit(fss):
