@@ -50,6 +50,14 @@ struct fss_ctx {
     bool fp64 = false;
     bool tree = true;
     bool resort = false;  // re-sort particles into their current leaves every RK4 step
+    // one problem sharded over ranks (shard_nranks == 0: not sharded): this
+    // rank's targets are units [shard_bounds[rank], shard_bounds[rank + 1]) --
+    // faces of level shard_unit_level (treecode) or blocks of target rows
+    // (direct sum) -- i.e. leaves or rows [shard_lo, shard_hi)
+    int shard_rank = 0, shard_nranks = 0, shard_unit_level = 0;
+    int64_t shard_lo = 0, shard_hi = 0;
+    std::vector<int64_t> shard_bounds;
+    std::vector<double> shard_cost;
     uint64_t wait_ns = 0;  // limit of the pair kernel's bounded waits
     int hold_block = -1;   // test hook: block of the next target-leaf launch that withholds a tile
 

@@ -150,7 +150,20 @@ int build_direct_lists(fss_ctx* c) {
     ListOutput& L = c->lists;
     L = ListOutput();
     for (int p = 0; p < P; p++) L.segs.push_back(Segment{1, int32_t(n * p / P), int32_t(n * (p + 1) / P), 0});
-    for (int64_t t = 0; t < tiles; t++) {
+    // sharded: this rank's blocks of target rows (direct_sum_mpi.cpp:74-82
+    // splits the rows over ranks in equal blocks)
+    int64_t t_lo = 0, t_hi = tiles;
+    if (c->shard_nranks > 0) {
+        c->shard_unit_level = 0;
+        c->shard_cost.assign(size_t(tiles), 0.0);
+        for (int64_t t = 0; t < tiles; t++) c->shard_cost[t] = double(std::min<int64_t>(TB, n - t * TB)) * double(n - 1);
+        c->shard_bounds = shard_partition(c->shard_cost, c->shard_nranks);
+        t_lo = c->shard_bounds[c->shard_rank];
+        t_hi = c->shard_bounds[c->shard_rank + 1];
+        c->shard_lo = t_lo * TB;
+        c->shard_hi = std::min<int64_t>(n, t_hi * TB);
+    }
+    for (int64_t t = t_lo; t < t_hi; t++) {
         const int64_t t0 = t * TB, nt = std::min<int64_t>(TB, n - t0);
         for (int p = 0; p < P; p++) {
             L.items.push_back(WorkItem{int32_t(t0), int32_t(nt), p, p + 1, p, -1});
@@ -158,7 +171,7 @@ int build_direct_lists(fss_ctx* c) {
         }
     }
     L.n_leaf_items = int64_t(L.items.size());
-    L.pp_pairs = double(n) * double(n - 1);
+    L.pp_pairs = double(c->shard_nranks > 0 ? c->shard_hi - c->shard_lo : n) * double(n - 1);
     c->direct_pairs = L.pp_pairs;
     TRY(upload(c, c->segs, L.segs));
     TRY(upload(c, c->items, L.items));
@@ -192,6 +205,66 @@ void make_alists(fss_ctx* c, const std::vector<int32_t>& dual_counts) {
     const int many = (c->cfg.many_count < 0) ? nproxy(c->cfg.degree) : c->cfg.many_count;
     c->alists = lists_from_pairs(c->geom, LL, dual_traverse(c->geom, cc, c->cfg.theta, many), many, c->cfg.degree,
                                  c->cfg.cluster_targets ? &c->tlists : nullptr);
+}
+
+// The lists of the current tree: the reference's pair list as built (static
+// tree, complete assignment, dual lists) or those of the configured mode.
+void make_lists(fss_ctx* c) {
+    const int LL = c->leaf_level;
+    const int many = (c->cfg.many_count < 0) ? nproxy(c->cfg.degree) : c->cfg.many_count;
+    if (c->cfg.list_mode == FSS_LIST_DUAL && !c->resort && c->cfg.assign_mode != FSS_ASSIGN_REFERENCE) {
+        c->tlists.clear();
+        c->alists = lists_from_pairs(c->geom, LL, c->pairs, many, c->cfg.degree,
+                                     c->cfg.cluster_targets ? &c->tlists : nullptr);
+    } else {
+        make_alists(c, c->counts_h);
+    }
+}
+
+// Sharded treecode: the units are the faces of the shallowest level holding
+// a target cluster (every target cluster and the downward pass below it then
+// lie within one unit), or the leaves; each unit costs the interactions of
+// its target leaves and clusters at the build's counts.  The ranks take
+// contiguous unit ranges of near-equal cost (every rank computes the same
+// plan from the same tree), and this rank keeps the source lists of its own
+// leaves and clusters only.
+int shard_filter(fss_ctx* c) {
+    if (c->shard_nranks <= 0) return FSS_OK;
+    const int LL = c->leaf_level;
+    int u = LL;
+    for (const TList& t : c->tlists) u = std::min(u, int(t.level));
+    const int64_t nunits = int64_t(20) << (2 * u);
+    if (nunits < c->shard_nranks)
+        return fail(c, FSS_ERR_INVALID, "more ranks than units (faces of level " + std::to_string(u) + ")");
+    auto count = [&](const ASrc& a) -> double {
+        return a.proxy ? double(nproxy(a.deg)) : double(c->counts_h[c->geom.lev_off[a.level] + a.node]);
+    };
+    std::vector<double> cost(size_t(nunits), 0.0);
+    for (int64_t lf = 0; lf < c->nleaf; lf++) {
+        double sc = 0;
+        for (const ASrc& a : c->alists[lf]) sc += count(a);
+        cost[size_t(lf >> (2 * (LL - u)))] += double(c->leaf_start_h[lf + 1] - c->leaf_start_h[lf]) * sc;
+    }
+    for (const TList& t : c->tlists) {
+        double sc = 0;
+        for (const ASrc& a : t.src) sc += count(a);
+        cost[size_t(t.node >> (2 * (t.level - u)))] += double(nproxy(t.deg)) * sc;
+    }
+    c->shard_unit_level = u;
+    c->shard_cost = cost;
+    c->shard_bounds = shard_partition(cost, c->shard_nranks);
+    const int64_t u0 = c->shard_bounds[c->shard_rank], u1 = c->shard_bounds[c->shard_rank + 1];
+    c->shard_lo = u0 << (2 * (LL - u));
+    c->shard_hi = u1 << (2 * (LL - u));
+    for (int64_t lf = 0; lf < c->nleaf; lf++)
+        if (lf < c->shard_lo || lf >= c->shard_hi) c->alists[lf].clear();
+    std::vector<TList> own;
+    for (TList& t : c->tlists) {
+        const int64_t unit = t.node >> (2 * (t.level - u));
+        if (unit >= u0 && unit < u1) own.push_back(std::move(t));
+    }
+    c->tlists = std::move(own);
+    return FSS_OK;
 }
 
 int ensure_particle_buffers(fss_ctx* c, int64_t n) {
@@ -350,13 +423,8 @@ int build_tree(fss_ctx* c) {
     // the reference-format pair list (fss_get_tree) of this build
     c->pairs = dual_traverse(c->geom, (c->cfg.assign_mode == FSS_ASSIGN_REFERENCE) ? ref_counts : c->counts_h,
                              c->cfg.theta, many);
-    if (c->cfg.list_mode == FSS_LIST_DUAL && !c->resort && c->cfg.assign_mode != FSS_ASSIGN_REFERENCE) {
-        c->tlists.clear();
-        c->alists = lists_from_pairs(c->geom, LL, c->pairs, many, c->cfg.degree,
-                                     c->cfg.cluster_targets ? &c->tlists : nullptr);
-    } else {
-        make_alists(c, c->counts_h);
-    }
+    make_lists(c);
+    TRY(shard_filter(c));
     TRY(materialize(c, choose_shape(c)));
     return FSS_OK;
 }
@@ -473,8 +541,10 @@ int launch_all_pairs(fss_ctx* c, bool want_psi) {
     return launch_cluster_pairs(c, c->stream, want_psi);
 }
 
-// One right-hand side on the current stage state (xs/src).
-int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
+// The partial sums of one right-hand side on the current stage state
+// (xs/src): every pair launch and the downward pass, joined on the
+// context's stream; *down is set when the downward pass wrote its slot.
+int eval_partials(fss_ctx* c, bool want_psi, bool* down_out) {
     // With target clusters, the target-leaf pair launch (compute-bound) runs
     // on the side stream beside the chain upward pass -> target-cluster
     // pairs -> downward pass (mostly latency-bound); it waits for the upward
@@ -545,6 +615,14 @@ int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
         CU(cudaEventRecord(c->ev_join, c->side));
         CU(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     }
+    *down_out = down;
+    return FSS_OK;
+}
+
+// One right-hand side on the current stage state (xs/src).
+int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
+    bool down = false;
+    TRY(eval_partials(c, want_psi, &down));
     if (want_psi) launch_wsum(c->stream, c->n, c->xs.as<double4>(), c->area_s.as<double>(), c->wtotal.as<double>());
     ea.n = c->n;
     ea.parts = c->parts + (down ? 1 : 0);
@@ -722,6 +800,7 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 int internal_relist(fss_ctx* c) {
     invalidate_graph(c);
     make_alists(c, c->counts_h);
+    TRY(shard_filter(c));
     TRY(materialize(c, choose_shape(c)));
     c->stage_dirty = true;
     TRY(refresh_stage(c));
@@ -1119,6 +1198,114 @@ int fss_tree_geometry(int32_t tree_levels, double* tri_info) {
         return fail(nullptr, FSS_ERR_INVALID, "bad tree_levels");
     TreeGeometry g = build_tree_geometry(tree_levels);
     std::memcpy(tri_info, g.tri_info.data(), sizeof(double) * 4 * g.lev_off[tree_levels]);
+    return FSS_OK;
+}
+
+// ------------------------------------------------------------------ sharding
+
+int fss_shard_partition(int64_t nunits, const double* cost, int32_t nranks, int64_t* bounds) {
+    if (nunits < 1 || nranks < 1 || !cost || !bounds) return fail(nullptr, FSS_ERR_INVALID, "bad partition arguments");
+    if (nranks > nunits) return fail(nullptr, FSS_ERR_INVALID, "more ranks than units");
+    const std::vector<int64_t> b = shard_partition(std::vector<double>(cost, cost + nunits), nranks);
+    std::memcpy(bounds, b.data(), sizeof(int64_t) * b.size());
+    return FSS_OK;
+}
+
+int fss_shard_set(fss_ctx* c, int32_t rank, int32_t nranks) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    if (nranks < 0 || (nranks > 0 && (rank < 0 || rank >= nranks))) return fail(c, FSS_ERR_INVALID, "bad rank");
+    CU(cudaSetDevice(c->dev));
+    invalidate_graph(c);
+    c->shard_rank = nranks > 0 ? rank : 0;
+    c->shard_nranks = nranks;
+    c->shard_bounds.clear();
+    c->shard_cost.clear();
+    c->shard_lo = 0;
+    c->shard_hi = c->tree ? c->nleaf : c->n;
+    if (!c->have) return FSS_OK;  // applied when the particles are set
+    if (c->tree) {
+        make_lists(c);
+        TRY(shard_filter(c));
+        TRY(materialize(c, c->shape));
+    } else {
+        TRY(build_direct_lists(c));
+    }
+    c->stage_dirty = true;
+    TRY(refresh_stage(c));
+    return check_device_error(c);
+}
+
+int fss_shard_get_info(fss_ctx* c, fss_shard_info* info) {
+    if (!c || !info) return fail(c, FSS_ERR_INVALID, "null argument");
+    std::memset(info, 0, sizeof(*info));
+    info->rank = c->shard_rank;
+    info->nranks = c->shard_nranks;
+    if (c->shard_nranks <= 0 || c->shard_bounds.empty()) return FSS_OK;
+    info->unit_level = c->tree ? c->shard_unit_level : -1;
+    info->units = int64_t(c->shard_cost.size());
+    info->unit_lo = c->shard_bounds[c->shard_rank];
+    info->unit_hi = c->shard_bounds[c->shard_rank + 1];
+    info->target_lo = c->shard_lo;
+    info->target_hi = c->shard_hi;
+    for (size_t u = 0; u < c->shard_cost.size(); u++) {
+        info->cost_total += c->shard_cost[u];
+        if (int64_t(u) >= info->unit_lo && int64_t(u) < info->unit_hi) info->cost_own += c->shard_cost[u];
+    }
+    return FSS_OK;
+}
+
+int fss_shard_stage(fss_ctx* c, int32_t stage, void* exchange) {
+    if (!c || !exchange) return fail(c, FSS_ERR_INVALID, "null argument");
+    if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    if (c->shard_nranks <= 0) return fail(c, FSS_ERR_STATE, "context not sharded (fss_shard_set)");
+    if (stage < 1 || stage > 4) return fail(c, FSS_ERR_INVALID, "stage must be 1..4");
+    CU(cudaSetDevice(c->dev));
+    if (stage == 1) {
+        TRY(refresh_stage(c));
+        if (c->tree && c->resort) TRY(resort(c));
+    }
+    bool down = false;
+    TRY(eval_partials(c, false, &down));
+    {
+        ProfScope ps(c, "shard_reduce");
+        launch_shard_reduce(c->stream, c->n, c->parts + (down ? 1 : 0), c->pstride, c->partials.as<double4>(),
+                            c->tree ? c->leaf_start.as<int32_t>() : nullptr, c->shard_lo, c->shard_hi, c->shard_lo,
+                            c->shard_hi, static_cast<double4*>(exchange));
+    }
+    CU(cudaGetLastError());
+    return FSS_OK;
+}
+
+int fss_shard_combine(fss_ctx* c, int32_t stage, double dt, double omega, const void* exchange) {
+    if (!c || !exchange) return fail(c, FSS_ERR_INVALID, "null argument");
+    if (!c->have) return fail(c, FSS_ERR_STATE, "no particles set");
+    if (c->shard_nranks <= 0) return fail(c, FSS_ERR_STATE, "context not sharded (fss_shard_set)");
+    if (stage < 1 || stage > 4) return fail(c, FSS_ERR_INVALID, "stage must be 1..4");
+    CU(cudaSetDevice(c->dev));
+    EpiArgs ea;
+    ea.mode = EPI_RK4;
+    ea.stage = stage;
+    ea.dt = dt;
+    ea.omega = omega;
+    ea.s0 = c->s0.as<double4>();
+    ea.acc = c->acc.as<double4>();
+    ea.n = c->n;
+    ea.parts = 1;
+    ea.pstride = c->n;
+    ea.partials = static_cast<const double4*>(exchange);
+    ea.xs = c->xs.as<double4>();
+    ea.area = c->area_s.as<double>();
+    ea.wtotal = c->wtotal.as<double>();
+    ea.perm = c->tree ? c->perm.as<int32_t>() : nullptr;
+    ea.src = c->src.p;
+    ea.leaf_of = nullptr;
+    ea.frame = nullptr;
+    {
+        ProfScope ps(c, "epilogue");
+        launch_epilogue(c->stream, c->fp64, ea);
+    }
+    CU(cudaGetLastError());
+    if (c->prof && stage == 4) prof_resolve(c);
     return FSS_OK;
 }
 

@@ -163,6 +163,34 @@ __global__ void k_epilogue(EpiArgs a) {
     static_cast<typename Vec4<T>::type*>(a.src)[s] = o;
 }
 
+// One rank's share of a sharded right-hand side: the partial slots of its own
+// targets -- rows [lo, hi) of the sorted order, read through leaf_start when
+// given (leaves [leaf_lo, leaf_hi): particles are re-sorted every step) --
+// summed in the epilogue's order, and -0.0 in every other row.  Summing the
+// buffers of all ranks then gives every row exactly, in any order
+// (x + -0.0 = x, and a sum started from +0.0 is never -0.0).
+__global__ void k_shard_reduce(int64_t n, int parts, int64_t pstride, const double4* __restrict__ partials,
+                               const int32_t* __restrict__ leaf_start, int64_t leaf_lo, int64_t leaf_hi,
+                               int64_t row_lo, int64_t row_hi, double4* __restrict__ out) {
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int64_t lo = row_lo, hi = row_hi;
+    if (leaf_start) {
+        lo = leaf_start[leaf_lo];
+        hi = leaf_start[leaf_hi];
+    }
+    if (s < lo || s >= hi) {
+        out[s] = make_double4(-0.0, -0.0, -0.0, -0.0);
+        return;
+    }
+    double Ax = 0, Ay = 0, Az = 0, Ap = 0;
+    for (int p = 0; p < parts; p++) {
+        const double4 v = partials[int64_t(p) * pstride + s];
+        Ax += v.x; Ay += v.y; Az += v.z; Ap += v.w;
+    }
+    out[s] = make_double4(Ax, Ay, Az, Ap);
+}
+
 // Stage state and interaction sources from the step state (after a
 // stand-alone right-hand side overwrote them).
 template <typename T>
@@ -416,6 +444,14 @@ void launch_epilogue(cudaStream_t st, bool fp64, const EpiArgs& a) {
         k_epilogue<double><<<g, 256, 0, st>>>(a);
     else
         k_epilogue<float><<<g, 256, 0, st>>>(a);
+}
+
+void launch_shard_reduce(cudaStream_t st, int64_t n, int parts, int64_t pstride, const double4* partials,
+                         const int32_t* leaf_start, int64_t leaf_lo, int64_t leaf_hi, int64_t row_lo, int64_t row_hi,
+                         double4* out) {
+    if (n == 0) return;
+    k_shard_reduce<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, parts, pstride, partials, leaf_start, leaf_lo,
+                                                              leaf_hi, row_lo, row_hi, out);
 }
 
 void launch_refresh(cudaStream_t st, bool fp64, int64_t n, const double4* s0, const double* area,

@@ -119,6 +119,12 @@ struct DownArgs {
 void launch_down(cudaStream_t st, bool psi, const DownArgs& d);
 int down_launch_count(const DownArgs& d);
 void launch_epilogue(cudaStream_t st, bool fp64, const EpiArgs& a);
+// Sharded RHS: this rank's rows (leaves [leaf_lo, leaf_hi) through
+// leaf_start, or rows [row_lo, row_hi) when leaf_start is null) summed over
+// the partial slots into out, -0.0 in the other rows.
+void launch_shard_reduce(cudaStream_t st, int64_t n, int parts, int64_t pstride, const double4* partials,
+                         const int32_t* leaf_start, int64_t leaf_lo, int64_t leaf_hi, int64_t row_lo, int64_t row_hi,
+                         double4* out);
 void launch_refresh(cudaStream_t st, bool fp64, int64_t n, const double4* s0, const double* area,
                     const uint32_t* leaf_of, const double4* frame, double4* xs, void* src);
 void launch_wsum(cudaStream_t st, int64_t n, const double4* xs, const double* area, double* w);

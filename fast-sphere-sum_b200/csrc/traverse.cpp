@@ -374,6 +374,76 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
     }
 }
 
+// ---------------------------------------------------------------- sharding
+
+std::vector<int64_t> shard_partition(const std::vector<double>& cost_in, int nranks) {
+    const int64_t U = int64_t(cost_in.size());
+    std::vector<double> cost(cost_in.size());
+    double total = 0, biggest = 0;
+    for (int64_t i = 0; i < U; i++) {
+        cost[i] = std::max(cost_in[i], 0.0);
+        total += cost[i];
+        biggest = std::max(biggest, cost[i]);
+    }
+    if (!(total > 0)) {
+        std::fill(cost.begin(), cost.end(), 1.0);
+        total = double(U);
+        biggest = 1.0;
+    }
+    // ranges a greedy left-to-right fill needs when no range may exceed t
+    auto greedy = [&](double t, std::vector<int64_t>* cuts) {
+        int64_t ranges = 1;
+        double acc = 0;
+        if (cuts) cuts->assign(1, 0);
+        for (int64_t i = 0; i < U; i++) {
+            if (acc + cost[i] > t && acc > 0) {
+                ranges++;
+                acc = 0;
+                if (cuts) cuts->push_back(i);
+            }
+            acc += cost[i];
+        }
+        if (cuts) cuts->push_back(U);
+        return ranges;
+    };
+    // the least bound on a range's cost that nranks ranges can meet
+    double lo = std::max(biggest, total / nranks), hi = total;
+    for (int it = 0; it < 100 && hi - lo > 1e-12 * total; it++) {
+        const double mid = 0.5 * (lo + hi);
+        if (greedy(mid, nullptr) <= nranks) hi = mid; else lo = mid;
+    }
+    std::vector<int64_t> b;
+    greedy(hi, &b);
+    // fewer ranges than ranks: split the costliest range of two or more units
+    // at its cost midpoint until every rank has one (when units allow)
+    while (int64_t(b.size()) - 1 < nranks) {
+        int best = -1;
+        double best_cost = -1;
+        for (size_t r = 0; r + 1 < b.size(); r++) {
+            if (b[r + 1] - b[r] < 2) continue;
+            double c = 0;
+            for (int64_t i = b[r]; i < b[r + 1]; i++) c += cost[i];
+            if (c > best_cost) {
+                best_cost = c;
+                best = int(r);
+            }
+        }
+        if (best < 0) {  // fewer units than ranks: empty ranges at the end
+            while (int64_t(b.size()) - 1 < nranks) b.push_back(U);
+            break;
+        }
+        double acc = 0;
+        int64_t k = b[best] + 1;
+        for (int64_t i = b[best]; i < b[best + 1] - 1; i++) {
+            acc += cost[i];
+            k = i + 1;
+            if (acc >= 0.5 * best_cost) break;
+        }
+        b.insert(b.begin() + best + 1, k);
+    }
+    return b;
+}
+
 // ---------------------------------------------------------------- interpolation
 
 void interp_nodes(int n, std::vector<double>& nodes, std::vector<double>& vinv) {

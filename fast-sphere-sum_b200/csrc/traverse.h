@@ -112,6 +112,12 @@ std::vector<std::vector<ASrc>> lists_per_leaf(const TreeGeometry& g, int leaf_le
 void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& lists,
                  const std::vector<TList>& clusters, ListOutput& out);
 
+// Contiguous ranges of units for nranks ranks with near-equal summed cost:
+// bounds[r] .. bounds[r + 1] for rank r (nranks + 1 entries, bounds[0] = 0,
+// bounds[nranks] = cost.size()); every rank gets at least one unit when
+// there are enough; uniform costs when they sum to zero.
+std::vector<int64_t> shard_partition(const std::vector<double>& cost, int nranks);
+
 // Proxy node set: barycentric interpolation points of degree n on a
 // triangle (Blyth-Pozrikidis construction on Chebyshev-Lobatto points) and
 // the inverse of the Vandermonde matrix of the Chebyshev product basis

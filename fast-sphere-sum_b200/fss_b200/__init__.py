@@ -44,6 +44,12 @@ class Config(C.Structure):
                 ("reserved", C.c_int32 * 3)]
 
 
+class ShardInfo(C.Structure):
+    _fields_ = [("rank", C.c_int32), ("nranks", C.c_int32), ("unit_level", C.c_int32), ("pad", C.c_int32),
+                ("units", C.c_int64), ("unit_lo", C.c_int64), ("unit_hi", C.c_int64), ("target_lo", C.c_int64),
+                ("target_hi", C.c_int64), ("cost_total", C.c_double), ("cost_own", C.c_double)]
+
+
 class TreeInfo(C.Structure):
     _fields_ = [("tree_levels", C.c_int32), ("leaf_count", C.c_int32), ("degree", C.c_int32),
                 ("n_proxy", C.c_int32), ("n_pairs", C.c_int64), ("n_list_entries", C.c_int64),
@@ -81,7 +87,8 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_ensemble_info", "fss_ensemble_time_pairs", "fss_amr_create", "fss_amr_destroy", "fss_amr_counts", "fss_amr_refine",
            "fss_amr_get_mesh", "fss_amr_remesh", "fss_amr_refine_current", "fss_remesh_lists", "fss_state_csv_append",
            "fss_point_count_append", "fss_output_name", "fss_state_bin_append", "fss_state_bin_read",
-           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_test_hold_tile", "fss_version"]
+           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_test_hold_tile", "fss_shard_partition", "fss_shard_set", "fss_shard_get_info",
+           "fss_shard_stage", "fss_shard_combine", "fss_version"]
 
 NOALLOC_MAX_PARTICLES = 262144  # FSS_NOALLOC_MAX_PARTICLES in include/fss.h
 
@@ -158,6 +165,11 @@ def lib():
     L.fss_read_vert_tris_csv.argtypes = [C.c_char_p, C.c_char_p, _i64, _I32, _I32, _i64]
     L.fss_version.restype = C.c_char_p
     L.fss_test_hold_tile.argtypes = [_vp, C.c_int32]
+    L.fss_shard_partition.argtypes = [_i64, _D, C.c_int32, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+    L.fss_shard_set.argtypes = [_vp, C.c_int32, C.c_int32]
+    L.fss_shard_get_info.argtypes = [_vp, P(ShardInfo)]
+    L.fss_shard_stage.argtypes = [_vp, C.c_int32, _vp]
+    L.fss_shard_combine.argtypes = [_vp, C.c_int32, C.c_double, C.c_double, _vp]
     _lib = L
     return L
 
@@ -414,11 +426,40 @@ class Context:
         self._c(lib().fss_work_per_rhs(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def shard(self, rank, nranks):
+        """Make this context rank `rank` of `nranks` of one sharded problem
+        (fss_shard_set; nranks = 0 undoes it)."""
+        self._c(lib().fss_shard_set(self.h, rank, nranks))
+
+    def shard_info(self):
+        i = ShardInfo()
+        self._c(lib().fss_shard_get_info(self.h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in ShardInfo._fields_ if k != "pad"}
+
+    def shard_stage(self, stage, exchange):
+        """Stage `stage` for this rank's targets into the exchange buffer (a
+        device pointer, or a tensor with data_ptr())."""
+        ptr = exchange if isinstance(exchange, int) else exchange.data_ptr()
+        self._c(lib().fss_shard_stage(self.h, stage, ptr))
+
+    def shard_combine(self, stage, dt, exchange, omega=OMEGA):
+        ptr = exchange if isinstance(exchange, int) else exchange.data_ptr()
+        self._c(lib().fss_shard_combine(self.h, stage, dt, omega, ptr))
+
     def test_hold_tile(self, block=0):
         """Test hook: the next evaluation's target-leaf pair block `block`
         withholds its first source tile, so that its bounded waits run out
         (fss_test_hold_tile)."""
         self._c(lib().fss_test_hold_tile(self.h, block))
+
+
+def shard_partition(cost, nranks):
+    """Contiguous unit ranges of near-equal cost (host only): bounds[r] ..
+    bounds[r + 1] for rank r."""
+    cost = np.ascontiguousarray(cost, dtype=np.float64)
+    b = np.zeros(nranks + 1, dtype=np.int64)
+    _check(lib().fss_shard_partition(cost.size, cost, nranks, b))
+    return b
 
 
 def rhs_direct_noalloc(n, state5_dev_ptr, area_dev_ptr, out5_dev_ptr, stream_handle=None, omega=OMEGA):

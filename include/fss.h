@@ -450,6 +450,58 @@ int fss_selector_apply(fss_ctx* ctx, fss_mlp* m, const float* feat_mean, const f
 int fss_rhs_direct_noalloc(int64_t n, const double* state5, const double* area, double omega, double* modify5,
                            void* stream);
 
+/* ------------------------------------------------------------ sharding
+ * One problem split over several GPUs, one process per GPU.  The reference
+ * splits the same work over MPI ranks: fast_sum_mpi.cpp:322-338 gives each
+ * rank a range of top-level target faces, direct_sum_mpi.cpp:74-82 a block
+ * of target rows, and mpi_utils.h:6-26 replicates the whole state again after
+ * every RK stage.  Here every rank holds the whole state and builds the same
+ * tree; it evaluates the right-hand side for its own targets only: a
+ * contiguous range of units -- the faces of the shallowest level that holds
+ * a target cluster, or the leaves (treecode); blocks of target rows (direct
+ * sum) -- balanced by their counted interactions, so that every target
+ * cluster and its downward pass lie with one rank.  Per RK stage the ranks
+ * exchange one device buffer of N x 4 doubles (the context's particle order):
+ * a rank writes the velocity sums of its own rows and -0.0 in every other
+ * row; the caller sums the buffers over the ranks (an all-reduce, e.g. NCCL
+ * through torch.distributed: x + -0.0 = x, so the sum is exact in any order);
+ * then every rank advances all particles identically.  One RK4 step:
+ *
+ *   for stage in 1..4:
+ *       fss_shard_stage(ctx, stage, exchange);             this rank's targets
+ *       all-reduce (sum) of exchange over the ranks;       the caller's collective
+ *       fss_shard_combine(ctx, stage, dt, omega, exchange);
+ *
+ * Each stage's launches go to the context's stream; the caller orders its
+ * collective after them (same stream, or an event).  With the same source
+ * split (src_parts) and degrees, the result equals an unsharded context's
+ * bit for bit.  No TMA load reads another GPU's memory: the exchange buffer
+ * is local and the collective belongs to the caller. */
+
+/* Contiguous unit ranges of near-equal summed cost: bounds[r] ..
+ * bounds[r + 1] for rank r (nranks + 1 entries).  Host only. */
+int fss_shard_partition(int64_t nunits, const double* cost, int32_t nranks, int64_t* bounds);
+/* Make the context rank `rank` of `nranks` (0 ranks: not sharded); applies
+ * to the current particles and to later builds. */
+int fss_shard_set(fss_ctx* ctx, int32_t rank, int32_t nranks);
+typedef struct fss_shard_info {
+    int32_t rank, nranks;
+    int32_t unit_level;            /* face level of the units (-1: direct-sum row blocks) */
+    int32_t pad;
+    int64_t units;                 /* units over all ranks */
+    int64_t unit_lo, unit_hi;      /* this rank's units */
+    int64_t target_lo, target_hi;  /* this rank's leaves (treecode) or rows (direct sum) */
+    double cost_total, cost_own;   /* counted interactions per RHS at the build */
+} fss_shard_info;
+int fss_shard_get_info(fss_ctx* ctx, fss_shard_info* info);
+/* Stage `stage` (1..4) of an RK4 step for this rank's targets (stage 1 first
+ * re-sorts the particles, as fss_rk4_step does): writes the exchange buffer
+ * (device, N x 4 doubles). */
+int fss_shard_stage(fss_ctx* ctx, int32_t stage, void* exchange);
+/* After the caller summed the exchange buffers of all ranks: the stage's
+ * combine and renormalisation for every particle. */
+int fss_shard_combine(fss_ctx* ctx, int32_t stage, double dt, double omega, const void* exchange);
+
 /* Test hook for the failure path (no counterpart in the reference, which has
  * no error path): in the next right-hand-side evaluation of this context,
  * block `block` of the target-leaf pair launch neither copies its first
