@@ -639,7 +639,7 @@ def main_shard(args, ws, rank, dev):
     from fss_b200 import shard
     state, area = fss.make_state(args.level, "rh_vortices", n_vortex=args.vortices, seed=args.seed)
     n = state.shape[0]
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(device=dev)   # every launch, the all-reduce and the events on it
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
     from fss_b200 import selector as _sel
     ctx = fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, list_mode=fss.LIST_LEAF,
@@ -651,15 +651,17 @@ def main_shard(args, ws, rank, dev):
     info = ctx.shard_info()
     ex = shard.exchange_buffer(ctx, f"cuda:{dev}")
     red = shard.torch_allreduce() if ws > 1 else None
+    torch.cuda.synchronize()
     shard.rk4_steps(ctx, ex, DT, nsteps=args.warmup, allreduce=red)
     torch.cuda.synchronize()
     barrier(ws)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for a, b in evs:
-        flush.zero_()
-        a.record(stream)
-        shard.rk4_steps(ctx, ex, DT, nsteps=1, allreduce=red)
-        b.record(stream)
+    with torch.cuda.stream(stream):
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            shard.rk4_steps(ctx, ex, DT, nsteps=1, allreduce=red)
+            b.record(stream)
     torch.cuda.synchronize()
     t = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs) / 1e3, ws)
     state_out = ctx.get_state()

@@ -905,6 +905,12 @@ int fss_set_stream(fss_ctx* c, void* s) {
     return FSS_OK;
 }
 
+int fss_get_stream(fss_ctx* c, void** s) {
+    if (!c || !s) return fail(c, FSS_ERR_INVALID, "null argument");
+    *s = static_cast<void*>(c->stream);
+    return FSS_OK;
+}
+
 int fss_set_particles(fss_ctx* c, int64_t n, const double* state5, const double* area) {
     if (!c) return fail(c, FSS_ERR_INVALID, "null context");
     CU(cudaSetDevice(c->dev));
@@ -1006,6 +1012,32 @@ int fss_rhs_current(fss_ctx* c, double omega, double* modify5, double* psi) {
     return check_device_error(c);
 }
 
+namespace {
+// Pair evaluations the consumer lanes of a pair launch perform on items
+// [i0, i1) with `targets` consumer threads per block: per chunk of targets,
+// every active warp evaluates every source of the item (padded to whole
+// quads), whether or not each of its lanes holds a target.
+double lane_pairs(const fss_ctx* c, int64_t i0, int64_t i1, int targets) {
+    const ListOutput& L = c->lists;
+    double sum = 0;
+    for (int64_t i = i0; i < i1; i++) {
+        const WorkItem& it = L.items[i];
+        double src = 0;
+        for (int g = it.g0; g < it.g1; g++) {
+            const Segment& sg = L.segs[g];
+            src += sg.kind == 0 ? double(c->leaf_start_h[sg.b] - c->leaf_start_h[sg.a]) : double(sg.b - sg.a);
+        }
+        src = 4.0 * std::ceil(src / 4.0);
+        const int nt = it.leaf >= 0 ? c->leaf_start_h[it.leaf + 1] - c->leaf_start_h[it.leaf] : it.nt;
+        for (int c0 = 0; c0 < nt; c0 += targets) {
+            const int cn = std::min(targets, nt - c0);
+            sum += 32.0 * double((cn + 31) / 32) * src;
+        }
+    }
+    return sum;
+}
+}  // namespace
+
 int fss_get_tree_info(fss_ctx* c, fss_tree_info* info) {
     if (!c || !info) return fail(c, FSS_ERR_INVALID, "null argument");
     std::memset(info, 0, sizeof(*info));
@@ -1026,6 +1058,12 @@ int fss_get_tree_info(fss_ctx* c, fss_tree_info* info) {
     info->target_clusters = int32_t(c->lists.down.size());
     info->cp_interactions = c->lists.cp_pairs;
     info->cc_interactions = c->lists.cc_pairs;
+    if (c->tree && c->have) {
+        const int64_t nl = c->lists.n_leaf_items, na = int64_t(c->lists.items.size());
+        info->lane_pairs_leaf = lane_pairs(c, 0, nl, c->shape.targets());
+        if (na > nl)
+            info->lane_pairs_cluster = lane_pairs(c, nl, na, cluster_shape(c->fp64, c->lists.max_cluster_k).targets());
+    }
     return FSS_OK;
 }
 

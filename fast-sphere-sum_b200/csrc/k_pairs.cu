@@ -33,11 +33,16 @@ namespace fss {
 constexpr int kDepth = 4;  // ring depth (tiles in flight)
 constexpr int TILE_F32 = tile_capacity(false);
 
-template <typename T, bool PSI, bool GUARD>
-__device__ __forceinline__ void tile_pairs(const typename Vec4<T>::type* __restrict__ s, int cnt, T tx, T ty, T tz,
-                                           T& ax, T& ay, T& az, T& ap) {
-#pragma unroll 8
-    for (int j = 0; j < cnt; j++) {
+// Sources j = j0, j0 + step, ... < cnt of an FP64 tile (step 1: all of them).
+template <typename T, bool PSI, bool GUARD, bool STRIDED>
+__device__ __forceinline__ void tile_pairs(const typename Vec4<T>::type* __restrict__ s, int cnt, int j0, int step,
+                                           T tx, T ty, T tz, T& ax, T& ay, T& az, T& ap) {
+    if (!STRIDED) {
+        j0 = 0;
+        step = 1;
+    }
+#pragma unroll(STRIDED ? 2 : 8)
+    for (int j = j0; j < cnt; j += step) {
         const typename Vec4<T>::type q = s[j];
         const T dx = q.x - tx, dy = q.y - ty, dz = q.z - tz;
         const T r2 = fma(dz, dz, fma(dy, dy, dx * dx));
@@ -60,12 +65,17 @@ __device__ __forceinline__ void tile_pairs(const typename Vec4<T>::type* __restr
 // contribution).  One 128-bit shared load brings a component of four
 // sources; each pair of sources goes through the packed f32x2 pipe: per
 // four sources 4 shared loads, 18 packed operations and 4 reciprocals.
-template <bool PSI, bool GUARD>
-__device__ __forceinline__ void tile_pairs_soa(const float* __restrict__ s, int nquad, f2 ntx, f2 nty, f2 ntz,
-                                               f2& ax, f2& ay, f2& az, float& ap) {
+// Quads q = q0, q0 + step, ... < nquad of the tile (step 1: all of them).
+template <bool PSI, bool GUARD, bool STRIDED>
+__device__ __forceinline__ void tile_pairs_soa(const float* __restrict__ s, int nquad, int q0, int step, f2 ntx,
+                                               f2 nty, f2 ntz, f2& ax, f2& ay, f2& az, float& ap) {
     constexpr int T = TILE_F32;
+    if (!STRIDED) {
+        q0 = 0;
+        step = 1;
+    }
 #pragma unroll 2
-    for (int q = 0; q < nquad; q++) {
+    for (int q = q0; q < nquad; q += step) {
         const float4 X = reinterpret_cast<const float4*>(s)[q];
         const float4 Y = reinterpret_cast<const float4*>(s + T)[q];
         const float4 Z = reinterpret_cast<const float4*>(s + 2 * T)[q];
@@ -135,6 +145,18 @@ __device__ __forceinline__ void kahan_add(T& sum, T& comp, T x) {
     const T t = sum + y;
     comp = (t - sum) - y;
     sum = t;
+}
+
+// Sum over the L lanes of each group [L t, L t + L) of the warp (segmented
+// tree of shuffles, L warp-uniform); the group's first lane (sub = 0) holds
+// the sum.
+template <typename T>
+__device__ __forceinline__ T group_sum(T x, int sub, int L) {
+    for (int off = 1; off < L; off <<= 1) {
+        const T y = __shfl_down_sync(0xffffffffu, x, off);
+        if (sub + off < L) x += y;
+    }
+    return x;
 }
 
 // Producer side of the ring: warp 0 packs the next tile of a work item's
@@ -229,7 +251,6 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
     constexpr bool kPacked = sizeof(T) == 4;
     constexpr int kTargets = THREADS - 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int ct = tid - 32;  // consumer thread index (warps 1..)
     int t0 = it.t0, nt = it.nt;
     if (it.leaf >= 0) {
         t0 = leaf_start[it.leaf];
@@ -288,8 +309,19 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
             rs.consumed = rs.issued;
         } else {
             // ------------------------------------------------ consumers
-            const bool active = (warp - 1) * 32 < cn;
-            const S4 v = src[t0 + c0 + ((ct < cn) ? ct : 0)];
+            // consumer warp cw takes targets [32 cw, 32 cw + 32) of the chunk;
+            // the last, partial warp (r < 32 targets) gives every target
+            // L = 32 / r lanes, which split each tile's sources between them
+            // and add their sums by shuffles, so that few of its lanes compute
+            // for no target (a block's time per tile is set by its full warps)
+            const int cw = warp - 1;
+            const int r = min(32, cn - 32 * cw);
+            const bool active = r > 0;
+            const int L = (r > 0 && r < 32) ? 32 / r : 1;
+            const int tl = lane / L, sub = lane - tl * L;
+            const bool has_t = active && tl < r;
+            const int tgt = 32 * cw + tl;
+            const S4 v = src[t0 + c0 + (has_t ? tgt : 0)];
             T ax = 0, ay = 0, az = 0, ap = 0, sx = 0, sy = 0, sz = 0, sp = 0, cx = 0, cy = 0, cz = 0, cp = 0;
             f2 ntx = 0, nty = 0, ntz = 0;
             if (kPacked) {
@@ -309,26 +341,50 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
                 if (active && h.count > 0) {
                     if constexpr (kPacked) {
                         const float* tile = soa + slot * 4 * TILE;
+                        const int nq = (h.count + 3) >> 2;
                         f2 px = 0, py = 0, pz = 0;
                         float pw = 0.f;
-                        if (h.guard)
-                            tile_pairs_soa<PSI, true>(tile, (h.count + 3) >> 2, ntx, nty, ntz, px, py, pz, pw);
-                        else
-                            tile_pairs_soa<PSI, false>(tile, (h.count + 3) >> 2, ntx, nty, ntz, px, py, pz, pw);
+                        if (L == 1) {
+                            if (h.guard)
+                                tile_pairs_soa<PSI, true, false>(tile, nq, 0, 1, ntx, nty, ntz, px, py, pz, pw);
+                            else
+                                tile_pairs_soa<PSI, false, false>(tile, nq, 0, 1, ntx, nty, ntz, px, py, pz, pw);
+                        } else {
+                            if (h.guard)
+                                tile_pairs_soa<PSI, true, true>(tile, nq, sub, L, ntx, nty, ntz, px, py, pz, pw);
+                            else
+                                tile_pairs_soa<PSI, false, true>(tile, nq, sub, L, ntx, nty, ntz, px, py, pz, pw);
+                        }
                         float a0, a1;
                         f2_unpack(px, a0, a1);
-                        kahan_add(sx, cx, T(a0 + a1));
+                        float tx = a0 + a1;
                         f2_unpack(py, a0, a1);
-                        kahan_add(sy, cy, T(a0 + a1));
+                        float ty = a0 + a1;
                         f2_unpack(pz, a0, a1);
-                        kahan_add(sz, cz, T(a0 + a1));
+                        float tz = a0 + a1;
+                        if (L > 1) {
+                            tx = group_sum(tx, sub, L);
+                            ty = group_sum(ty, sub, L);
+                            tz = group_sum(tz, sub, L);
+                            if (PSI) pw = group_sum(pw, sub, L);
+                        }
+                        kahan_add(sx, cx, T(tx));
+                        kahan_add(sy, cy, T(ty));
+                        kahan_add(sz, cz, T(tz));
                         if (PSI) kahan_add(sp, cp, T(pw));
                     } else {
                         const S4* tile = ring + slot * TILE;
-                        if (h.guard)
-                            tile_pairs<T, PSI, true>(tile, h.count, v.x, v.y, v.z, ax, ay, az, ap);
-                        else
-                            tile_pairs<T, PSI, false>(tile, h.count, v.x, v.y, v.z, ax, ay, az, ap);
+                        if (L == 1) {
+                            if (h.guard)
+                                tile_pairs<T, PSI, true, false>(tile, h.count, 0, 1, v.x, v.y, v.z, ax, ay, az, ap);
+                            else
+                                tile_pairs<T, PSI, false, false>(tile, h.count, 0, 1, v.x, v.y, v.z, ax, ay, az, ap);
+                        } else {
+                            if (h.guard)
+                                tile_pairs<T, PSI, true, true>(tile, h.count, sub, L, v.x, v.y, v.z, ax, ay, az, ap);
+                            else
+                                tile_pairs<T, PSI, false, true>(tile, h.count, sub, L, v.x, v.y, v.z, ax, ay, az, ap);
+                        }
                     }
                 }
                 __syncwarp();
@@ -336,14 +392,20 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
                 rs.consumed++;
                 if (h.count == 0) break;
             }
-            if (!rs.failed && ct < cn) {
+            if (!kPacked && L > 1) {  // the FP64 path sums plainly: add the lanes' shares once
+                ax = group_sum(ax, sub, L);
+                ay = group_sum(ay, sub, L);
+                az = group_sum(az, sub, L);
+                if (PSI) ap = group_sum(ap, sub, L);
+            }
+            if (!rs.failed && has_t && sub == 0) {
                 double4 o;
                 if (kPacked)
                     o = make_double4(double(sx) - double(cx), double(sy) - double(cy), double(sz) - double(cz),
                                      double(sp) - double(cp));
                 else
                     o = make_double4(double(ax), double(ay), double(az), double(ap));
-                partials[int64_t(it.part) * pstride + t0 + c0 + ct] = o;
+                partials[int64_t(it.part) * pstride + t0 + c0 + tgt] = o;
             }
             rs.issued = rs.consumed;
         }

@@ -251,69 +251,73 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
     const int P = std::max(1, in.parts);
     struct Cost { double cost; WorkItem it; };
     std::vector<Cost> items;
-    std::vector<Segment> sg;
-    std::vector<double> est;  // sources per segment at the build
-    // segments of one source list for nt targets; `self_leaf` is the target
-    // leaf (-1 for a target cluster); returns pp and proxy pair counts
-    auto make_segments = [&](const std::vector<ASrc>& list, double nt, int64_t self_leaf, double& npp, double& npc) {
-        sg.clear();
+    // sources of every entry of one list for nt targets; `self_leaf` is the
+    // target leaf (-1 for a target cluster); returns pp and proxy pair counts
+    std::vector<double> est;
+    auto count_sources = [&](const std::vector<ASrc>& list, double nt, int64_t self_leaf, double& npp, double& npc) {
         est.clear();
         npp = npc = 0;
         for (const ASrc& a : list) {
-            const int64_t gf = g.lev_off[a.level] + a.node;
-            Segment e{};
             double cnt;
             if (a.proxy) {
-                e.kind = 1;
-                e.a = int32_t(in.n + slot[std::make_pair(gf, a.deg)]);
-                e.b = e.a + nproxy(a.deg);
                 cnt = nproxy(a.deg);
                 npc += nt * cnt;
             } else {
                 const int64_t span = int64_t(1) << (2 * (LL - a.level));
-                e.kind = 0;
-                e.a = int32_t(a.node * span);
-                e.b = int32_t((a.node + 1) * span);
-                // the particles of a face are contiguous in leaf order
-                const int32_t s0 = in.leaf_start[e.a], s1 = in.leaf_start[e.b];
-                cnt = s1 - s0;
-                const bool self = (self_leaf >= e.a && self_leaf < e.b);
+                const int32_t lo = int32_t(a.node * span), hi = int32_t((a.node + 1) * span);
+                cnt = in.leaf_start[hi] - in.leaf_start[lo];
+                const bool self = (self_leaf >= lo && self_leaf < hi);
                 npp += nt * cnt - (self ? nt : 0);
             }
-            if (!sg.empty() && sg.back().kind == e.kind && sg.back().b == e.a) {
-                sg.back().b = e.b;
-                est.back() += cnt;
-            } else {
-                sg.push_back(e);
-                est.push_back(cnt);
-            }
+            est.push_back(cnt);
         }
     };
-    // split the current segments into P parts of similar source counts and
-    // queue one item per part
-    auto add_items = [&](int32_t t0, int32_t nt_item, int32_t leaf, int nt_est) {
-        const int32_t base = int32_t(out.segs.size());
-        out.segs.insert(out.segs.end(), sg.begin(), sg.end());
+    // the list split into P parts of similar source counts -- cut between
+    // entries of the list itself, so that the cut does not depend on which
+    // proxy slots happen to be adjacent -- each part merged into segments (a
+    // face's particles as a kind-0 run over its leaves, adjacent ones merged;
+    // a face's proxies as a kind-1 run over its slots) and queued as one item
+    auto add_items = [&](const std::vector<ASrc>& list, int32_t t0, int32_t nt_item, int32_t leaf, int nt_est) {
         double total = 0;
         for (double c : est) total += c;
-        std::vector<int32_t> cut(P + 1, int32_t(sg.size()));
+        std::vector<size_t> cut(P + 1, list.size());
         cut[0] = 0;
         {
             double acc = 0;
             int p = 1;
-            for (size_t k = 0; k < sg.size() && p < P; k++) {
+            for (size_t k = 0; k < list.size() && p < P; k++) {
                 acc += est[k];
-                if (acc >= total * p / P) cut[p++] = int32_t(k + 1);
+                if (acc >= total * p / P) cut[p++] = k + 1;
             }
         }
         const int chunks = std::max(1, (nt_est + TB - 1) / TB);
         for (int p = 0; p < P; p++) {
+            const int32_t base = int32_t(out.segs.size());
             double w = 0;
-            for (int32_t k = cut[p]; k < cut[p + 1]; k++) w += est[k];
+            for (size_t k = cut[p]; k < cut[p + 1]; k++) {
+                const ASrc& a = list[k];
+                const int64_t gf = g.lev_off[a.level] + a.node;
+                Segment e{};
+                if (a.proxy) {
+                    e.kind = 1;
+                    e.a = int32_t(in.n + slot[std::make_pair(gf, a.deg)]);
+                    e.b = e.a + nproxy(a.deg);
+                } else {
+                    const int64_t span = int64_t(1) << (2 * (LL - a.level));
+                    e.kind = 0;
+                    e.a = int32_t(a.node * span);
+                    e.b = int32_t((a.node + 1) * span);
+                }
+                if (int32_t(out.segs.size()) > base && out.segs.back().kind == e.kind && out.segs.back().b == e.a)
+                    out.segs.back().b = e.b;
+                else
+                    out.segs.push_back(e);
+                w += est[k];
+            }
             out.n_tiles += int64_t(chunks) * (int64_t(w + in.tile - 1) / in.tile);
             // a block's run time follows its source count (its warps run
             // side by side), so the longest source lists go first
-            items.push_back({w * chunks, WorkItem{t0, nt_item, base + cut[p], base + cut[p + 1], p, leaf}});
+            items.push_back({w * chunks, WorkItem{t0, nt_item, base, int32_t(out.segs.size()), p, leaf}});
         }
     };
     auto flush_items = [&]() {
@@ -325,10 +329,10 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
         const int32_t nt = in.leaf_start[lf + 1] - in.leaf_start[lf];
         if (lists[lf].empty() || (nt == 0 && !in.all_leaves)) continue;
         double npp, npc;
-        make_segments(lists[lf], nt, lf, npp, npc);
+        count_sources(lists[lf], nt, lf, npp, npc);
         out.pp_pairs += npp;
         out.pc_pairs += npc;
-        add_items(0, 0, int32_t(lf), nt);
+        add_items(lists[lf], 0, 0, int32_t(lf), nt);
     }
     flush_items();
     out.n_leaf_items = int64_t(out.items.size());
@@ -344,10 +348,10 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
         const int64_t gf = g.lev_off[t.level] + t.node;
         const int32_t s0 = int32_t(in.n + slot[std::make_pair(gf, t.deg)]);
         double npp, npc;
-        make_segments(t.src, K, -1, npp, npc);
+        count_sources(t.src, K, -1, npp, npc);
         out.cp_pairs += npp;
         out.cc_pairs += npc;
-        add_items(s0, K, -1, K);
+        add_items(t.src, s0, K, -1, K);
         own_slot[gf] = s0;
         own_deg[gf] = t.deg;
         out.max_cluster_k = std::max(out.max_cluster_k, K);

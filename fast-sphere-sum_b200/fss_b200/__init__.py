@@ -56,7 +56,8 @@ class TreeInfo(C.Structure):
                 ("n_items", C.c_int64), ("n_tiles", C.c_int64), ("unassigned", C.c_int64), ("pp_interactions", C.c_double),
                 ("pc_interactions", C.c_double), ("block_threads", C.c_int32),
                 ("targets_per_thread", C.c_int32), ("src_parts", C.c_int32), ("target_clusters", C.c_int32),
-                ("cp_interactions", C.c_double), ("cc_interactions", C.c_double)]
+                ("cp_interactions", C.c_double), ("cc_interactions", C.c_double),
+                ("lane_pairs_leaf", C.c_double), ("lane_pairs_cluster", C.c_double)]
 
 
 def build():
@@ -87,7 +88,7 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_ensemble_info", "fss_ensemble_time_pairs", "fss_amr_create", "fss_amr_destroy", "fss_amr_counts", "fss_amr_refine",
            "fss_amr_get_mesh", "fss_amr_remesh", "fss_amr_refine_current", "fss_remesh_lists", "fss_state_csv_append",
            "fss_point_count_append", "fss_output_name", "fss_state_bin_append", "fss_state_bin_read",
-           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_test_hold_tile", "fss_shard_partition", "fss_shard_set", "fss_shard_get_info",
+           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_test_hold_tile", "fss_get_stream", "fss_shard_partition", "fss_shard_set", "fss_shard_get_info",
            "fss_shard_stage", "fss_shard_combine", "fss_version"]
 
 NOALLOC_MAX_PARTICLES = 262144  # FSS_NOALLOC_MAX_PARTICLES in include/fss.h
@@ -165,6 +166,7 @@ def lib():
     L.fss_read_vert_tris_csv.argtypes = [C.c_char_p, C.c_char_p, _i64, _I32, _I32, _i64]
     L.fss_version.restype = C.c_char_p
     L.fss_test_hold_tile.argtypes = [_vp, C.c_int32]
+    L.fss_get_stream.argtypes = [_vp, P(_vp)]
     L.fss_shard_partition.argtypes = [_i64, _D, C.c_int32, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
     L.fss_shard_set.argtypes = [_vp, C.c_int32, C.c_int32]
     L.fss_shard_get_info.argtypes = [_vp, P(ShardInfo)]
@@ -425,6 +427,12 @@ class Context:
         a, b = C.c_double(), C.c_double()
         self._c(lib().fss_work_per_rhs(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def stream_handle(self):
+        """The cudaStream_t the context launches on (an int)."""
+        h = _vp()
+        self._c(lib().fss_get_stream(self.h, C.byref(h)))
+        return h.value or 0
 
     def shard(self, rank, nranks):
         """Make this context rank `rank` of `nranks` of one sharded problem

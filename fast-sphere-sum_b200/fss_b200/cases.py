@@ -74,8 +74,13 @@ def main(argv=None):
                 out = ctx.rhs(s, area)
         info = ctx.tree_info()
     assert np.all(np.isfinite(out))
+    alg_leaf = info["pp_interactions"] + info["pc_interactions"]
+    alg_cl = info["cp_interactions"] + info["cc_interactions"]
     print(f"case={a.case} level={a.level} n={s.shape[0]} precision={a.precision} "
-          f"items={info['n_items']} wall={time.perf_counter() - t0:.3f}s")
+          f"items={info['n_items']} block={info['block_threads']} "
+          f"pairs_leaf={alg_leaf:.4g} lane_pairs_leaf={info['lane_pairs_leaf']:.4g} "
+          f"pairs_cluster={alg_cl:.4g} lane_pairs_cluster={info['lane_pairs_cluster']:.4g} "
+          f"wall={time.perf_counter() - t0:.3f}s")
 
 
 def ensemble_case(a):

@@ -35,14 +35,24 @@ def torch_allreduce(group=None):
 
 def rk4_steps(ctx, exchange, dt, nsteps=1, allreduce=None, omega=OMEGA):
     """`nsteps` RK4 steps of a sharded context: per stage its own targets,
-    one all-reduce of `exchange` (a torch tensor on the context's device, on
-    whose stream the context launches), then the combine for every particle.
-    With allreduce=None the buffer is used as it is (one rank)."""
+    one all-reduce of `exchange` (a torch tensor on the context's device),
+    then the combine for every particle.  The all-reduce is issued on the
+    stream the context launches on, so that it follows the stage's kernels
+    and precedes the combine.  With allreduce=None the buffer is used as it
+    is (one rank)."""
+    on_device = getattr(exchange, "is_cuda", False)
+    if on_device:
+        import torch
+        ctx_stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=exchange.device)
     for _ in range(nsteps):
         for stage in (1, 2, 3, 4):
             ctx.shard_stage(stage, exchange)
             if allreduce is not None:
-                allreduce(exchange)
+                if on_device:
+                    with torch.cuda.stream(ctx_stream):
+                        allreduce(exchange)
+                else:
+                    allreduce(exchange)
             ctx.shard_combine(stage, dt, exchange, omega)
 
 

@@ -133,6 +133,10 @@ void fss_destroy(fss_ctx* ctx);
 const char* fss_last_error(const fss_ctx* ctx);
 /* Launch stream for all later work (a cudaStream_t; NULL = the context's own). */
 int fss_set_stream(fss_ctx* ctx, void* cuda_stream);
+/* The stream the context launches on now (its own unless fss_set_stream gave
+ * one), for ordering the caller's work -- e.g. the collective of a sharded
+ * step -- after the context's. */
+int fss_get_stream(fss_ctx* ctx, void** cuda_stream);
 
 /* Upload a particle set (host, 5 doubles per particle, in the caller's order)
  * and, for the treecode, build the tree, as the reference does before its
@@ -289,6 +293,10 @@ typedef struct fss_tree_info {
     int32_t target_clusters; /* faces evaluated at interpolation points (cp/cc) */
     double cp_interactions;  /* interpolation point-particle pairs per RHS */
     double cc_interactions;  /* interpolation point-proxy pairs per RHS */
+    double lane_pairs_leaf;    /* pair evaluations the target-leaf launch's
+                                  consumer lanes perform per RHS at the build's
+                                  leaf counts, discarded lanes included */
+    double lane_pairs_cluster; /* the same for the target-cluster launch */
 } fss_tree_info;
 int fss_get_tree_info(fss_ctx* ctx, fss_tree_info* info);
 

@@ -24,7 +24,7 @@ CASES = [
 
 def run_sharded(fss, kw, s, a, nranks, steps, dt=0.01):
     import torch
-    st = torch.cuda.current_stream()
+    st = torch.cuda.Stream()               # a real stream (the legacy default would mean "the context's own")
     ctxs = []
     for r in range(nranks):
         c = fss.Context(**kw)
@@ -36,15 +36,16 @@ def run_sharded(fss, kw, s, a, nranks, steps, dt=0.01):
     bufs = [torch.empty((n, 4), dtype=torch.float64, device="cuda") for _ in range(nranks)]
     total = torch.empty((n, 4), dtype=torch.float64, device="cuda")
     try:
-        for _ in range(steps):
-            for stage in (1, 2, 3, 4):
-                for c, b in zip(ctxs, bufs):
-                    c.shard_stage(stage, b)
-                total.copy_(bufs[0])
-                for b in bufs[1:]:
-                    total += b                 # what the all-reduce computes
-                for c in ctxs:
-                    c.shard_combine(stage, dt, total)
+        with torch.cuda.stream(st):
+            for _ in range(steps):
+                for stage in (1, 2, 3, 4):
+                    for c, b in zip(ctxs, bufs):
+                        c.shard_stage(stage, b)
+                    total.copy_(bufs[0])
+                    for b in bufs[1:]:
+                        total += b                 # what the all-reduce computes
+                    for c in ctxs:
+                        c.shard_combine(stage, dt, total)
         st.synchronize()
         states = [c.get_state() for c in ctxs]
         infos = [c.shard_info() for c in ctxs]
@@ -90,10 +91,10 @@ def test_one_rank_shard_equals_unsharded(fss):
         one.rk4_step(0.01, nsteps=2)
         want = one.get_state()
     with fss.Context(**kw) as c:
-        c.set_stream(torch.cuda.current_stream().cuda_stream)
-        c.set_particles(s, a)
+        c.set_particles(s, a)                     # the context's own stream
         c.shard(0, 1)
         ex = shard.exchange_buffer(c, "cuda")
+        torch.cuda.synchronize()                  # the buffer exists before the context's stream uses it
         shard.rk4_steps(c, ex, 0.01, nsteps=2)
         got = c.get_state()
         c.shard(0, 0)                         # unshard: the full lists again
