@@ -476,8 +476,8 @@ int materialize(fss_ctx* c, PairShape shape) {
         for (int d = 0; d <= kMaxDegree; d++)
             if ((j.degmask >> d) & 1) c->nmax = std::max(c->nmax, d);
     }
-    std::vector<double> vinv_all, vinvT_all, bary_all;
-    std::vector<int32_t> vinv_off(kMaxDegree + 1, 0), bary_off(kMaxDegree + 1, 0);
+    std::vector<double> vinv_all, vinvT_all;
+    std::vector<int32_t> vinv_off(kMaxDegree + 1, 0);
     for (int d = 0; d <= c->nmax; d++) {
         std::vector<double> nodes, vi;
         interp_nodes(d, nodes, vi);
@@ -486,19 +486,15 @@ int materialize(fss_ctx* c, PairShape shape) {
         const int K = nproxy(d);
         for (int k = 0; k < K; k++)
             for (int m = 0; m < K; m++) vinvT_all.push_back(vi[size_t(m) * K + k]);
-        bary_off[d] = int32_t(bary_all.size());
-        bary_all.insert(bary_all.end(), nodes.begin(), nodes.end());
     }
     TRY(upload(c, c->vinv, vinv_all));
     TRY(upload(c, c->vinvT, vinvT_all));
-    TRY(upload(c, c->bary, bary_all));
-    TRY(upload(c, c->bary_off, bary_off));
     TRY(upload(c, c->vinv_off, vinv_off));
     TRY(upload(c, c->segs, L.segs));
     TRY(upload(c, c->items, L.items));
     TRY(upload(c, c->jobs, L.jobs));
     TRY(upload(c, c->down_jobs, L.down));
-    TRY(upload(c, c->down_of_face, L.down_of_face));
+    TRY(upload(c, c->down_anc, L.leaf_anc));
     CU(c->down_coef.ensure(sizeof(double4) * size_t(std::max<int64_t>(L.n_coef, 1))));
     std::vector<double4> pp(L.proxy_pos.size() / 4);
     for (size_t i = 0; i < pp.size(); i++)
@@ -589,24 +585,17 @@ int eval_partials(fss_ctx* c, bool want_psi, bool* down_out) {
         DownArgs d;
         d.njobs = int(c->lists.down.size());
         d.jobs = c->down_jobs.as<DownJob>();
-        d.level_off = c->lists.down_level_off.data();
         d.partials = c->partials.as<double4>();
         d.parts = c->parts;
         d.pstride = c->pstride;
         d.vinvT = c->vinvT.as<double>();
         d.vinv_off = c->vinv_off.as<int32_t>();
-        d.bary = c->bary.as<double>();
-        d.bary_off = c->bary_off.as<int32_t>();
-        d.verts = c->verts.as<double>();
-        d.tri_verts = c->tri_verts.as<int32_t>();
         d.node = c->node.as<NodeGeom>();
         d.coef = c->down_coef.as<double4>();
         d.nleaf = int(c->nleaf);
-        d.leaf_level = c->leaf_level;
-        d.leaf_off = c->geom.lev_off[c->leaf_level];
         d.xs = c->xs.as<double4>();
         d.leaf_start = c->leaf_start.as<int32_t>();
-        d.down_of_face = c->down_of_face.as<int32_t>();
+        d.leaf_anc = c->down_anc.as<LeafAnc>();
         d.out = c->partials.as<double4>() + int64_t(c->parts) * c->pstride;
         ProfScope ps(c, "downward", down_launch_count(d));
         launch_down(c->stream, want_psi, d);
@@ -1015,8 +1004,9 @@ int fss_rhs_current(fss_ctx* c, double omega, double* modify5, double* psi) {
 namespace {
 // Pair evaluations the consumer lanes of a pair launch perform on items
 // [i0, i1) with `targets` consumer threads per block: per chunk of targets,
-// every active warp evaluates every source of the item (padded to whole
-// quads), whether or not each of its lanes holds a target.
+// every full warp evaluates every source of the item (padded to whole
+// quads) on each lane; the last, partial warp (r targets) splits them over
+// 32 / r lanes per target, each lane taking every (32 / r)-th quad.
 double lane_pairs(const fss_ctx* c, int64_t i0, int64_t i1, int targets) {
     const ListOutput& L = c->lists;
     double sum = 0;
@@ -1027,11 +1017,12 @@ double lane_pairs(const fss_ctx* c, int64_t i0, int64_t i1, int targets) {
             const Segment& sg = L.segs[g];
             src += sg.kind == 0 ? double(c->leaf_start_h[sg.b] - c->leaf_start_h[sg.a]) : double(sg.b - sg.a);
         }
-        src = 4.0 * std::ceil(src / 4.0);
+        const double quads = std::ceil(src / 4.0);
         const int nt = it.leaf >= 0 ? c->leaf_start_h[it.leaf + 1] - c->leaf_start_h[it.leaf] : it.nt;
         for (int c0 = 0; c0 < nt; c0 += targets) {
             const int cn = std::min(targets, nt - c0);
-            sum += 32.0 * double((cn + 31) / 32) * src;
+            sum += 32.0 * double(cn / 32) * 4.0 * quads;
+            if (cn % 32) sum += 32.0 * 4.0 * std::ceil(quads / double(32 / (cn % 32)));
         }
     }
     return sum;

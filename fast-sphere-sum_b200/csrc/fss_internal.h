@@ -80,18 +80,24 @@ struct EnsLeaf {
     int64_t part_base;
 };
 
-// Downward pass: a face that receives far sources at its K = nproxy(deg)
-// interpolation points (a target cluster, fast_rhs.h cp and cc; slot >= 0:
-// unified indices [slot, slot + K)), or a face below one (slot = -1).  Its
-// field is held as coefficients of the Chebyshev product basis (K double4
-// from `coef`): its own points' values, plus its parent's polynomial
-// re-interpolated at its points (parent = job index, -1 at the top).
+// Downward pass: a target cluster, a face that receives far sources at its
+// K = nproxy(deg) interpolation points (fast_rhs.h cp and cc): unified
+// indices [slot, slot + K).  Its field there becomes K coefficients of the
+// Chebyshev product basis (double4 from `coef`), which every particle below
+// the face evaluates directly (as cp evaluates the interpolant at the
+// targets, fast_rhs.h:228-235).
 struct DownJob {
-    int32_t level, node, local, deg;  // node = global face index
-    int32_t slot;                     // first own interpolation point (unified index), or -1
-    int32_t coef;                     // first coefficient (double4 units)
-    int32_t parent;                   // parent's job, or -1
-    int32_t pad;
+    int32_t level, node, deg;  // node = global face index
+    int32_t slot;              // first interpolation point (unified index)
+    int32_t coef;              // first coefficient (double4 units)
+    int32_t pad[3];
+};
+
+// One target cluster above a leaf, as the leaf's evaluation reads it:
+// coefficients from `coef`, degree, face (global index); coef < 0 ends a
+// leaf's list.
+struct LeafAnc {
+    int32_t coef, deg, node, pad;
 };
 
 // Per-node geometry for the upward pass: inverse of [v1 v2 v3] (columns),

@@ -46,9 +46,20 @@ __global__ void __launch_bounds__(128) k_up_combine_batch(const ProxyJob* __rest
     const int tid = threadIdx.x;
     const int KM = nproxy(nmax);
     if (tid < KM) {
-        double s = 0;
-        for (int lf = job.leaf_lo; lf < job.leaf_hi; lf++) s += part[leaves[lf].part_base + int64_t(job.level) * KM + tid];
-        M[tid] = s;
+        // four independent sums over the face's leaves, as the single
+        // problem's combine forms them (same order, same result)
+        const int64_t off = int64_t(job.level) * KM + tid;
+        const int nl = job.leaf_hi - job.leaf_lo;
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        int lf = 0;
+        for (; lf + 4 <= nl; lf += 4) {
+            s0 += part[leaves[job.leaf_lo + lf + 0].part_base + off];
+            s1 += part[leaves[job.leaf_lo + lf + 1].part_base + off];
+            s2 += part[leaves[job.leaf_lo + lf + 2].part_base + off];
+            s3 += part[leaves[job.leaf_lo + lf + 3].part_base + off];
+        }
+        for (; lf < nl; lf++) s0 += part[leaves[job.leaf_lo + lf].part_base + off];
+        M[tid] = (s0 + s1) + (s2 + s3);
     }
     __syncthreads();
     for (int d = 0; d <= nmax; d++) {

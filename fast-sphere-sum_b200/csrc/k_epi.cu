@@ -56,9 +56,20 @@ __global__ void __launch_bounds__(kUpThreads) k_up_combine(const ProxyJob* __res
     const int tid = threadIdx.x;
     const int KM = nproxy(nmax);
     if (tid < KM) {
-        double s = 0;
-        for (int lf = job.leaf_lo; lf < job.leaf_hi; lf++) s += part[(int64_t(lf) * (leaf_level + 1) + job.level) * KM + tid];
-        M[tid] = s;
+        // four independent sums over the face's leaves (four rows in flight)
+        const int64_t stride = int64_t(leaf_level + 1) * KM;
+        const double* p = part + (int64_t(job.leaf_lo) * (leaf_level + 1) + job.level) * KM + tid;
+        const int nl = job.leaf_hi - job.leaf_lo;
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        int lf = 0;
+        for (; lf + 4 <= nl; lf += 4) {
+            s0 += p[(lf + 0) * stride];
+            s1 += p[(lf + 1) * stride];
+            s2 += p[(lf + 2) * stride];
+            s3 += p[(lf + 3) * stride];
+        }
+        for (; lf < nl; lf++) s0 += p[lf * stride];
+        M[tid] = (s0 + s1) + (s2 + s3);
     }
     __syncthreads();
     double cx = 0, cy = 0, cz = 0;
@@ -253,34 +264,98 @@ __global__ void k_scatter_state(int64_t n, const int32_t* __restrict__ perm, con
 // down-pass partial slot.  x, y, z and, when the stream function is wanted,
 // its log term.  FP64.
 
-// Interpolant with coefficients C (degree deg) of face geometry ng at x:
-// sum_a T_a(u) sum_b c_ab T_b(v) (a + b <= deg), both Chebyshev families by
-// their three-term recurrences.
+// Downward pass, part 1: the coefficients of every target cluster at once,
+// one warp per cluster: y_k = the cluster's field at its K interpolation
+// points (its partial slots summed), c_m = sum_k Vinv[m][k] y_k (VT = Vinv
+// transposed, so that consecutive lanes read consecutive entries).  A lane
+// forms its NQ = ceil(K / 32) outputs m = lane + 32 q in one pass over k
+// (independent chains, several loads in flight).
+constexpr int kCoefWarps = 4;
+template <bool PSI, int NQ>
+__device__ __forceinline__ void coef_outputs(const double* __restrict__ VT, int K, int lane,
+                                             const double4* __restrict__ Y, double4* __restrict__ out) {
+    double4 c[NQ];
+    int mm[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        c[q] = make_double4(0.0, 0.0, 0.0, 0.0);
+        mm[q] = min(lane + 32 * q, K - 1);  // a lane past K repeats the last output (not stored)
+    }
+#pragma unroll 4
+    for (int k = 0; k < K; k++) {
+        const double4 y = Y[k];
+        const double* row = VT + k * K;
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            const double t = __ldg(row + mm[q]);
+            c[q].x = fma(t, y.x, c[q].x);
+            c[q].y = fma(t, y.y, c[q].y);
+            c[q].z = fma(t, y.z, c[q].z);
+            if (PSI) c[q].w = fma(t, y.w, c[q].w);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; q++)
+        if (lane + 32 * q < K) out[lane + 32 * q] = c[q];
+}
+
 template <bool PSI>
-__device__ __forceinline__ double4 eval_interp(const NodeGeom& ng, double x, double y, double z,
-                                               const double4* C, int deg) {
-    const double c0 = ng.minv[0] * x + ng.minv[1] * y + ng.minv[2] * z;
-    const double c1 = ng.minv[3] * x + ng.minv[4] * y + ng.minv[5] * z;
-    const double c2 = ng.minv[6] * x + ng.minv[7] * y + ng.minv[8] * z;
-    const double inv = 1.0 / (c0 + c1 + c2);
-    const double u = 2.0 * (c0 * inv) - 1.0, v = 2.0 * (c1 * inv) - 1.0;
-    const double u2 = 2.0 * u, v2 = 2.0 * v;
+__global__ void __launch_bounds__(32 * kCoefWarps) k_down_coef(const DownJob* __restrict__ jobs, int njobs,
+                                                               const double4* __restrict__ partials, int parts,
+                                                               int64_t pstride, const double* __restrict__ vinvT,
+                                                               const int32_t* __restrict__ vinv_off,
+                                                               double4* __restrict__ coef) {
+    static_assert(kMaxK <= 96, "at most three outputs per lane");
+    __shared__ double4 Y[kCoefWarps][kMaxK];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int j = blockIdx.x * kCoefWarps + w;
+    if (j >= njobs) return;  // whole warps only; no block-wide barrier follows
+    const DownJob job = jobs[j];
+    const int K = nproxy(job.deg);
+    for (int k = lane; k < K; k += 32) {
+        double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int p = 0; p < parts; p++) {
+            const double4 q = partials[int64_t(p) * pstride + job.slot + k];
+            v.x += q.x; v.y += q.y; v.z += q.z; v.w += q.w;
+        }
+        Y[w][k] = v;
+    }
+    __syncwarp();
+    const double* VT = vinvT + vinv_off[job.deg];
+    double4* out = coef + job.coef;
+    if (K <= 32)
+        coef_outputs<PSI, 1>(VT, K, lane, Y[w], out);
+    else if (K <= 64)
+        coef_outputs<PSI, 2>(VT, K, lane, Y[w], out);
+    else
+        coef_outputs<PSI, 3>(VT, K, lane, Y[w], out);
+}
+
+// The interpolant of degree D with coefficients C at barycentric (u, v)
+// (both mapped to [-1, 1]): sum_a T_a(u) sum_b C[m(a, b)] T_b(v), a + b <= D,
+// m(a, b) = (a + b)(a + b + 1)/2 + b, both Chebyshev families by their
+// three-term recurrences; the degree is known at compile time, so that the
+// loops unroll and C is read at fixed offsets.
+template <int D, bool PSI>
+__device__ __forceinline__ double4 eval_deg(double u, double v, const double4* __restrict__ C) {
+    double tv[D + 1];
+    tv[0] = 1.0;
+    if (D >= 1) tv[1] = v;
+    const double v2 = 2.0 * v, u2 = 2.0 * u;
+#pragma unroll
+    for (int b = 2; b <= D; b++) tv[b] = fma(v2, tv[b - 1], -tv[b - 2]);
     double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
     double ta = 1.0, ta_prev = u;  // T_a(u), T_{a-1}(u) (T_{-1} = T_1)
-    for (int a = 0; a <= deg; a++) {
+#pragma unroll
+    for (int a = 0; a <= D; a++) {
         double4 s = make_double4(0.0, 0.0, 0.0, 0.0);
-        double tb = 1.0, tb_prev = v;
-        int m = a * (a + 1) / 2;  // index of (a, 0): g = a, b = 0
-        for (int b = 0; a + b <= deg; b++) {
-            const double4 cm = C[m];
-            s.x = fma(tb, cm.x, s.x);
-            s.y = fma(tb, cm.y, s.y);
-            s.z = fma(tb, cm.z, s.z);
-            if (PSI) s.w = fma(tb, cm.w, s.w);
-            const double tn = fma(v2, tb, -tb_prev);
-            tb_prev = tb;
-            tb = tn;
-            m += a + b + 2;  // (g, b) -> (g + 1, b + 1)
+#pragma unroll
+        for (int b = 0; a + b <= D; b++) {
+            const double4 cm = C[(a + b) * (a + b + 1) / 2 + b];
+            s.x = fma(tv[b], cm.x, s.x);
+            s.y = fma(tv[b], cm.y, s.y);
+            s.z = fma(tv[b], cm.z, s.z);
+            if (PSI) s.w = fma(tv[b], cm.w, s.w);
         }
         acc.x = fma(ta, s.x, acc.x);
         acc.y = fma(ta, s.y, acc.y);
@@ -293,121 +368,67 @@ __device__ __forceinline__ double4 eval_interp(const NodeGeom& ng, double x, dou
     return acc;
 }
 
-// One level of the downward pass: block b takes the level's jobs [j0 + 4b,
-// j0 + 4b + 4).  A face's values at its points y_k are its own far field
-// (partial slots at [slot, slot + K), when it is a target cluster) plus its
-// parent's interpolant there; c = Vinv values (VT = Vinv transposed, so that
-// consecutive threads read consecutive entries).
-constexpr int kDownGroup = 4;
-constexpr int kDownThreads = 256;
 template <bool PSI>
-__global__ void __launch_bounds__(kDownThreads) k_down_level(const DownJob* __restrict__ jobs, int j0, int nj,
-                                                             const double4* __restrict__ partials, int parts,
-                                                             int64_t pstride, const NodeGeom* __restrict__ node,
-                                                             const double* __restrict__ verts,
-                                                             const int32_t* __restrict__ tri_verts,
-                                                             const double* __restrict__ bary,
-                                                             const int32_t* __restrict__ bary_off,
-                                                             const double* __restrict__ vinvT,
-                                                             const int32_t* __restrict__ vinv_off,
-                                                             double4* __restrict__ coef) {
-    __shared__ double4 Cp[kDownGroup][kMaxK];
-    __shared__ double4 Y[kDownGroup][kMaxK];
-    __shared__ DownJob J[kDownGroup], P[kDownGroup];
-    const int tid = threadIdx.x;
-    const int jb = j0 + kDownGroup * blockIdx.x;
-    const int nq = min(kDownGroup, j0 + nj - jb);
-    if (tid < nq) {
-        J[tid] = jobs[jb + tid];
-        if (J[tid].parent >= 0) P[tid] = jobs[J[tid].parent];
+__device__ __forceinline__ double4 eval_any(int deg, double u, double v, const double4* C) {
+    switch (deg) {
+#define FSS_DEG(D) \
+    case D: return eval_deg<D, PSI>(u, v, C);
+        FSS_DEG(0) FSS_DEG(1) FSS_DEG(2) FSS_DEG(3) FSS_DEG(4) FSS_DEG(5) FSS_DEG(6)
+        FSS_DEG(7) FSS_DEG(8) FSS_DEG(9) FSS_DEG(10) FSS_DEG(11) FSS_DEG(12)
+#undef FSS_DEG
     }
-    __syncthreads();
-    for (int idx = tid; idx < nq * kMaxK; idx += kDownThreads) {
-        const int q = idx / kMaxK, m = idx % kMaxK;
-        if (J[q].parent >= 0 && m < nproxy(P[q].deg)) Cp[q][m] = coef[int64_t(P[q].coef) + m];
-    }
-    __syncthreads();
-    for (int idx = tid; idx < nq * kMaxK; idx += kDownThreads) {
-        const int q = idx / kMaxK, k = idx % kMaxK;
-        const DownJob& job = J[q];
-        if (k >= nproxy(job.deg)) continue;
-        double4 val = make_double4(0.0, 0.0, 0.0, 0.0);
-        if (job.slot >= 0)
-            for (int p = 0; p < parts; p++) {
-                const double4 v = partials[int64_t(p) * pstride + job.slot + k];
-                val.x += v.x; val.y += v.y; val.z += v.z; val.w += v.w;
-            }
-        if (job.parent >= 0) {
-            const int32_t* tv = tri_verts + 3 * int64_t(job.node);
-            const double* v0 = verts + 3 * int64_t(tv[0]);
-            const double* v1 = verts + 3 * int64_t(tv[1]);
-            const double* v2 = verts + 3 * int64_t(tv[2]);
-            const double* nd = bary + bary_off[job.deg] + 3 * k;
-            double y[3];
-            for (int c = 0; c < 3; c++) y[c] = nd[0] * v0[c] + nd[1] * v1[c] + nd[2] * v2[c];
-            const double r = 1.0 / sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
-            const double4 e = eval_interp<PSI>(node[P[q].node], y[0] * r, y[1] * r, y[2] * r, Cp[q], P[q].deg);
-            val.x += e.x; val.y += e.y; val.z += e.z; val.w += e.w;
-        }
-        Y[q][k] = val;
-    }
-    __syncthreads();
-    // c_m = sum_k Vinv[m][k] Y_k: four threads per output, each a quarter of
-    // the k range (short independent chains), combined by shuffles
-    const int total = nq * kMaxK * 4;
-    for (int base = 0; base < total; base += kDownThreads) {  // same trip count in every lane
-        const int idx = base + tid;
-        const int o = idx >> 2, part = idx & 3;
-        const int q = (idx < total) ? o / kMaxK : 0, m = (idx < total) ? o % kMaxK : kMaxK;
-        const DownJob& job = J[q];
-        const int K = nproxy(job.deg);
-        const double* VT = vinvT + vinv_off[job.deg];
-        double4 c = make_double4(0.0, 0.0, 0.0, 0.0);
-        if (m < K) {
-#pragma unroll 4
-            for (int k = part; k < K; k += 4) {
-                const double w = __ldg(&VT[k * K + m]);
-                const double4 v = Y[q][k];
-                c.x = fma(w, v.x, c.x); c.y = fma(w, v.y, c.y); c.z = fma(w, v.z, c.z);
-                if (PSI) c.w = fma(w, v.w, c.w);
-            }
-        }
-        // the four parts of one output are consecutive lanes of one warp
-        for (int d = 1; d < 4; d <<= 1) {
-            c.x += __shfl_xor_sync(0xffffffffu, c.x, d);
-            c.y += __shfl_xor_sync(0xffffffffu, c.y, d);
-            c.z += __shfl_xor_sync(0xffffffffu, c.z, d);
-            if (PSI) c.w += __shfl_xor_sync(0xffffffffu, c.w, d);
-        }
-        if (part == 0 && m < K) coef[int64_t(job.coef) + m] = c;
-    }
+    return make_double4(0.0, 0.0, 0.0, 0.0);
 }
+static_assert(kMaxDegree == 12, "eval_any instantiates degrees 0..12");
 
+// Downward pass, part 2: one block per leaf; every particle sums the
+// interpolants of the target clusters above its leaf (coarse to fine),
+// evaluated where it is (barycentric coordinates of its central projection
+// in each cluster's frame).  A leaf below none writes zeros.
 template <bool PSI>
-__global__ void __launch_bounds__(kUpThreads) k_down_leaf(const double4* __restrict__ xs,
-                                                          const int32_t* __restrict__ leaf_start,
-                                                          const NodeGeom* __restrict__ node, int64_t leaf_off,
-                                                          const int32_t* __restrict__ down_of_face,
-                                                          const DownJob* __restrict__ jobs,
-                                                          const double4* __restrict__ coef,
-                                                          double4* __restrict__ out) {
-    __shared__ double4 C[kMaxK];
+__global__ void __launch_bounds__(kUpThreads) k_down_direct(const double4* __restrict__ xs,
+                                                            const int32_t* __restrict__ leaf_start,
+                                                            const NodeGeom* __restrict__ node,
+                                                            const LeafAnc* __restrict__ leaf_anc,
+                                                            const double4* __restrict__ coef,
+                                                            double4* __restrict__ out) {
+    __shared__ double4 C[kMaxLevels * kMaxK];
+    __shared__ LeafAnc A[kMaxLevels];
+    __shared__ NodeGeom G[kMaxLevels];
+    __shared__ int off[kMaxLevels + 1];
     const int leaf = blockIdx.x, tid = threadIdx.x;
     const int a0 = leaf_start[leaf], a1 = leaf_start[leaf + 1];
     if (a0 == a1) return;
-    const int j = down_of_face[leaf_off + leaf];
-    if (j < 0) {
-        for (int i = a0 + tid; i < a1; i += kUpThreads) out[i] = make_double4(0.0, 0.0, 0.0, 0.0);
-        return;
-    }
-    const DownJob job = jobs[j];
-    const int K = nproxy(job.deg);
-    for (int k = tid; k < K; k += kUpThreads) C[k] = coef[int64_t(job.coef) + k];
+    if (tid < kMaxLevels) A[tid] = leaf_anc[int64_t(leaf) * kMaxLevels + tid];
     __syncthreads();
-    const NodeGeom& ng = node[leaf_off + leaf];
+    int nanc = 0;
+    while (nanc < kMaxLevels && A[nanc].coef >= 0) nanc++;
+    if (tid < nanc) G[tid] = node[A[tid].node];
+    if (tid == 0) {
+        int o = 0;
+        for (int k = 0; k < nanc; k++) {
+            off[k] = o;
+            o += nproxy(A[k].deg);
+        }
+        off[nanc] = o;
+    }
+    __syncthreads();
+    for (int a = 0; a < nanc; a++)
+        for (int m = tid; m < off[a + 1] - off[a]; m += kUpThreads) C[off[a] + m] = coef[int64_t(A[a].coef) + m];
+    __syncthreads();
     for (int i = a0 + tid; i < a1; i += kUpThreads) {
         const double4 x = xs[i];
-        out[i] = eval_interp<PSI>(ng, x.x, x.y, x.z, C, job.deg);
+        double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int a = 0; a < nanc; a++) {
+            const NodeGeom& ng = G[a];
+            const double c0 = ng.minv[0] * x.x + ng.minv[1] * x.y + ng.minv[2] * x.z;
+            const double c1 = ng.minv[3] * x.x + ng.minv[4] * x.y + ng.minv[5] * x.z;
+            const double c2 = ng.minv[6] * x.x + ng.minv[7] * x.y + ng.minv[8] * x.z;
+            const double inv = 1.0 / (c0 + c1 + c2);
+            const double4 e = eval_any<PSI>(A[a].deg, 2.0 * (c0 * inv) - 1.0, 2.0 * (c1 * inv) - 1.0, C + off[a]);
+            acc.x += e.x; acc.y += e.y; acc.z += e.z; acc.w += e.w;
+        }
+        out[i] = acc;
     }
 }
 
@@ -476,32 +497,18 @@ void launch_scatter_state(cudaStream_t st, int64_t n, const int32_t* perm, const
 
 void launch_down(cudaStream_t st, bool psi, const DownArgs& d) {
     if (d.njobs == 0) return;
-    for (int l = 0; l <= d.leaf_level; l++) {
-        const int j0 = d.level_off[l], nj = d.level_off[l + 1] - j0;
-        if (nj == 0) continue;
-        const int nb = (nj + kDownGroup - 1) / kDownGroup;
-        if (psi)
-            k_down_level<true><<<nb, kDownThreads, 0, st>>>(d.jobs, j0, nj, d.partials, d.parts, d.pstride, d.node,
-                                                            d.verts, d.tri_verts, d.bary, d.bary_off, d.vinvT,
-                                                            d.vinv_off, d.coef);
-        else
-            k_down_level<false><<<nb, kDownThreads, 0, st>>>(d.jobs, j0, nj, d.partials, d.parts, d.pstride, d.node,
-                                                             d.verts, d.tri_verts, d.bary, d.bary_off, d.vinvT,
-                                                             d.vinv_off, d.coef);
+    const unsigned nb = unsigned((d.njobs + kCoefWarps - 1) / kCoefWarps);
+    if (psi) {
+        k_down_coef<true><<<nb, 32 * kCoefWarps, 0, st>>>(d.jobs, d.njobs, d.partials, d.parts, d.pstride, d.vinvT,
+                                                          d.vinv_off, d.coef);
+        k_down_direct<true><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc, d.coef, d.out);
+    } else {
+        k_down_coef<false><<<nb, 32 * kCoefWarps, 0, st>>>(d.jobs, d.njobs, d.partials, d.parts, d.pstride, d.vinvT,
+                                                           d.vinv_off, d.coef);
+        k_down_direct<false><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc, d.coef, d.out);
     }
-    if (psi)
-        k_down_leaf<true><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_off, d.down_of_face,
-                                                          d.jobs, d.coef, d.out);
-    else
-        k_down_leaf<false><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_off, d.down_of_face,
-                                                           d.jobs, d.coef, d.out);
 }
 
-int down_launch_count(const DownArgs& d) {
-    if (d.njobs == 0) return 0;
-    int n = 1;
-    for (int l = 0; l <= d.leaf_level; l++) n += (d.level_off[l + 1] > d.level_off[l]) ? 1 : 0;
-    return n;
-}
+int down_launch_count(const DownArgs& d) { return d.njobs == 0 ? 0 : 2; }
 
 }  // namespace fss

@@ -74,7 +74,7 @@ __device__ __forceinline__ void tile_pairs_soa(const float* __restrict__ s, int 
         q0 = 0;
         step = 1;
     }
-#pragma unroll 2
+#pragma unroll 4
     for (int q = q0; q < nquad; q += step) {
         const float4 X = reinterpret_cast<const float4*>(s)[q];
         const float4 Y = reinterpret_cast<const float4*>(s + T)[q];

@@ -95,25 +95,19 @@ void launch_up_combine(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jo
                        const NodeGeom* node, int local_frames, int64_t n, void* src);
 // Downward pass of the target clusters and the faces below them.
 struct DownArgs {
-    int njobs = 0;
+    int njobs = 0;                       // target clusters
     const DownJob* jobs = nullptr;
-    const int32_t* level_off = nullptr;  // host array: first job of each level (leaf_level + 2)
     const double4* partials = nullptr;   // field at the interpolation points: parts slots of stride pstride
     int parts = 1;
     int64_t pstride = 0;
     const double* vinvT = nullptr;       // inverse Vandermonde matrices transposed, by degree
     const int32_t* vinv_off = nullptr;
-    const double* bary = nullptr;        // interpolation nodes (barycentric, 3 per point) by degree
-    const int32_t* bary_off = nullptr;
-    const double* verts = nullptr;
-    const int32_t* tri_verts = nullptr;
     const NodeGeom* node = nullptr;
     double4* coef = nullptr;
-    int nleaf = 0, leaf_level = 0;
-    int64_t leaf_off = 0;                // global index of the first leaf face
+    int nleaf = 0;
     const double4* xs = nullptr;
     const int32_t* leaf_start = nullptr;
-    const int32_t* down_of_face = nullptr;
+    const LeafAnc* leaf_anc = nullptr;   // kMaxLevels per leaf
     double4* out = nullptr;              // down-pass partial slot, one per particle
 };
 void launch_down(cudaStream_t st, bool psi, const DownArgs& d);

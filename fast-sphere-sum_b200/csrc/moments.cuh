@@ -14,7 +14,9 @@ constexpr int kUpLd = kUpThreads + 4;    // padded row: 8 rows of 4 doubles hit 
 // particle's basis W[a][j] = w T_a(u), V[b][j] = T_b(v); then M = W V^T
 // (16 x 16, a + b <= n used) on the FP64 tensor cores, warp w taking the 8 x 8
 // tile (w / 2, w % 2).  Lane (4 g + t) ends holding M[8 (w/2) + g][8 (w%2) +
-// 2t + {0, 1}], written to out[m], m = (a + b)(a + b + 1) / 2 + b.
+// 2t + {0, 1}], written to out[m], m = (a + b)(a + b + 1) / 2 + b.  A tile
+// holding no a + b <= n is not formed: (1, 1) never (n <= 12 < 16), (0, 1) and
+// (1, 0) not for n < 8.
 template <typename T>
 __device__ __forceinline__ void leaf_moments(const typename Vec4<T>::type* __restrict__ src, int a0, int a1,
                                              double fx, double fy, double fz, const NodeGeom& ng, int nmax,
@@ -47,8 +49,9 @@ __device__ __forceinline__ void leaf_moments(const typename Vec4<T>::type* __res
         }
         __syncthreads();
         const int nk = (min(kUpThreads, a1 - c0) + 3) >> 2;  // same in every thread
-        for (int k = 0; k < nk; k++)
-            dmma_8x8x4(d0, d1, W[8 * ta + g][4 * k + t], V[8 * tb + g][4 * k + t]);
+        if (8 * (ta + tb) <= nmax)                            // warp-uniform
+            for (int k = 0; k < nk; k++)
+                dmma_8x8x4(d0, d1, W[8 * ta + g][4 * k + t], V[8 * tb + g][4 * k + t]);
         __syncthreads();
     }
     const int a = 8 * ta + g;

@@ -338,11 +338,8 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
     out.n_leaf_items = int64_t(out.items.size());
     // target clusters: their interpolation points are the targets
     const int64_t nfaces = g.lev_off[LL + 1];
-    std::vector<int32_t> own_slot, own_deg;
-    if (!clusters.empty()) {
-        own_slot.assign(nfaces, -1);
-        own_deg.assign(nfaces, -1);
-    }
+    std::vector<int32_t> job_of_face;
+    if (!clusters.empty()) job_of_face.assign(nfaces, -1);
     for (const TList& t : clusters) {
         const int K = nproxy(t.deg);
         const int64_t gf = g.lev_off[t.level] + t.node;
@@ -352,29 +349,26 @@ void build_lists(const ListInput& in, const std::vector<std::vector<ASrc>>& list
         out.cp_pairs += npp;
         out.cc_pairs += npc;
         add_items(t.src, s0, K, -1, K);
-        own_slot[gf] = s0;
-        own_deg[gf] = t.deg;
+        job_of_face[gf] = int32_t(out.down.size());
+        out.down.push_back(DownJob{t.level, int32_t(gf), t.deg, s0, int32_t(out.n_coef), {0, 0, 0}});
+        out.n_coef += K;
         out.max_cluster_k = std::max(out.max_cluster_k, K);
     }
     flush_items();
-    // downward pass: every target cluster and every face below one, level by
-    // level (a face below takes its parent's degree unless it has its own)
+    // downward pass: every leaf below a target cluster evaluates that
+    // cluster's interpolant at its particles; per leaf the clusters on its
+    // path to the root, coarse to fine
     if (!clusters.empty()) {
-        out.down_of_face.assign(nfaces, -1);
-        out.down_level_off.assign(LL + 2, 0);
-        for (int l = 0; l <= LL; l++) {
-            out.down_level_off[l] = int32_t(out.down.size());
-            for (int64_t f = 0; f < g.level_count(l); f++) {
-                const int64_t gf = g.lev_off[l] + f;
-                const int32_t pj = (l > 0) ? out.down_of_face[g.lev_off[l - 1] + f / 4] : -1;
-                const int deg = own_deg[gf] >= 0 ? own_deg[gf] : (pj >= 0 ? out.down[pj].deg : -1);
-                if (deg < 0) continue;
-                out.down_of_face[gf] = int32_t(out.down.size());
-                out.down.push_back(DownJob{l, int32_t(gf), int32_t(f), deg, own_slot[gf], int32_t(out.n_coef), pj, 0});
-                out.n_coef += nproxy(deg);
+        out.leaf_anc.assign(size_t(nleaf) * kMaxLevels, LeafAnc{-1, 0, 0, 0});
+        for (int64_t lf = 0; lf < nleaf; lf++) {
+            int k = 0;
+            for (int l = 0; l <= LL; l++) {
+                const int64_t gf = g.lev_off[l] + (lf >> (2 * (LL - l)));
+                const int32_t j = job_of_face[gf];
+                if (j < 0) continue;
+                out.leaf_anc[size_t(lf) * kMaxLevels + k++] = LeafAnc{out.down[j].coef, out.down[j].deg, int32_t(gf), 0};
             }
         }
-        out.down_level_off[LL + 1] = int32_t(out.down.size());
     }
 }
 

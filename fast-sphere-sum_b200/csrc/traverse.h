@@ -68,9 +68,8 @@ struct ListOutput {
     int64_t n_leaf_items = 0;
     int max_cluster_k = 0;          // largest interpolation point count of a target cluster
     std::vector<ProxyJob> jobs;
-    std::vector<DownJob> down;      // target clusters and the faces below them, by level
-    std::vector<int32_t> down_level_off;  // first down job of each level (leaf_level + 2 entries)
-    std::vector<int32_t> down_of_face;  // global face -> down job, or -1 (empty without target clusters)
+    std::vector<DownJob> down;      // target clusters
+    std::vector<LeafAnc> leaf_anc;  // per leaf, kMaxLevels records: the target clusters above it, coarse to fine
     int64_t n_coef = 0;             // down-pass coefficients (double4)
     std::vector<double> proxy_pos;  // 4 doubles per proxy slot: y (on sphere) and pad
     std::vector<int32_t> proxy_node;  // proxy slot -> face (global index)

@@ -16,8 +16,8 @@ Gaussian vortices; mixed-precision BLTC n=8, theta=0.7; one CUDA graph per
 RK4 step for all members.
 
 --learned: the learned per-leaf (degree, theta) choice (tolerance 1e-6,
-safety 2) and the autotuned block shape, with target clusters (the
-reference's cp/cc types) unless --no-clusters.
+safety 2) and the autotuned block shape (--block N: that shape instead),
+with target clusters (the reference's cp/cc types) unless --no-clusters.
 
 Inputs: icosahedral grid of the given level, RH4 wave + seeded vortices.
 Prints one line with the wall time; exits non-zero on any library error.
@@ -48,6 +48,9 @@ def main(argv=None):
     p.add_argument("--learned", action="store_true")
     p.add_argument("--clusters", action="store_true", help="target clusters with fixed degree/theta")
     p.add_argument("--no-clusters", action="store_true")
+    p.add_argument("--block", type=int, default=0,
+                   help="pair-kernel block threads (no autotuning: the only pair launches before the steps are "
+                        "the two of the selector's one right-hand side)")
     a = p.parse_args(argv)
     prec = PREC_MIXED if a.precision == "mixed" else PREC_FP64
     if a.case == "ensemble":
@@ -57,7 +60,9 @@ def main(argv=None):
     s, area = make_state(a.level, "rh_vortices", n_vortex=a.vortices, seed=2)
     method = METHOD_DIRECT if a.case == "direct" else METHOD_TREECODE
     t0 = time.perf_counter()
-    extra = dict(list_mode=1, autotune=1) if a.learned else {}
+    extra = dict(list_mode=1, autotune=0 if a.block else 1) if a.learned else {}
+    if a.block:
+        extra["block_threads"] = a.block
     if (a.learned and not a.no_clusters) or a.clusters:
         extra["cluster_targets"] = 1
     with Context(method=method, precision=prec, degree=a.degree, theta=a.theta,
