@@ -215,21 +215,35 @@ def time_steps(ctx, stream, steps, flush):
 
 
 def make_arm(fss, state, area, stream, prec, args, dev, clusters=False):
-    """Fixed degree/theta treecode; block shape chosen by the autotuner."""
+    """Fixed degree/theta treecode; tree depth, source split and block shape
+    chosen by the autotuner."""
     ctx = fss.Context(method=fss.METHOD_TREECODE, precision=prec, degree=args.degree, theta=args.theta,
-                      cluster_targets=int(clusters), device=dev, autotune=1)
+                      cluster_targets=int(clusters), device=dev, autotune=2)
     ctx.set_stream(stream.cuda_stream)
     ctx.set_particles(state, area)
     return ctx
 
 
+def auto_tree_levels(n, leaf_target=64, max_levels=8):
+    """The library's automatic depth: the smallest whose mean leaf holds at
+    least leaf_target particles (fixed for the learned arm, whose network
+    was trained on leaves of that size)."""
+    ll = 0
+    while ll + 1 < max_levels and n / (20.0 * 4 ** (ll + 1)) >= leaf_target:
+        ll += 1
+    return ll + 1
+
+
 def make_learned_arm(fss, state, area, stream, args, dev, clusters=True):
     """Mixed precision with the learned per-leaf (degree, theta) (with target
-    clusters: carried up to the faces of a dual traversal); block shape
-    chosen by the autotuner."""
+    clusters: carried up to the faces of a dual traversal); block shape and
+    source split chosen by the autotuner on the learned lists (the tree
+    depth stays the automatic one, on which the selector's network was
+    trained)."""
     from fss_b200 import selector
     ctx = fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, list_mode=fss.LIST_LEAF,
-                      cluster_targets=int(clusters), degree=args.degree, theta=args.theta, device=dev, autotune=1)
+                      cluster_targets=int(clusters), degree=args.degree, theta=args.theta, device=dev, autotune=2,
+                      tree_levels=auto_tree_levels(state.shape[0]))
     ctx.set_stream(stream.cuda_stream)
     ctx.set_particles(state, area)
     choice = selector.apply(ctx, tol=args.tol, safety=args.safety, device=dev)
@@ -789,8 +803,11 @@ def main():
         c2 = make_arm(fss, state, area, stream, prec, args, dev, clusters=cl)
         e2 = rel_err(c2)
         v2, ms2 = time_arm(c2, stream, flush, args, ws)
+        ti = c2.tree_info()
         res[name] = {"value": v2, "ms_per_step": ms2, "rel_l2": e2[0], "rel_max": e2[1], "degree": args.degree,
-                     "theta": args.theta, "target_clusters": cl, "precision": "fp64" if prec == fss.PREC_FP64 else "mixed"}
+                     "theta": args.theta, "target_clusters": cl, "precision": "fp64" if prec == fss.PREC_FP64 else "mixed",
+                     "tuned": {"tree_levels": ti["tree_levels"], "src_parts": ti["src_parts"],
+                               "block_threads": ti["block_threads"]}}
         c2.close()
     fp64, fp64c, fixc = res.get("fp64_plain"), res.get("fp64_same_algorithm"), res.get("mixed_fixed_clusters")
 

@@ -78,6 +78,11 @@ struct fss_ctx {
     std::vector<std::vector<ASrc>> alists;  // per-leaf sources before packing
     std::vector<fss::TList> tlists;         // target clusters (cp/cc) and their sources
     std::vector<std::pair<fss::PairShape, double>> tuned;  // autotuner: shape, ms per pair pass
+    std::vector<std::pair<int, double>> tuned_depth;       // autotuner: tree levels, ms per RHS
+    std::vector<std::pair<int, double>> tuned_parts;       // autotuner: src_parts, ms per pair pass
+    int64_t depth_n = -1;  // particle count the tuned depth belongs to
+    int depth_tl = 0;      // tuned tree levels (0: none)
+    int src_parts_given = 0;  // src_parts of the configuration (0: the autotuner may choose)
     std::vector<int32_t> leaf_deg;
     std::vector<double> leaf_theta;
     int nmax = 0, level_mask = 0;

@@ -285,7 +285,7 @@ int ensure_particle_buffers(fss_ctx* c, int64_t n) {
 int build_tree(fss_ctx* c);
 PairShape choose_shape(fss_ctx* c);
 int materialize(fss_ctx* c, PairShape shape);
-int autotune(fss_ctx* c);
+int autotune(fss_ctx* c, bool depth);
 int refresh_stage(fss_ctx* c);
 int eval(fss_ctx* c, EpiArgs& ea, bool want_psi);
 
@@ -327,14 +327,16 @@ int set_particles(fss_ctx* c, int64_t n, const double* state5, const double* are
     TRY(gather(c, true));
     c->have = true;
     c->stage_dirty = false;
-    if (c->tree && c->cfg.autotune) TRY(autotune(c));
+    if (c->tree && c->cfg.autotune) TRY(autotune(c, true));
     TRY(refresh_stage(c));
     return check_device_error(c);
 }
 
 int build_tree(fss_ctx* c) {
     const int64_t n = c->n;
-    const int TL = auto_tree_levels(c->cfg, n);
+    // automatic depth: the autotuner's choice for this particle count, if any
+    const int TL = (c->cfg.tree_levels == 0 && c->depth_n == n && c->depth_tl > 0) ? c->depth_tl
+                                                                                   : auto_tree_levels(c->cfg, n);
     c->resort = c->cfg.rebuild == FSS_REBUILD_RESORT ||
                 (c->cfg.rebuild == FSS_REBUILD_AUTO && c->cfg.assign_mode != FSS_ASSIGN_REFERENCE);
     if (TL < 1 || TL > kMaxLevels) return fail(c, FSS_ERR_INVALID, "tree_levels out of range");
@@ -632,39 +634,112 @@ int eval(fss_ctx* c, EpiArgs& ea, bool want_psi) {
     return FSS_OK;
 }
 
-// Autotuner: time the pair kernel (after the upward pass) for every
-// supported block shape on the current lists and keep the fastest.
-int autotune(fss_ctx* c) {
+// Device time (ms, mean of `reps`) of `step` on the context's stream, after
+// one untimed run.
+struct TuneEvents {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~TuneEvents() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+template <class Step>
+int time_ms(fss_ctx* c, TuneEvents& ev, int reps, Step&& step, double* ms) {
+    TRY(step());
+    CU(cudaEventRecord(ev.a, c->stream));
+    for (int r = 0; r < reps; r++) TRY(step());
+    CU(cudaEventRecord(ev.b, c->stream));
+    CU(cudaEventSynchronize(ev.b));
+    float t = 0;
+    CU(cudaEventElapsedTime(&t, ev.a, ev.b));
+    *ms = double(t) / reps;
+    return FSS_OK;
+}
+
+// One whole right-hand side on the current stage state (for tuning).
+int tune_rhs(fss_ctx* c) {
+    EpiArgs ea;
+    ea.mode = EPI_RHS;
+    ea.out5 = c->out5.as<double>();
+    return eval(c, ea, false);
+}
+
+// Autotuner, run by fss_set_particles.  autotune >= 1: the pair kernel's
+// block shape -- every supported shape timed on the current lists (after
+// the upward pass), the fastest kept.  autotune >= 2 also: the tree depth
+// (leaf size), when the configuration leaves it automatic -- the automatic
+// depth and one level either side, each built and timed on a whole
+// right-hand side (the fastest is kept for this particle count); and the
+// source split (src_parts 1, 2, 4), when automatic, timed on the pairs.
+// depth = false (lists rebuilt for per-leaf parameters, which belong to the
+// current leaves) keeps the tree.
+int autotune(fss_ctx* c, bool depth) {
     c->tuned.clear();
     const bool prof_was = c->prof;
     c->prof = false;
-    cudaEvent_t a, b;
-    CU(cudaEventCreate(&a));
-    CU(cudaEventCreate(&b));
+    TuneEvents ev;
+    CU(cudaEventCreate(&ev.a));
+    CU(cudaEventCreate(&ev.b));
+    if (depth && c->cfg.autotune >= 2 && c->tree && c->cfg.tree_levels == 0 && c->depth_n != c->n) {
+        const int base = c->tree_levels;
+        int best_tl = base;
+        double best_ms = 1e30;
+        c->depth_n = c->n;
+        for (int tl = base - 1; tl <= base + 1; tl++) {
+            if (tl < 2 || tl > kMaxLevels) continue;
+            if (double(c->n) / (20.0 * std::pow(4.0, tl - 1)) < 8.0) continue;  // leaves under 8 particles
+            c->depth_tl = tl;
+            TRY(build_tree(c));
+            TRY(gather(c, true));
+            c->stage_dirty = false;
+            double ms = 0;
+            TRY(time_ms(c, ev, 2, [&] { return tune_rhs(c); }, &ms));
+            c->tuned_depth.push_back({tl, ms});
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_tl = tl;
+            }
+        }
+        c->depth_tl = best_tl;
+        if (c->tree_levels != best_tl) {
+            TRY(build_tree(c));
+            TRY(gather(c, true));
+            c->stage_dirty = false;
+        }
+    }
     PairShape best = c->shape;
     double best_ms = 1e30;
     for (const PairShape& sh : pair_shapes(c->fp64)) {
         TRY(materialize(c, sh));
         TRY(refresh_stage(c));
-        EpiArgs ea;
-        ea.mode = EPI_RHS;
-        ea.out5 = c->out5.as<double>();
-        TRY(eval(c, ea, false));  // warm (and proxies)
-        CU(cudaEventRecord(a, c->stream));
-        for (int r = 0; r < 2; r++)
-            TRY(launch_all_pairs(c, false));
-        CU(cudaEventRecord(b, c->stream));
-        CU(cudaEventSynchronize(b));
-        float ms = 0;
-        CU(cudaEventElapsedTime(&ms, a, b));
-        c->tuned.push_back({sh, ms / 2});
-        if (ms / 2 < best_ms) {
-            best_ms = ms / 2;
+        TRY(tune_rhs(c));  // proxies of the upward pass for the pair launches
+        double ms = 0;
+        TRY(time_ms(c, ev, 2, [&] { return launch_all_pairs(c, false); }, &ms));
+        c->tuned.push_back({sh, ms});
+        if (ms < best_ms) {
+            best_ms = ms;
             best = sh;
         }
     }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
+    if (c->cfg.autotune >= 2 && c->cfg.src_parts == 0) {
+        int best_p = 0;
+        double best_p_ms = 1e30;
+        for (int p : {1, 2, 4}) {
+            c->cfg.src_parts = p;
+            TRY(materialize(c, best));
+            TRY(refresh_stage(c));
+            TRY(tune_rhs(c));
+            double ms = 0;
+            TRY(time_ms(c, ev, 2, [&] { return launch_all_pairs(c, false); }, &ms));
+            c->tuned_parts.push_back({p, ms});
+            if (ms < best_p_ms) {
+                best_p_ms = ms;
+                best_p = p;
+            }
+        }
+        c->cfg.src_parts = best_p;
+    }
     TRY(materialize(c, best));
     c->prof = prof_was;
     c->stage_dirty = true;  // the timing passes overwrote the stage sources
@@ -792,6 +867,10 @@ int internal_relist(fss_ctx* c) {
     TRY(shard_filter(c));
     TRY(materialize(c, choose_shape(c)));
     c->stage_dirty = true;
+    if (c->cfg.autotune) {  // block shape (and source split) for the new lists
+        if (c->cfg.autotune >= 2 && c->src_parts_given == 0) c->cfg.src_parts = 0;  // tune it again
+        TRY(autotune(c, false));
+    }
     TRY(refresh_stage(c));
     return check_device_error(c);
 }
@@ -855,6 +934,7 @@ int fss_create(const fss_config* cfg, fss_ctx** out) {
     c->fp64 = cfg->precision == FSS_PREC_FP64;
     c->tree = cfg->method == FSS_METHOD_TREECODE;
     c->wait_ns = cfg->wait_limit_us > 0 ? uint64_t(cfg->wait_limit_us) * 1000ull : kWaitLimitNs;
+    c->src_parts_given = cfg->src_parts;
     CU(cudaSetDevice(c->dev));
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, c->dev));

@@ -101,8 +101,14 @@ typedef struct fss_config {
                               224 or 288 (0 = automatic: the smallest block
                               whose consumers hold the largest leaf) */
     int32_t targets_per_thread; /* 1 */
-    int32_t autotune;      /* at fss_set_particles, time every supported block
-                              shape on the actual lists and keep the fastest */
+    int32_t autotune;      /* at fss_set_particles: 1 = time every supported
+                              block shape of the pair kernel on the actual
+                              lists and keep the fastest; 2 = also, when
+                              tree_levels is 0, the tree depth (leaf size: the
+                              automatic depth and one level either side, each
+                              timed on a whole right-hand side, the fastest kept
+                              for this particle count) and, when src_parts is
+                              0, the source split (1, 2, 4: the fastest kept) */
     int32_t rebuild;       /* fss_rebuild_policy */
     int32_t cluster_targets; /* 1 = the reference's cp/cc interaction types
                               (fast_rhs.h cp, cc): a well-separated target face

@@ -78,3 +78,26 @@ def test_treecode_level7_sampled(fss, oracle):
             ctx.set_particles(s, a)
             out = ctx.rhs(s, a)
         assert rel_l2(out[rows, :3], ref) < 1e-6, prec
+
+
+def test_autotune_depth_and_split(fss, oracle):
+    """autotune = 2: the tree depth (automatic depth and one level either
+    side, timed on a whole right-hand side) and the source split are chosen
+    by timing; the result stays within the treecode's tolerance, and a later
+    fss_set_particles with the same particle count keeps the tuned depth."""
+    s, a = fss.make_state(6, "rh_vortices", n_vortex=8, seed=3)
+    rows = np.arange(0, s.shape[0], 17)
+    ref = oracle.rhs_direct_rows(s, a, rows)
+    with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as auto:
+        auto.set_particles(s, a)
+        base = auto.tree_info()["tree_levels"]
+    with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, autotune=2) as ctx:
+        ctx.set_particles(s, a)
+        info = ctx.tree_info()
+        out = ctx.rhs(s, a)
+        ctx.set_particles(s, a)
+        again = ctx.tree_info()
+    assert abs(info["tree_levels"] - base) <= 1
+    assert info["src_parts"] in (1, 2, 4)
+    assert again["tree_levels"] == info["tree_levels"]
+    assert rel_l2(out[rows, :3], ref) < 1e-6

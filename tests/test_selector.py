@@ -87,9 +87,11 @@ def test_selector_gain_over_fixed_degree(fss):
     if not os.path.exists(S.WEIGHTS):
         pytest.skip("no trained weights")
     r = S.evaluate(S.WEIGHTS, level=7, seed=4242, tol=1e-6, safety=2.0, n_vortex=16)
+    print("selector gain, target leaves:", r)
     assert r["learned"]["rel_l2"] <= 1e-6, r
     assert r["fixed"]["rel_l2"] <= 1e-6, r
-    assert r["interaction_ratio"] > 1.0, r
+    # measured 1.19 (exact interaction counts; deterministic for these weights and this field)
+    assert r["interaction_ratio"] > 1.15, r
 
 
 def test_class_tables_agree_with_library(fss):
@@ -121,5 +123,7 @@ def test_selector_gain_with_target_clusters(fss):
     if not os.path.exists(S.WEIGHTS_CLUSTERS):
         pytest.skip("no trained weights")
     r = S.evaluate(S.WEIGHTS_CLUSTERS, level=8, seed=4243, tol=1e-6, safety=2.0, n_vortex=24, clusters=True)
+    print("selector gain, target clusters:", r)
     assert r["learned"]["rel_l2"] <= 1e-6, r
-    assert r["interaction_ratio"] > 1.0, r
+    # measured 1.19 (exact interaction counts; deterministic for these weights and this field)
+    assert r["interaction_ratio"] > 1.15, r
