@@ -491,7 +491,7 @@ def kernel_rooflines(prof, steps, n, info, up_bytes, peaks):
         add("RK4 combine (k_epilogue, 4 per step)", prof["epilogue"][0] / steps,
             float(n) * (5 * 8 * 5 + 5 * 8 + 16), "step")
     if "downward" in prof:
-        out.append({"kernel": "downward pass (k_down_level, k_down_leaf)", "bound": "latency",
+        out.append({"kernel": "downward pass (k_down_coef, k_down_direct)", "bound": "latency",
                     "ms": prof["downward"][0] / (4 * steps), "per": "RHS"})
     return out
 

@@ -94,7 +94,7 @@ struct fss_ctx {
     // device
     DBuf in5, area_in, perm, key, key_tmp, vals_tmp, hist, leaf_start, s0, xs, acc, area_s, tracer_s, src, partials,
         segs, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
-        wtotal, err_flag, loc, sortq, grid3, rm_target, rm_tris, rm_off, rm_adj, down_jobs, down_anc, down_coef, vinvT;
+        wtotal, err_flag, loc, sortq, grid3, rm_target, rm_tris, rm_off, rm_adj, down_jobs, down_anc, down_coef, vinvT, up_deg;
     int64_t src_count = 0;
 
     // graph

@@ -473,11 +473,18 @@ int materialize(fss_ctx* c, PairShape shape) {
     // interpolation tables for the degrees in use
     c->nmax = std::max(L.max_degree, 0);
     c->level_mask = 0;
+    // per face, the highest proxy degree it serves (-1: no proxies), so the
+    // upward pass forms only the moments some list uses
+    std::vector<int8_t> up_deg(c->geom.node.size(), int8_t(-1));
     for (const ProxyJob& j : L.jobs) {
         c->level_mask |= 1 << j.level;
         for (int d = 0; d <= kMaxDegree; d++)
-            if ((j.degmask >> d) & 1) c->nmax = std::max(c->nmax, d);
+            if ((j.degmask >> d) & 1) {
+                c->nmax = std::max(c->nmax, d);
+                up_deg[size_t(j.node)] = int8_t(std::max<int>(up_deg[size_t(j.node)], d));
+            }
     }
+    TRY(upload(c, c->up_deg, up_deg));
     std::vector<double> vinv_all, vinvT_all;
     std::vector<int32_t> vinv_off(kMaxDegree + 1, 0);
     for (int d = 0; d <= c->nmax; d++) {
@@ -561,7 +568,7 @@ int eval_partials(fss_ctx* c, bool want_psi, bool* down_out) {
             ProfScope ps(c, "upward_leaf");
             launch_up_leaf(c->stream, c->fp64, int(c->nleaf), c->src.p, c->leaf_start.as<int32_t>(), nullptr,
                            c->node.as<NodeGeom>(), c->lev_off.as<int64_t>(),
-                           c->leaf_level, c->nmax, c->level_mask, c->part_up.as<double>());
+                           c->leaf_level, c->nmax, c->level_mask, c->up_deg.as<int8_t>(), c->part_up.as<double>());
         }
         {
             ProfScope ps(c, "upward_combine");

@@ -17,17 +17,20 @@ namespace fss {
 __global__ void __launch_bounds__(kUpThreads) k_up_leaf_batch(const float4* __restrict__ src, const EnsLeaf* __restrict__ leaves,
                                                        const int32_t* __restrict__ leaf_start,
                                                        const NodeGeom* __restrict__ node,
-                                                       const int64_t* __restrict__ lev_off, int nmax,
+                                                       const int64_t* __restrict__ lev_off, int nmax, int nleaf,
                                                        double* __restrict__ part) {
-    __shared__ double W[kUpRows][kUpLd];
-    __shared__ double V[kUpRows][kUpLd];
-    const EnsLeaf lf = leaves[blockIdx.x];
+    __shared__ double W[kUpLeaves][kUpRows][kUpLd];
+    __shared__ double V[kUpLeaves][kUpRows][kUpLd];
+    const int w = threadIdx.x >> 5;
+    const int i = blockIdx.x * kUpLeaves + w;
+    if (i >= nleaf) return;  // whole warps; no block-wide barrier follows
+    const EnsLeaf lf = leaves[i];
     const int a0 = leaf_start[lf.gleaf], a1 = leaf_start[lf.gleaf + 1];
     const int KM = nproxy(nmax);
     for (int l = 0; l <= lf.leaf_level; l++) {
         if (!((lf.level_mask >> l) & 1)) continue;
         const NodeGeom ng = node[lev_off[l] + (lf.local >> (2 * (lf.leaf_level - l)))];
-        leaf_moments<float>(src, a0, a1, 0.0, 0.0, 0.0, ng, nmax, W, V, part + lf.part_base + int64_t(l) * KM);
+        leaf_moments<float>(src, a0, a1, 0.0, 0.0, 0.0, ng, nmax, W[w], V[w], part + lf.part_base + int64_t(l) * KM);
     }
 }
 
@@ -80,8 +83,8 @@ void launch_up_leaf_batch(cudaStream_t st, int nleaf, const void* src, const Ens
                           const int32_t* leaf_start, const NodeGeom* node, const int64_t* lev_off, int nmax,
                           double* part) {
     if (nleaf == 0) return;
-    k_up_leaf_batch<<<nleaf, 128, 0, st>>>(static_cast<const float4*>(src), leaves, leaf_start, node, lev_off, nmax,
-                                           part);
+    k_up_leaf_batch<<<unsigned((nleaf + kUpLeaves - 1) / kUpLeaves), kUpThreads, 0, st>>>(
+        static_cast<const float4*>(src), leaves, leaf_start, node, lev_off, nmax, nleaf, part);
 }
 
 void launch_up_combine_batch(cudaStream_t st, int njobs, const ProxyJob* jobs, const EnsLeaf* leaves,

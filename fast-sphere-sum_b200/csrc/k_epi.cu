@@ -18,16 +18,23 @@ namespace fss {
 // level), summed over the leaves of each face and contracted with Vinv
 // (kernel 2).  FP64.
 
+// One warp per leaf: the leaf's moments in the frame of every ancestor level
+// in level_mask, up to the degree up_deg[node] its proxies need (none when
+// -1; nmax everywhere without up_deg).  Slots keep the stride nproxy(nmax);
+// moments above a node's degree are not written and never read.
 template <typename T>
 __global__ void __launch_bounds__(kUpThreads) k_up_leaf(const typename Vec4<T>::type* __restrict__ src,
                                                         const int32_t* __restrict__ leaf_start,
                                                         const double4* __restrict__ frame,
                                                         const NodeGeom* __restrict__ node,
                                                         const int64_t* __restrict__ lev_off, int leaf_level,
-                                                        int nmax, int level_mask, double* __restrict__ part) {
-    __shared__ double W[kUpRows][kUpLd];
-    __shared__ double V[kUpRows][kUpLd];
-    const int leaf = blockIdx.x;
+                                                        int nmax, int level_mask, const int8_t* __restrict__ up_deg,
+                                                        int nleaf, double* __restrict__ part) {
+    __shared__ double W[kUpLeaves][kUpRows][kUpLd];
+    __shared__ double V[kUpLeaves][kUpRows][kUpLd];
+    const int w = threadIdx.x >> 5;
+    const int leaf = blockIdx.x * kUpLeaves + w;
+    if (leaf >= nleaf) return;  // whole warps; no block-wide barrier follows
     const int KM = nproxy(nmax);
     const int a0 = leaf_start[leaf], a1 = leaf_start[leaf + 1];
     double fx = 0, fy = 0, fz = 0;
@@ -37,8 +44,11 @@ __global__ void __launch_bounds__(kUpThreads) k_up_leaf(const typename Vec4<T>::
     }
     for (int l = 0; l <= leaf_level; l++) {
         if (!((level_mask >> l) & 1)) continue;
-        const NodeGeom ng = node[lev_off[l] + (leaf >> (2 * (leaf_level - l)))];
-        leaf_moments<T>(src, a0, a1, fx, fy, fz, ng, nmax, W, V,
+        const int64_t gi = lev_off[l] + (leaf >> (2 * (leaf_level - l)));
+        const int nm = up_deg ? int(up_deg[gi]) : nmax;  // warp-uniform
+        if (nm < 0) continue;
+        const NodeGeom ng = node[gi];
+        leaf_moments<T>(src, a0, a1, fx, fy, fz, ng, nm, W[w], V[w],
                         part + (int64_t(leaf) * (leaf_level + 1) + l) * KM);
     }
 }
@@ -54,8 +64,9 @@ __global__ void __launch_bounds__(kUpThreads) k_up_combine(const ProxyJob* __res
     // read in place: a copy indexed by a run-time degree (job.off[d]) would sit in local memory
     const ProxyJob& job = jobs[blockIdx.x];
     const int tid = threadIdx.x;
-    const int KM = nproxy(nmax);
-    if (tid < KM) {
+    const int KM = nproxy(nmax);                       // slot stride
+    const int KJ = nproxy(31 - __clz(job.degmask));    // moments this face's degrees use
+    if (tid < KJ) {
         // four independent sums over the face's leaves (four rows in flight)
         const int64_t stride = int64_t(leaf_level + 1) * KM;
         const double* p = part + (int64_t(job.leaf_lo) * (leaf_level + 1) + job.level) * KM + tid;
@@ -436,14 +447,15 @@ __global__ void __launch_bounds__(kUpThreads) k_down_direct(const double4* __res
 
 void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, const int32_t* leaf_start,
                     const double4* frame, const NodeGeom* node, const int64_t* lev_off, int leaf_level, int nmax,
-                    int level_mask, double* part) {
+                    int level_mask, const int8_t* up_deg, double* part) {
     if (nleaf == 0 || level_mask == 0) return;
+    const unsigned nb = unsigned((nleaf + kUpLeaves - 1) / kUpLeaves);
     if (fp64)
-        k_up_leaf<double><<<nleaf, kUpThreads, 0, st>>>(static_cast<const double4*>(src), leaf_start, frame, node,
-                                                        lev_off, leaf_level, nmax, level_mask, part);
+        k_up_leaf<double><<<nb, kUpThreads, 0, st>>>(static_cast<const double4*>(src), leaf_start, frame, node,
+                                                     lev_off, leaf_level, nmax, level_mask, up_deg, nleaf, part);
     else
-        k_up_leaf<float><<<nleaf, kUpThreads, 0, st>>>(static_cast<const float4*>(src), leaf_start, frame, node,
-                                                       lev_off, leaf_level, nmax, level_mask, part);
+        k_up_leaf<float><<<nb, kUpThreads, 0, st>>>(static_cast<const float4*>(src), leaf_start, frame, node,
+                                                    lev_off, leaf_level, nmax, level_mask, up_deg, nleaf, part);
 }
 
 void launch_up_combine(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part, int leaf_level,

@@ -89,7 +89,7 @@ int persistent_blocks_per_sm();
 // k_epi.cu
 void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, const int32_t* leaf_start,
                     const double4* frame, const NodeGeom* node, const int64_t* lev_off, int leaf_level, int nmax,
-                    int level_mask, double* part);
+                    int level_mask, const int8_t* up_deg, double* part);
 void launch_up_combine(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part, int leaf_level,
                        int nmax, const double* vinv, const int32_t* vinv_off, const double4* proxy_pos,
                        const NodeGeom* node, int local_frames, int64_t n, void* src);

@@ -38,6 +38,21 @@ def test_treecode_converges_with_degree(fss, field5):
     assert errs[-1] < 1e-7, errs
 
 
+def test_treecode_high_degrees(fss, field5):
+    """Degrees 9 and 11 form the moments beyond the 8 x 8 corner in one
+    permuted tile, degree 12 (the maximum) in two.  Both must beat degree 9
+    by far (a wrong moment costs digits, not a factor); 11 and 12 need not be
+    ordered (at theta = 0.7 on this field, 1.5e-9 and 3.0e-9)."""
+    s, a, ref = field5
+    errs = {}
+    for n in (9, 11, 12):
+        with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_FP64, degree=n, theta=0.7) as ctx:
+            ctx.set_particles(s, a)
+            errs[n] = rel_l2(ctx.rhs(s, a)[:, :3], ref[:, :3])
+    assert errs[9] < 1e-7, errs
+    assert max(errs[11], errs[12]) < errs[9] / 4, errs
+
+
 def test_treecode_theta_tightens(fss, field5):
     s, a, ref = field5
     e = {}
