@@ -39,6 +39,7 @@ struct fss_ensemble {
     std::vector<int64_t> poff, pxoff, loff;  // particle, proxy-slot and leaf offsets per member
     int64_t ntot = 0, nprox = 0, nleaf = 0;
     int nmax = 0, blocks = 0;
+    int max_leaf_level = 0;  // deepest member's leaf level
     double interactions = 0;
     bool built = false, resort = false;
     DBuf s0, xs, acc, area, tracer, perm, src, partials, segs, items, jobs, leaves, leaf_start, part, proxy_pos, vinv,
@@ -100,7 +101,8 @@ int stage(fss_ensemble* e, int st, double dt, double omega) {
         if (r) return r;
     }
     launch_up_leaf_batch(e->stream, int(e->nleaf), e->src.p, e->leaves.as<EnsLeaf>(), e->leaf_start.as<int32_t>(),
-                         e->node.as<NodeGeom>(), e->lev_off.as<int64_t>(), e->nmax, e->part.as<double>());
+                         e->node.as<NodeGeom>(), e->lev_off.as<int64_t>(), e->nmax, e->max_leaf_level,
+                         e->part.as<double>());
     launch_up_combine_batch(e->stream, int(e->njobs), e->jobs.as<ProxyJob>(), e->leaves.as<EnsLeaf>(),
                             e->part.as<double>(), e->nmax, e->vinv.as<double>(), e->vinv_off.as<int32_t>(),
                             e->proxy_pos.as<double4>(), e->ntot, e->src.p);
@@ -276,6 +278,7 @@ int fss_ensemble_build(fss_ensemble* e) {
         e->interactions += L.pp_pairs + L.pc_pairs;
     }
     lstart.push_back(int32_t(e->ntot));
+    e->max_leaf_level = maxTL - 1;
     // longest source lists first across all members
     {
         std::vector<size_t> order(items.size());

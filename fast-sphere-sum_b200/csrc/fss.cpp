@@ -1136,6 +1136,8 @@ int fss_get_tree_info(fss_ctx* c, fss_tree_info* info) {
     info->target_clusters = int32_t(c->lists.down.size());
     info->cp_interactions = c->lists.cp_pairs;
     info->cc_interactions = c->lists.cc_pairs;
+    info->max_degree = c->tree ? c->nmax : 0;
+    info->max_cluster_points = c->lists.down.empty() ? 0 : int32_t(c->lists.max_cluster_k);
     if (c->tree && c->have) {
         const int64_t nl = c->lists.n_leaf_items, na = int64_t(c->lists.items.size());
         info->lane_pairs_leaf = lane_pairs(c, 0, nl, c->shape.targets());

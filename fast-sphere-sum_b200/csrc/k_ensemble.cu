@@ -9,11 +9,13 @@
 
 namespace fss {
 
-// Upward pass over the leaves of every member.  Leaf g: particles
-// [leaf_start[g], leaf_start[g+1]) of the concatenated arrays (current after
-// each re-sort), leaf level LL, index within its member's leaf level, and
-// the start of its moment slots (LL + 1 levels x KM); moments as for one
-// problem (leaf_moments).
+// Upward pass over the leaves of every member.  Leaf i: particles
+// [leaf_start[g], leaf_start[g+1]) of the concatenated arrays (g = its
+// gleaf, current after each re-sort), its member's leaf level LL, index on
+// that level, and the start of its moment slots (LL + 1 levels x KM).
+// Every member has 20 * 4^LL leaves and starts at a multiple of four, so
+// entries 4 b .. 4 b + 3 are one member's sibling group; block (b, level)
+// forms its rows as the single problem's k_up_leaf does (up_row_step).
 __global__ void __launch_bounds__(kUpThreads) k_up_leaf_batch(const float4* __restrict__ src, const EnsLeaf* __restrict__ leaves,
                                                        const int32_t* __restrict__ leaf_start,
                                                        const NodeGeom* __restrict__ node,
@@ -21,21 +23,35 @@ __global__ void __launch_bounds__(kUpThreads) k_up_leaf_batch(const float4* __re
                                                        double* __restrict__ part) {
     __shared__ double W[kUpLeaves][kUpRows][kUpLd];
     __shared__ double V[kUpLeaves][kUpRows][kUpLd];
+    __shared__ double O[kUpLeaves][kMaxK];
+    const int l = blockIdx.y;
     const int w = threadIdx.x >> 5;
     const int i = blockIdx.x * kUpLeaves + w;
-    if (i >= nleaf) return;  // whole warps; no block-wide barrier follows
-    const EnsLeaf lf = leaves[i];
-    const int a0 = leaf_start[lf.gleaf], a1 = leaf_start[lf.gleaf + 1];
+    const EnsLeaf lf = leaves[min(i, nleaf - 1)];
+    // block-uniform: the group's member (its leaf level and level mask)
+    if (l > lf.leaf_level || !((lf.level_mask >> l) & 1)) return;
     const int KM = nproxy(nmax);
-    for (int l = 0; l <= lf.leaf_level; l++) {
-        if (!((lf.level_mask >> l) & 1)) continue;
-        const NodeGeom ng = node[lev_off[l] + (lf.local >> (2 * (lf.leaf_level - l)))];
-        leaf_moments<float>(src, a0, a1, 0.0, 0.0, 0.0, ng, nmax, W[w], V[w], part + lf.part_base + int64_t(l) * KM);
+    const NodeGeom& ng = node[lev_off[l] + (lf.local >> (2 * (lf.leaf_level - l)))];
+    if (l == lf.leaf_level) {
+        if (i >= nleaf) return;
+        leaf_moments<float>(src, leaf_start[lf.gleaf], leaf_start[lf.gleaf + 1], 0.0, 0.0, 0.0, ng, nmax, W[w], V[w],
+                            part + lf.part_base + int64_t(l) * KM);
+        return;
     }
+    if (i < nleaf) {
+        leaf_moments<float>(src, leaf_start[lf.gleaf], leaf_start[lf.gleaf + 1], 0.0, 0.0, 0.0, ng, nmax, W[w], V[w],
+                            O[w]);
+    } else {
+        for (int m = threadIdx.x & 31; m < KM; m += 32) O[w][m] = 0.0;
+    }
+    __syncthreads();
+    double* out = part + leaves[blockIdx.x * kUpLeaves].part_base + int64_t(l) * KM;
+    for (int m = threadIdx.x; m < KM; m += kUpThreads) out[m] = (O[0][m] + O[1][m]) + (O[2][m] + O[3][m]);
 }
 
-// Proxy charges of every member's far clusters: job j sums the moments of
-// its leaves (global leaf indices, slots through EnsLeaf::part_base).
+// Proxy charges of every member's far clusters: job j sums the rows of its
+// leaves (global leaf indices, slots through EnsLeaf::part_base) as the
+// single problem's k_up_combine does.
 __global__ void __launch_bounds__(128) k_up_combine_batch(const ProxyJob* __restrict__ jobs,
                                                           const EnsLeaf* __restrict__ leaves,
                                                           const double* __restrict__ part, int nmax,
@@ -49,20 +65,10 @@ __global__ void __launch_bounds__(128) k_up_combine_batch(const ProxyJob* __rest
     const int tid = threadIdx.x;
     const int KM = nproxy(nmax);
     if (tid < KM) {
-        // four independent sums over the face's leaves, as the single
-        // problem's combine forms them (same order, same result)
+        const int step = up_row_step(job.level, leaves[job.leaf_lo].leaf_level);
         const int64_t off = int64_t(job.level) * KM + tid;
-        const int nl = job.leaf_hi - job.leaf_lo;
-        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-        int lf = 0;
-        for (; lf + 4 <= nl; lf += 4) {
-            s0 += part[leaves[job.leaf_lo + lf + 0].part_base + off];
-            s1 += part[leaves[job.leaf_lo + lf + 1].part_base + off];
-            s2 += part[leaves[job.leaf_lo + lf + 2].part_base + off];
-            s3 += part[leaves[job.leaf_lo + lf + 3].part_base + off];
-        }
-        for (; lf < nl; lf++) s0 += part[leaves[job.leaf_lo + lf].part_base + off];
-        M[tid] = (s0 + s1) + (s2 + s3);
+        M[tid] = sum_rows4([&](int r) { return part[leaves[job.leaf_lo + r * step].part_base + off]; },
+                           (job.leaf_hi - job.leaf_lo) / step);
     }
     __syncthreads();
     for (int d = 0; d <= nmax; d++) {
@@ -81,9 +87,10 @@ __global__ void __launch_bounds__(128) k_up_combine_batch(const ProxyJob* __rest
 
 void launch_up_leaf_batch(cudaStream_t st, int nleaf, const void* src, const EnsLeaf* leaves,
                           const int32_t* leaf_start, const NodeGeom* node, const int64_t* lev_off, int nmax,
-                          double* part) {
+                          int max_leaf_level, double* part) {
     if (nleaf == 0) return;
-    k_up_leaf_batch<<<unsigned((nleaf + kUpLeaves - 1) / kUpLeaves), kUpThreads, 0, st>>>(
+    const dim3 grid(unsigned((nleaf + kUpLeaves - 1) / kUpLeaves), unsigned(max_leaf_level + 1));
+    k_up_leaf_batch<<<grid, kUpThreads, 0, st>>>(
         static_cast<const float4*>(src), leaves, leaf_start, node, lev_off, nmax, nleaf, part);
 }
 

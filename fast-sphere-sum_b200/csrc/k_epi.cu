@@ -18,10 +18,12 @@ namespace fss {
 // level), summed over the leaves of each face and contracted with Vinv
 // (kernel 2).  FP64.
 
-// One warp per leaf: the leaf's moments in the frame of every ancestor level
-// in level_mask, up to the degree up_deg[node] its proxies need (none when
-// -1; nmax everywhere without up_deg).  Slots keep the stride nproxy(nmax);
-// moments above a node's degree are not written and never read.
+// Block (group g of four sibling leaves, level l = blockIdx.y): warp w takes
+// leaf 4 g + w, its moments in the frame of its ancestor on level l (levels
+// outside level_mask: no work), up to the degree up_deg[face] its proxies
+// need (none when -1; nmax everywhere without up_deg).  Rows as described
+// at up_row_step; slots keep the stride nproxy(nmax), and moments above a
+// face's degree are neither written nor read.
 template <typename T>
 __global__ void __launch_bounds__(kUpThreads) k_up_leaf(const typename Vec4<T>::type* __restrict__ src,
                                                         const int32_t* __restrict__ leaf_start,
@@ -32,25 +34,35 @@ __global__ void __launch_bounds__(kUpThreads) k_up_leaf(const typename Vec4<T>::
                                                         int nleaf, double* __restrict__ part) {
     __shared__ double W[kUpLeaves][kUpRows][kUpLd];
     __shared__ double V[kUpLeaves][kUpRows][kUpLd];
+    __shared__ double O[kUpLeaves][kMaxK];
+    const int l = blockIdx.y;
+    if (!((level_mask >> l) & 1)) return;  // block-uniform
     const int w = threadIdx.x >> 5;
     const int leaf = blockIdx.x * kUpLeaves + w;
-    if (leaf >= nleaf) return;  // whole warps; no block-wide barrier follows
     const int KM = nproxy(nmax);
-    const int a0 = leaf_start[leaf], a1 = leaf_start[leaf + 1];
+    const int64_t gi = lev_off[l] + (min(leaf, nleaf - 1) >> (2 * (leaf_level - l)));
+    const int nm = up_deg ? int(up_deg[gi]) : nmax;  // block-uniform above the leaf level
     double fx = 0, fy = 0, fz = 0;
-    if (frame) {
+    if (frame && leaf < nleaf) {
         const double4 f = frame[leaf];
         fx = f.x; fy = f.y; fz = f.z;
     }
-    for (int l = 0; l <= leaf_level; l++) {
-        if (!((level_mask >> l) & 1)) continue;
-        const int64_t gi = lev_off[l] + (leaf >> (2 * (leaf_level - l)));
-        const int nm = up_deg ? int(up_deg[gi]) : nmax;  // warp-uniform
-        if (nm < 0) continue;
-        const NodeGeom ng = node[gi];
-        leaf_moments<T>(src, a0, a1, fx, fy, fz, ng, nm, W[w], V[w],
+    if (l == leaf_level) {  // one row per leaf; warps independent
+        if (leaf >= nleaf || nm < 0) return;
+        leaf_moments<T>(src, leaf_start[leaf], leaf_start[leaf + 1], fx, fy, fz, node[gi], nm, W[w], V[w],
                         part + (int64_t(leaf) * (leaf_level + 1) + l) * KM);
+        return;
     }
+    if (nm < 0) return;  // the group's common ancestor takes no proxies
+    const int KJ = nproxy(nm);
+    if (leaf < nleaf) {
+        leaf_moments<T>(src, leaf_start[leaf], leaf_start[leaf + 1], fx, fy, fz, node[gi], nm, W[w], V[w], O[w]);
+    } else {
+        for (int m = threadIdx.x & 31; m < KJ; m += 32) O[w][m] = 0.0;
+    }
+    __syncthreads();
+    double* out = part + (int64_t(blockIdx.x) * kUpLeaves * (leaf_level + 1) + l) * KM;
+    for (int m = threadIdx.x; m < KJ; m += kUpThreads) out[m] = (O[0][m] + O[1][m]) + (O[2][m] + O[3][m]);
 }
 
 template <typename T>
@@ -67,20 +79,11 @@ __global__ void __launch_bounds__(kUpThreads) k_up_combine(const ProxyJob* __res
     const int KM = nproxy(nmax);                       // slot stride
     const int KJ = nproxy(31 - __clz(job.degmask));    // moments this face's degrees use
     if (tid < KJ) {
-        // four independent sums over the face's leaves (four rows in flight)
-        const int64_t stride = int64_t(leaf_level + 1) * KM;
+        // the face's rows (one per group of four leaves above the leaf level)
+        const int step = up_row_step(job.level, leaf_level);
+        const int64_t stride = int64_t(step) * (leaf_level + 1) * KM;
         const double* p = part + (int64_t(job.leaf_lo) * (leaf_level + 1) + job.level) * KM + tid;
-        const int nl = job.leaf_hi - job.leaf_lo;
-        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-        int lf = 0;
-        for (; lf + 4 <= nl; lf += 4) {
-            s0 += p[(lf + 0) * stride];
-            s1 += p[(lf + 1) * stride];
-            s2 += p[(lf + 2) * stride];
-            s3 += p[(lf + 3) * stride];
-        }
-        for (; lf < nl; lf++) s0 += p[lf * stride];
-        M[tid] = (s0 + s1) + (s2 + s3);
+        M[tid] = sum_rows4([&](int i) { return p[i * stride]; }, (job.leaf_hi - job.leaf_lo) / step);
     }
     __syncthreads();
     double cx = 0, cy = 0, cz = 0;
@@ -449,7 +452,7 @@ void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, cons
                     const double4* frame, const NodeGeom* node, const int64_t* lev_off, int leaf_level, int nmax,
                     int level_mask, const int8_t* up_deg, double* part) {
     if (nleaf == 0 || level_mask == 0) return;
-    const unsigned nb = unsigned((nleaf + kUpLeaves - 1) / kUpLeaves);
+    const dim3 nb(unsigned((nleaf + kUpLeaves - 1) / kUpLeaves), unsigned(leaf_level + 1));
     if (fp64)
         k_up_leaf<double><<<nb, kUpThreads, 0, st>>>(static_cast<const double4*>(src), leaf_start, frame, node,
                                                      lev_off, leaf_level, nmax, level_mask, up_deg, nleaf, part);

@@ -32,6 +32,7 @@ namespace fss {
 
 constexpr int kDepth = 4;  // ring depth (tiles in flight)
 constexpr int TILE_F32 = tile_capacity(false);
+constexpr float kSelfR2 = 1e-30f;  // r^2 bias of the FP32 loop (a normal float; 1 / kSelfR2 finite)
 
 // Sources j = j0, j0 + step, ... < cnt of an FP64 tile (step 1: all of them).
 template <typename T, bool PSI, bool GUARD, bool STRIDED>
@@ -64,7 +65,13 @@ __device__ __forceinline__ void tile_pairs(const typename Vec4<T>::type* __restr
 // multiple of 4 sources with w = 0 at the origin (|x_i - 0|^2 = 1, no
 // contribution).  One 128-bit shared load brings a component of four
 // sources; each pair of sources goes through the packed f32x2 pipe: per
-// four sources 4 shared loads, 18 packed operations and 4 reciprocals.
+// four sources 4 shared loads, 20 packed operations and 4 reciprocals.
+// The self pair (and any source at the target's position) needs no select:
+// r^2 starts from kSelfR2 = 1e-30 inside the first FMA, so it gets
+// 1 / r^2 = 1e30 and w 1e30 * (x_j - x_i) = 0; every other pair's r^2 (at
+// least ~1e-12 between distinct particles on the unit sphere) is unchanged
+// by the bias except when the exact d_x^2 falls on a rounding tie.  Only
+// the stream function's log needs the guard (GUARD: tiles holding targets).
 // Quads q = q0, q0 + step, ... < nquad of the tile (step 1: all of them).
 template <bool PSI, bool GUARD, bool STRIDED>
 __device__ __forceinline__ void tile_pairs_soa(const float* __restrict__ s, int nquad, int q0, int step, f2 ntx,
@@ -74,6 +81,7 @@ __device__ __forceinline__ void tile_pairs_soa(const float* __restrict__ s, int 
         q0 = 0;
         step = 1;
     }
+    const f2 eps = f2_pack(kSelfR2, kSelfR2);
 #pragma unroll 4
     for (int q = q0; q < nquad; q += step) {
         const float4 X = reinterpret_cast<const float4*>(s)[q];
@@ -89,14 +97,10 @@ __device__ __forceinline__ void tile_pairs_soa(const float* __restrict__ s, int 
             const f2 dx = f2_add(qx[h], ntx);
             const f2 dy = f2_add(qy[h], nty);
             const f2 dz = f2_add(qz[h], ntz);
-            const f2 r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+            const f2 r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_fma(dx, dx, eps)));
             float r0, r1;
             f2_unpack(r2, r0, r1);
-            float i0 = rcp_fast(r0), i1 = rcp_fast(r1);
-            if (GUARD) {
-                i0 = (r0 > 0.f) ? i0 : 0.f;
-                i1 = (r1 > 0.f) ? i1 : 0.f;
-            }
+            const float i0 = rcp_fast(r0), i1 = rcp_fast(r1);
             const f2 sc = f2_mul(qw[h], f2_pack(i0, i1));
             ax = f2_fma(sc, dx, ax);
             ay = f2_fma(sc, dy, ay);
@@ -104,8 +108,8 @@ __device__ __forceinline__ void tile_pairs_soa(const float* __restrict__ s, int 
             if (PSI) {
                 float l0 = lg2_fast(r0), l1 = lg2_fast(r1);
                 if (GUARD) {
-                    l0 = (r0 > 0.f) ? l0 : 0.f;
-                    l1 = (r1 > 0.f) ? l1 : 0.f;
+                    l0 = (r0 > kSelfR2) ? l0 : 0.f;
+                    l1 = (r1 > kSelfR2) ? l1 : 0.f;
                 }
                 float w0, w1;
                 f2_unpack(qw[h], w0, w1);
@@ -344,13 +348,14 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
                         const int nq = (h.count + 3) >> 2;
                         f2 px = 0, py = 0, pz = 0;
                         float pw = 0.f;
+                        // (the velocity needs no guard; only the stream function's log does)
                         if (L == 1) {
-                            if (h.guard)
+                            if (PSI && h.guard)
                                 tile_pairs_soa<PSI, true, false>(tile, nq, 0, 1, ntx, nty, ntz, px, py, pz, pw);
                             else
                                 tile_pairs_soa<PSI, false, false>(tile, nq, 0, 1, ntx, nty, ntz, px, py, pz, pw);
                         } else {
-                            if (h.guard)
+                            if (PSI && h.guard)
                                 tile_pairs_soa<PSI, true, true>(tile, nq, sub, L, ntx, nty, ntz, px, py, pz, pw);
                             else
                                 tile_pairs_soa<PSI, false, true>(tile, nq, sub, L, ntx, nty, ntz, px, py, pz, pw);

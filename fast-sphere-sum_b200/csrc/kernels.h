@@ -175,7 +175,7 @@ void launch_scan_u32(cudaStream_t st, uint32_t* a, int64_t m, uint32_t* part);
 // k_ensemble.cu
 void launch_up_leaf_batch(cudaStream_t st, int nleaf, const void* src, const EnsLeaf* leaves,
                           const int32_t* leaf_start, const NodeGeom* node, const int64_t* lev_off, int nmax,
-                          double* part);
+                          int max_leaf_level, double* part);
 void launch_up_combine_batch(cudaStream_t st, int njobs, const ProxyJob* jobs, const EnsLeaf* leaves,
                              const double* part, int nmax, const double* vinv, const int32_t* vinv_off,
                              const double4* proxy_pos, int64_t n, void* src);

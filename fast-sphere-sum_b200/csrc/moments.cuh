@@ -11,33 +11,31 @@ constexpr int kUpRows = 16;              // basis rows (degree <= 15), zero beyo
 constexpr int kUpLd = 32 + 4;            // padded row: the 8 rows x 4 doubles a DMMA operand reads hit distinct banks
 
 // Moments of the particles [a0, a1) of one leaf in the frame of one
-// ancestor face (FP64), by one warp.  Per chunk of 32 particles each lane
-// writes its particle's basis W[a][j] = w T_a(u), V[b][j] = T_b(v) into the
-// warp's own shared rows; then the moments M_ab (a + b <= n) as 8 x 8 tiles
-// of W V^T on the FP64 tensor cores, over the chunk's groups of four
-// particles.  Tile 0 is a, b < 8.  The rest (a >= 8 or b >= 8, so the other
-// index <= n - 8) is one tile with rows a = 8..n, 0..n-8 and columns
-// b = 0..n-8, 8..n when n <= 11, else the two tiles a >= 8, b < 8 and
-// a < 8, b >= 8 (none for n < 8).  Lane (4 g + t) holds D[g][2t + {0, 1}]
-// of each tile; every moment is written once, to out[m], m = (a + b)(a + b +
-// 1) / 2 + b.  The groups of four particles are taken in particle order, so
-// a moment's sum does not depend on which tile forms it or on the chunking.
-template <typename T>
-__device__ __forceinline__ void leaf_moments(const typename Vec4<T>::type* __restrict__ src, int a0, int a1,
-                                             double fx, double fy, double fz, const NodeGeom& ng, int nmax,
-                                             double (*W)[kUpLd], double (*V)[kUpLd], double* __restrict__ out) {
+// ancestor face (FP64), by one warp, up to degree NM.  Per chunk of 32
+// particles each lane writes its particle's basis W[a][j] = w T_a(u),
+// V[b][j] = T_b(v), a, b <= NM, into the warp's own shared rows; then the
+// moments M_ab (a + b <= NM) as 8 x 8 tiles of W V^T on the FP64 tensor
+// cores, over the chunk's groups of four particles.  Tile 0 is a, b < 8.
+// The rest (a >= 8 or b >= 8, so the other index <= NM - 8) is one tile
+// with rows a = 8..NM, 0..NM-8 and columns b = 0..NM-8, 8..NM when NM <= 11,
+// else the two tiles a >= 8, b < 8 and a < 8, b >= 8 (none for NM < 8).
+// Rows above NM are neither formed nor stored: a tile may read such a row
+// (left from earlier chunks), but it only reaches outputs with a + b > NM,
+// which are dropped.  Lane (4 g + t) holds D[g][2t + {0, 1}] of each tile;
+// every moment is written once, to out[m], m = (a + b)(a + b + 1) / 2 + b.
+// The groups of four particles are taken in particle order, so a moment's
+// sum does not depend on which tile forms it, on NM or on the chunking.
+template <typename T, int NM>
+__device__ __forceinline__ void leaf_moments_n(const typename Vec4<T>::type* __restrict__ src, int a0, int a1,
+                                               double fx, double fy, double fz, const NodeGeom& ng,
+                                               double (*W)[kUpLd], double (*V)[kUpLd], double* __restrict__ out) {
+    static_assert(NM >= 0 && NM < kUpRows, "degree beyond the basis rows");
+    constexpr int NT = NM < 8 ? 1 : (NM <= 11 ? 2 : 3);  // tiles
+    constexpr int H = NM - 7;                            // rows 8..NM when NT == 2
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    // the rows (of W) and columns (of V) of the tiles beyond tile 0
-    const int ntiles = nmax < 8 ? 1 : (nmax <= 11 ? 2 : 3);  // warp-uniform
-    const int h = nmax - 7;                                    // rows 8..nmax when nmax <= 11
-    int ra1, cb1;                                             // tile 1, this lane's row and B column
-    if (ntiles == 2) {
-        ra1 = g < h ? 8 + g : g - h;
-        cb1 = g < h ? g : 8 + (g - h);
-    } else {
-        ra1 = 8 + g;  // a >= 8, b < 8
-        cb1 = g;
-    }
+    // tile 1: this lane's row of W and column of V
+    const int ra1 = NT == 2 ? (g < H ? 8 + g : g - H) : 8 + g;
+    const int cb1 = NT == 2 ? (g < H ? g : 8 + (g - H)) : g;
     double d00 = 0.0, d01 = 0.0, e00 = 0.0, e01 = 0.0, f00 = 0.0, f01 = 0.0;
     for (int c0 = a0; c0 < a1; c0 += 32) {
         const int j = c0 + lane;
@@ -55,40 +53,85 @@ __device__ __forceinline__ void leaf_moments(const typename Vec4<T>::type* __res
         }
         double ta0 = 1.0, ta1 = u, tb0 = 1.0, tb1 = v;
 #pragma unroll
-        for (int r = 0; r < kUpRows; r++) {
+        for (int r = 0; r <= NM; r++) {
             const double tu = (r == 0) ? 1.0 : (r == 1 ? u : 2.0 * u * ta1 - ta0);
             const double tv = (r == 0) ? 1.0 : (r == 1 ? v : 2.0 * v * tb1 - tb0);
             if (r >= 2) { ta0 = ta1; ta1 = tu; tb0 = tb1; tb1 = tv; }
-            W[r][lane] = (r <= nmax) ? w * tu : 0.0;
-            V[r][lane] = (r <= nmax) ? tv : 0.0;
+            W[r][lane] = w * tu;
+            V[r][lane] = tv;
         }
         __syncwarp();
         const int nk = (min(32, a1 - c0) + 3) >> 2;
         for (int k = 0; k < nk; k++) {
             const int p = 4 * k + t;
             dmma_8x8x4(d00, d01, W[g][p], V[g][p]);
-            if (ntiles >= 2) dmma_8x8x4(e00, e01, W[ra1][p], V[cb1][p]);
-            if (ntiles == 3) dmma_8x8x4(f00, f01, W[g][p], V[8 + g][p]);  // a < 8, b >= 8
+            if constexpr (NT >= 2) dmma_8x8x4(e00, e01, W[ra1][p], V[cb1][p]);
+            if constexpr (NT == 3) dmma_8x8x4(f00, f01, W[g][p], V[8 + g][p]);  // a < 8, b >= 8
         }
         __syncwarp();
     }
-    // column index of this lane's two accumulators in tile 1
-    auto col1 = [&](int c) { return ntiles == 2 ? (c < h ? c : 8 + (c - h)) : c; };
+#pragma unroll
     for (int i = 0; i < 2; i++) {
         const int c = 2 * t + i;
         int a = g, b = c;  // tile 0
-        if (a + b <= nmax) out[(a + b) * (a + b + 1) / 2 + b] = i ? d01 : d00;
-        if (ntiles >= 2) {
+        if (a + b <= NM) out[(a + b) * (a + b + 1) / 2 + b] = i ? d01 : d00;
+        if constexpr (NT >= 2) {
             a = ra1;
-            b = col1(c);
-            if (a + b <= nmax && (a >= 8 || b >= 8)) out[(a + b) * (a + b + 1) / 2 + b] = i ? e01 : e00;
+            b = NT == 2 ? (c < H ? c : 8 + (c - H)) : c;
+            if (a + b <= NM && (a >= 8 || b >= 8)) out[(a + b) * (a + b + 1) / 2 + b] = i ? e01 : e00;
         }
-        if (ntiles == 3) {
+        if constexpr (NT == 3) {
             a = g;
             b = 8 + c;
-            if (a + b <= nmax) out[(a + b) * (a + b + 1) / 2 + b] = i ? f01 : f00;
+            if (a + b <= NM) out[(a + b) * (a + b + 1) / 2 + b] = i ? f01 : f00;
         }
     }
 }
+
+// leaf_moments_n for a run-time (warp-uniform) degree nm <= kMaxDegree.
+template <typename T>
+__device__ __forceinline__ void leaf_moments(const typename Vec4<T>::type* __restrict__ src, int a0, int a1,
+                                             double fx, double fy, double fz, const NodeGeom& ng, int nm,
+                                             double (*W)[kUpLd], double (*V)[kUpLd], double* __restrict__ out) {
+    static_assert(kMaxDegree == 12, "extend the dispatch");
+    switch (nm) {
+#define FSS_MOMENTS_CASE(N) \
+    case N: leaf_moments_n<T, N>(src, a0, a1, fx, fy, fz, ng, W, V, out); break;
+        FSS_MOMENTS_CASE(0) FSS_MOMENTS_CASE(1) FSS_MOMENTS_CASE(2) FSS_MOMENTS_CASE(3) FSS_MOMENTS_CASE(4)
+        FSS_MOMENTS_CASE(5) FSS_MOMENTS_CASE(6) FSS_MOMENTS_CASE(7) FSS_MOMENTS_CASE(8) FSS_MOMENTS_CASE(9)
+        FSS_MOMENTS_CASE(10) FSS_MOMENTS_CASE(11) FSS_MOMENTS_CASE(12)
+#undef FSS_MOMENTS_CASE
+        default: break;
+    }
+}
+
+// Sum of R rows, row(i) for i < R, as four chains (rows i = 0, 4, 8, ...;
+// 1, 5, ...; ...) added as (s0 + s1) + (s2 + s3): four loads in flight.
+// The single problem's and the ensemble's combines both sum this way.
+template <typename F>
+__device__ __forceinline__ double sum_rows4(F row, int R) {
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    int i = 0;
+    for (; i + 4 <= R; i += 4) {
+        s0 += row(i + 0);
+        s1 += row(i + 1);
+        s2 += row(i + 2);
+        s3 += row(i + 3);
+    }
+    for (; i < R; i++) s0 += row(i);
+    return (s0 + s1) + (s2 + s3);
+}
+
+// Moment rows of the upward pass.  The leaves of a member are numbered so
+// that leaves 4g .. 4g + 3 are the four children of one face (and share
+// every ancestor above the leaf level).  A block of four warps takes one
+// such group on one level l: on the leaf level each warp writes its own
+// leaf's row; above it the four rows are added in shared memory as
+// (r0 + r1) + (r2 + r3) and written once, into the slot of the group's
+// first leaf.  A face on level l < leaf level then sums the rows of every
+// fourth leaf of its range (its groups), a leaf-level face its one row.
+// The same below for the single problem and the ensemble, so that both
+// form every proxy charge from the same additions.
+__device__ __forceinline__ int up_row_step(int level, int leaf_level) { return level < leaf_level ? 4 : 1; }
 
 }  // namespace fss

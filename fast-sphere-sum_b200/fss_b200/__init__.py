@@ -57,7 +57,8 @@ class TreeInfo(C.Structure):
                 ("pc_interactions", C.c_double), ("block_threads", C.c_int32),
                 ("targets_per_thread", C.c_int32), ("src_parts", C.c_int32), ("target_clusters", C.c_int32),
                 ("cp_interactions", C.c_double), ("cc_interactions", C.c_double),
-                ("lane_pairs_leaf", C.c_double), ("lane_pairs_cluster", C.c_double)]
+                ("lane_pairs_leaf", C.c_double), ("lane_pairs_cluster", C.c_double),
+                ("max_degree", C.c_int32), ("max_cluster_points", C.c_int32)]
 
 
 def build():

@@ -303,6 +303,10 @@ typedef struct fss_tree_info {
                                   consumer lanes perform per RHS at the build's
                                   leaf counts, discarded lanes included */
     double lane_pairs_cluster; /* the same for the target-cluster launch */
+    int32_t max_degree;        /* highest degree among the lists' proxies and
+                                  target clusters (the upward pass forms
+                                  moments up to it) */
+    int32_t max_cluster_points; /* largest target cluster (interpolation points) */
 } fss_tree_info;
 int fss_get_tree_info(fss_ctx* ctx, fss_tree_info* info);
 
