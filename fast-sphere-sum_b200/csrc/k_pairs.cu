@@ -31,6 +31,7 @@
 namespace fss {
 
 constexpr int kDepth = 4;  // ring depth (tiles in flight)
+constexpr int kClusterDepth = 3;  // ring depth of the target-cluster launch
 constexpr int TILE_F32 = tile_capacity(false);
 constexpr float kSelfR2 = 1e-30f;  // r^2 bias of the FP32 loop (a normal float; 1 / kSelfR2 finite)
 
@@ -244,7 +245,7 @@ struct RingState {
 // ready_bar; it computes nothing.  Warps 1.. are the consumers, one target
 // per thread (THREADS - 32 targets per chunk); they wait on ready_bar (FP32)
 // or full_bar (FP64) and release a slot through empty_bar.
-template <typename T, int THREADS, int TILE, bool PSI>
+template <typename T, int THREADS, int TILE, bool PSI, int DEPTH>
 __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4<T>::type* __restrict__ src,
                                          const Segment* __restrict__ segs, const int32_t* __restrict__ leaf_start,
                                          double4* __restrict__ partials, int64_t pstride,
@@ -269,8 +270,8 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
             for (;;) {
                 // convert every produced tile (each waits for its copies)
                 while (kPacked && rs.converted < rs.issued && !rs.failed) {
-                    const int slot = int(rs.converted % kDepth);
-                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full_bar[slot], uint32_t(rs.converted / kDepth) & 1,
+                    const int slot = int(rs.converted % DEPTH);
+                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full_bar[slot], uint32_t(rs.converted / DEPTH) & 1,
                                                                    ctl.wait_ns))) {
                         rs.failed = true;
                         break;
@@ -284,10 +285,10 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
                 if (pdone || rs.failed) break;
                 // the next tile, once its slot is free (then the empty tile
                 // that ends the chunk)
-                const int slot = int(rs.issued % kDepth);
+                const int slot = int(rs.issued % DEPTH);
                 bool ok = true;
-                if (rs.issued >= kDepth)
-                    ok = mbar_wait_bounded(&empty_bar[slot], uint32_t((rs.issued / kDepth) - 1) & 1, ctl.wait_ns);
+                if (rs.issued >= DEPTH)
+                    ok = mbar_wait_bounded(&empty_bar[slot], uint32_t((rs.issued / DEPTH) - 1) & 1, ctl.wait_ns);
                 if (!__all_sync(0xffffffffu, ok)) {
                     rs.failed = true;
                     break;
@@ -334,10 +335,10 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
                 ntz = f2_pack(-float(v.z), -float(v.z));
             }
             for (;;) {
-                const int slot = int(rs.consumed % kDepth);
+                const int slot = int(rs.consumed % DEPTH);
                 uint64_t* wait_bar = kPacked ? &ready_bar[slot] : &full_bar[slot];
                 if (!__all_sync(0xffffffffu,
-                                mbar_wait_bounded(wait_bar, uint32_t(rs.consumed / kDepth) & 1, ctl.wait_ns))) {
+                                mbar_wait_bounded(wait_bar, uint32_t(rs.consumed / DEPTH) & 1, ctl.wait_ns))) {
                     rs.failed = true;
                     break;
                 }
@@ -420,30 +421,31 @@ __device__ __forceinline__ void run_item(const WorkItem& it, const typename Vec4
         if (rs.failed) {
             // no bulk copy may still be landing in this block's shared memory
             // when it exits: the producer waits (bounded) for the tiles not
-            // known to have landed -- at most the last kDepth it issued
+            // known to have landed -- at most the last DEPTH it issued
             if (warp == 0) {
-                int64_t t = rs.issued - kDepth;
+                int64_t t = rs.issued - DEPTH;
                 if (kPacked && rs.converted > t) t = rs.converted;
                 for (t = (t < 0) ? 0 : t; t < rs.issued; t++)
-                    mbar_wait_bounded(&full_bar[t % kDepth], uint32_t(t / kDepth) & 1, ctl.wait_ns);
+                    mbar_wait_bounded(&full_bar[t % DEPTH], uint32_t(t / DEPTH) & 1, ctl.wait_ns);
             }
             return;
         }
     }
 }
 
-// Shared memory of a pair block: the landing ring (kDepth tiles as copied)
+// Shared memory of a pair block: the landing ring (DEPTH tiles as copied)
 // and, in FP32, the SoA ring the consumers read.
-template <typename T, int TILE>
-FSS_HD constexpr size_t ring_bytes() { return size_t(kDepth) * TILE * sizeof(typename Vec4<T>::type); }
-template <typename T, int TILE>
+template <typename T, int TILE, int DEPTH = kDepth>
+FSS_HD constexpr size_t ring_bytes() { return size_t(DEPTH) * TILE * sizeof(typename Vec4<T>::type); }
+template <typename T, int TILE, int DEPTH = kDepth>
 FSS_HD constexpr size_t pair_smem_bytes() {
-    return ring_bytes<T, TILE>() + (sizeof(T) == 4 ? size_t(kDepth) * 4 * TILE * sizeof(float) : 0);
+    return ring_bytes<T, TILE, DEPTH>() + (sizeof(T) == 4 ? size_t(DEPTH) * 4 * TILE * sizeof(float) : 0);
 }
 
-__device__ __forceinline__ void init_ring(uint64_t* full_bar, uint64_t* empty_bar, uint64_t* ready_bar, int warps) {
+__device__ __forceinline__ void init_ring(uint64_t* full_bar, uint64_t* empty_bar, uint64_t* ready_bar, int warps,
+                                          int depth) {
     if (threadIdx.x == 0) {
-        for (int d = 0; d < kDepth; d++) {
+        for (int d = 0; d < depth; d++) {
             mbar_init(&full_bar[d], 1);
             mbar_init(&empty_bar[d], warps - 1);  // consumer warps
             mbar_init(&ready_bar[d], 1);
@@ -453,8 +455,8 @@ __device__ __forceinline__ void init_ring(uint64_t* full_bar, uint64_t* empty_ba
     __syncthreads();
 }
 
-// One block per work item.
-template <typename T, int THREADS, bool PSI, int TILE>
+// One block per work item; a ring of DEPTH tile slots.
+template <typename T, int THREADS, bool PSI, int TILE, int DEPTH>
 __global__ void __launch_bounds__(THREADS) k_pairs(const typename Vec4<T>::type* __restrict__ src,
                                                    const Segment* __restrict__ segs,
                                                    const int32_t* __restrict__ leaf_start,
@@ -462,14 +464,16 @@ __global__ void __launch_bounds__(THREADS) k_pairs(const typename Vec4<T>::type*
                                                    int64_t pstride, int* __restrict__ err, const PairCtl ctl) {
     using S4 = typename Vec4<T>::type;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth], ready_bar[kDepth];
-    __shared__ SlotHdr hdr[kDepth];
-    init_ring(full_bar, empty_bar, ready_bar, THREADS / 32);
+    __shared__ __align__(8) uint64_t full_bar[DEPTH], empty_bar[DEPTH], ready_bar[DEPTH];
+    __shared__ SlotHdr hdr[DEPTH];
+    init_ring(full_bar, empty_bar, ready_bar, THREADS / 32, DEPTH);
     RingState rs{0, 0, 0, false};
     const WorkItem it = items[blockIdx.x];
-    run_item<T, THREADS, TILE, PSI>(it, src, segs, leaf_start, partials, pstride, reinterpret_cast<S4*>(smem_raw),
-                                    reinterpret_cast<float*>(smem_raw + ring_bytes<T, TILE>()), hdr, full_bar,
-                                    empty_bar, ready_bar, rs, ctl, int(blockIdx.x) == ctl.hold_block);
+    run_item<T, THREADS, TILE, PSI, DEPTH>(it, src, segs, leaf_start, partials, pstride,
+                                           reinterpret_cast<S4*>(smem_raw),
+                                           reinterpret_cast<float*>(smem_raw + ring_bytes<T, TILE, DEPTH>()), hdr,
+                                           full_bar, empty_bar, ready_bar, rs, ctl,
+                                           int(blockIdx.x) == ctl.hold_block);
     if (rs.failed && threadIdx.x == 0) set_error(err, kErrTimeout);
 }
 
@@ -488,7 +492,7 @@ __global__ void __launch_bounds__(THREADS) k_pairs_persistent(const typename Vec
     __shared__ __align__(8) uint64_t full_bar[kDepth], empty_bar[kDepth], ready_bar[kDepth];
     __shared__ SlotHdr hdr[kDepth];
     __shared__ int next_item;
-    init_ring(full_bar, empty_bar, ready_bar, THREADS / 32);
+    init_ring(full_bar, empty_bar, ready_bar, THREADS / 32, kDepth);
     RingState rs{0, 0, 0, false};
     for (;;) {
         if (threadIdx.x == 0) next_item = atomicAdd(queue, 1);
@@ -497,7 +501,7 @@ __global__ void __launch_bounds__(THREADS) k_pairs_persistent(const typename Vec
         __syncthreads();
         if (item >= nitems) break;
         const WorkItem it = items[item];
-        run_item<T, THREADS, TILE, false>(it, src, segs, leaf_start, partials, pstride,
+        run_item<T, THREADS, TILE, false, kDepth>(it, src, segs, leaf_start, partials, pstride,
                                           reinterpret_cast<S4*>(smem_raw),
                                           reinterpret_cast<float*>(smem_raw + ring_bytes<T, TILE>()), hdr, full_bar,
                                           empty_bar, ready_bar, rs, ctl, false);
@@ -508,15 +512,15 @@ __global__ void __launch_bounds__(THREADS) k_pairs_persistent(const typename Vec
 
 // ---------------------------------------------------------------- dispatch
 
-template <typename T, int THREADS, bool PSI>
+template <typename T, int THREADS, bool PSI, int DEPTH>
 static cudaError_t run_pairs(cudaStream_t st, int nitems, const void* src, const Segment* segs,
                              const int32_t* leaf_start, const WorkItem* items, double4* partials, int64_t pstride,
                              int* err, PairCtl ctl) {
     constexpr int TILE = tile_capacity(sizeof(T) == 8);
-    constexpr size_t smem = pair_smem_bytes<T, TILE>();
+    constexpr size_t smem = pair_smem_bytes<T, TILE, DEPTH>();
     static_assert(smem <= 48 * 1024, "ring must fit the default dynamic shared memory limit");
     if (nitems == 0) return cudaSuccess;
-    k_pairs<T, THREADS, PSI, TILE><<<nitems, THREADS, smem, st>>>(static_cast<const typename Vec4<T>::type*>(src),
+    k_pairs<T, THREADS, PSI, TILE, DEPTH><<<nitems, THREADS, smem, st>>>(static_cast<const typename Vec4<T>::type*>(src),
                                                                    segs, leaf_start, items, partials,
                                                                    pstride, err, ctl);
     return cudaGetLastError();
@@ -537,10 +541,11 @@ PairShape pairs_shape(bool fp64, int threads, int per_thread) {
 
 PairShape cluster_shape(bool fp64, int k) {
     const int tile = tile_capacity(fp64);
-    if (k <= 32) return PairShape{64, 1, tile};
-    if (k <= 64) return PairShape{96, 1, tile};
-    if (k <= 96) return PairShape{128, 1, tile};
-    return PairShape{160, 1, tile};
+    const int depth = kClusterDepth;
+    if (k <= 32) return PairShape{64, 1, tile, depth};
+    if (k <= 64) return PairShape{96, 1, tile, depth};
+    if (k <= 96) return PairShape{128, 1, tile, depth};
+    return PairShape{160, 1, tile, depth};
 }
 
 template <typename T, bool PSI>
@@ -549,7 +554,15 @@ static cudaError_t dispatch(cudaStream_t st, PairShape sh, int nitems, const voi
                             int64_t pstride, int* err, PairCtl ctl) {
 #define FSS_SHAPE(TH)                                                                                            \
     if (sh.threads == TH)                                                                                        \
-        return run_pairs<T, TH, PSI>(st, nitems, src, segs, leaf_start, items, partials, pstride, err, ctl);
+        return run_pairs<T, TH, PSI, kDepth>(st, nitems, src, segs, leaf_start, items, partials, pstride, err, ctl);
+#define FSS_SHAPE3(TH)                                                                                           \
+    if (sh.threads == TH && sh.depth == 3)                                                                       \
+        return run_pairs<T, TH, PSI, 3>(st, nitems, src, segs, leaf_start, items, partials, pstride, err, ctl);
+    FSS_SHAPE3(64)
+    FSS_SHAPE3(96)
+    FSS_SHAPE3(128)
+    FSS_SHAPE3(160)
+#undef FSS_SHAPE3
     FSS_SHAPE(64)
     FSS_SHAPE(96)
     FSS_SHAPE(128)

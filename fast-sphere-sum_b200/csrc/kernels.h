@@ -42,6 +42,7 @@ struct PairShape {
     int threads = 160;
     int per_thread = 1;
     int tile = 256;
+    int depth = 4;  // ring slots (tiles in flight)
     int targets() const { return (threads - 32) * per_thread; }
 };
 
