@@ -88,13 +88,16 @@ struct fss_ctx {
     int nmax = 0, level_mask = 0;
     int parts = 1;
     int64_t pstride = 0;  // partial slot stride: n, or n + proxy slots with target clusters
+    int n_up_blocks = 0, n_dn_blocks = 0;  // blocks of the batched V^-1 products
+    int down_max_deg = 0;                  // highest target-cluster degree
     PairShape shape;
     double direct_pairs = 0;
 
     // device
     DBuf in5, area_in, perm, key, key_tmp, vals_tmp, hist, leaf_start, s0, xs, acc, area_s, tracer_s, src, partials,
-        segs, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, vinv, vinv_off, proxy_pos, out5, psi,
-        wtotal, err_flag, loc, sortq, grid3, rm_target, rm_tris, rm_off, rm_adj, down_jobs, down_anc, down_coef, vinvT, up_deg;
+        segs, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, proxy_pos, out5, psi,
+        wtotal, err_flag, loc, sortq, grid3, rm_target, rm_tris, rm_off, rm_adj, down_jobs, down_anc, down_coef, vpad, vtpad, vpad_off, up_deg, up_tblocks, up_tasks,
+        dn_tblocks, dn_tasks, msum;
     int64_t src_count = 0;
 
     // graph

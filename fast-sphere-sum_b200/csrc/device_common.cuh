@@ -152,4 +152,25 @@ __device__ __forceinline__ void set_error(int* err, int code) {
     if (err) atomicCAS(err, 0, code);
 }
 
+// A block's one-shot bulk staging: thread 0 initialises `bar` and copies
+// `bytes` (a multiple of 16; both addresses 16-byte aligned) of global memory
+// into shared memory; after a __syncthreads every thread calls stage_wait.
+__device__ __forceinline__ void stage_issue(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_init_fence();
+        mbar_arrive_expect_tx(bar, bytes);
+        bulk_g2s(dst, src, bytes, bar);
+    }
+}
+
+// Waits (bounded) for the staged copy; false in every thread of the block
+// when it did not land in time, after a second bounded wait, so that no copy
+// is left in flight when the block returns.
+__device__ __forceinline__ bool stage_wait(uint64_t* bar, uint64_t limit_ns) {
+    const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0, limit_ns)) != 0;
+    if (!ok) mbar_wait_bounded(bar, 0, limit_ns);
+    return ok;
+}
+
 }  // namespace fss

@@ -116,6 +116,22 @@ int upload(fss_ctx* c, DBuf& b, const std::vector<T>& v) {
     return FSS_OK;
 }
 
+// Blocks of the batched V^-1 products: tasks (index, degree) grouped by
+// degree (stable, so a block's tasks keep list order), at most per_block a
+// block.
+void make_task_blocks(const std::vector<std::pair<int32_t, int32_t>>& tasks, int per_block,
+                      std::vector<TaskBlock>& blocks, std::vector<int32_t>& index) {
+    blocks.clear();
+    index.clear();
+    for (int d = 0; d <= kMaxDegree; d++) {
+        const int32_t first = int32_t(index.size());
+        for (const auto& t : tasks)
+            if (t.second == d) index.push_back(t.first);
+        for (int32_t b = first; b < int32_t(index.size()); b += per_block)
+            blocks.push_back(TaskBlock{d, b, std::min<int32_t>(per_block, int32_t(index.size()) - b), 0});
+    }
+}
+
 int auto_tree_levels(const fss_config& cfg, int64_t n) {
     if (cfg.tree_levels > 0) return cfg.tree_levels;
     const int target = cfg.leaf_target > 0 ? cfg.leaf_target : 64;
@@ -485,24 +501,52 @@ int materialize(fss_ctx* c, PairShape shape) {
             }
     }
     TRY(upload(c, c->up_deg, up_deg));
-    std::vector<double> vinv_all, vinvT_all;
-    std::vector<int32_t> vinv_off(kMaxDegree + 1, 0);
+    // Vinv of every degree in use for the batched products, rows padded to a
+    // multiple of 4 doubles (Vinv[m][k] by rows m, and the transpose by rows
+    // k), each a bulk copy of K * Kp doubles
+    std::vector<double> vpad_all, vtpad_all;
+    std::vector<int32_t> vpad_off(kMaxDegree + 1, 0);
     for (int d = 0; d <= c->nmax; d++) {
         std::vector<double> nodes, vi;
         interp_nodes(d, nodes, vi);
-        vinv_off[d] = int32_t(vinv_all.size());
-        vinv_all.insert(vinv_all.end(), vi.begin(), vi.end());
-        const int K = nproxy(d);
-        for (int k = 0; k < K; k++)
-            for (int m = 0; m < K; m++) vinvT_all.push_back(vi[size_t(m) * K + k]);
+        const int K = nproxy(d), Kp = (K + 3) & ~3;
+        vpad_off[d] = int32_t(vpad_all.size());
+        for (int r = 0; r < K; r++)
+            for (int q = 0; q < Kp; q++) {
+                vpad_all.push_back(q < K ? vi[size_t(r) * K + q] : 0.0);
+                vtpad_all.push_back(q < K ? vi[size_t(q) * K + r] : 0.0);
+            }
     }
-    TRY(upload(c, c->vinv, vinv_all));
-    TRY(upload(c, c->vinvT, vinvT_all));
-    TRY(upload(c, c->vinv_off, vinv_off));
+    TRY(upload(c, c->vpad, vpad_all));
+    TRY(upload(c, c->vtpad, vtpad_all));
+    TRY(upload(c, c->vpad_off, vpad_off));
     TRY(upload(c, c->segs, L.segs));
     TRY(upload(c, c->items, L.items));
     TRY(upload(c, c->jobs, L.jobs));
     TRY(upload(c, c->down_jobs, L.down));
+    {
+        std::vector<std::pair<int32_t, int32_t>> up, dn;
+        for (size_t j = 0; j < L.jobs.size(); j++)
+            for (int d = 0; d <= kMaxDegree; d++)
+                if ((L.jobs[j].degmask >> d) & 1) up.emplace_back(int32_t(j), d);
+        c->down_max_deg = 0;
+        for (size_t j = 0; j < L.down.size(); j++) {
+            dn.emplace_back(int32_t(j), L.down[j].deg);
+            c->down_max_deg = std::max(c->down_max_deg, int(L.down[j].deg));
+        }
+        CU(batch_prepare());
+        CU(c->msum.ensure(sizeof(double) * std::max<size_t>(L.jobs.size(), 1) * size_t(nproxy(c->nmax))));
+        std::vector<TaskBlock> blocks;
+        std::vector<int32_t> index;
+        make_task_blocks(up, batch_tasks(), blocks, index);
+        c->n_up_blocks = int(blocks.size());
+        TRY(upload(c, c->up_tblocks, blocks));
+        TRY(upload(c, c->up_tasks, index));
+        make_task_blocks(dn, batch_tasks(), blocks, index);
+        c->n_dn_blocks = int(blocks.size());
+        TRY(upload(c, c->dn_tblocks, blocks));
+        TRY(upload(c, c->dn_tasks, index));
+    }
     TRY(upload(c, c->down_anc, L.leaf_anc));
     CU(c->down_coef.ensure(sizeof(double4) * size_t(std::max<int64_t>(L.n_coef, 1))));
     std::vector<double4> pp(L.proxy_pos.size() / 4);
@@ -572,10 +616,11 @@ int eval_partials(fss_ctx* c, bool want_psi, bool* down_out) {
         }
         {
             ProfScope ps(c, "upward_combine");
-            launch_up_combine(c->stream, c->fp64, int(c->lists.jobs.size()), c->jobs.as<ProxyJob>(),
-                              c->part_up.as<double>(), c->leaf_level, c->nmax, c->vinv.as<double>(),
-                              c->vinv_off.as<int32_t>(), c->proxy_pos.as<double4>(), c->node.as<NodeGeom>(), 0,
-                              c->n, c->src.p);
+            launch_up_proxies(c->stream, c->fp64, int(c->lists.jobs.size()), c->jobs.as<ProxyJob>(),
+                              c->part_up.as<double>(), c->leaf_level, c->nmax, c->msum.as<double>(),
+                              c->n_up_blocks, c->up_tblocks.as<TaskBlock>(), c->up_tasks.as<int32_t>(),
+                              c->vpad.as<double>(), c->vpad_off.as<int32_t>(), c->proxy_pos.as<double4>(), c->n,
+                              c->src.p, c->err_flag.as<int>(), c->wait_ns);
         }
     }
     if (overlap) {
@@ -594,11 +639,17 @@ int eval_partials(fss_ctx* c, bool want_psi, bool* down_out) {
         DownArgs d;
         d.njobs = int(c->lists.down.size());
         d.jobs = c->down_jobs.as<DownJob>();
+        d.ncoef_blocks = c->n_dn_blocks;
+        d.max_deg = c->down_max_deg;
+        d.coef_blocks = c->dn_tblocks.as<TaskBlock>();
+        d.coef_tasks = c->dn_tasks.as<int32_t>();
         d.partials = c->partials.as<double4>();
         d.parts = c->parts;
         d.pstride = c->pstride;
-        d.vinvT = c->vinvT.as<double>();
-        d.vinv_off = c->vinv_off.as<int32_t>();
+        d.vtpad = c->vtpad.as<double>();
+        d.vpad_off = c->vpad_off.as<int32_t>();
+        d.err = c->err_flag.as<int>();
+        d.wait_ns = c->wait_ns;
         d.node = c->node.as<NodeGeom>();
         d.coef = c->down_coef.as<double4>();
         d.nleaf = int(c->nleaf);

@@ -93,6 +93,13 @@ struct DownJob {
     int32_t pad[3];
 };
 
+// A block of the batched V^-1 products (proxy charges of the upward pass,
+// coefficients of the downward pass): `count` tasks of degree `deg`, task
+// indices tasks[first .. first + count) (a proxy job or a target cluster).
+struct TaskBlock {
+    int32_t deg, first, count, pad;
+};
+
 // One target cluster above a leaf, as the leaf's evaluation reads it:
 // coefficients from `coef`, degree, face (global index); coef < 0 ends a
 // leaf's list.

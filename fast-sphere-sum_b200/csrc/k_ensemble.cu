@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kUpThreads) k_up_leaf_batch(const float4* __re
 
 // Proxy charges of every member's far clusters: job j sums the rows of its
 // leaves (global leaf indices, slots through EnsLeaf::part_base) as the
-// single problem's k_up_combine does.
+// single problem's k_up_proxies does (each q_k the same FMA chain).
 __global__ void __launch_bounds__(128) k_up_combine_batch(const ProxyJob* __restrict__ jobs,
                                                           const EnsLeaf* __restrict__ leaves,
                                                           const double* __restrict__ part, int nmax,

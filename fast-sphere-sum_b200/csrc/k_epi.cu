@@ -65,50 +65,100 @@ __global__ void __launch_bounds__(kUpThreads) k_up_leaf(const typename Vec4<T>::
     for (int m = threadIdx.x; m < KJ; m += kUpThreads) out[m] = (O[0][m] + O[1][m]) + (O[2][m] + O[3][m]);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kUpThreads) k_up_combine(const ProxyJob* __restrict__ jobs, const double* __restrict__ part,
-                                                           int leaf_level, int nmax, const double* __restrict__ vinv,
-                                                           const int32_t* __restrict__ vinv_off,
-                                                           const double4* __restrict__ proxy_pos,
-                                                           const NodeGeom* __restrict__ node, int local_frames,
-                                                           int64_t n, typename Vec4<T>::type* __restrict__ src) {
-    __shared__ double M[kMaxK];
-    // read in place: a copy indexed by a run-time degree (job.off[d]) would sit in local memory
+// Batched V^-1 products.  A block takes up to kBatchTasks tasks (faces or
+// clusters) of one degree, K = nproxy(deg): it stages the K x K matrix, its
+// rows padded to Kp = 4 ceil(K / 4) doubles, and the tasks' inputs in shared
+// memory, and gives each thread a tile of 2 outputs x 4 tasks, so that every
+// staged value it reads feeds several FMA chains.  Each output is the chain
+// of FMAs over the inner index in order, as a per-task product forms it (so
+// the single problem and the ensemble stay bit-identical).
+constexpr int kBatchThreads = 192;
+constexpr int kBatchTasks = 16;
+__host__ __device__ constexpr int batch_pad(int K) { return (K + 3) & ~3; }
+static_assert((batch_pad(kMaxK) / 2) * (kBatchTasks / 4) <= kBatchThreads, "one tile per thread at the largest degree");
+
+// Upward pass, part 2a: the moments of every proxy face, its rows summed
+// (up_row_step, sum_rows4), one thread per (face, moment): msum[j][m].
+__global__ void __launch_bounds__(kMaxK) k_up_sums(const ProxyJob* __restrict__ jobs, const double* __restrict__ part,
+                                                   int leaf_level, int nmax, double* __restrict__ msum) {
     const ProxyJob& job = jobs[blockIdx.x];
-    const int tid = threadIdx.x;
-    const int KM = nproxy(nmax);                       // slot stride
-    const int KJ = nproxy(31 - __clz(job.degmask));    // moments this face's degrees use
-    if (tid < KJ) {
-        // the face's rows (one per group of four leaves above the leaf level)
-        const int step = up_row_step(job.level, leaf_level);
-        const int64_t stride = int64_t(step) * (leaf_level + 1) * KM;
-        const double* p = part + (int64_t(job.leaf_lo) * (leaf_level + 1) + job.level) * KM + tid;
-        M[tid] = sum_rows4([&](int i) { return p[i * stride]; }, (job.leaf_hi - job.leaf_lo) / step);
+    const int m = threadIdx.x;
+    const int KM = nproxy(nmax);
+    if (m >= nproxy(31 - __clz(job.degmask))) return;  // moments this face's degrees use
+    const int step = up_row_step(job.level, leaf_level);
+    const int64_t stride = int64_t(step) * (leaf_level + 1) * KM;
+    const double* pr = part + (int64_t(job.leaf_lo) * (leaf_level + 1) + job.level) * KM + m;
+    msum[int64_t(blockIdx.x) * KM + m] = sum_rows4([&](int r) { return pr[r * stride]; }, (job.leaf_hi - job.leaf_lo) / step);
+}
+
+// Upward pass, part 2b: proxy charges q_k = sum_m Vinv[m][k] M_m of every
+// (face, degree) task, written with the proxy positions at the face's slots
+// of the unified source array (absolute coordinates).  Shared memory:
+// A[m][k] = Vinv[m][k] (K rows of Kp; one bulk copy of the padded matrix
+// `vpad`), then X[t][m] = the task's moments.
+template <typename T>
+__global__ void __launch_bounds__(kBatchThreads) k_up_proxies(const TaskBlock* __restrict__ blocks,
+                                                              const int32_t* __restrict__ tasks,
+                                                              const ProxyJob* __restrict__ jobs,
+                                                              const double* __restrict__ msum, int nmax,
+                                                              const double* __restrict__ vpad,
+                                                              const int32_t* __restrict__ vpad_off,
+                                                              const double4* __restrict__ proxy_pos, int64_t n,
+                                                              typename Vec4<T>::type* __restrict__ src, int* err,
+                                                              uint64_t wait_ns) {
+    extern __shared__ __align__(32) double bsm[];
+    __shared__ __align__(8) uint64_t bar;
+    const TaskBlock tb = blocks[blockIdx.x];
+    const int d = tb.deg, K = nproxy(d), Kp = batch_pad(K), nt = tb.count;
+    const int KM = nproxy(nmax);
+    double* A = bsm;
+    double* X = bsm + K * Kp;
+    stage_issue(A, vpad + vpad_off[d], uint32_t(sizeof(double)) * K * Kp, &bar);
+    for (int i = threadIdx.x; i < nt * K; i += kBatchThreads) {
+        const int t = i / K, m = i - t * K;
+        X[i] = msum[int64_t(tasks[tb.first + t]) * KM + m];
     }
     __syncthreads();
-    double cx = 0, cy = 0, cz = 0;
-    if (local_frames) {
-        const NodeGeom& ng = node[job.node];
-        cx = ng.cx; cy = ng.cy; cz = ng.cz;
+    if (!stage_wait(&bar, wait_ns)) {
+        if (threadIdx.x == 0) set_error(err, kErrTimeout);
+        return;
     }
-    for (int d = 0; d <= nmax; d++) {
-        if (!((job.degmask >> d) & 1)) continue;
-        const int K = nproxy(d);
-        const double* V = vinv + vinv_off[d];
-        for (int k = tid; k < K; k += kUpThreads) {
-            double q = 0;
-            for (int m = 0; m < K; m++) q = fma(V[m * K + k], M[m], q);
-            const int64_t slot = int64_t(job.off[d]) + k;
+    const int npair = Kp / 2, tid = threadIdx.x;
+    if (tid >= npair * ((nt + 3) / 4)) return;  // no barrier follows
+    const int k0 = 2 * (tid % npair), t0 = 4 * (tid / npair);
+    double q[4][2];
+#pragma unroll
+    for (int j = 0; j < 4; j++) q[j][0] = q[j][1] = 0.0;
+    const double* Xt = X + t0 * K;
+    for (int m = 0; m < K; m++) {
+        const double2 a = *reinterpret_cast<const double2*>(A + m * Kp + k0);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const double x = (t0 + j < nt) ? Xt[j * K + m] : 0.0;
+            q[j][0] = fma(a.x, x, q[j][0]);
+            q[j][1] = fma(a.y, x, q[j][1]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (t0 + j >= nt) break;
+        const ProxyJob& job = jobs[tasks[tb.first + t0 + j]];
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            if (k0 + r >= K) break;
+            const int64_t slot = int64_t(job.off[d]) + k0 + r;
             const double4 y = proxy_pos[slot - n];
             typename Vec4<T>::type o;
-            o.x = T(y.x - cx);
-            o.y = T(y.y - cy);
-            o.z = T(y.z - cz);
-            o.w = T(q);
+            o.x = T(y.x);
+            o.y = T(y.y);
+            o.z = T(y.z);
+            o.w = T(q[j][r]);
             src[slot] = o;
         }
     }
 }
+
+size_t up_proxies_smem(int K) { return sizeof(double) * size_t(K * batch_pad(K) + kBatchTasks * K); }
 
 // ---------------------------------------------------------------- epilogue
 
@@ -279,71 +329,75 @@ __global__ void k_scatter_state(int64_t n, const int32_t* __restrict__ perm, con
 // its log term.  FP64.
 
 // Downward pass, part 1: the coefficients of every target cluster at once,
-// one warp per cluster: y_k = the cluster's field at its K interpolation
-// points (its partial slots summed), c_m = sum_k Vinv[m][k] y_k (VT = Vinv
-// transposed, so that consecutive lanes read consecutive entries).  A lane
-// forms its NQ = ceil(K / 32) outputs m = lane + 32 q in one pass over k
-// (independent chains, several loads in flight).
-constexpr int kCoefWarps = 4;
-template <bool PSI, int NQ>
-__device__ __forceinline__ void coef_outputs(const double* __restrict__ VT, int K, int lane,
-                                             const double4* __restrict__ Y, double4* __restrict__ out) {
-    double4 c[NQ];
-    int mm[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; q++) {
-        c[q] = make_double4(0.0, 0.0, 0.0, 0.0);
-        mm[q] = min(lane + 32 * q, K - 1);  // a lane past K repeats the last output (not stored)
+// batched by degree (kBatchThreads above): y_k = the cluster's field at its
+// K interpolation points (its partial slots summed, in slot order), c_m =
+// sum_k Vinv[m][k] y_k over k in order.  Shared memory: A[k][m] =
+// Vinv[m][k] (K rows of Kp; one bulk copy of the padded transpose `vtpad`),
+// then Y[t][k].
+template <bool PSI>
+__global__ void __launch_bounds__(kBatchThreads) k_down_coef(const TaskBlock* __restrict__ blocks,
+                                                             const int32_t* __restrict__ tasks,
+                                                             const DownJob* __restrict__ jobs,
+                                                             const double4* __restrict__ partials, int parts,
+                                                             int64_t pstride, const double* __restrict__ vtpad,
+                                                             const int32_t* __restrict__ vpad_off,
+                                                             double4* __restrict__ coef, int* err, uint64_t wait_ns) {
+    extern __shared__ __align__(32) double bsm[];
+    __shared__ __align__(8) uint64_t bar;
+    const TaskBlock tb = blocks[blockIdx.x];
+    const int d = tb.deg, K = nproxy(d), Kp = batch_pad(K), nt = tb.count;
+    double* A = bsm;
+    double4* Y = reinterpret_cast<double4*>(bsm + K * Kp);  // K * Kp is a multiple of 4
+    stage_issue(A, vtpad + vpad_off[d], uint32_t(sizeof(double)) * K * Kp, &bar);
+    for (int i = threadIdx.x; i < nt * K; i += kBatchThreads) {
+        const int t = i / K, k = i - t * K;
+        const int32_t slot = jobs[tasks[tb.first + t]].slot;
+        double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int q = 0; q < parts; q++) {
+            const double4 y = partials[int64_t(q) * pstride + slot + k];
+            v.x += y.x; v.y += y.y; v.z += y.z; v.w += y.w;
+        }
+        Y[i] = v;
     }
-#pragma unroll 4
-    for (int k = 0; k < K; k++) {
-        const double4 y = Y[k];
-        const double* row = VT + k * K;
+    __syncthreads();
+    if (!stage_wait(&bar, wait_ns)) {
+        if (threadIdx.x == 0) set_error(err, kErrTimeout);
+        return;
+    }
+    const int npair = Kp / 2, tid = threadIdx.x;
+    if (tid >= npair * ((nt + 3) / 4)) return;  // no barrier follows
+    const int m0 = 2 * (tid % npair), t0 = 4 * (tid / npair);
+    double4 c[4][2];
 #pragma unroll
-        for (int q = 0; q < NQ; q++) {
-            const double t = __ldg(row + mm[q]);
-            c[q].x = fma(t, y.x, c[q].x);
-            c[q].y = fma(t, y.y, c[q].y);
-            c[q].z = fma(t, y.z, c[q].z);
-            if (PSI) c[q].w = fma(t, y.w, c[q].w);
+    for (int j = 0; j < 4; j++) c[j][0] = c[j][1] = make_double4(0.0, 0.0, 0.0, 0.0);
+    const double4* Yt = Y + t0 * K;
+    for (int k = 0; k < K; k++) {
+        const double2 a = *reinterpret_cast<const double2*>(A + k * Kp + m0);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const double4 y = (t0 + j < nt) ? Yt[j * K + k] : make_double4(0.0, 0.0, 0.0, 0.0);
+            c[j][0].x = fma(a.x, y.x, c[j][0].x);
+            c[j][0].y = fma(a.x, y.y, c[j][0].y);
+            c[j][0].z = fma(a.x, y.z, c[j][0].z);
+            c[j][1].x = fma(a.y, y.x, c[j][1].x);
+            c[j][1].y = fma(a.y, y.y, c[j][1].y);
+            c[j][1].z = fma(a.y, y.z, c[j][1].z);
+            if (PSI) {
+                c[j][0].w = fma(a.x, y.w, c[j][0].w);
+                c[j][1].w = fma(a.y, y.w, c[j][1].w);
+            }
         }
     }
 #pragma unroll
-    for (int q = 0; q < NQ; q++)
-        if (lane + 32 * q < K) out[lane + 32 * q] = c[q];
+    for (int j = 0; j < 4; j++) {
+        if (t0 + j >= nt) break;
+        double4* out = coef + jobs[tasks[tb.first + t0 + j]].coef;
+        if (m0 < K) out[m0] = c[j][0];
+        if (m0 + 1 < K) out[m0 + 1] = c[j][1];
+    }
 }
 
-template <bool PSI>
-__global__ void __launch_bounds__(32 * kCoefWarps) k_down_coef(const DownJob* __restrict__ jobs, int njobs,
-                                                               const double4* __restrict__ partials, int parts,
-                                                               int64_t pstride, const double* __restrict__ vinvT,
-                                                               const int32_t* __restrict__ vinv_off,
-                                                               double4* __restrict__ coef) {
-    static_assert(kMaxK <= 96, "at most three outputs per lane");
-    __shared__ double4 Y[kCoefWarps][kMaxK];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int j = blockIdx.x * kCoefWarps + w;
-    if (j >= njobs) return;  // whole warps only; no block-wide barrier follows
-    const DownJob job = jobs[j];
-    const int K = nproxy(job.deg);
-    for (int k = lane; k < K; k += 32) {
-        double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
-        for (int p = 0; p < parts; p++) {
-            const double4 q = partials[int64_t(p) * pstride + job.slot + k];
-            v.x += q.x; v.y += q.y; v.z += q.z; v.w += q.w;
-        }
-        Y[w][k] = v;
-    }
-    __syncwarp();
-    const double* VT = vinvT + vinv_off[job.deg];
-    double4* out = coef + job.coef;
-    if (K <= 32)
-        coef_outputs<PSI, 1>(VT, K, lane, Y[w], out);
-    else if (K <= 64)
-        coef_outputs<PSI, 2>(VT, K, lane, Y[w], out);
-    else
-        coef_outputs<PSI, 3>(VT, K, lane, Y[w], out);
-}
+size_t down_coef_smem(int K) { return sizeof(double) * size_t(K * batch_pad(K)) + sizeof(double4) * size_t(kBatchTasks * K); }
 
 // The interpolant of degree D with coefficients C at barycentric (u, v)
 // (both mapped to [-1, 1]): sum_a T_a(u) sum_b C[m(a, b)] T_b(v), a + b <= D,
@@ -461,16 +515,35 @@ void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, cons
                                                     lev_off, leaf_level, nmax, level_mask, up_deg, nleaf, part);
 }
 
-void launch_up_combine(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part, int leaf_level,
-                       int nmax, const double* vinv, const int32_t* vinv_off, const double4* proxy_pos,
-                       const NodeGeom* node, int local_frames, int64_t n, void* src) {
+void launch_up_proxies(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part,
+                       int leaf_level, int nmax, double* msum, int nblocks, const TaskBlock* blocks,
+                       const int32_t* tasks, const double* vpad, const int32_t* vpad_off, const double4* proxy_pos,
+                       int64_t n, void* src, int* err, uint64_t wait_ns) {
     if (njobs == 0) return;
+    k_up_sums<<<njobs, kMaxK, 0, st>>>(jobs, part, leaf_level, nmax, msum);
+    const size_t smem = up_proxies_smem(nproxy(nmax));
     if (fp64)
-        k_up_combine<double><<<njobs, kUpThreads, 0, st>>>(jobs, part, leaf_level, nmax, vinv, vinv_off, proxy_pos,
-                                                           node, local_frames, n, static_cast<double4*>(src));
+        k_up_proxies<double><<<nblocks, kBatchThreads, smem, st>>>(blocks, tasks, jobs, msum, nmax, vpad, vpad_off,
+                                                                   proxy_pos, n, static_cast<double4*>(src), err,
+                                                                   wait_ns);
     else
-        k_up_combine<float><<<njobs, kUpThreads, 0, st>>>(jobs, part, leaf_level, nmax, vinv, vinv_off, proxy_pos,
-                                                          node, local_frames, n, static_cast<float4*>(src));
+        k_up_proxies<float><<<nblocks, kBatchThreads, smem, st>>>(blocks, tasks, jobs, msum, nmax, vpad, vpad_off,
+                                                                  proxy_pos, n, static_cast<float4*>(src), err,
+                                                                  wait_ns);
+}
+
+int batch_tasks() { return kBatchTasks; }
+
+cudaError_t batch_prepare() {
+    // dynamic shared memory above the default 48 KB, sized for the largest degree
+    const int up = int(up_proxies_smem(kMaxK)), dn = int(down_coef_smem(kMaxK));
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_up_proxies<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, up)) ||
+        (e = cudaFuncSetAttribute(k_up_proxies<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, up)) ||
+        (e = cudaFuncSetAttribute(k_down_coef<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dn)) ||
+        (e = cudaFuncSetAttribute(k_down_coef<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dn)))
+        return e;
+    return cudaSuccess;
 }
 
 void launch_epilogue(cudaStream_t st, bool fp64, const EpiArgs& a) {
@@ -512,14 +585,16 @@ void launch_scatter_state(cudaStream_t st, int64_t n, const int32_t* perm, const
 
 void launch_down(cudaStream_t st, bool psi, const DownArgs& d) {
     if (d.njobs == 0) return;
-    const unsigned nb = unsigned((d.njobs + kCoefWarps - 1) / kCoefWarps);
+    const unsigned nb = unsigned(d.ncoef_blocks);
+    const size_t smem = down_coef_smem(nproxy(d.max_deg));
     if (psi) {
-        k_down_coef<true><<<nb, 32 * kCoefWarps, 0, st>>>(d.jobs, d.njobs, d.partials, d.parts, d.pstride, d.vinvT,
-                                                          d.vinv_off, d.coef);
+        k_down_coef<true><<<nb, kBatchThreads, smem, st>>>(d.coef_blocks, d.coef_tasks, d.jobs, d.partials, d.parts,
+                                                           d.pstride, d.vtpad, d.vpad_off, d.coef, d.err, d.wait_ns);
         k_down_direct<true><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc, d.coef, d.out);
     } else {
-        k_down_coef<false><<<nb, 32 * kCoefWarps, 0, st>>>(d.jobs, d.njobs, d.partials, d.parts, d.pstride, d.vinvT,
-                                                           d.vinv_off, d.coef);
+        k_down_coef<false><<<nb, kBatchThreads, smem, st>>>(d.coef_blocks, d.coef_tasks, d.jobs, d.partials,
+                                                            d.parts, d.pstride, d.vtpad, d.vpad_off, d.coef, d.err,
+                                                            d.wait_ns);
         k_down_direct<false><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc, d.coef, d.out);
     }
 }

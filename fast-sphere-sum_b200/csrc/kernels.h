@@ -91,18 +91,36 @@ int persistent_blocks_per_sm();
 void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, const int32_t* leaf_start,
                     const double4* frame, const NodeGeom* node, const int64_t* lev_off, int leaf_level, int nmax,
                     int level_mask, const int8_t* up_deg, double* part);
-void launch_up_combine(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part, int leaf_level,
-                       int nmax, const double* vinv, const int32_t* vinv_off, const double4* proxy_pos,
-                       const NodeGeom* node, int local_frames, int64_t n, void* src);
+// Upward pass, part 2: every proxy face's moments (its rows summed into
+// msum, njobs x nproxy(nmax)), then the proxy charges of every (face,
+// degree) task, batched by degree (`blocks` of at most batch_tasks() tasks).
+// vpad: Vinv of every degree with rows padded to a multiple of 4 doubles
+// (vpad_off by degree); a failed wait sets kErrTimeout in err.
+void launch_up_proxies(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part,
+                       int leaf_level, int nmax, double* msum, int nblocks, const TaskBlock* blocks,
+                       const int32_t* tasks, const double* vpad, const int32_t* vpad_off, const double4* proxy_pos,
+                       int64_t n, void* src, int* err, uint64_t wait_ns);
+// Tasks per block of the batched V^-1 products (upward proxy charges,
+// downward coefficients).
+int batch_tasks();
+// Allows the batched V^-1 kernels the dynamic shared memory of the largest
+// degree (host only; before their first launch).
+cudaError_t batch_prepare();
 // Downward pass of the target clusters and the faces below them.
 struct DownArgs {
     int njobs = 0;                       // target clusters
     const DownJob* jobs = nullptr;
+    int ncoef_blocks = 0;                // their coefficient tasks, batched by degree
+    int max_deg = 0;                     // highest target-cluster degree
+    const TaskBlock* coef_blocks = nullptr;
+    const int32_t* coef_tasks = nullptr;
     const double4* partials = nullptr;   // field at the interpolation points: parts slots of stride pstride
     int parts = 1;
     int64_t pstride = 0;
-    const double* vinvT = nullptr;       // inverse Vandermonde matrices transposed, by degree
-    const int32_t* vinv_off = nullptr;
+    const double* vtpad = nullptr;       // inverse Vandermonde matrices transposed, rows padded
+    const int32_t* vpad_off = nullptr;   // to a multiple of 4 doubles, by degree
+    int* err = nullptr;                  // kErrTimeout when a staging wait runs out
+    uint64_t wait_ns = 0;
     const NodeGeom* node = nullptr;
     double4* coef = nullptr;
     int nleaf = 0;
