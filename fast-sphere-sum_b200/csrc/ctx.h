@@ -79,7 +79,7 @@ struct fss_ctx {
     std::vector<fss::TList> tlists;         // target clusters (cp/cc) and their sources
     std::vector<std::pair<fss::PairShape, double>> tuned;  // autotuner: shape, ms per pair pass
     std::vector<std::pair<int, double>> tuned_depth;       // autotuner: tree levels, ms per RHS
-    std::vector<std::pair<int, double>> tuned_parts;       // autotuner: src_parts, ms per pair pass
+    std::vector<std::pair<int, double>> tuned_parts;       // autotuner: src_parts, ms per right-hand side
     int64_t depth_n = -1;  // particle count the tuned depth belongs to
     int depth_tl = 0;      // tuned tree levels (0: none)
     int src_parts_given = 0;  // src_parts of the configuration (0: the autotuner may choose)

@@ -729,7 +729,9 @@ int tune_rhs(fss_ctx* c) {
 // (leaf size), when the configuration leaves it automatic -- the automatic
 // depth and one level either side, each built and timed on a whole
 // right-hand side (the fastest is kept for this particle count); and the
-// source split (src_parts 1, 2, 4), when automatic, timed on the pairs.
+// source split (src_parts 1, 2, 4), when automatic, timed on a whole
+// right-hand side (more parts balance the pair launches but add partial
+// slots for the epilogue to sum).
 // depth = false (lists rebuilt for per-leaf parameters, which belong to the
 // current leaves) keeps the tree.
 int autotune(fss_ctx* c, bool depth) {
@@ -781,15 +783,15 @@ int autotune(fss_ctx* c, bool depth) {
         }
     }
     if (c->cfg.autotune >= 2 && c->cfg.src_parts == 0) {
-        int best_p = 0;
+        c->tuned_parts.clear();
+        int best_p = 1;
         double best_p_ms = 1e30;
         for (int p : {1, 2, 4}) {
             c->cfg.src_parts = p;
             TRY(materialize(c, best));
             TRY(refresh_stage(c));
-            TRY(tune_rhs(c));
             double ms = 0;
-            TRY(time_ms(c, ev, 2, [&] { return launch_all_pairs(c, false); }, &ms));
+            TRY(time_ms(c, ev, 3, [&] { return tune_rhs(c); }, &ms));
             c->tuned_parts.push_back({p, ms});
             if (ms < best_p_ms) {
                 best_p_ms = ms;

@@ -25,7 +25,7 @@ namespace fss {
 // at up_row_step; slots keep the stride nproxy(nmax), and moments above a
 // face's degree are neither written nor read.
 template <typename T>
-__global__ void __launch_bounds__(kUpThreads) k_up_leaf(const typename Vec4<T>::type* __restrict__ src,
+__global__ void __launch_bounds__(kUpThreads, 6) k_up_leaf(const typename Vec4<T>::type* __restrict__ src,
                                                         const int32_t* __restrict__ leaf_start,
                                                         const double4* __restrict__ frame,
                                                         const NodeGeom* __restrict__ node,

@@ -7,7 +7,7 @@ namespace fss {
 
 constexpr int kUpThreads = 128;          // four warps, one leaf each
 constexpr int kUpLeaves = kUpThreads / 32;
-constexpr int kUpRows = 16;              // basis rows (degree <= 15), zero beyond n
+constexpr int kUpRows = kMaxDegree + 1;  // basis rows (degree <= kMaxDegree)
 constexpr int kUpLd = 32 + 4;            // padded row: the 8 rows x 4 doubles a DMMA operand reads hit distinct banks
 
 // Moments of the particles [a0, a1) of one leaf in the frame of one
@@ -19,9 +19,9 @@ constexpr int kUpLd = 32 + 4;            // padded row: the 8 rows x 4 doubles a
 // The rest (a >= 8 or b >= 8, so the other index <= NM - 8) is one tile
 // with rows a = 8..NM, 0..NM-8 and columns b = 0..NM-8, 8..NM when NM <= 11,
 // else the two tiles a >= 8, b < 8 and a < 8, b >= 8 (none for NM < 8).
-// Rows above NM are neither formed nor stored: a tile may read such a row
-// (left from earlier chunks), but it only reaches outputs with a + b > NM,
-// which are dropped.  Lane (4 g + t) holds D[g][2t + {0, 1}] of each tile;
+// Rows above NM are neither formed nor stored: a tile row or column index
+// above NM is clamped to NM (a row of this chunk), and it only reaches
+// outputs with a + b > NM, which are dropped.  Lane (4 g + t) holds D[g][2t + {0, 1}] of each tile;
 // every moment is written once, to out[m], m = (a + b)(a + b + 1) / 2 + b.
 // The groups of four particles are taken in particle order, so a moment's
 // sum does not depend on which tile forms it, on NM or on the chunking.
@@ -34,8 +34,11 @@ __device__ __forceinline__ void leaf_moments_n(const typename Vec4<T>::type* __r
     constexpr int H = NM - 7;                            // rows 8..NM when NT == 2
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     // tile 1: this lane's row of W and column of V
-    const int ra1 = NT == 2 ? (g < H ? 8 + g : g - H) : 8 + g;
-    const int cb1 = NT == 2 ? (g < H ? g : 8 + (g - H)) : g;
+    const int ra1u = NT == 2 ? (g < H ? 8 + g : g - H) : 8 + g;  // the row this lane's outputs belong to
+    const int ra1 = min(ra1u, NM);
+    const int cb1 = min(NT == 2 ? (g < H ? g : 8 + (g - H)) : g, NM);
+    const int g0 = min(g, NM);      // tile 0's row and column (a, b < 8)
+    const int c2 = min(8 + g, NM);  // tile 2's column (b >= 8)
     double d00 = 0.0, d01 = 0.0, e00 = 0.0, e01 = 0.0, f00 = 0.0, f01 = 0.0;
     for (int c0 = a0; c0 < a1; c0 += 32) {
         const int j = c0 + lane;
@@ -64,9 +67,9 @@ __device__ __forceinline__ void leaf_moments_n(const typename Vec4<T>::type* __r
         const int nk = (min(32, a1 - c0) + 3) >> 2;
         for (int k = 0; k < nk; k++) {
             const int p = 4 * k + t;
-            dmma_8x8x4(d00, d01, W[g][p], V[g][p]);
+            dmma_8x8x4(d00, d01, W[g0][p], V[g0][p]);
             if constexpr (NT >= 2) dmma_8x8x4(e00, e01, W[ra1][p], V[cb1][p]);
-            if constexpr (NT == 3) dmma_8x8x4(f00, f01, W[g][p], V[8 + g][p]);  // a < 8, b >= 8
+            if constexpr (NT == 3) dmma_8x8x4(f00, f01, W[g0][p], V[c2][p]);  // a < 8, b >= 8
         }
         __syncwarp();
     }
@@ -76,7 +79,7 @@ __device__ __forceinline__ void leaf_moments_n(const typename Vec4<T>::type* __r
         int a = g, b = c;  // tile 0
         if (a + b <= NM) out[(a + b) * (a + b + 1) / 2 + b] = i ? d01 : d00;
         if constexpr (NT >= 2) {
-            a = ra1;
+            a = ra1u;
             b = NT == 2 ? (c < H ? c : 8 + (c - H)) : c;
             if (a + b <= NM && (a >= 8 || b >= 8)) out[(a + b) * (a + b + 1) / 2 + b] = i ? e01 : e00;
         }
