@@ -641,6 +641,7 @@ int eval_partials(fss_ctx* c, bool want_psi, bool* down_out) {
         d.jobs = c->down_jobs.as<DownJob>();
         d.ncoef_blocks = c->n_dn_blocks;
         d.max_deg = c->down_max_deg;
+        d.fp32_eval = !c->fp64;
         d.coef_blocks = c->dn_tblocks.as<TaskBlock>();
         d.coef_tasks = c->dn_tasks.as<int32_t>();
         d.partials = c->partials.as<double4>();

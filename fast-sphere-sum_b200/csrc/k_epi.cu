@@ -449,11 +449,57 @@ __device__ __forceinline__ double4 eval_any(int deg, double u, double v, const d
 }
 static_assert(kMaxDegree == 12, "eval_any instantiates degrees 0..12");
 
+// FP32 form of eval_deg for the mixed-precision path (velocity only): the
+// recurrences and the K x 3 contraction in FP32 on coefficients rounded to
+// FP32; the caller adds the result in FP64.
+template <int D>
+__device__ __forceinline__ float3 eval_deg_f(float u, float v, const float4* __restrict__ C) {
+    float tv[D + 1];
+    tv[0] = 1.f;
+    if (D >= 1) tv[1] = v;
+    const float v2 = 2.f * v, u2 = 2.f * u;
+#pragma unroll
+    for (int b = 2; b <= D; b++) tv[b] = fmaf(v2, tv[b - 1], -tv[b - 2]);
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    float ta = 1.f, ta_prev = u;  // T_a(u), T_{a-1}(u) (T_{-1} = T_1)
+#pragma unroll
+    for (int a = 0; a <= D; a++) {
+        float3 sa = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+        for (int b = 0; a + b <= D; b++) {
+            const float4 cm = C[(a + b) * (a + b + 1) / 2 + b];
+            sa.x = fmaf(tv[b], cm.x, sa.x);
+            sa.y = fmaf(tv[b], cm.y, sa.y);
+            sa.z = fmaf(tv[b], cm.z, sa.z);
+        }
+        acc.x = fmaf(ta, sa.x, acc.x);
+        acc.y = fmaf(ta, sa.y, acc.y);
+        acc.z = fmaf(ta, sa.z, acc.z);
+        const float tn = fmaf(u2, ta, -ta_prev);
+        ta_prev = ta;
+        ta = tn;
+    }
+    return acc;
+}
+
+__device__ __forceinline__ float3 eval_any_f(int deg, float u, float v, const float4* C) {
+    switch (deg) {
+#define FSS_DEG(D) \
+    case D: return eval_deg_f<D>(u, v, C);
+        FSS_DEG(0) FSS_DEG(1) FSS_DEG(2) FSS_DEG(3) FSS_DEG(4) FSS_DEG(5) FSS_DEG(6)
+        FSS_DEG(7) FSS_DEG(8) FSS_DEG(9) FSS_DEG(10) FSS_DEG(11) FSS_DEG(12)
+#undef FSS_DEG
+    }
+    return make_float3(0.f, 0.f, 0.f);
+}
+
 // Downward pass, part 2: one block per leaf; every particle sums the
 // interpolants of the target clusters above its leaf (coarse to fine),
 // evaluated where it is (barycentric coordinates of its central projection
-// in each cluster's frame).  A leaf below none writes zeros.
-template <bool PSI>
+// in each cluster's frame).  A leaf below none writes zeros.  F32 (mixed
+// precision, velocity only): the interpolants evaluated in FP32
+// (eval_deg_f), the coordinates and the sum over the clusters in FP64.
+template <bool PSI, bool F32>
 __global__ void __launch_bounds__(kUpThreads) k_down_direct(const double4* __restrict__ xs,
                                                             const int32_t* __restrict__ leaf_start,
                                                             const NodeGeom* __restrict__ node,
@@ -481,8 +527,15 @@ __global__ void __launch_bounds__(kUpThreads) k_down_direct(const double4* __res
         off[nanc] = o;
     }
     __syncthreads();
+    float4* Cf = reinterpret_cast<float4*>(C);  // F32: the same coefficients rounded, 16 B each
     for (int a = 0; a < nanc; a++)
-        for (int m = tid; m < off[a + 1] - off[a]; m += kUpThreads) C[off[a] + m] = coef[int64_t(A[a].coef) + m];
+        for (int m = tid; m < off[a + 1] - off[a]; m += kUpThreads) {
+            const double4 cd = coef[int64_t(A[a].coef) + m];
+            if (F32)
+                Cf[off[a] + m] = make_float4(float(cd.x), float(cd.y), float(cd.z), 0.f);
+            else
+                C[off[a] + m] = cd;
+        }
     __syncthreads();
     for (int i = a0 + tid; i < a1; i += kUpThreads) {
         const double4 x = xs[i];
@@ -493,8 +546,14 @@ __global__ void __launch_bounds__(kUpThreads) k_down_direct(const double4* __res
             const double c1 = ng.minv[3] * x.x + ng.minv[4] * x.y + ng.minv[5] * x.z;
             const double c2 = ng.minv[6] * x.x + ng.minv[7] * x.y + ng.minv[8] * x.z;
             const double inv = 1.0 / (c0 + c1 + c2);
-            const double4 e = eval_any<PSI>(A[a].deg, 2.0 * (c0 * inv) - 1.0, 2.0 * (c1 * inv) - 1.0, C + off[a]);
-            acc.x += e.x; acc.y += e.y; acc.z += e.z; acc.w += e.w;
+            const double u = 2.0 * (c0 * inv) - 1.0, v = 2.0 * (c1 * inv) - 1.0;
+            if (F32) {
+                const float3 e = eval_any_f(A[a].deg, float(u), float(v), Cf + off[a]);
+                acc.x += double(e.x); acc.y += double(e.y); acc.z += double(e.z);
+            } else {
+                const double4 e = eval_any<PSI>(A[a].deg, u, v, C + off[a]);
+                acc.x += e.x; acc.y += e.y; acc.z += e.z; acc.w += e.w;
+            }
         }
         out[i] = acc;
     }
@@ -590,12 +649,18 @@ void launch_down(cudaStream_t st, bool psi, const DownArgs& d) {
     if (psi) {
         k_down_coef<true><<<nb, kBatchThreads, smem, st>>>(d.coef_blocks, d.coef_tasks, d.jobs, d.partials, d.parts,
                                                            d.pstride, d.vtpad, d.vpad_off, d.coef, d.err, d.wait_ns);
-        k_down_direct<true><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc, d.coef, d.out);
+        k_down_direct<true, false><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc, d.coef,
+                                                                   d.out);
     } else {
         k_down_coef<false><<<nb, kBatchThreads, smem, st>>>(d.coef_blocks, d.coef_tasks, d.jobs, d.partials,
                                                             d.parts, d.pstride, d.vtpad, d.vpad_off, d.coef, d.err,
                                                             d.wait_ns);
-        k_down_direct<false><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc, d.coef, d.out);
+        if (d.fp32_eval)
+            k_down_direct<false, true><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc,
+                                                                       d.coef, d.out);
+        else
+            k_down_direct<false, false><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc,
+                                                                        d.coef, d.out);
     }
 }
 

@@ -128,6 +128,7 @@ struct DownArgs {
     const int32_t* leaf_start = nullptr;
     const LeafAnc* leaf_anc = nullptr;   // kMaxLevels per leaf
     double4* out = nullptr;              // down-pass partial slot, one per particle
+    bool fp32_eval = false;              // mixed precision: interpolants evaluated in FP32 (velocity)
 };
 void launch_down(cudaStream_t st, bool psi, const DownArgs& d);
 int down_launch_count(const DownArgs& d);
