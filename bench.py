@@ -483,7 +483,7 @@ def kernel_rooflines(prof, steps, n, info, up_bytes, peaks):
 
     up_ms = sum(prof[k][0] for k in ("upward_leaf", "upward_combine") if k in prof) / (4 * steps)
     if up_ms > 0:
-        add("upward pass (k_up_leaf + k_up_combine)", up_ms, float(up_bytes), "RHS")
+        add("upward pass (k_up_leaf, k_up_sums, k_up_proxies)", up_ms, float(up_bytes), "RHS")
     if "resort" in prof:
         add("tree build: per-step re-sort (k_reassign, radix sort, k_resort_*, k_leaf_bounds)",
             prof["resort"][0] / steps, float(n) * (24 + 8 + 16) + 2.0 * n * 12 * passes, "step")
