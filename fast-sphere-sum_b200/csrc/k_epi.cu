@@ -78,17 +78,22 @@ __host__ __device__ constexpr int batch_pad(int K) { return (K + 3) & ~3; }
 static_assert((batch_pad(kMaxK) / 2) * (kBatchTasks / 4) <= kBatchThreads, "one tile per thread at the largest degree");
 
 // Upward pass, part 2a: the moments of every proxy face, its rows summed
-// (up_row_step, sum_rows4), one thread per (face, moment): msum[j][m].
-__global__ void __launch_bounds__(kMaxK) k_up_sums(const ProxyJob* __restrict__ jobs, const double* __restrict__ part,
-                                                   int leaf_level, int nmax, double* __restrict__ msum) {
-    const ProxyJob& job = jobs[blockIdx.x];
-    const int m = threadIdx.x;
+// (up_row_step, sum_rows4), one thread per (face, moment) over a flat grid
+// of njobs x nproxy(nmax) items: msum[j][m].
+constexpr int kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads) k_up_sums(const ProxyJob* __restrict__ jobs, int njobs,
+                                                         const double* __restrict__ part, int leaf_level, int nmax,
+                                                         double* __restrict__ msum) {
     const int KM = nproxy(nmax);
+    const int64_t item = int64_t(blockIdx.x) * kSumThreads + threadIdx.x;
+    if (item >= int64_t(njobs) * KM) return;
+    const int j = int(item / KM), m = int(item - int64_t(j) * KM);
+    const ProxyJob& job = jobs[j];
     if (m >= nproxy(31 - __clz(job.degmask))) return;  // moments this face's degrees use
     const int step = up_row_step(job.level, leaf_level);
     const int64_t stride = int64_t(step) * (leaf_level + 1) * KM;
     const double* pr = part + (int64_t(job.leaf_lo) * (leaf_level + 1) + job.level) * KM + m;
-    msum[int64_t(blockIdx.x) * KM + m] = sum_rows4([&](int r) { return pr[r * stride]; }, (job.leaf_hi - job.leaf_lo) / step);
+    msum[item] = sum_rows4([&](int r) { return pr[r * stride]; }, (job.leaf_hi - job.leaf_lo) / step);
 }
 
 // Upward pass, part 2b: proxy charges q_k = sum_m Vinv[m][k] M_m of every
@@ -579,7 +584,9 @@ void launch_up_proxies(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jo
                        const int32_t* tasks, const double* vpad, const int32_t* vpad_off, const double4* proxy_pos,
                        int64_t n, void* src, int* err, uint64_t wait_ns) {
     if (njobs == 0) return;
-    k_up_sums<<<njobs, kMaxK, 0, st>>>(jobs, part, leaf_level, nmax, msum);
+    const int64_t items = int64_t(njobs) * nproxy(nmax);
+    k_up_sums<<<unsigned((items + kSumThreads - 1) / kSumThreads), kSumThreads, 0, st>>>(jobs, njobs, part, leaf_level,
+                                                                                          nmax, msum);
     const size_t smem = up_proxies_smem(nproxy(nmax));
     if (fp64)
         k_up_proxies<double><<<nblocks, kBatchThreads, smem, st>>>(blocks, tasks, jobs, msum, nmax, vpad, vpad_off,
