@@ -9,9 +9,10 @@
 // read at run time) or a fixed range of far-cluster proxies -- which warp 0
 // packs back to back into shared-memory tiles as it goes, issuing one bulk
 // TMA copy (cp.async.bulk, no multicast) per piece with completion counted
-// on the tile slot's mbarrier.  Tiles circulate in a ring of kDepth slots
-// released by the consumer warps through a second mbarrier; an empty tile
-// ends a chunk.  Warp 0 only produces (and, in FP32, converts each landed
+// on the tile slot's mbarrier.  Tiles circulate in a ring of DEPTH slots
+// (kDepth = 4; kClusterDepth = 3 for the target-cluster launch's small
+// blocks) released by the consumer warps through a second mbarrier; an
+// empty tile ends a chunk.  Warp 0 only produces (and, in FP32, converts each landed
 // tile to pair-interleaved order for the packed f32x2 pipe); the other warps
 // consume, one target per thread.  Per pair (23 algorithmic flops):
 //

@@ -119,10 +119,11 @@ typedef struct fss_config {
                               FSS_LIST_LEAF the per-leaf (n, theta) are carried
                               up to the faces of a dual traversal (theta = min,
                               n = max over a face's leaves) */
-    int32_t wait_limit_us; /* every wait of the pair kernel on its tile ring
-                              gives up after this many microseconds and the
-                              call returns FSS_ERR_TIMEOUT, the context staying
-                              usable (0 = 2 s) */
+    int32_t wait_limit_us; /* every wait of the pair kernel on its tile ring,
+                              and of the batched V^-1 kernels on their bulk
+                              copy, gives up after this many microseconds and
+                              the call returns FSS_ERR_TIMEOUT, the context
+                              staying usable (0 = 2 s) */
     int32_t reserved[3];
 } fss_config;
 
