@@ -60,6 +60,7 @@ struct fss_ctx {
     std::vector<double> shard_cost;
     uint64_t wait_ns = 0;  // limit of the pair kernel's bounded waits
     int hold_block = -1;   // test hook: block of the next target-leaf launch that withholds a tile
+    int hold_stage = -1;   // test hook: 0 / 1, block 0 of the next proxy / coefficient launch withholds its matrix
 
     int64_t n = 0;
     bool have = false;

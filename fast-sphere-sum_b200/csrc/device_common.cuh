@@ -155,12 +155,15 @@ __device__ __forceinline__ void set_error(int* err, int code) {
 // A block's one-shot bulk staging: thread 0 initialises `bar` and copies
 // `bytes` (a multiple of 16; both addresses 16-byte aligned) of global memory
 // into shared memory; after a __syncthreads every thread calls stage_wait.
-__device__ __forceinline__ void stage_issue(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+// hold (test hook): the bytes are expected but no copy is issued, so the
+// wait runs out with nothing in flight.
+__device__ __forceinline__ void stage_issue(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
+                                            bool hold = false) {
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         mbar_init_fence();
         mbar_arrive_expect_tx(bar, bytes);
-        bulk_g2s(dst, src, bytes, bar);
+        if (!hold) bulk_g2s(dst, src, bytes, bar);
     }
 }
 

@@ -620,7 +620,8 @@ int eval_partials(fss_ctx* c, bool want_psi, bool* down_out) {
                               c->part_up.as<double>(), c->leaf_level, c->nmax, c->msum.as<double>(),
                               c->n_up_blocks, c->up_tblocks.as<TaskBlock>(), c->up_tasks.as<int32_t>(),
                               c->vpad.as<double>(), c->vpad_off.as<int32_t>(), c->proxy_pos.as<double4>(), c->n,
-                              c->src.p, c->err_flag.as<int>(), c->wait_ns);
+                              c->src.p, c->err_flag.as<int>(), c->wait_ns, c->hold_stage == 0 ? 0 : -1);
+            if (c->hold_stage == 0) c->hold_stage = -1;  // the test hook holds one launch only
         }
     }
     if (overlap) {
@@ -651,6 +652,8 @@ int eval_partials(fss_ctx* c, bool want_psi, bool* down_out) {
         d.vpad_off = c->vpad_off.as<int32_t>();
         d.err = c->err_flag.as<int>();
         d.wait_ns = c->wait_ns;
+        d.hold_block = c->hold_stage == 1 ? 0 : -1;
+        if (c->hold_stage == 1) c->hold_stage = -1;  // the test hook holds one launch only
         d.node = c->node.as<NodeGeom>();
         d.coef = c->down_coef.as<double4>();
         d.nleaf = int(c->nleaf);
@@ -858,7 +861,7 @@ int rk4_steps(fss_ctx* c, double dt, double omega, int nsteps) {
     if (nsteps < 0) return fail(c, FSS_ERR_INVALID, "nsteps < 0");
     TRY(refresh_stage(c));
     // a held tile (test hook) is taken by one eager step, never baked into a graph
-    const bool use_graph = c->cfg.use_graph && !c->prof && c->hold_block < 0;
+    const bool use_graph = c->cfg.use_graph && !c->prof && c->hold_block < 0 && c->hold_stage < 0;
     if (!use_graph) {
         for (int s = 0; s < nsteps; s++) TRY(rk4_once(c, dt, omega));
         return FSS_OK;
@@ -1485,6 +1488,14 @@ int fss_test_hold_tile(fss_ctx* c, int32_t block) {
     if (!c) return fail(c, FSS_ERR_INVALID, "null context");
     invalidate_graph(c);
     c->hold_block = block < 0 ? -1 : block;
+    return FSS_OK;
+}
+
+int fss_test_hold_stage(fss_ctx* c, int32_t which) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    if (which > 1) return fail(c, FSS_ERR_INVALID, "which must be 0 (proxy charges) or 1 (cluster coefficients)");
+    invalidate_graph(c);
+    c->hold_stage = which < 0 ? -1 : which;
     return FSS_OK;
 }
 

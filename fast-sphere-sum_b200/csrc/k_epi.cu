@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(kBatchThreads) k_up_proxies(const TaskBlock* _
                                                               const int32_t* __restrict__ vpad_off,
                                                               const double4* __restrict__ proxy_pos, int64_t n,
                                                               typename Vec4<T>::type* __restrict__ src, int* err,
-                                                              uint64_t wait_ns) {
+                                                              uint64_t wait_ns, int hold_block) {
     extern __shared__ __align__(32) double bsm[];
     __shared__ __align__(8) uint64_t bar;
     const TaskBlock tb = blocks[blockIdx.x];
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kBatchThreads) k_up_proxies(const TaskBlock* _
     const int KM = nproxy(nmax);
     double* A = bsm;
     double* X = bsm + K * Kp;
-    stage_issue(A, vpad + vpad_off[d], uint32_t(sizeof(double)) * K * Kp, &bar);
+    stage_issue(A, vpad + vpad_off[d], uint32_t(sizeof(double)) * K * Kp, &bar, int(blockIdx.x) == hold_block);
     for (int i = threadIdx.x; i < nt * K; i += kBatchThreads) {
         const int t = i / K, m = i - t * K;
         X[i] = msum[int64_t(tasks[tb.first + t]) * KM + m];
@@ -346,14 +346,15 @@ __global__ void __launch_bounds__(kBatchThreads) k_down_coef(const TaskBlock* __
                                                              const double4* __restrict__ partials, int parts,
                                                              int64_t pstride, const double* __restrict__ vtpad,
                                                              const int32_t* __restrict__ vpad_off,
-                                                             double4* __restrict__ coef, int* err, uint64_t wait_ns) {
+                                                             double4* __restrict__ coef, int* err, uint64_t wait_ns,
+                                                             int hold_block) {
     extern __shared__ __align__(32) double bsm[];
     __shared__ __align__(8) uint64_t bar;
     const TaskBlock tb = blocks[blockIdx.x];
     const int d = tb.deg, K = nproxy(d), Kp = batch_pad(K), nt = tb.count;
     double* A = bsm;
     double4* Y = reinterpret_cast<double4*>(bsm + K * Kp);  // K * Kp is a multiple of 4
-    stage_issue(A, vtpad + vpad_off[d], uint32_t(sizeof(double)) * K * Kp, &bar);
+    stage_issue(A, vtpad + vpad_off[d], uint32_t(sizeof(double)) * K * Kp, &bar, int(blockIdx.x) == hold_block);
     for (int i = threadIdx.x; i < nt * K; i += kBatchThreads) {
         const int t = i / K, k = i - t * K;
         const int32_t slot = jobs[tasks[tb.first + t]].slot;
@@ -582,7 +583,7 @@ void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, cons
 void launch_up_proxies(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part,
                        int leaf_level, int nmax, double* msum, int nblocks, const TaskBlock* blocks,
                        const int32_t* tasks, const double* vpad, const int32_t* vpad_off, const double4* proxy_pos,
-                       int64_t n, void* src, int* err, uint64_t wait_ns) {
+                       int64_t n, void* src, int* err, uint64_t wait_ns, int hold_block) {
     if (njobs == 0) return;
     const int64_t items = int64_t(njobs) * nproxy(nmax);
     k_up_sums<<<unsigned((items + kSumThreads - 1) / kSumThreads), kSumThreads, 0, st>>>(jobs, njobs, part, leaf_level,
@@ -591,11 +592,11 @@ void launch_up_proxies(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jo
     if (fp64)
         k_up_proxies<double><<<nblocks, kBatchThreads, smem, st>>>(blocks, tasks, jobs, msum, nmax, vpad, vpad_off,
                                                                    proxy_pos, n, static_cast<double4*>(src), err,
-                                                                   wait_ns);
+                                                                   wait_ns, hold_block);
     else
         k_up_proxies<float><<<nblocks, kBatchThreads, smem, st>>>(blocks, tasks, jobs, msum, nmax, vpad, vpad_off,
                                                                   proxy_pos, n, static_cast<float4*>(src), err,
-                                                                  wait_ns);
+                                                                  wait_ns, hold_block);
 }
 
 int batch_tasks() { return kBatchTasks; }
@@ -655,13 +656,14 @@ void launch_down(cudaStream_t st, bool psi, const DownArgs& d) {
     const size_t smem = down_coef_smem(nproxy(d.max_deg));
     if (psi) {
         k_down_coef<true><<<nb, kBatchThreads, smem, st>>>(d.coef_blocks, d.coef_tasks, d.jobs, d.partials, d.parts,
-                                                           d.pstride, d.vtpad, d.vpad_off, d.coef, d.err, d.wait_ns);
+                                                           d.pstride, d.vtpad, d.vpad_off, d.coef, d.err, d.wait_ns,
+                                                           d.hold_block);
         k_down_direct<true, false><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc, d.coef,
                                                                    d.out);
     } else {
         k_down_coef<false><<<nb, kBatchThreads, smem, st>>>(d.coef_blocks, d.coef_tasks, d.jobs, d.partials,
                                                             d.parts, d.pstride, d.vtpad, d.vpad_off, d.coef, d.err,
-                                                            d.wait_ns);
+                                                            d.wait_ns, d.hold_block);
         if (d.fp32_eval)
             k_down_direct<false, true><<<d.nleaf, kUpThreads, 0, st>>>(d.xs, d.leaf_start, d.node, d.leaf_anc,
                                                                        d.coef, d.out);

@@ -99,7 +99,7 @@ void launch_up_leaf(cudaStream_t st, bool fp64, int nleaf, const void* src, cons
 void launch_up_proxies(cudaStream_t st, bool fp64, int njobs, const ProxyJob* jobs, const double* part,
                        int leaf_level, int nmax, double* msum, int nblocks, const TaskBlock* blocks,
                        const int32_t* tasks, const double* vpad, const int32_t* vpad_off, const double4* proxy_pos,
-                       int64_t n, void* src, int* err, uint64_t wait_ns);
+                       int64_t n, void* src, int* err, uint64_t wait_ns, int hold_block = -1);
 // Tasks per block of the batched V^-1 products (upward proxy charges,
 // downward coefficients).
 int batch_tasks();
@@ -121,6 +121,7 @@ struct DownArgs {
     const int32_t* vpad_off = nullptr;   // to a multiple of 4 doubles, by degree
     int* err = nullptr;                  // kErrTimeout when a staging wait runs out
     uint64_t wait_ns = 0;
+    int hold_block = -1;                 // test hook: coefficient block that withholds its staging copy
     const NodeGeom* node = nullptr;
     double4* coef = nullptr;
     int nleaf = 0;

@@ -89,7 +89,7 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_ensemble_info", "fss_ensemble_time_pairs", "fss_amr_create", "fss_amr_destroy", "fss_amr_counts", "fss_amr_refine",
            "fss_amr_get_mesh", "fss_amr_remesh", "fss_amr_refine_current", "fss_remesh_lists", "fss_state_csv_append",
            "fss_point_count_append", "fss_output_name", "fss_state_bin_append", "fss_state_bin_read",
-           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_test_hold_tile", "fss_get_stream", "fss_shard_partition", "fss_shard_set", "fss_shard_get_info",
+           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_test_hold_tile", "fss_test_hold_stage", "fss_get_stream", "fss_shard_partition", "fss_shard_set", "fss_shard_get_info",
            "fss_shard_stage", "fss_shard_combine", "fss_version"]
 
 NOALLOC_MAX_PARTICLES = 262144  # FSS_NOALLOC_MAX_PARTICLES in include/fss.h
@@ -167,6 +167,7 @@ def lib():
     L.fss_read_vert_tris_csv.argtypes = [C.c_char_p, C.c_char_p, _i64, _I32, _I32, _i64]
     L.fss_version.restype = C.c_char_p
     L.fss_test_hold_tile.argtypes = [_vp, C.c_int32]
+    L.fss_test_hold_stage.argtypes = [_vp, C.c_int32]
     L.fss_get_stream.argtypes = [_vp, P(_vp)]
     L.fss_shard_partition.argtypes = [_i64, _D, C.c_int32, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
     L.fss_shard_set.argtypes = [_vp, C.c_int32, C.c_int32]
@@ -460,6 +461,12 @@ class Context:
         withholds its first source tile, so that its bounded waits run out
         (fss_test_hold_tile)."""
         self._c(lib().fss_test_hold_tile(self.h, block))
+
+    def test_hold_stage(self, which=0):
+        """Test hook: block 0 of the next evaluation's proxy-charge (0) or
+        cluster-coefficient (1) launch withholds the bulk copy of its matrix,
+        so that its bounded wait runs out (fss_test_hold_stage)."""
+        self._c(lib().fss_test_hold_stage(self.h, which))
 
 
 def shard_partition(cost, nranks):

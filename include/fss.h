@@ -531,6 +531,15 @@ int fss_shard_combine(fss_ctx* ctx, int32_t stage, double dt, double omega, cons
  * copies it did issue before it exits.  block < 0 clears the hook. */
 int fss_test_hold_tile(fss_ctx* ctx, int32_t block);
 
+/* Test hook for the batched V^-1 kernels' bounded wait: in the next
+ * right-hand-side evaluation, block 0 of the proxy-charge launch (which = 0)
+ * or of the cluster-coefficient launch (which = 1) expects the bulk copy of
+ * its matrix but does not issue it, so that its wait runs out.  The call
+ * returns FSS_ERR_TIMEOUT; the hook is then cleared and the context stays
+ * usable.  No copy is left in flight (none was issued).  which < 0 clears
+ * the hook. */
+int fss_test_hold_stage(fss_ctx* ctx, int32_t which);
+
 /* Library build string (architecture, features). */
 const char* fss_version(void);
 

@@ -7,7 +7,10 @@ source tile (no copy issued, arrival never signalled -- a flag that nothing
 sets), so that block's waits run out; the block waits for the copies it did
 issue, then exits.  The call must report FSS_ERR_TIMEOUT, the error word must
 be cleared, and the next call on the same context must give the normal
-result.  No GPU fault is involved: the kernel returns on its own.
+result.  No GPU fault is involved: the kernel returns on its own.  The same
+for the batched V^-1 kernels' one wait, on the bulk copy of their matrix:
+fss_test_hold_stage makes block 0 of the proxy-charge or cluster-coefficient
+launch expect that copy without issuing it.
 """
 import numpy as np
 import pytest
@@ -60,3 +63,18 @@ def test_default_limit_is_two_seconds(fss, field):
         ctx.set_particles(s, a)
         ctx.rk4_step(0.01, nsteps=3)
         assert np.all(np.isfinite(ctx.get_state()))
+
+
+@pytest.mark.parametrize("which", [0, 1], ids=["proxy charges", "cluster coefficients"])
+def test_batched_staging_wait_runs_out_then_context_recovers(fss, field, which):
+    s, a = field
+    with fss.Context(method=1, precision=1, degree=8, cluster_targets=1, wait_limit_us=LIMIT_US) as ctx:
+        ctx.set_particles(s, a)
+        assert ctx.tree_info()["target_clusters"] > 0
+        expect = ctx.rhs(s, a)
+        ctx.test_hold_stage(which)
+        with pytest.raises(fss.FssError) as e:
+            ctx.rhs(s, a)
+        assert e.value.code == TIMEOUT, str(e.value)
+        got = ctx.rhs(s, a)  # hook cleared, error word cleared
+        assert np.array_equal(got.view(np.uint64), expect.view(np.uint64))
