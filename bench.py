@@ -462,18 +462,17 @@ def amr_measure(fss, level=5, reps=3):
     return out
 
 
-def kernel_rooflines(prof, steps, n, info, up_bytes, peaks):
+def kernel_rooflines(prof, steps, n, up_bytes, peaks):
     """HBM roofline of the memory-bound ranges with the algorithmic byte
     units of the scope table: upward pass = N 16 B read per level + K (4 +
     12) B per proxy (per RHS, from fss_work_per_rhs); tree build (the
-    per-step re-sort) = N (24 + 8 + 16) B + 2 N 12 B per 8-bit radix pass;
-    RK4 combine = N (5 x 8 x (1 + 4) + 5 x 8 + 16) B per step.  The
+    per-step re-sort) = N (24 + 8 + 16) B + 2 N 12 B per radix pass executed
+    (none: the re-sort partitions the old order instead of sorting); RK4
+    combine = N (5 x 8 x (1 + 4) + 5 x 8 + 16) B per step.  The
     downward pass has no byte unit (FP64, latency-bound): time only.  Times
     from the kernel-level pass (events around every launch)."""
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     src = "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
-    leaves = max(int(info.get("leaf_count", 1)), 2)
-    passes = (max((leaves - 1).bit_length(), 1) + 7) // 8
     out = []
 
     def add(name, ms, nbytes, per):
@@ -485,8 +484,8 @@ def kernel_rooflines(prof, steps, n, info, up_bytes, peaks):
     if up_ms > 0:
         add("upward pass (k_up_leaf, k_up_sums, k_up_proxies)", up_ms, float(up_bytes), "RHS")
     if "resort" in prof:
-        add("tree build: per-step re-sort (k_reassign, radix sort, k_resort_*, k_leaf_bounds)",
-            prof["resort"][0] / steps, float(n) * (24 + 8 + 16) + 2.0 * n * 12 * passes, "step")
+        add("tree build: per-step re-sort (k_part_check, k_part_descend, k_part_bucket, k_part_place, "
+            "k_resort_commit)", prof["resort"][0] / steps, float(n) * (24 + 8 + 16), "step")
     if "epilogue" in prof:
         add("RK4 combine (k_epilogue, 4 per step)", prof["epilogue"][0] / steps,
             float(n) * (5 * 8 * 5 + 5 * 8 + 16), "step")
@@ -785,7 +784,7 @@ def main():
     roofline_detail = {"frac_at_sampled_clock": (achieved / (fp32_peak * clocks["sm_mhz"] / sm_max)) if clocks.get("sm_mhz") else None,
                        "kernel_shares": {k: round(v[0] / total_ms, 4) for k, v in prof.items()},
                        "upward_bytes_per_rhs": up_bytes,
-                       "kernels": kernel_rooflines(prof, args.steps, n, info, up_bytes, peaks)}
+                       "kernels": kernel_rooflines(prof, args.steps, n, up_bytes, peaks)}
 
     # ---------------- the other arms on the same GPU: the plain FP64 BLTC (the
     # ratio's denominator: fixed n, theta, far sources summed at the target

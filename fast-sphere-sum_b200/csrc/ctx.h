@@ -61,6 +61,7 @@ struct fss_ctx {
     uint64_t wait_ns = 0;  // limit of the pair kernel's bounded waits
     int hold_block = -1;   // test hook: block of the next target-leaf launch that withholds a tile
     int hold_stage = -1;   // test hook: 0 / 1, block 0 of the next proxy / coefficient launch withholds its matrix
+    int resort_mode = 0;   // test hook: per-step re-sort by partition of the old order (0) or radix key sort (1)
 
     int64_t n = 0;
     bool have = false;
@@ -98,7 +99,7 @@ struct fss_ctx {
     DBuf in5, area_in, perm, key, key_tmp, vals_tmp, hist, leaf_start, s0, xs, acc, area_s, tracer_s, src, partials,
         segs, items, jobs, frame, node, lev_off, verts, tri_verts, part_up, proxy_pos, out5, psi,
         wtotal, err_flag, loc, sortq, grid3, rm_target, rm_tris, rm_off, rm_adj, down_jobs, down_anc, down_coef, vpad, vtpad, vpad_off, up_deg, up_tblocks, up_tasks,
-        dn_tblocks, dn_tasks, msum;
+        dn_tblocks, dn_tasks, msum, part_scratch;
     int64_t src_count = 0;
 
     // graph

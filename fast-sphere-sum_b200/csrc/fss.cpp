@@ -385,6 +385,7 @@ int build_tree(fss_ctx* c) {
     CU(c->vals_tmp.ensure(sizeof(int32_t) * n));
     CU(c->sortq.ensure(sizeof(int32_t) * n));
     CU(c->hist.ensure(sizeof(uint32_t) * sort_scratch_words(n)));
+    CU(c->part_scratch.ensure(sizeof(uint32_t) * partition_scratch_words(c->nleaf)));
     CU(c->leaf_start.ensure(sizeof(int32_t) * (c->nleaf + 1)));
     c->ref_loc_h.clear();
     c->unassigned = 0;
@@ -811,15 +812,31 @@ int autotune(fss_ctx* c, bool depth) {
 }
 
 // Particles into the leaves they are in now (start of an RK4 step): keys,
-// stable key sort (order q), state permuted in place, leaf ranges, stage-1
-// sources.
+// the stable order of the new keys, state permuted in place, leaf ranges,
+// stage-1 sources.  The order comes from partitioning the old one (few
+// particles change leaves in a step); the radix key sort of the initial
+// build gives the same order and stays selectable by a test hook.
 int resort(fss_ctx* c) {
+    const int64_t n = c->n;
+    if (c->resort_mode == 0) {
+        // check, descent + scan, bucket, place, commit
+        ProfScope ps(c, "resort", 5);
+        const NodeGeom* node = c->node.as<NodeGeom>();
+        launch_resort_partition(c->stream, c->fp64, n, c->nleaf, c->leaf_level, node,
+                                node + c->geom.lev_off[c->leaf_level], c->lev_off.as<int64_t>(),
+                                c->key.as<uint32_t>(), c->key_tmp.as<uint32_t>(), c->leaf_start.as<int32_t>(),
+                                c->sortq.as<int32_t>(), c->vals_tmp.as<int32_t>(), c->part_scratch.as<uint32_t>(),
+                                c->s0.as<double4>(), c->area_s.as<double>(), c->tracer_s.as<double>(),
+                                c->perm.as<int32_t>(), c->xs.as<double4>(), c->acc.as<double4>(), c->src.p,
+                                c->err_flag.as<int>());
+        CU(cudaGetLastError());
+        return FSS_OK;
+    }
     int bits = 0;
     while ((int64_t(1) << bits) < c->nleaf) bits++;
     bits = std::max(bits, 1);
     // reassign, 3 per 8-bit sort pass, gather + commit, leaf bounds
     ProfScope ps(c, "resort", 1 + sort_launch_count(c->n, bits) + 2 + 1);
-    const int64_t n = c->n;
     launch_reassign(c->stream, n, c->s0.as<double4>(), nullptr, c->leaf_level, c->node.as<NodeGeom>(),
                     c->lev_off.as<int64_t>(), c->key.as<uint32_t>(), c->err_flag.as<int>());
     launch_sort(c->stream, n, bits, c->key.as<uint32_t>(), c->key_tmp.as<uint32_t>(),
@@ -1496,6 +1513,14 @@ int fss_test_hold_stage(fss_ctx* c, int32_t which) {
     if (which > 1) return fail(c, FSS_ERR_INVALID, "which must be 0 (proxy charges) or 1 (cluster coefficients)");
     invalidate_graph(c);
     c->hold_stage = which < 0 ? -1 : which;
+    return FSS_OK;
+}
+
+int fss_test_resort_mode(fss_ctx* c, int32_t mode) {
+    if (!c) return fail(c, FSS_ERR_INVALID, "null context");
+    if (mode != 0 && mode != 1) return fail(c, FSS_ERR_INVALID, "mode must be 0 (partition) or 1 (radix key sort)");
+    invalidate_graph(c);
+    c->resort_mode = mode;
     return FSS_OK;
 }
 

@@ -292,6 +292,25 @@ __device__ __forceinline__ double min_cone(const NodeGeom& g, double x, double y
     return fmin(c0, fmin(c1, c2));
 }
 
+// Leaf index on level LL reached from the 20 root faces: on each level the
+// first child that contains the point, else the most-inside one.
+__device__ __forceinline__ int descend(const NodeGeom* __restrict__ node, const int64_t* __restrict__ lev_off, int LL,
+                                       double4 q) {
+    int prev = 0;
+    for (int l = 0; l <= LL; l++) {
+        const int lb = (l > 0) ? 4 * prev : 0, ub = (l > 0) ? lb + 4 : 20;
+        int best = lb;
+        double best_min = -1e300;
+        for (int j = lb; j < ub; j++) {
+            const double m = min_cone(node[lev_off[l] + j], q.x, q.y, q.z);
+            if (m >= 0.0) { best = j; break; }
+            if (m > best_min) { best_min = m; best = j; }
+        }
+        prev = best;
+    }
+    return prev;
+}
+
 __global__ void k_reassign(int64_t n, const double4* __restrict__ pos, const EnsLeaf* __restrict__ leaves,
                            int leaf_level, const NodeGeom* __restrict__ node, const int64_t* __restrict__ lev_off,
                            uint32_t* __restrict__ key, int* __restrict__ err) {
@@ -314,19 +333,7 @@ __global__ void k_reassign(int64_t n, const double4* __restrict__ pos, const Ens
         local = lf.local;
     }
     if (min_cone(node[lev_off[LL] + local], q.x, q.y, q.z) >= 0.0) return;
-    int prev = 0;
-    for (int l = 0; l <= LL; l++) {
-        const int lb = (l > 0) ? 4 * prev : 0, ub = (l > 0) ? lb + 4 : 20;
-        int best = lb;
-        double best_min = -1e300;
-        for (int j = lb; j < ub; j++) {
-            const double m = min_cone(node[lev_off[l] + j], q.x, q.y, q.z);
-            if (m >= 0.0) { best = j; break; }
-            if (m > best_min) { best_min = m; best = j; }
-        }
-        prev = best;
-    }
-    key[i] = uint32_t(int64_t(g) - local + prev);
+    key[i] = uint32_t(int64_t(g) - local + descend(node, lev_off, LL, q));
 }
 
 // New order q (sorted position -> old position): the step state, areas,
@@ -343,12 +350,15 @@ __global__ void k_resort_gather(int64_t n, const int32_t* __restrict__ q, const 
 }
 
 // Back into place, with the stage-1 state (xs = s0) and interaction
-// sources (x, y, z, zeta A) of the new order.
+// sources (x, y, z, zeta A) of the new order; with ls_new, the new leaf
+// ranges (nls entries) copied into leaf_start as well.
 template <typename T>
 __global__ void k_resort_commit(int64_t n, const double4* __restrict__ xs, const double4* __restrict__ acc,
                                 double4* __restrict__ s0, double* __restrict__ area, double* __restrict__ tracer,
-                                int32_t* __restrict__ perm, typename Vec4<T>::type* __restrict__ src) {
+                                int32_t* __restrict__ perm, typename Vec4<T>::type* __restrict__ src,
+                                const uint32_t* __restrict__ ls_new, int32_t* __restrict__ leaf_start, int64_t nls) {
     const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (ls_new && s < nls) leaf_start[s] = int32_t(ls_new[s]);
     if (s >= n) return;
     const double4 v = xs[s];
     const double4 t = acc[s];
@@ -362,6 +372,202 @@ __global__ void k_resort_commit(int64_t n, const double4* __restrict__ xs, const
     o.z = T(v.z);
     o.w = T(v.w * t.x);
     src[s] = o;
+}
+
+// ---------------------------------------------------------------- re-sort by partition
+// Between two steps few particles change leaves, so the stable key sort of
+// the new leaf keys is built from the old order instead of sorted again:
+// within new leaf k, a stable sort puts first the particles that come from
+// old positions before leaf k's old range, then the ones that stayed (in
+// their old order), then the ones from after it (each group in old order).
+// The stayers' places follow from the old ranges and one scan of the new
+// leaf counts; only the movers are bucketed by new leaf and ranked there by
+// old position.  The result is the unique stable order, the same as the
+// radix sort's.
+//
+// Scratch words: [0] blocks done (descent), [1] movers listed, then in[m],
+// out[m], fill[m] (zeroed before every re-sort), ns[m + 1] (new leaf
+// starts), mo[m + 1] (bucket starts), m = leaf count.
+constexpr int kPartThreads = 256;
+
+// Fast path for every particle: still inside its old leaf (kept), else
+// listed as a mover.  key_new[i] = old key for now.
+__global__ void __launch_bounds__(kPartThreads) k_part_check(int64_t n, const double4* __restrict__ pos,
+                                                             const NodeGeom* __restrict__ leaf_node,
+                                                             const uint32_t* __restrict__ key,
+                                                             uint32_t* __restrict__ key_new,
+                                                             int32_t* __restrict__ movers, uint32_t* __restrict__ ctl,
+                                                             int* __restrict__ err) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool mover = false;
+    if (i < n) {
+        const double4 q = pos[i];
+        const uint32_t g = key[i];
+        key_new[i] = g;
+        // a non-finite position keeps its leaf (see k_reassign)
+        if (!isfinite(q.x) || !isfinite(q.y) || !isfinite(q.z))
+            set_error(err, kErrNonFinite);
+        else
+            mover = min_cone(leaf_node[g], q.x, q.y, q.z) < 0.0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, mover);
+    if (m == 0u) return;
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd(&ctl[1], uint32_t(__popc(m)));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (mover) movers[base + __popc(m & ((1u << lane) - 1u))] = int32_t(i);
+}
+
+// One block: ns = exclusive scan of the new leaf counts (old count - out +
+// in), mo = exclusive scan of in; entry m holds the totals.
+__device__ void part_scan(int64_t m, const int32_t* __restrict__ ls, const uint32_t* __restrict__ in,
+                          const uint32_t* __restrict__ out, uint32_t* __restrict__ ns, uint32_t* __restrict__ mo) {
+    constexpr int R = 8;
+    __shared__ uint32_t wa[kPartThreads / 32], wb[kPartThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    uint32_t ca = 0, cb = 0;  // carries (block-uniform)
+    for (int64_t base = 0; base < m; base += int64_t(kPartThreads) * R) {
+        uint32_t va[R], vb[R], sa = 0, sb = 0;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int64_t k = base + int64_t(t) * R + r;
+            va[r] = vb[r] = 0;
+            if (k < m) {
+                const uint32_t a_in = __ldcg(in + k), a_out = __ldcg(out + k);
+                va[r] = uint32_t(ls[k + 1] - ls[k]) - a_out + a_in;
+                vb[r] = a_in;
+            }
+            sa += va[r];
+            sb += vb[r];
+        }
+        uint32_t xa = sa, xb = sb;  // inclusive warp scan
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t ya = __shfl_up_sync(0xffffffffu, xa, d), yb = __shfl_up_sync(0xffffffffu, xb, d);
+            if (lane >= d) { xa += ya; xb += yb; }
+        }
+        if (lane == 31) { wa[w] = xa; wb[w] = xb; }
+        __syncthreads();
+        uint32_t oa = ca, ob = cb, ta = 0, tb = 0;
+        for (int v = 0; v < kPartThreads / 32; v++) {
+            if (v < w) { oa += wa[v]; ob += wb[v]; }
+            ta += wa[v];
+            tb += wb[v];
+        }
+        oa += xa - sa;
+        ob += xb - sb;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int64_t k = base + int64_t(t) * R + r;
+            if (k < m) { ns[k] = oa; mo[k] = ob; }
+            oa += va[r];
+            ob += vb[r];
+        }
+        ca += ta;
+        cb += tb;
+        __syncthreads();
+    }
+    if (t == 0) { ns[m] = ca; mo[m] = cb; }
+}
+
+// The movers' new leaves (descent from the root faces), their counts into
+// and out of every leaf; the last block to finish scans the counts.
+__global__ void __launch_bounds__(kPartThreads) k_part_descend(const double4* __restrict__ pos,
+                                                               const NodeGeom* __restrict__ node,
+                                                               const int64_t* __restrict__ lev_off, int leaf_level,
+                                                               const uint32_t* __restrict__ key,
+                                                               uint32_t* __restrict__ key_new,
+                                                               const int32_t* __restrict__ movers,
+                                                               uint32_t* __restrict__ scratch, int64_t m,
+                                                               const int32_t* __restrict__ ls) {
+    uint32_t* ctl = scratch;
+    uint32_t* in = scratch + 2;
+    uint32_t* out = in + m;
+    const uint32_t nmov = ctl[1];
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < nmov; j += stride) {
+        const int32_t i = movers[j];
+        const uint32_t g = key[i];
+        const uint32_t g2 = uint32_t(descend(node, lev_off, leaf_level, pos[i]));
+        key_new[i] = g2;
+        if (g2 != g) {
+            atomicAdd(&in[g2], 1u);
+            atomicAdd(&out[g], 1u);
+        }
+    }
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&ctl[0], 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    uint32_t* ns = out + 2 * m;  // after fill
+    part_scan(m, ls, in, out, ns, ns + m + 1);
+}
+
+// Movers into their new leaf's bucket (unordered within it).
+__global__ void __launch_bounds__(kPartThreads) k_part_bucket(const uint32_t* __restrict__ key,
+                                                              const uint32_t* __restrict__ key_new,
+                                                              const int32_t* __restrict__ movers,
+                                                              uint32_t* __restrict__ scratch, int64_t m,
+                                                              int32_t* __restrict__ bucket) {
+    const uint32_t nmov = scratch[1];
+    uint32_t* fill = scratch + 2 + 2 * m;
+    const uint32_t* mo = fill + m + (m + 1);
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < nmov; j += stride) {
+        const int32_t i = movers[j];
+        const uint32_t g2 = key_new[i];
+        if (g2 == key[i]) continue;
+        bucket[mo[g2] + atomicAdd(&fill[g2], 1u)] = i;
+    }
+}
+
+// One warp per new leaf k: its movers ranked by old position, its stayers
+// in old order, each particle's state gathered into its new place (xs, and
+// acc as {area, tracer, caller index, 0}), the new sorted keys written.
+constexpr int kPlaceWarps = 4;
+__global__ void __launch_bounds__(kPlaceWarps * 32) k_part_place(
+    int64_t m, const int32_t* __restrict__ ls, const uint32_t* __restrict__ key_new,
+    const uint32_t* __restrict__ scratch, const int32_t* __restrict__ bucket, const double4* __restrict__ s0,
+    const double* __restrict__ area, const double* __restrict__ tracer, const int32_t* __restrict__ perm,
+    double4* __restrict__ xs, double4* __restrict__ acc, uint32_t* __restrict__ key) {
+    const int64_t k = int64_t(blockIdx.x) * kPlaceWarps + (threadIdx.x >> 5);
+    if (k >= m) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t* in = scratch + 2;
+    const uint32_t* out = in + m;
+    const uint32_t* ns = out + 2 * m;
+    const uint32_t* mo = ns + m + 1;
+    const int32_t a = ls[k], b = ls[k + 1];
+    const uint32_t base = ns[k], c = in[k], m0 = mo[k];
+    const uint32_t stays = uint32_t(b - a) - out[k];
+    auto place = [&](int64_t p, int64_t dst) {
+        xs[dst] = s0[p];
+        acc[dst] = make_double4(area[p], tracer[p], double(perm[p]), 0.0);
+    };
+    // movers: rank = number of movers into k with a smaller old position
+    uint32_t below = 0;
+    for (uint32_t t = lane; t < c; t += 32) below += bucket[m0 + t] < a ? 1u : 0u;
+    for (int d = 16; d > 0; d >>= 1) below += __shfl_xor_sync(0xffffffffu, below, d);
+    for (uint32_t t = lane; t < c; t += 32) {
+        const int32_t p = bucket[m0 + t];
+        uint32_t r = 0;
+        for (uint32_t u = 0; u < c; u++) r += bucket[m0 + u] < p ? 1u : 0u;
+        place(p, int64_t(base) + r + (p >= a ? stays : 0u));
+    }
+    // stayers, in old order after the movers from below
+    uint32_t run = base + below;
+    for (int32_t p0 = a; p0 < b; p0 += 32) {
+        const int32_t p = p0 + lane;
+        const bool st = p < b && key_new[p] == uint32_t(k);
+        const unsigned bal = __ballot_sync(0xffffffffu, st);
+        if (st) place(p, int64_t(run) + __popc(bal & ((1u << lane) - 1u)));
+        run += __popc(bal);
+    }
+    const uint32_t cnt = stays + c;
+    for (uint32_t j = lane; j < cnt; j += 32) key[base + j] = uint32_t(k);
 }
 
 // ---------------------------------------------------------------- launchers
@@ -455,9 +661,42 @@ void launch_resort(cudaStream_t st, bool fp64, int64_t n, const int32_t* q, doub
     const unsigned g = unsigned((n + 255) / 256);
     k_resort_gather<<<g, 256, 0, st>>>(n, q, s0, area, tracer, perm, xs, acc);
     if (fp64)
-        k_resort_commit<double><<<g, 256, 0, st>>>(n, xs, acc, s0, area, tracer, perm, static_cast<double4*>(src));
+        k_resort_commit<double><<<g, 256, 0, st>>>(n, xs, acc, s0, area, tracer, perm, static_cast<double4*>(src),
+                                                   nullptr, nullptr, 0);
     else
-        k_resort_commit<float><<<g, 256, 0, st>>>(n, xs, acc, s0, area, tracer, perm, static_cast<float4*>(src));
+        k_resort_commit<float><<<g, 256, 0, st>>>(n, xs, acc, s0, area, tracer, perm, static_cast<float4*>(src),
+                                                  nullptr, nullptr, 0);
+}
+
+int64_t partition_scratch_words(int64_t nleaf) { return 2 + 3 * nleaf + 2 * (nleaf + 1); }
+
+void launch_resort_partition(cudaStream_t st, bool fp64, int64_t n, int64_t nleaf, int leaf_level,
+                             const NodeGeom* node, const NodeGeom* leaf_node, const int64_t* lev_off, uint32_t* key,
+                             uint32_t* key_new, int32_t* leaf_start, int32_t* movers, int32_t* bucket,
+                             uint32_t* scratch, double4* s0, double* area, double* tracer, int32_t* perm,
+                             double4* xs, double4* acc, void* src, int* err) {
+    if (n == 0) return;
+    cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * size_t(2 + 3 * nleaf), st);
+    k_part_check<<<unsigned((n + kPartThreads - 1) / kPartThreads), kPartThreads, 0, st>>>(
+        n, s0, leaf_node, key, key_new, movers, scratch, err);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+    const unsigned grid = unsigned(std::min<int64_t>(int64_t(sms) * 4, (n + kPartThreads - 1) / kPartThreads));
+    k_part_descend<<<grid, kPartThreads, 0, st>>>(s0, node, lev_off, leaf_level, key, key_new, movers, scratch, nleaf,
+                                                  leaf_start);
+    k_part_bucket<<<grid, kPartThreads, 0, st>>>(key, key_new, movers, scratch, nleaf, bucket);
+    k_part_place<<<unsigned((nleaf + kPlaceWarps - 1) / kPlaceWarps), kPlaceWarps * 32, 0, st>>>(
+        nleaf, leaf_start, key_new, scratch, bucket, s0, area, tracer, perm, xs, acc, key);
+    const uint32_t* ns = scratch + 2 + 3 * nleaf;
+    const unsigned g = unsigned((std::max(n, nleaf + 1) + 255) / 256);
+    if (fp64)
+        k_resort_commit<double><<<g, 256, 0, st>>>(n, xs, acc, s0, area, tracer, perm, static_cast<double4*>(src),
+                                                   ns, leaf_start, nleaf + 1);
+    else
+        k_resort_commit<float><<<g, 256, 0, st>>>(n, xs, acc, s0, area, tracer, perm, static_cast<float4*>(src), ns,
+                                                  leaf_start, nleaf + 1);
 }
 
 }  // namespace fss

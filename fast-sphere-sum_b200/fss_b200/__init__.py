@@ -89,7 +89,7 @@ SYMBOLS = ["fss_config_init", "fss_create", "fss_destroy", "fss_last_error", "fs
            "fss_ensemble_info", "fss_ensemble_time_pairs", "fss_amr_create", "fss_amr_destroy", "fss_amr_counts", "fss_amr_refine",
            "fss_amr_get_mesh", "fss_amr_remesh", "fss_amr_refine_current", "fss_remesh_lists", "fss_state_csv_append",
            "fss_point_count_append", "fss_output_name", "fss_state_bin_append", "fss_state_bin_read",
-           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_test_hold_tile", "fss_test_hold_stage", "fss_get_stream", "fss_shard_partition", "fss_shard_set", "fss_shard_get_info",
+           "fss_read_points_csv", "fss_read_tris_csv", "fss_read_vert_tris_csv", "fss_test_hold_tile", "fss_test_hold_stage", "fss_test_resort_mode", "fss_get_stream", "fss_shard_partition", "fss_shard_set", "fss_shard_get_info",
            "fss_shard_stage", "fss_shard_combine", "fss_version"]
 
 NOALLOC_MAX_PARTICLES = 262144  # FSS_NOALLOC_MAX_PARTICLES in include/fss.h
@@ -168,6 +168,7 @@ def lib():
     L.fss_version.restype = C.c_char_p
     L.fss_test_hold_tile.argtypes = [_vp, C.c_int32]
     L.fss_test_hold_stage.argtypes = [_vp, C.c_int32]
+    L.fss_test_resort_mode.argtypes = [_vp, C.c_int32]
     L.fss_get_stream.argtypes = [_vp, P(_vp)]
     L.fss_shard_partition.argtypes = [_i64, _D, C.c_int32, np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
     L.fss_shard_set.argtypes = [_vp, C.c_int32, C.c_int32]
@@ -467,6 +468,11 @@ class Context:
         cluster-coefficient (1) launch withholds the bulk copy of its matrix,
         so that its bounded wait runs out (fss_test_hold_stage)."""
         self._c(lib().fss_test_hold_stage(self.h, which))
+
+    def test_resort_mode(self, mode=0):
+        """Test hook: the per-step re-sort by partition of the old order (0,
+        the default) or by the radix key sort (1) (fss_test_resort_mode)."""
+        self._c(lib().fss_test_resort_mode(self.h, mode))
 
 
 def shard_partition(cost, nranks):

@@ -540,6 +540,15 @@ int fss_test_hold_tile(fss_ctx* ctx, int32_t block);
  * the hook. */
 int fss_test_hold_stage(fss_ctx* ctx, int32_t which);
 
+/* Test hook for the per-step re-sort (FSS_REBUILD_RESORT): mode 0 (the
+ * default) builds the new leaf order by partitioning the old one (particles
+ * that stay in their leaf keep their order; the few that move are bucketed
+ * by new leaf and ranked by old position), mode 1 by the two-pass radix key
+ * sort of the initial tree build.  Both give the unique stable order of the
+ * new leaf keys, so every later result is the same to the bit.  Other modes
+ * return FSS_ERR_INVALID. */
+int fss_test_resort_mode(fss_ctx* ctx, int32_t mode);
+
 /* Library build string (architecture, features). */
 const char* fss_version(void);
 

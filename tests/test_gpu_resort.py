@@ -64,3 +64,41 @@ def test_resort_graph_equals_eager(fss):
     outs = [_steps(fss, s, a, 4, method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED, use_graph=g,
                    rebuild=fss.REBUILD_RESORT)[0] for g in (0, 1)]
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("precision,use_graph,dt,level,tree_levels",
+                         [("mixed", 1, 0.01, 6, 5), ("mixed", 0, 0.01, 6, 5), ("fp64", 1, 0.01, 6, 5),
+                          ("mixed", 1, 0.05, 6, 3)])
+def test_partition_resort_equals_radix_sort(fss, precision, use_graph, dt, level, tree_levels):
+    """The per-step re-sort by partition of the old order (the default) and
+    the radix key sort both give the stable order of the new leaf keys: the
+    states, the leaf membership and the leaf counts agree to the bit.  The
+    second step's re-sort moves the particles that crossed leaves in the
+    first; with 128 particles per leaf at dt = 0.05 about a quarter of them
+    change leaves and some leaf receives more than a warp's 32 movers (69
+    in the oracle's step)."""
+    s, a = fss.make_state(level, "rh_vortices", n_vortex=16, seed=21)
+    prec = fss.PREC_MIXED if precision == "mixed" else fss.PREC_FP64
+    outs = []
+    for mode in (0, 1):
+        with fss.Context(method=fss.METHOD_TREECODE, precision=prec, tree_levels=tree_levels, use_graph=use_graph,
+                         rebuild=fss.REBUILD_RESORT) as ctx:
+            ctx.test_resort_mode(mode)
+            ctx.set_particles(s, a)
+            loc0 = ctx.get_tree()[0][-1]
+            ctx.rk4_step(dt, nsteps=2)
+            loc, counts, _ = ctx.get_tree()
+            outs.append((ctx.get_state(), loc, counts))
+    moved = loc[-1] != loc0
+    assert moved.any()
+    if tree_levels == 3:
+        assert np.bincount(loc[-1][moved]).max() > 32
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(outs[0][2], outs[1][2])
+
+
+def test_resort_mode_rejects_unknown(fss):
+    with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as ctx:
+        with pytest.raises(fss.FssError):
+            ctx.test_resort_mode(2)
