@@ -484,7 +484,7 @@ def kernel_rooflines(prof, steps, n, up_bytes, peaks):
     if up_ms > 0:
         add("upward pass (k_up_leaf, k_up_sums, k_up_proxies)", up_ms, float(up_bytes), "RHS")
     if "resort" in prof:
-        add("tree build: per-step re-sort (k_part_check, k_part_descend, k_part_bucket, k_part_place, "
+        add("tree build: per-step re-sort (k_part_keys, k_part_scan, k_part_bucket, k_part_place, "
             "k_resort_commit)", prof["resort"][0] / steps, float(n) * (24 + 8 + 16), "step")
     if "epilogue" in prof:
         add("RK4 combine (k_epilogue, 4 per step)", prof["epilogue"][0] / steps,

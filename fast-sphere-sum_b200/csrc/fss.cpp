@@ -819,16 +819,14 @@ int autotune(fss_ctx* c, bool depth) {
 int resort(fss_ctx* c) {
     const int64_t n = c->n;
     if (c->resort_mode == 0) {
-        // check, descent + scan, bucket, place, commit
+        // keys, scan, bucket, place, commit
         ProfScope ps(c, "resort", 5);
-        const NodeGeom* node = c->node.as<NodeGeom>();
-        launch_resort_partition(c->stream, c->fp64, n, c->nleaf, c->leaf_level, node,
-                                node + c->geom.lev_off[c->leaf_level], c->lev_off.as<int64_t>(),
-                                c->key.as<uint32_t>(), c->key_tmp.as<uint32_t>(), c->leaf_start.as<int32_t>(),
-                                c->sortq.as<int32_t>(), c->vals_tmp.as<int32_t>(), c->part_scratch.as<uint32_t>(),
-                                c->s0.as<double4>(), c->area_s.as<double>(), c->tracer_s.as<double>(),
-                                c->perm.as<int32_t>(), c->xs.as<double4>(), c->acc.as<double4>(), c->src.p,
-                                c->err_flag.as<int>());
+        launch_resort_partition(c->stream, c->fp64, n, c->nleaf, c->leaf_level, c->node.as<NodeGeom>(),
+                                c->lev_off.as<int64_t>(), c->key.as<uint32_t>(), c->key_tmp.as<uint32_t>(),
+                                c->leaf_start.as<int32_t>(), c->vals_tmp.as<int32_t>(),
+                                c->part_scratch.as<uint32_t>(), c->s0.as<double4>(), c->area_s.as<double>(),
+                                c->tracer_s.as<double>(), c->perm.as<int32_t>(), c->xs.as<double4>(),
+                                c->acc.as<double4>(), c->src.p, c->err_flag.as<int>());
         CU(cudaGetLastError());
         return FSS_OK;
     }

@@ -293,11 +293,11 @@ __device__ __forceinline__ double min_cone(const NodeGeom& g, double x, double y
 }
 
 // Leaf index on level LL reached from the 20 root faces: on each level the
-// first child that contains the point, else the most-inside one.
+// first child that contains the point, else the most-inside one.  With l0 >
+// 0 the walk starts below face `prev` of level l0 - 1.
 __device__ __forceinline__ int descend(const NodeGeom* __restrict__ node, const int64_t* __restrict__ lev_off, int LL,
-                                       double4 q) {
-    int prev = 0;
-    for (int l = 0; l <= LL; l++) {
+                                       double4 q, int l0 = 0, int prev = 0) {
+    for (int l = l0; l <= LL; l++) {
         const int lb = (l > 0) ? 4 * prev : 0, ub = (l > 0) ? lb + 4 : 20;
         int best = lb;
         double best_min = -1e300;
@@ -385,59 +385,96 @@ __global__ void k_resort_commit(int64_t n, const double4* __restrict__ xs, const
 // old position.  The result is the unique stable order, the same as the
 // radix sort's.
 //
-// Scratch words: [0] blocks done (descent), [1] movers listed, then in[m],
-// out[m], fill[m] (zeroed before every re-sort), ns[m + 1] (new leaf
-// starts), mo[m + 1] (bucket starts), m = leaf count.
+// Scratch words: in[m], out[m], fill[m] (zeroed before every re-sort),
+// ns[m + 1] (new leaf starts), mo[m + 1] (bucket starts), m = leaf count.
 constexpr int kPartThreads = 256;
+// Cone-coordinate margin of the descent's shortcut.  Cone coordinates of a
+// point inside a face are O(1) at every level; their FP64 rounding error is
+// a few ulp times the row sums of M^-1, which grow like 1 / face size (at
+// most 243 on level 7), so about 1e-13: far below the margin.  A face of a
+// coarser level is at most 2^7 times larger, so a point that far inside
+// one face is still clearly outside every other face of the levels above.
+constexpr double kInsideMargin = 1e-6;
+constexpr uint32_t kNoLeaf = 0xffffffffu;
 
-// Fast path for every particle: still inside its old leaf (kept), else
-// listed as a mover.  key_new[i] = old key for now.
-__global__ void __launch_bounds__(kPartThreads) k_part_check(int64_t n, const double4* __restrict__ pos,
-                                                             const NodeGeom* __restrict__ leaf_node,
-                                                             const uint32_t* __restrict__ key,
-                                                             uint32_t* __restrict__ key_new,
-                                                             int32_t* __restrict__ movers, uint32_t* __restrict__ ctl,
-                                                             int* __restrict__ err) {
+// Lanes of a warp that add 1 to the same counter add their count once
+// (movers of a warp mostly share their old and their new leaf).  idx =
+// kNoLeaf adds nothing.  All 32 lanes call it.
+__device__ __forceinline__ void warp_count_add(uint32_t* __restrict__ cnt, uint32_t idx) {
+    const unsigned peers = __match_any_sync(0xffffffffu, idx);
+    if (idx != kNoLeaf && int(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&cnt[idx], uint32_t(__popc(peers)));
+}
+
+// Every particle's new leaf: the old one while the particle is still
+// inside it, else the descent's; the counts into and out of every leaf.
+__global__ void __launch_bounds__(kPartThreads) k_part_keys(int64_t n, const double4* __restrict__ pos,
+                                                            const NodeGeom* __restrict__ node,
+                                                            const int64_t* __restrict__ lev_off, int leaf_level,
+                                                            const uint32_t* __restrict__ key,
+                                                            uint32_t* __restrict__ key_new,
+                                                            uint32_t* __restrict__ scratch, int64_t m,
+                                                            int* __restrict__ err) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    bool mover = false;
+    uint32_t from = kNoLeaf, to = kNoLeaf;
     if (i < n) {
         const double4 q = pos[i];
         const uint32_t g = key[i];
-        key_new[i] = g;
+        uint32_t g2 = g;
         // a non-finite position keeps its leaf (see k_reassign)
-        if (!isfinite(q.x) || !isfinite(q.y) || !isfinite(q.z))
+        if (!isfinite(q.x) || !isfinite(q.y) || !isfinite(q.z)) {
             set_error(err, kErrNonFinite);
-        else
-            mover = min_cone(leaf_node[g], q.x, q.y, q.z) < 0.0;
+        } else if (min_cone(node[lev_off[leaf_level] + g], q.x, q.y, q.z) < 0.0) {
+            // The lowest ancestor of the old leaf that holds the particle
+            // with a margin: every other face of its level and of the levels
+            // above lies at least that far away, so each of them fails its
+            // test and the descent from the root passes through this
+            // ancestor.  Start below it (the root's walk when none qualifies).
+            int l = leaf_level - 1;
+            uint32_t f = g >> 2;
+            for (; l >= 0; l--, f >>= 2)
+                if (min_cone(node[lev_off[l] + f], q.x, q.y, q.z) > kInsideMargin) break;
+            g2 = uint32_t(l >= 0 ? descend(node, lev_off, leaf_level, q, l + 1, int(f))
+                                 : descend(node, lev_off, leaf_level, q));
+        }
+        key_new[i] = g2;
+        if (g2 != g) {
+            from = g;
+            to = g2;
+        }
     }
-    const unsigned m = __ballot_sync(0xffffffffu, mover);
-    if (m == 0u) return;
-    const int lane = threadIdx.x & 31;
-    uint32_t base = 0;
-    if (lane == __ffs(m) - 1) base = atomicAdd(&ctl[1], uint32_t(__popc(m)));
-    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-    if (mover) movers[base + __popc(m & ((1u << lane) - 1u))] = int32_t(i);
+    warp_count_add(scratch, to);        // in
+    warp_count_add(scratch + m, from);  // out
 }
 
-// One block: ns = exclusive scan of the new leaf counts (old count - out +
-// in), mo = exclusive scan of in; entry m holds the totals.
+// One block of 1024 threads: ns = exclusive scan of the new leaf counts
+// (old count - out + in), mo = exclusive scan of in; entry m holds the
+// totals.  Chunks of 4096 entries pass through shared memory, so that the
+// global loads and stores are coalesced.
 __device__ void part_scan(int64_t m, const int32_t* __restrict__ ls, const uint32_t* __restrict__ in,
                           const uint32_t* __restrict__ out, uint32_t* __restrict__ ns, uint32_t* __restrict__ mo) {
-    constexpr int R = 8;
-    __shared__ uint32_t wa[kPartThreads / 32], wb[kPartThreads / 32];
+    constexpr int R = 4, T = 1024, C = R * T;
+    __shared__ uint32_t ba[C], bb[C];
+    __shared__ uint32_t wa[T / 32], wb[T / 32];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     uint32_t ca = 0, cb = 0;  // carries (block-uniform)
-    for (int64_t base = 0; base < m; base += int64_t(kPartThreads) * R) {
-        uint32_t va[R], vb[R], sa = 0, sb = 0;
+    for (int64_t base = 0; base < m; base += C) {
 #pragma unroll
         for (int r = 0; r < R; r++) {
-            const int64_t k = base + int64_t(t) * R + r;
-            va[r] = vb[r] = 0;
+            const int64_t k = base + int64_t(r) * T + t;
+            uint32_t va = 0, vb = 0;
             if (k < m) {
-                const uint32_t a_in = __ldcg(in + k), a_out = __ldcg(out + k);
-                va[r] = uint32_t(ls[k + 1] - ls[k]) - a_out + a_in;
-                vb[r] = a_in;
+                vb = in[k];
+                va = uint32_t(ls[k + 1] - ls[k]) - out[k] + vb;
             }
+            ba[r * T + t] = va;
+            bb[r * T + t] = vb;
+        }
+        __syncthreads();
+        uint32_t va[R], vb[R], sa = 0, sb = 0;  // thread t: entries [R t, R t + R) of the chunk
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            va[r] = ba[t * R + r];
+            vb[r] = bb[t * R + r];
             sa += va[r];
             sb += vb[r];
         }
@@ -449,7 +486,7 @@ __device__ void part_scan(int64_t m, const int32_t* __restrict__ ls, const uint3
         if (lane == 31) { wa[w] = xa; wb[w] = xb; }
         __syncthreads();
         uint32_t oa = ca, ob = cb, ta = 0, tb = 0;
-        for (int v = 0; v < kPartThreads / 32; v++) {
+        for (int v = 0; v < T / 32; v++) {
             if (v < w) { oa += wa[v]; ob += wb[v]; }
             ta += wa[v];
             tb += wb[v];
@@ -458,87 +495,75 @@ __device__ void part_scan(int64_t m, const int32_t* __restrict__ ls, const uint3
         ob += xb - sb;
 #pragma unroll
         for (int r = 0; r < R; r++) {
-            const int64_t k = base + int64_t(t) * R + r;
-            if (k < m) { ns[k] = oa; mo[k] = ob; }
+            ba[t * R + r] = oa;
+            bb[t * R + r] = ob;
             oa += va[r];
             ob += vb[r];
         }
         ca += ta;
         cb += tb;
         __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int64_t k = base + int64_t(r) * T + t;
+            if (k < m) {
+                ns[k] = ba[r * T + t];
+                mo[k] = bb[r * T + t];
+            }
+        }
+        __syncthreads();
     }
     if (t == 0) { ns[m] = ca; mo[m] = cb; }
 }
 
-// The movers' new leaves (descent from the root faces), their counts into
-// and out of every leaf; the last block to finish scans the counts.
-__global__ void __launch_bounds__(kPartThreads) k_part_descend(const double4* __restrict__ pos,
-                                                               const NodeGeom* __restrict__ node,
-                                                               const int64_t* __restrict__ lev_off, int leaf_level,
-                                                               const uint32_t* __restrict__ key,
-                                                               uint32_t* __restrict__ key_new,
-                                                               const int32_t* __restrict__ movers,
-                                                               uint32_t* __restrict__ scratch, int64_t m,
-                                                               const int32_t* __restrict__ ls) {
-    uint32_t* ctl = scratch;
-    uint32_t* in = scratch + 2;
-    uint32_t* out = in + m;
-    const uint32_t nmov = ctl[1];
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < nmov; j += stride) {
-        const int32_t i = movers[j];
-        const uint32_t g = key[i];
-        const uint32_t g2 = uint32_t(descend(node, lev_off, leaf_level, pos[i]));
-        key_new[i] = g2;
-        if (g2 != g) {
-            atomicAdd(&in[g2], 1u);
-            atomicAdd(&out[g], 1u);
-        }
-    }
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(&ctl[0], 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    uint32_t* ns = out + 2 * m;  // after fill
-    part_scan(m, ls, in, out, ns, ns + m + 1);
+// The scan of the counts, by one block of kScanThreads.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) k_part_scan(uint32_t* __restrict__ scratch, int64_t m,
+                                                           const int32_t* __restrict__ ls) {
+    uint32_t* ns = scratch + 3 * m;
+    part_scan(m, ls, scratch, scratch + m, ns, ns + m + 1);
 }
 
 // Movers into their new leaf's bucket (unordered within it).
-__global__ void __launch_bounds__(kPartThreads) k_part_bucket(const uint32_t* __restrict__ key,
+__global__ void __launch_bounds__(kPartThreads) k_part_bucket(int64_t n, const uint32_t* __restrict__ key,
                                                               const uint32_t* __restrict__ key_new,
-                                                              const int32_t* __restrict__ movers,
                                                               uint32_t* __restrict__ scratch, int64_t m,
                                                               int32_t* __restrict__ bucket) {
-    const uint32_t nmov = scratch[1];
-    uint32_t* fill = scratch + 2 + 2 * m;
-    const uint32_t* mo = fill + m + (m + 1);
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < nmov; j += stride) {
-        const int32_t i = movers[j];
+    uint32_t* fill = scratch + 2 * m;
+    const uint32_t* mo = scratch + 3 * m + (m + 1);
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    uint32_t to = kNoLeaf;
+    if (i < n) {
         const uint32_t g2 = key_new[i];
-        if (g2 == key[i]) continue;
-        bucket[mo[g2] + atomicAdd(&fill[g2], 1u)] = i;
+        if (g2 != key[i]) to = g2;
     }
+    // lanes bound for the same leaf reserve their slots with one atomic
+    const unsigned peers = __match_any_sync(0xffffffffu, to);
+    const int leader = __ffs(peers) - 1;
+    uint32_t slot = 0;
+    if (to != kNoLeaf && lane == leader) slot = atomicAdd(&fill[to], uint32_t(__popc(peers)));
+    slot = __shfl_sync(0xffffffffu, slot, leader);
+    if (to != kNoLeaf) bucket[mo[to] + slot + uint32_t(__popc(peers & ((1u << lane) - 1u)))] = int32_t(i);
 }
 
-// One warp per new leaf k: its movers ranked by old position, its stayers
+// One block per new leaf k: its movers ranked by old position, its stayers
 // in old order, each particle's state gathered into its new place (xs, and
 // acc as {area, tracer, caller index, 0}), the new sorted keys written.
-constexpr int kPlaceWarps = 4;
-__global__ void __launch_bounds__(kPlaceWarps * 32) k_part_place(
+constexpr int kPlaceThreads = 128;
+constexpr int kPlaceStage = 512;  // movers into one leaf ranked from shared memory
+__global__ void __launch_bounds__(kPlaceThreads) k_part_place(
     int64_t m, const int32_t* __restrict__ ls, const uint32_t* __restrict__ key_new,
     const uint32_t* __restrict__ scratch, const int32_t* __restrict__ bucket, const double4* __restrict__ s0,
     const double* __restrict__ area, const double* __restrict__ tracer, const int32_t* __restrict__ perm,
     double4* __restrict__ xs, double4* __restrict__ acc, uint32_t* __restrict__ key) {
-    const int64_t k = int64_t(blockIdx.x) * kPlaceWarps + (threadIdx.x >> 5);
-    if (k >= m) return;
-    const int lane = threadIdx.x & 31;
-    const uint32_t* in = scratch + 2;
-    const uint32_t* out = in + m;
-    const uint32_t* ns = out + 2 * m;
+    constexpr int W = kPlaceThreads / 32;
+    __shared__ uint32_t wcnt[W];
+    const int64_t k = blockIdx.x;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const uint32_t* in = scratch;
+    const uint32_t* out = scratch + m;
+    const uint32_t* ns = scratch + 3 * m;
     const uint32_t* mo = ns + m + 1;
     const int32_t a = ls[k], b = ls[k + 1];
     const uint32_t base = ns[k], c = in[k], m0 = mo[k];
@@ -548,26 +573,46 @@ __global__ void __launch_bounds__(kPlaceWarps * 32) k_part_place(
         acc[dst] = make_double4(area[p], tracer[p], double(perm[p]), 0.0);
     };
     // movers: rank = number of movers into k with a smaller old position
+    // (the bucket staged in shared memory when it fits)
+    __shared__ int32_t bk[kPlaceStage];
+    const bool staged = c <= uint32_t(kPlaceStage);
+    if (staged)
+        for (uint32_t u = t; u < c; u += kPlaceThreads) bk[u] = bucket[m0 + u];
     uint32_t below = 0;
-    for (uint32_t t = lane; t < c; t += 32) below += bucket[m0 + t] < a ? 1u : 0u;
-    for (int d = 16; d > 0; d >>= 1) below += __shfl_xor_sync(0xffffffffu, below, d);
-    for (uint32_t t = lane; t < c; t += 32) {
-        const int32_t p = bucket[m0 + t];
+    for (uint32_t u0 = 0; u0 < c; u0 += kPlaceThreads) {
+        const uint32_t u = u0 + t;
+        below += uint32_t(__syncthreads_count(u < c && (staged ? bk[u] : bucket[m0 + u]) < a));
+    }
+    for (uint32_t j = t; j < c; j += kPlaceThreads) {
+        const int32_t p = staged ? bk[j] : bucket[m0 + j];
         uint32_t r = 0;
-        for (uint32_t u = 0; u < c; u++) r += bucket[m0 + u] < p ? 1u : 0u;
+        if (staged)
+            for (uint32_t u = 0; u < c; u++) r += bk[u] < p ? 1u : 0u;
+        else
+            for (uint32_t u = 0; u < c; u++) r += bucket[m0 + u] < p ? 1u : 0u;
         place(p, int64_t(base) + r + (p >= a ? stays : 0u));
     }
     // stayers, in old order after the movers from below
     uint32_t run = base + below;
-    for (int32_t p0 = a; p0 < b; p0 += 32) {
-        const int32_t p = p0 + lane;
+    for (int32_t p0 = a; p0 < b; p0 += kPlaceThreads) {
+        const int32_t p = p0 + t;
         const bool st = p < b && key_new[p] == uint32_t(k);
         const unsigned bal = __ballot_sync(0xffffffffu, st);
-        if (st) place(p, int64_t(run) + __popc(bal & ((1u << lane) - 1u)));
-        run += __popc(bal);
+        if (lane == 0) wcnt[w] = uint32_t(__popc(bal));
+        __syncthreads();
+        uint32_t off = 0, tot = 0;
+#pragma unroll
+        for (int v = 0; v < W; v++) {
+            const uint32_t x = wcnt[v];
+            if (v < w) off += x;
+            tot += x;
+        }
+        if (st) place(p, int64_t(run) + off + uint32_t(__popc(bal & ((1u << lane) - 1u))));
+        run += tot;
+        __syncthreads();
     }
     const uint32_t cnt = stays + c;
-    for (uint32_t j = lane; j < cnt; j += 32) key[base + j] = uint32_t(k);
+    for (uint32_t j = t; j < cnt; j += kPlaceThreads) key[base + j] = uint32_t(k);
 }
 
 // ---------------------------------------------------------------- launchers
@@ -668,28 +713,21 @@ void launch_resort(cudaStream_t st, bool fp64, int64_t n, const int32_t* q, doub
                                                   nullptr, nullptr, 0);
 }
 
-int64_t partition_scratch_words(int64_t nleaf) { return 2 + 3 * nleaf + 2 * (nleaf + 1); }
+int64_t partition_scratch_words(int64_t nleaf) { return 3 * nleaf + 2 * (nleaf + 1); }
 
 void launch_resort_partition(cudaStream_t st, bool fp64, int64_t n, int64_t nleaf, int leaf_level,
-                             const NodeGeom* node, const NodeGeom* leaf_node, const int64_t* lev_off, uint32_t* key,
-                             uint32_t* key_new, int32_t* leaf_start, int32_t* movers, int32_t* bucket,
-                             uint32_t* scratch, double4* s0, double* area, double* tracer, int32_t* perm,
-                             double4* xs, double4* acc, void* src, int* err) {
+                             const NodeGeom* node, const int64_t* lev_off, uint32_t* key, uint32_t* key_new,
+                             int32_t* leaf_start, int32_t* bucket, uint32_t* scratch, double4* s0, double* area,
+                             double* tracer, int32_t* perm, double4* xs, double4* acc, void* src, int* err) {
     if (n == 0) return;
-    cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * size_t(2 + 3 * nleaf), st);
-    k_part_check<<<unsigned((n + kPartThreads - 1) / kPartThreads), kPartThreads, 0, st>>>(
-        n, s0, leaf_node, key, key_new, movers, scratch, err);
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-    const unsigned grid = unsigned(std::min<int64_t>(int64_t(sms) * 4, (n + kPartThreads - 1) / kPartThreads));
-    k_part_descend<<<grid, kPartThreads, 0, st>>>(s0, node, lev_off, leaf_level, key, key_new, movers, scratch, nleaf,
-                                                  leaf_start);
-    k_part_bucket<<<grid, kPartThreads, 0, st>>>(key, key_new, movers, scratch, nleaf, bucket);
-    k_part_place<<<unsigned((nleaf + kPlaceWarps - 1) / kPlaceWarps), kPlaceWarps * 32, 0, st>>>(
+    cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * size_t(3 * nleaf), st);
+    const unsigned grid = unsigned((n + kPartThreads - 1) / kPartThreads);
+    k_part_keys<<<grid, kPartThreads, 0, st>>>(n, s0, node, lev_off, leaf_level, key, key_new, scratch, nleaf, err);
+    k_part_scan<<<1, kScanThreads, 0, st>>>(scratch, nleaf, leaf_start);
+    k_part_bucket<<<grid, kPartThreads, 0, st>>>(n, key, key_new, scratch, nleaf, bucket);
+    k_part_place<<<unsigned(nleaf), kPlaceThreads, 0, st>>>(
         nleaf, leaf_start, key_new, scratch, bucket, s0, area, tracer, perm, xs, acc, key);
-    const uint32_t* ns = scratch + 2 + 3 * nleaf;
+    const uint32_t* ns = scratch + 3 * nleaf;
     const unsigned g = unsigned((std::max(n, nleaf + 1) + 255) / 256);
     if (fp64)
         k_resort_commit<double><<<g, 256, 0, st>>>(n, xs, acc, s0, area, tracer, perm, static_cast<double4*>(src),

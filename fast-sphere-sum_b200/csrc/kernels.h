@@ -68,15 +68,14 @@ void launch_resort(cudaStream_t st, bool fp64, int64_t n, const int32_t* q, doub
                    double* tracer, int32_t* perm, double4* xs, double4* acc, void* src);
 // The same re-sort without a key sort: the old order partitioned into the
 // new leaves (stayers in place order, movers bucketed and ranked by old
-// position), which is the stable sort's order.  key_new, movers and bucket
-// take n words each; scratch partition_scratch_words(nleaf); leaf_node =
-// node + the leaf level's offset.  key and leaf_start are updated.
+// position), which is the stable sort's order.  key_new and bucket take n
+// words each, scratch partition_scratch_words(nleaf).  key and leaf_start
+// are updated.
 int64_t partition_scratch_words(int64_t nleaf);
 void launch_resort_partition(cudaStream_t st, bool fp64, int64_t n, int64_t nleaf, int leaf_level,
-                             const NodeGeom* node, const NodeGeom* leaf_node, const int64_t* lev_off, uint32_t* key,
-                             uint32_t* key_new, int32_t* leaf_start, int32_t* movers, int32_t* bucket,
-                             uint32_t* scratch, double4* s0, double* area, double* tracer, int32_t* perm,
-                             double4* xs, double4* acc, void* src, int* err);
+                             const NodeGeom* node, const int64_t* lev_off, uint32_t* key, uint32_t* key_new,
+                             int32_t* leaf_start, int32_t* bucket, uint32_t* scratch, double4* s0, double* area,
+                             double* tracer, int32_t* perm, double4* xs, double4* acc, void* src, int* err);
 void launch_gather(cudaStream_t st, bool fp64, int64_t n, const double* in5, const double* area_in, const int32_t* perm,
                    const uint32_t* leaf_of, const double4* frame, double4* s0, double4* xs, double* area_s,
                    double* tracer_s, void* src);
