@@ -350,14 +350,25 @@ __global__ void __launch_bounds__(kBatchThreads) k_down_coef(const TaskBlock* __
                                                              int hold_block) {
     extern __shared__ __align__(32) double bsm[];
     __shared__ __align__(8) uint64_t bar;
+    __shared__ int32_t slot_of[kBatchTasks];
+    __shared__ int64_t coef_of[kBatchTasks];
     const TaskBlock tb = blocks[blockIdx.x];
     const int d = tb.deg, K = nproxy(d), Kp = batch_pad(K), nt = tb.count;
     double* A = bsm;
     double4* Y = reinterpret_cast<double4*>(bsm + K * Kp);  // K * Kp is a multiple of 4
     stage_issue(A, vtpad + vpad_off[d], uint32_t(sizeof(double)) * K * Kp, &bar, int(blockIdx.x) == hold_block);
+    // the block's jobs looked up once (their point slots and coefficient rows)
+    if (threadIdx.x < nt) {
+        const DownJob jb = jobs[tasks[tb.first + threadIdx.x]];
+        slot_of[threadIdx.x] = jb.slot;
+        coef_of[threadIdx.x] = jb.coef;
+    }
+    __syncthreads();
+    // unrolled: the partial-slot loads of several points in flight at once
+#pragma unroll 4
     for (int i = threadIdx.x; i < nt * K; i += kBatchThreads) {
         const int t = i / K, k = i - t * K;
-        const int32_t slot = jobs[tasks[tb.first + t]].slot;
+        const int32_t slot = slot_of[t];
         double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
         for (int q = 0; q < parts; q++) {
             const double4 y = partials[int64_t(q) * pstride + slot + k];
@@ -397,7 +408,7 @@ __global__ void __launch_bounds__(kBatchThreads) k_down_coef(const TaskBlock* __
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         if (t0 + j >= nt) break;
-        double4* out = coef + jobs[tasks[tb.first + t0 + j]].coef;
+        double4* out = coef + coef_of[t0 + j];
         if (m0 < K) out[m0] = c[j][0];
         if (m0 + 1 < K) out[m0 + 1] = c[j][1];
     }

@@ -102,3 +102,28 @@ def test_resort_mode_rejects_unknown(fss):
     with fss.Context(method=fss.METHOD_TREECODE, precision=fss.PREC_MIXED) as ctx:
         with pytest.raises(fss.FssError):
             ctx.test_resort_mode(2)
+
+
+@pytest.mark.parametrize("level,tree_levels,precision", [(4, 1, "mixed"), (4, 2, "fp64"), (3, 5, "mixed")])
+def test_partition_resort_edge_trees(fss, level, tree_levels, precision):
+    """The partition re-sort against the radix sort on the trees at its
+    edges: leaves on level 0 (the root faces: every mover descends from the
+    root, no ancestor to start below), leaves on level 1, and more leaves
+    (5,120) than particles (642), so that most leaves are empty and stay or
+    become empty between steps."""
+    s, a = fss.make_state(level, "rh_vortices", n_vortex=8, seed=5)
+    prec = fss.PREC_MIXED if precision == "mixed" else fss.PREC_FP64
+    outs = []
+    for mode in (0, 1):
+        with fss.Context(method=fss.METHOD_TREECODE, precision=prec, tree_levels=tree_levels,
+                         rebuild=fss.REBUILD_RESORT) as ctx:
+            ctx.test_resort_mode(mode)
+            ctx.set_particles(s, a)
+            loc0 = ctx.get_tree()[0][-1]
+            ctx.rk4_step(0.05, nsteps=3)
+            loc, counts, _ = ctx.get_tree()
+            outs.append((ctx.get_state(), loc, counts))
+    assert np.any(loc[-1] != loc0)
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(outs[0][2], outs[1][2])
