@@ -616,7 +616,7 @@ int eval_partials(fss_ctx* c, bool want_psi, bool* down_out) {
                            c->leaf_level, c->nmax, c->level_mask, c->up_deg.as<int8_t>(), c->part_up.as<double>());
         }
         {
-            ProfScope ps(c, "upward_combine");
+            ProfScope ps(c, "upward_combine", 2);  // k_up_sums, k_up_proxies
             launch_up_proxies(c->stream, c->fp64, int(c->lists.jobs.size()), c->jobs.as<ProxyJob>(),
                               c->part_up.as<double>(), c->leaf_level, c->nmax, c->msum.as<double>(),
                               c->n_up_blocks, c->up_tblocks.as<TaskBlock>(), c->up_tasks.as<int32_t>(),
