@@ -23,9 +23,11 @@ namespace fss {
 // outside level_mask: no work), up to the degree up_deg[face] its proxies
 // need (none when -1; nmax everywhere without up_deg).  Rows as described
 // at up_row_step; slots keep the stride nproxy(nmax), and moments above a
-// face's degree are neither written nor read.
+// face's degree are neither written nor read.  Five blocks per SM: the
+// per-lane moment sums of degrees 8-11 need 96 registers (80, for six
+// blocks, spilled 320 bytes; 118, for four, ran 0.7% slower in the step).
 template <typename T>
-__global__ void __launch_bounds__(kUpThreads, 6) k_up_leaf(const typename Vec4<T>::type* __restrict__ src,
+__global__ void __launch_bounds__(kUpThreads, 5) k_up_leaf(const typename Vec4<T>::type* __restrict__ src,
                                                         const int32_t* __restrict__ leaf_start,
                                                         const double4* __restrict__ frame,
                                                         const NodeGeom* __restrict__ node,

@@ -14,32 +14,38 @@ constexpr int kUpLd = 32 + 4;            // padded row: the 8 rows x 4 doubles a
 // ancestor face (FP64), by one warp, up to degree NM.  Per chunk of 32
 // particles each lane writes its particle's basis W[a][j] = w T_a(u),
 // V[b][j] = T_b(v), a, b <= NM, into the warp's own shared rows; then the
-// moments M_ab (a + b <= NM) as 8 x 8 tiles of W V^T on the FP64 tensor
-// cores, over the chunk's groups of four particles.  Tile 0 is a, b < 8.
-// The rest (a >= 8 or b >= 8, so the other index <= NM - 8) is one tile
-// with rows a = 8..NM, 0..NM-8 and columns b = 0..NM-8, 8..NM when NM <= 11,
-// else the two tiles a >= 8, b < 8 and a < 8, b >= 8 (none for NM < 8).
-// Rows above NM are neither formed nor stored: a tile row or column index
-// above NM is clamped to NM (a row of this chunk), and it only reaches
-// outputs with a + b > NM, which are dropped.  Lane (4 g + t) holds D[g][2t + {0, 1}] of each tile;
-// every moment is written once, to out[m], m = (a + b)(a + b + 1) / 2 + b.
-// The groups of four particles are taken in particle order, so a moment's
-// sum does not depend on which tile forms it, on NM or on the chunking.
+// moments M_ab (a + b <= NM) with a, b < 8 as one 8 x 8 tile of W V^T on the
+// FP64 tensor cores, over the chunk's groups of four particles.  The rest
+// (a >= 8 or b >= 8, so the other index <= NM - 8): for NM <= 11 at most 20
+// moments, each a per-lane FP64 sum of the lane's own particles, added over
+// the warp by shuffles at the end (a second tile would be mostly unused,
+// and on B200 an FP64 tensor tile costs the FP64 pipe as much as its 256
+// FMA); for NM = 12 the two tiles a >= 8, b < 8 and a < 8, b >= 8.  A tile
+// row or column index above NM is clamped to NM (a row of this chunk), and
+// it only reaches outputs with a + b > NM, which are dropped.  Lane (4 g +
+// t) holds D[g][2t + {0, 1}] of each tile; every moment is written once, to
+// out[m], m = (a + b)(a + b + 1) / 2 + b.
 template <typename T, int NM>
 __device__ __forceinline__ void leaf_moments_n(const typename Vec4<T>::type* __restrict__ src, int a0, int a1,
                                                double fx, double fy, double fz, const NodeGeom& ng,
                                                double (*W)[kUpLd], double (*V)[kUpLd], double* __restrict__ out) {
     static_assert(NM >= 0 && NM < kUpRows, "degree beyond the basis rows");
-    constexpr int NT = NM < 8 ? 1 : (NM <= 11 ? 2 : 3);  // tiles
-    constexpr int H = NM - 7;                            // rows 8..NM when NT == 2
+    constexpr int NT = NM < 8 ? 1 : (NM <= 11 ? 2 : 3);  // tiles (NT == 2: one tile and lane sums)
+    // NM 8..11: the moments with a or b >= 8 (the other index <= NM - 8 <= 3),
+    // XE of them, are per-lane FP64 sums of this lane's particles, added
+    // across the warp at the end, instead of a second 8x8x4 tile per four
+    // particles that would be mostly unused.  Entry order: for r = 8..NM and
+    // s = 0..NM - r, (a, b) = (r, s) then (s, r).
+    constexpr int H = NM - 7;
+    constexpr int XE = NT == 2 ? H * (H + 1) : 0;
+    constexpr int XL = NT == 2 ? H : 1;  // low rows kept in registers (s <= NM - 8)
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    // tile 1: this lane's row of W and column of V
-    const int ra1u = NT == 2 ? (g < H ? 8 + g : g - H) : 8 + g;  // the row this lane's outputs belong to
-    const int ra1 = min(ra1u, NM);
-    const int cb1 = min(NT == 2 ? (g < H ? g : 8 + (g - H)) : g, NM);
     const int g0 = min(g, NM);      // tile 0's row and column (a, b < 8)
-    const int c2 = min(8 + g, NM);  // tile 2's column (b >= 8)
+    const int r1 = min(8 + g, NM);  // NT == 3: tile 1's row (a >= 8), tile 2's column (b >= 8)
     double d00 = 0.0, d01 = 0.0, e00 = 0.0, e01 = 0.0, f00 = 0.0, f01 = 0.0;
+    double xs[XE > 0 ? XE : 1];
+#pragma unroll
+    for (int e = 0; e < (XE > 0 ? XE : 1); e++) xs[e] = 0.0;
     for (int c0 = a0; c0 < a1; c0 += 32) {
         const int j = c0 + lane;
         double u = 0.0, v = 0.0, w = 0.0;
@@ -55,21 +61,41 @@ __device__ __forceinline__ void leaf_moments_n(const typename Vec4<T>::type* __r
             v = 2.0 * (e1 * inv) - 1.0;
         }
         double ta0 = 1.0, ta1 = u, tb0 = 1.0, tb1 = v;
+        double wlo[XL], vlo[XL];  // w T_s(u), T_s(v) for s < XL
 #pragma unroll
         for (int r = 0; r <= NM; r++) {
             const double tu = (r == 0) ? 1.0 : (r == 1 ? u : 2.0 * u * ta1 - ta0);
             const double tv = (r == 0) ? 1.0 : (r == 1 ? v : 2.0 * v * tb1 - tb0);
             if (r >= 2) { ta0 = ta1; ta1 = tu; tb0 = tb1; tb1 = tv; }
-            W[r][lane] = w * tu;
-            V[r][lane] = tv;
+            const double wt = w * tu;
+            if (r < 8 || NT == 3) {
+                W[r][lane] = wt;
+                V[r][lane] = tv;
+            }
+            if constexpr (NT == 2) {
+                if (r < XL) {
+                    wlo[r] = wt;
+                    vlo[r] = tv;
+                }
+                if (r >= 8) {
+                    const int e0 = (r - 8) * (2 * H - (r - 8) + 1);  // entries before row r
+#pragma unroll
+                    for (int s2 = 0; s2 <= NM - r; s2++) {
+                        xs[e0 + 2 * s2] = fma(wt, vlo[s2], xs[e0 + 2 * s2]);
+                        xs[e0 + 2 * s2 + 1] = fma(wlo[s2], tv, xs[e0 + 2 * s2 + 1]);
+                    }
+                }
+            }
         }
         __syncwarp();
         const int nk = (min(32, a1 - c0) + 3) >> 2;
         for (int k = 0; k < nk; k++) {
             const int p = 4 * k + t;
             dmma_8x8x4(d00, d01, W[g0][p], V[g0][p]);
-            if constexpr (NT >= 2) dmma_8x8x4(e00, e01, W[ra1][p], V[cb1][p]);
-            if constexpr (NT == 3) dmma_8x8x4(f00, f01, W[g0][p], V[c2][p]);  // a < 8, b >= 8
+            if constexpr (NT == 3) {
+                dmma_8x8x4(e00, e01, W[r1][p], V[g0][p]);  // a >= 8, b < 8
+                dmma_8x8x4(f00, f01, W[g0][p], V[r1][p]);  // a < 8, b >= 8
+            }
         }
         __syncwarp();
     }
@@ -78,15 +104,29 @@ __device__ __forceinline__ void leaf_moments_n(const typename Vec4<T>::type* __r
         const int c = 2 * t + i;
         int a = g, b = c;  // tile 0
         if (a + b <= NM) out[(a + b) * (a + b + 1) / 2 + b] = i ? d01 : d00;
-        if constexpr (NT >= 2) {
-            a = ra1u;
-            b = NT == 2 ? (c < H ? c : 8 + (c - H)) : c;
-            if (a + b <= NM && (a >= 8 || b >= 8)) out[(a + b) * (a + b + 1) / 2 + b] = i ? e01 : e00;
-        }
         if constexpr (NT == 3) {
+            a = 8 + g;
+            b = c;
+            if (a + b <= NM) out[(a + b) * (a + b + 1) / 2 + b] = i ? e01 : e00;
             a = g;
             b = 8 + c;
             if (a + b <= NM) out[(a + b) * (a + b + 1) / 2 + b] = i ? f01 : f00;
+        }
+    }
+    if constexpr (NT == 2) {
+#pragma unroll
+        for (int e = 0; e < XE; e++)
+            for (int o = 16; o > 0; o >>= 1) xs[e] += __shfl_xor_sync(0xffffffffu, xs[e], o);
+        if (lane == 0) {
+#pragma unroll
+            for (int r = 8; r <= NM; r++) {
+                const int e0 = (r - 8) * (2 * H - (r - 8) + 1);
+#pragma unroll
+                for (int s2 = 0; s2 <= NM - r; s2++) {
+                    out[(r + s2) * (r + s2 + 1) / 2 + s2] = xs[e0 + 2 * s2];  // (a, b) = (r, s2)
+                    out[(r + s2) * (r + s2 + 1) / 2 + r] = xs[e0 + 2 * s2 + 1];  // (a, b) = (s2, r)
+                }
+            }
         }
     }
 }
